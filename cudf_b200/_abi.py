@@ -1,0 +1,219 @@
+"""ctypes mirror of include/gbx.h (the C ABI of libgbx).
+
+Only type and constant definitions live here; loading the shared library is
+done by :mod:`cudf_b200._lib`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+
+class TypeId(enum.IntEnum):
+    """cudf::type_id (cpp/include/cudf/types.hpp:203-235)."""
+
+    EMPTY = 0
+    INT8 = 1
+    INT16 = 2
+    INT32 = 3
+    INT64 = 4
+    UINT8 = 5
+    UINT16 = 6
+    UINT32 = 7
+    UINT64 = 8
+    FLOAT32 = 9
+    FLOAT64 = 10
+    BOOL8 = 11
+    TIMESTAMP_DAYS = 12
+    TIMESTAMP_SECONDS = 13
+    TIMESTAMP_MILLISECONDS = 14
+    TIMESTAMP_MICROSECONDS = 15
+    TIMESTAMP_NANOSECONDS = 16
+    DURATION_DAYS = 17
+    DURATION_SECONDS = 18
+    DURATION_MILLISECONDS = 19
+    DURATION_MICROSECONDS = 20
+    DURATION_NANOSECONDS = 21
+    DICTIONARY32 = 22
+    STRING = 23
+    LIST = 24
+    DECIMAL32 = 25
+    DECIMAL64 = 26
+    DECIMAL128 = 27
+    STRUCT = 28
+
+
+class Kind(enum.IntEnum):
+    """cudf::aggregation::Kind (cpp/include/cudf/aggregation.hpp:86-124)."""
+
+    SUM = 0
+    PRODUCT = 1
+    MIN = 2
+    MAX = 3
+    COUNT_VALID = 4
+    COUNT_ALL = 5
+    ANY = 6
+    ALL = 7
+    SUM_OF_SQUARES = 8
+    MEAN = 9
+    M2 = 10
+    VARIANCE = 11
+    STD = 12
+    MEDIAN = 13
+    QUANTILE = 14
+    ARGMAX = 15
+    ARGMIN = 16
+    NUNIQUE = 17
+    NTH_ELEMENT = 18
+
+
+class NullPolicy(enum.IntEnum):
+    """cudf::null_policy (types.hpp:126)."""
+
+    EXCLUDE = 0
+    INCLUDE = 1
+
+
+class Sorted(enum.IntEnum):
+    """cudf::sorted (types.hpp:167)."""
+
+    NO = 0
+    YES = 1
+
+
+class Status(enum.IntEnum):
+    OK = 0
+    ERR_LOGIC = 1
+    ERR_CUDA = 2
+    ERR_ALLOC = 3
+    ERR_UNSUPPORTED = 4
+    ERR_DEVICE = 5
+
+
+class Strategy(enum.IntEnum):
+    AUTO = 0
+    PRIVATIZED = 1
+    GLOBAL = 2
+    PARTITIONED = 3
+
+
+# element width in bytes of each fixed-width type (0: not fixed width)
+TYPE_WIDTH = {
+    TypeId.INT8: 1, TypeId.INT16: 2, TypeId.INT32: 4, TypeId.INT64: 8,
+    TypeId.UINT8: 1, TypeId.UINT16: 2, TypeId.UINT32: 4, TypeId.UINT64: 8,
+    TypeId.FLOAT32: 4, TypeId.FLOAT64: 8, TypeId.BOOL8: 1,
+    TypeId.TIMESTAMP_DAYS: 4, TypeId.TIMESTAMP_SECONDS: 8, TypeId.TIMESTAMP_MILLISECONDS: 8,
+    TypeId.TIMESTAMP_MICROSECONDS: 8, TypeId.TIMESTAMP_NANOSECONDS: 8,
+    TypeId.DURATION_DAYS: 4, TypeId.DURATION_SECONDS: 8, TypeId.DURATION_MILLISECONDS: 8,
+    TypeId.DURATION_MICROSECONDS: 8, TypeId.DURATION_NANOSECONDS: 8,
+    TypeId.DECIMAL32: 4, TypeId.DECIMAL64: 8,
+}
+
+
+class gbx_column_view(C.Structure):
+    pass
+
+
+gbx_column_view._fields_ = [
+    ("type_id", C.c_int32),
+    ("scale", C.c_int32),
+    ("size", C.c_int64),
+    ("offset", C.c_int64),
+    ("data", C.c_void_p),
+    ("null_mask", C.c_void_p),
+    ("null_count", C.c_int64),
+    ("index_type_id", C.c_int32),
+    ("reserved0", C.c_int32),
+    ("dict_keys", C.POINTER(gbx_column_view)),
+]
+
+
+class gbx_table_view(C.Structure):
+    _fields_ = [
+        ("num_columns", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("columns", C.POINTER(gbx_column_view)),
+    ]
+
+
+class gbx_aggregation(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("ddof", C.c_int32)]
+
+
+class gbx_request(C.Structure):
+    _fields_ = [
+        ("values", gbx_column_view),
+        ("num_aggregations", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("aggregations", C.POINTER(gbx_aggregation)),
+    ]
+
+
+ALLOC_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
+DEALLOC_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
+
+
+class gbx_allocator(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("allocate", ALLOC_FN), ("deallocate", DEALLOC_FN)]
+
+
+class gbx_column(C.Structure):
+    _fields_ = [
+        ("view", gbx_column_view),
+        ("data", C.c_void_p),
+        ("null_mask", C.c_void_p),
+        ("data_bytes", C.c_size_t),
+        ("mask_bytes", C.c_size_t),
+    ]
+
+
+class gbx_aggregation_result(C.Structure):
+    _fields_ = [
+        ("num_results", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("results", C.POINTER(gbx_column)),
+    ]
+
+
+class gbx_result(C.Structure):
+    _fields_ = [
+        ("num_groups", C.c_int64),
+        ("num_key_columns", C.c_int32),
+        ("num_requests", C.c_int32),
+        ("keys", C.POINTER(gbx_column)),
+        ("requests", C.POINTER(gbx_aggregation_result)),
+        ("internal", C.c_void_p),
+    ]
+
+
+class gbx_stats(C.Structure):
+    _fields_ = [
+        ("num_rows", C.c_int64),
+        ("num_groups", C.c_int64),
+        ("estimated_groups", C.c_int64),
+        ("table_capacity", C.c_int64),
+        ("strategy", C.c_int32),
+        ("retries", C.c_int32),
+        ("scratch_bytes", C.c_int64),
+        ("kernel_launches", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+# Every entry point include/gbx.h declares, with (restype, argtypes).
+SIGNATURES = {
+    "gbx_groupby_create": (C.c_int, [C.POINTER(gbx_table_view), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "gbx_groupby_aggregate": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(gbx_request), C.c_int32, C.c_void_p, C.POINTER(gbx_allocator),
+         C.POINTER(C.POINTER(gbx_result))],
+    ),
+    "gbx_can_use_hash_groupby": (C.c_int, [C.POINTER(gbx_request), C.c_int32]),
+    "gbx_target_type": (C.c_int32, [C.c_int32, C.c_int32]),
+    "gbx_result_release": (None, [C.POINTER(gbx_result)]),
+    "gbx_groupby_destroy": (None, [C.c_void_p]),
+    "gbx_last_error": (C.c_char_p, []),
+    "gbx_abi_version": (C.c_int32, []),
+    "gbx_groupby_set_strategy": (C.c_int, [C.c_void_p, C.c_int32]),
+    "gbx_groupby_last_stats": (C.c_int, [C.c_void_p, C.POINTER(gbx_stats)]),
+}

@@ -1,0 +1,927 @@
+// gbx_abi.cpp -- host side of libgbx: the C ABI (include/gbx.h) over the
+// sm_100a kernels.  Restates the reference's host flow of
+// cudf::groupby::groupby::aggregate (cpp/src/groupby/groupby.cu:150-221) and
+// detail::hash::groupby (cpp/src/groupby/hash/groupby.cu:548-667):
+// validation, empty-input shortcut, flattening of compound aggregations,
+// table build + single-pass aggregation, compaction and finalisation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gbx.h"
+#include "gbx_kernels.hpp"
+
+namespace gbx {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Failure {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int code, const char* fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw Failure{code, buf};
+}
+
+#define GBX_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      if (e_ == cudaErrorMemoryAllocation)                                                  \
+        fail(GBX_ERR_ALLOC, "CUDA error at %s:%d: %s", __FILE__, __LINE__,                  \
+             cudaGetErrorString(e_));                                                       \
+      fail(GBX_ERR_CUDA, "CUDA error at %s:%d: %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+    }                                                                                       \
+  } while (0)
+
+#define GBX_EXPECTS(cond, ...)               \
+  do {                                       \
+    if (!(cond)) fail(GBX_ERR_LOGIC, __VA_ARGS__); \
+  } while (0)
+
+template <class F>
+int guarded(F&& f)
+{
+  try {
+    f();
+    g_last_error.clear();
+    return GBX_OK;
+  } catch (Failure& e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return GBX_ERR_ALLOC;
+  }
+}
+
+// ------------------------------------------------------------------- types
+
+int type_width(int32_t t)
+{
+  switch (t) {
+    case GBX_TYPE_INT8:
+    case GBX_TYPE_UINT8:
+    case GBX_TYPE_BOOL8: return 1;
+    case GBX_TYPE_INT16:
+    case GBX_TYPE_UINT16: return 2;
+    case GBX_TYPE_INT32:
+    case GBX_TYPE_UINT32:
+    case GBX_TYPE_FLOAT32:
+    case GBX_TYPE_TIMESTAMP_DAYS:
+    case GBX_TYPE_DURATION_DAYS:
+    case GBX_TYPE_DECIMAL32: return 4;
+    case GBX_TYPE_INT64:
+    case GBX_TYPE_UINT64:
+    case GBX_TYPE_FLOAT64:
+    case GBX_TYPE_TIMESTAMP_SECONDS:
+    case GBX_TYPE_TIMESTAMP_MILLISECONDS:
+    case GBX_TYPE_TIMESTAMP_MICROSECONDS:
+    case GBX_TYPE_TIMESTAMP_NANOSECONDS:
+    case GBX_TYPE_DURATION_SECONDS:
+    case GBX_TYPE_DURATION_MILLISECONDS:
+    case GBX_TYPE_DURATION_MICROSECONDS:
+    case GBX_TYPE_DURATION_NANOSECONDS:
+    case GBX_TYPE_DECIMAL64: return 8;
+    default: return 0;
+  }
+}
+
+bool is_integral(int32_t t) { return (t >= GBX_TYPE_INT8 && t <= GBX_TYPE_UINT64) || t == GBX_TYPE_BOOL8; }
+bool is_floating(int32_t t) { return t == GBX_TYPE_FLOAT32 || t == GBX_TYPE_FLOAT64; }
+bool is_duration(int32_t t) { return t >= GBX_TYPE_DURATION_DAYS && t <= GBX_TYPE_DURATION_NANOSECONDS; }
+bool is_decimal(int32_t t) { return t == GBX_TYPE_DECIMAL32 || t == GBX_TYPE_DECIMAL64; }
+bool is_fixed_width(int32_t t) { return type_width(t) > 0; }
+bool is_unsigned(int32_t t) { return t >= GBX_TYPE_UINT8 && t <= GBX_TYPE_UINT64; }
+
+// Physical code of a fixed-width element type.
+int8_t phys_of(int32_t t)
+{
+  if (t == GBX_TYPE_BOOL8) return P_BOOL;
+  if (t == GBX_TYPE_FLOAT32) return P_F32;
+  if (t == GBX_TYPE_FLOAT64) return P_F64;
+  int w = type_width(t);
+  if (is_unsigned(t)) return w == 1 ? P_U8 : w == 2 ? P_U16 : w == 4 ? P_U32 : P_U64;
+  return w == 1 ? P_I8 : w == 2 ? P_I16 : w == 4 ? P_I32 : P_I64;
+}
+
+// cudf::detail::target_type restated (detail/aggregation/aggregation.hpp:1212-1335)
+// for the kinds the hash path computes (hash/groupby.cu:73-84); GBX_TYPE_EMPTY
+// when the combination is invalid.
+int32_t target_type(int32_t t, int32_t kind)
+{
+  if (!is_fixed_width(t)) return GBX_TYPE_EMPTY;
+  switch (kind) {
+    case GBX_AGG_SUM:
+      if (is_integral(t)) return GBX_TYPE_INT64;
+      if (is_floating(t) || is_duration(t) || is_decimal(t)) return t;
+      return GBX_TYPE_EMPTY;
+    case GBX_AGG_PRODUCT:
+    case GBX_AGG_SUM_OF_SQUARES:
+      if (is_integral(t)) return GBX_TYPE_INT64;
+      if (is_floating(t)) return t;
+      return GBX_TYPE_EMPTY;
+    case GBX_AGG_MIN:
+    case GBX_AGG_MAX: return t;
+    case GBX_AGG_COUNT_VALID:
+    case GBX_AGG_COUNT_ALL: return GBX_TYPE_INT32;
+    case GBX_AGG_MEAN:
+      if (is_integral(t) || is_floating(t)) return GBX_TYPE_FLOAT64;
+      if (is_duration(t) || is_decimal(t)) return t;
+      return GBX_TYPE_EMPTY;
+    case GBX_AGG_VARIANCE:
+    case GBX_AGG_STD:
+      if (is_integral(t) || is_floating(t)) return GBX_TYPE_FLOAT64;
+      return GBX_TYPE_EMPTY;
+    default: return GBX_TYPE_EMPTY;
+  }
+}
+
+// Kinds libcudf accepts on its hash path (hash/groupby.cu:73-84).  ARGMIN /
+// ARGMAX are hash kinds there too but are not provided by this library.
+bool is_hash_kind(int32_t k)
+{
+  switch (k) {
+    case GBX_AGG_SUM:
+    case GBX_AGG_PRODUCT:
+    case GBX_AGG_MIN:
+    case GBX_AGG_MAX:
+    case GBX_AGG_COUNT_VALID:
+    case GBX_AGG_COUNT_ALL:
+    case GBX_AGG_SUM_OF_SQUARES:
+    case GBX_AGG_MEAN:
+    case GBX_AGG_STD:
+    case GBX_AGG_VARIANCE: return true;
+    default: return false;
+  }
+}
+
+int32_t value_type(const gbx_column_view& c)
+{
+  if (c.type_id == GBX_TYPE_DICTIONARY32) return c.dict_keys ? c.dict_keys->type_id : GBX_TYPE_EMPTY;
+  return c.type_id;
+}
+
+bool same_view(const gbx_column_view& a, const gbx_column_view& b)
+{
+  return a.type_id == b.type_id && a.size == b.size && a.offset == b.offset && a.data == b.data &&
+         a.null_mask == b.null_mask && a.index_type_id == b.index_type_id && a.dict_keys == b.dict_keys &&
+         a.scale == b.scale;
+}
+
+// -------------------------------------------------------------- allocation
+
+struct Alloc {
+  gbx_allocator user{};
+  bool has_user = false;
+  cudaStream_t st = nullptr;
+
+  void* allocate(size_t bytes)
+  {
+    if (bytes == 0) bytes = 8;
+    bytes = (bytes + 255) & ~size_t(255);
+    void* p = nullptr;
+    if (has_user) {
+      p = user.allocate(user.ctx, bytes, st);
+      if (!p) fail(GBX_ERR_ALLOC, "allocator returned null for %zu bytes", bytes);
+      return p;
+    }
+    cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      fail(GBX_ERR_ALLOC, "cudaMallocAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return p;
+  }
+  void release(void* p, size_t bytes)
+  {
+    if (!p) return;
+    if (bytes == 0) bytes = 8;
+    bytes = (bytes + 255) & ~size_t(255);
+    if (has_user) user.deallocate(user.ctx, p, bytes, st);
+    else cudaFreeAsync(p, st);
+  }
+};
+
+// Scratch buffers released (stream-ordered) when the call ends.
+struct Scratch {
+  Alloc* a;
+  std::vector<std::pair<void*, size_t>> bufs;
+  explicit Scratch(Alloc* al) : a(al) {}
+  void* get(size_t bytes)
+  {
+    void* p = a->allocate(bytes);
+    bufs.emplace_back(p, bytes);
+    return p;
+  }
+  size_t total() const
+  {
+    size_t s = 0;
+    for (auto& b : bufs) s += b.second;
+    return s;
+  }
+  void release_all()
+  {
+    for (auto& b : bufs) a->release(b.first, b.second);
+    bufs.clear();
+  }
+  ~Scratch() { release_all(); }
+};
+
+struct DeviceInfo {
+  int device = -1;
+  int num_sms = 0;
+  size_t smem_optin = 0;
+};
+
+DeviceInfo current_device()
+{
+  DeviceInfo d;
+  GBX_CUDA(cudaGetDevice(&d.device));
+  GBX_CUDA(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, d.device));
+  int optin = 0;
+  GBX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device));
+  d.smem_optin = static_cast<size_t>(optin);
+  return d;
+}
+
+uint64_t next_pow2(uint64_t v)
+{
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+}  // namespace
+}  // namespace gbx
+
+using namespace gbx;
+
+// ------------------------------------------------------------- the object
+
+struct gbx_groupby {
+  std::vector<gbx_column_view> keys;
+  std::vector<gbx_column_view> dict_keys;  // copies of each key column's dictionary keys
+  int32_t null_policy = GBX_NULL_EXCLUDE;
+  int32_t keys_are_sorted = 0;
+  int32_t strategy = GBX_STRATEGY_AUTO;
+  gbx_stats stats{};
+};
+
+struct ResultInternal {
+  Alloc alloc;
+};
+
+namespace gbx {
+namespace {
+
+// Output column allocation helper.
+void alloc_column(Alloc& a, gbx_column& c, int32_t type_id, int32_t scale, int64_t n, bool with_mask)
+{
+  std::memset(&c, 0, sizeof(c));
+  int w          = type_width(type_id == GBX_TYPE_DICTIONARY32 ? GBX_TYPE_INT32 : type_id);
+  c.data_bytes   = static_cast<size_t>(n) * w;
+  c.data         = n > 0 ? a.allocate(c.data_bytes) : nullptr;
+  if (with_mask) {
+    size_t words = static_cast<size_t>((n + 31) / 32);
+    c.mask_bytes = ((words * 4 + 63) / 64) * 64;  // padded like cudf's bitmask allocations
+    c.null_mask  = n > 0 ? static_cast<uint32_t*>(a.allocate(c.mask_bytes)) : nullptr;
+  }
+  c.view.type_id    = type_id;
+  c.view.scale      = scale;
+  c.view.size       = n;
+  c.view.offset     = 0;
+  c.view.data       = c.data;
+  c.view.null_mask  = c.null_mask;
+  c.view.null_count = with_mask ? -1 : 0;
+}
+
+struct ReqMap {
+  int chan;
+};
+
+void validate(const gbx_groupby* gb, const gbx_request* reqs, int32_t nreq)
+{
+  GBX_EXPECTS(nreq >= 0 && (nreq == 0 || reqs != nullptr), "invalid request array");
+  const int64_t n = gb->keys.empty() ? 0 : gb->keys[0].size;
+  for (int32_t q = 0; q < nreq; ++q) {
+    const gbx_request& r = reqs[q];
+    // groupby.cu:210-214
+    GBX_EXPECTS(r.values.size == n, "Size mismatch between request values and groupby keys.");
+    GBX_EXPECTS(r.num_aggregations >= 0 && (r.num_aggregations == 0 || r.aggregations != nullptr),
+                "invalid aggregation array");
+    if (r.values.type_id == GBX_TYPE_DICTIONARY32)
+      GBX_EXPECTS(r.values.dict_keys != nullptr, "dictionary column without keys");
+    int32_t vt = value_type(r.values);
+    for (int32_t k = 0; k < r.num_aggregations; ++k) {
+      int32_t kind = r.aggregations[k].kind;
+      // verify_valid_requests (groupby.cu:176-192)
+      if (!is_hash_kind(kind)) {
+        if (kind == GBX_AGG_ARGMIN || kind == GBX_AGG_ARGMAX || kind == GBX_AGG_NTH_ELEMENT ||
+            kind == GBX_AGG_MEDIAN || kind == GBX_AGG_QUANTILE || kind == GBX_AGG_NUNIQUE ||
+            kind == GBX_AGG_M2 || kind == GBX_AGG_ANY || kind == GBX_AGG_ALL || kind > GBX_AGG_NTH_ELEMENT)
+          fail(GBX_ERR_UNSUPPORTED,
+               "aggregation kind %d is computed by libcudf's sort-based groupby, which this library does not "
+               "provide",
+               kind);
+        fail(GBX_ERR_LOGIC, "Invalid type/aggregation combination.");
+      }
+      if (vt == GBX_TYPE_STRING || vt == GBX_TYPE_LIST || vt == GBX_TYPE_STRUCT || vt == GBX_TYPE_DECIMAL128)
+        fail(GBX_ERR_UNSUPPORTED,
+             "value type %d is aggregated by libcudf's sort-based groupby, which this library does not provide", vt);
+      GBX_EXPECTS(target_type(vt, kind) != GBX_TYPE_EMPTY, "Invalid type/aggregation combination.");
+    }
+  }
+}
+
+int64_t exact_null_count_or_neg(const gbx_column_view& c)
+{
+  if (c.null_mask == nullptr) return 0;
+  return c.null_count;  // -1 when unknown
+}
+
+struct Call {
+  gbx_groupby* gb;
+  const gbx_request* reqs;
+  int32_t nreq;
+  Alloc alloc;
+  DeviceInfo dev;
+  int64_t n = 0;
+};
+
+// Builds the key plan.  `key_nulls[c]` is the null count of key column c.
+KeyPlan make_key_plan(const gbx_groupby* gb, const std::vector<int64_t>& key_nulls, bool& ok)
+{
+  KeyPlan kp{};
+  ok                   = true;
+  kp.ncols             = static_cast<int32_t>(gb->keys.size());
+  bool any_nulls       = false;
+  for (auto v : key_nulls) any_nulls |= (v != 0);
+  const bool include   = gb->null_policy == GBX_NULL_INCLUDE;
+  kp.skip_null_rows    = (!include && any_nulls) ? 1 : 0;
+  // value fields first (never split across a word), then the null bits in
+  // the first free bits of either word
+  int word = 0, bit = 0;
+  for (int c = 0; c < kp.ncols; ++c) {
+    const gbx_column_view& col = gb->keys[c];
+    KeyCol& kc                 = kp.cols[c];
+    int32_t phys_type          = col.type_id == GBX_TYPE_DICTIONARY32
+                                   ? (col.index_type_id ? col.index_type_id : GBX_TYPE_INT32)
+                                   : col.type_id;
+    kc.data      = col.data;
+    kc.mask      = key_nulls[c] != 0 ? col.null_mask : nullptr;
+    kc.offset    = col.offset;
+    kc.width     = static_cast<int8_t>(type_width(phys_type));
+    kc.is_float  = is_floating(phys_type) ? 1 : 0;
+    kc.is_bool   = phys_type == GBX_TYPE_BOOL8 ? 1 : 0;
+    kc.null_bit  = (include && key_nulls[c] != 0) ? 1 : 0;
+    kc.is_signed = (!is_unsigned(phys_type) && phys_type != GBX_TYPE_BOOL8) ? 1 : 0;
+    int need     = kc.width * 8;
+    if (bit + need > 64) {
+      ++word;
+      bit = 0;
+    }
+    if (word > 1) {
+      ok = false;
+      return kp;
+    }
+    kc.word  = static_cast<int8_t>(word);
+    kc.shift = static_cast<int8_t>(bit);
+    bit += need;
+    kp.bits_used += need;
+  }
+  int used[2] = {word == 0 ? bit : 64, word == 1 ? bit : 0};
+  int nwords  = word + 1;
+  for (int c = 0; c < kp.ncols; ++c) {
+    KeyCol& kc = kp.cols[c];
+    if (!kc.null_bit) continue;
+    int w = used[0] < 64 ? 0 : 1;
+    if (w == 1 && used[1] >= 64) {
+      ok = false;
+      return kp;
+    }
+    nwords         = std::max(nwords, w + 1);
+    kc.null_word   = static_cast<int8_t>(w);
+    kc.null_shift  = static_cast<int8_t>(used[w]++);
+    kp.bits_used  += 1;
+  }
+  kp.nwords = nwords;
+  return kp;
+}
+
+}  // namespace
+}  // namespace gbx
+
+// ================================================================== C ABI
+
+extern "C" {
+
+const char* gbx_last_error(void) { return g_last_error.c_str(); }
+int32_t gbx_abi_version(void) { return GBX_ABI_VERSION; }
+int32_t gbx_target_type(int32_t type_id, int32_t kind)
+{
+  if (!is_hash_kind(kind)) return GBX_TYPE_EMPTY;
+  return target_type(type_id, kind);
+}
+
+int gbx_groupby_create(const gbx_table_view* keys, int32_t null_policy, int32_t keys_are_sorted, gbx_groupby** out)
+{
+  return guarded([&] {
+    GBX_EXPECTS(out != nullptr, "out is null");
+    *out = nullptr;
+    GBX_EXPECTS(keys != nullptr && keys->num_columns >= 0 && (keys->num_columns == 0 || keys->columns),
+                "invalid keys table");
+    GBX_EXPECTS(null_policy == GBX_NULL_EXCLUDE || null_policy == GBX_NULL_INCLUDE, "invalid null_policy");
+    auto* gb            = new gbx_groupby();
+    gb->null_policy     = null_policy;
+    gb->keys_are_sorted = keys_are_sorted;
+    try {
+      gb->keys.assign(keys->columns, keys->columns + keys->num_columns);
+      gb->dict_keys.resize(gb->keys.size());
+      for (size_t c = 0; c < gb->keys.size(); ++c) {
+        gbx_column_view& k = gb->keys[c];
+        GBX_EXPECTS(k.size == gb->keys[0].size, "key columns differ in size");
+        if (k.type_id == GBX_TYPE_DICTIONARY32) {
+          GBX_EXPECTS(k.dict_keys != nullptr, "dictionary key column without keys");
+          gb->dict_keys[c] = *k.dict_keys;
+          k.dict_keys      = &gb->dict_keys[c];
+          int32_t it       = k.index_type_id ? k.index_type_id : GBX_TYPE_INT32;
+          GBX_EXPECTS(is_integral(it) && it != GBX_TYPE_BOOL8, "dictionary indices must be integers");
+        } else if (!is_fixed_width(k.type_id)) {
+          fail(GBX_ERR_UNSUPPORTED,
+               "key type %d (string / list / struct / decimal128) is not supported by this library", k.type_id);
+        }
+        GBX_EXPECTS(k.size >= 0 && k.offset >= 0, "negative size or offset");
+        GBX_EXPECTS(k.size <= INT32_MAX, "row count exceeds cudf::size_type");
+      }
+    } catch (...) {
+      delete gb;
+      throw;
+    }
+    *out = gb;
+  });
+}
+
+void gbx_groupby_destroy(gbx_groupby* gb) { delete gb; }
+
+int gbx_groupby_set_strategy(gbx_groupby* gb, int32_t strategy)
+{
+  return guarded([&] {
+    GBX_EXPECTS(gb != nullptr, "null groupby");
+    GBX_EXPECTS(strategy >= GBX_STRATEGY_AUTO && strategy <= GBX_STRATEGY_GLOBAL,
+                "strategy %d not available", strategy);
+    gb->strategy = strategy;
+  });
+}
+
+int gbx_groupby_last_stats(const gbx_groupby* gb, gbx_stats* out)
+{
+  return guarded([&] {
+    GBX_EXPECTS(gb != nullptr && out != nullptr, "null argument");
+    *out = gb->stats;
+  });
+}
+
+int gbx_can_use_hash_groupby(const gbx_request* requests, int32_t num_requests)
+{
+  int rv = 1;
+  int st = guarded([&] {
+    GBX_EXPECTS(num_requests >= 0 && (num_requests == 0 || requests), "invalid request array");
+    for (int32_t q = 0; q < num_requests; ++q) {
+      int32_t vt = value_type(requests[q].values);
+      if (vt == GBX_TYPE_STRUCT || vt == GBX_TYPE_LIST) rv = 0;
+      for (int32_t k = 0; k < requests[q].num_aggregations; ++k) {
+        int32_t kind = requests[q].aggregations[k].kind;
+        if (!is_hash_kind(kind) || target_type(vt, kind) == GBX_TYPE_EMPTY) rv = 0;
+      }
+    }
+  });
+  return st == GBX_OK ? rv : -1;
+}
+
+void gbx_result_release(gbx_result* r)
+{
+  if (!r) return;
+  auto* in = static_cast<ResultInternal*>(r->internal);
+  auto free_col = [&](gbx_column& c) {
+    if (in) {
+      in->alloc.release(c.data, c.data_bytes);
+      in->alloc.release(c.null_mask, c.mask_bytes);
+    }
+  };
+  for (int c = 0; c < r->num_key_columns; ++c) free_col(r->keys[c]);
+  for (int q = 0; q < r->num_requests; ++q) {
+    for (int k = 0; k < r->requests[q].num_results; ++k) free_col(r->requests[q].results[k]);
+    delete[] r->requests[q].results;
+  }
+  delete[] r->keys;
+  delete[] r->requests;
+  delete in;
+  delete r;
+}
+
+int gbx_groupby_aggregate(gbx_groupby* gb,
+                          const gbx_request* requests,
+                          int32_t num_requests,
+                          void* stream,
+                          const gbx_allocator* mr,
+                          gbx_result** out)
+{
+  gbx_result* res = nullptr;
+  int st          = guarded([&] {
+    GBX_EXPECTS(gb != nullptr && out != nullptr, "null argument");
+    *out = nullptr;
+    validate(gb, requests, num_requests);
+
+    Call call{gb, requests, num_requests};
+    call.alloc.st = static_cast<cudaStream_t>(stream);
+    if (mr && mr->allocate && mr->deallocate) {
+      call.alloc.user     = *mr;
+      call.alloc.has_user = true;
+    }
+    call.dev = current_device();
+    call.n   = gb->keys.empty() ? 0 : gb->keys[0].size;
+    cudaStream_t s = call.alloc.st;
+    const int nkeys = static_cast<int>(gb->keys.size());
+
+    res                  = new gbx_result();
+    std::memset(res, 0, sizeof(*res));
+    auto* internal       = new ResultInternal{call.alloc};
+    res->internal        = internal;
+    res->num_key_columns = nkeys;
+    res->num_requests    = num_requests;
+    res->keys            = new gbx_column[nkeys > 0 ? nkeys : 1]();
+    res->requests        = new gbx_aggregation_result[num_requests > 0 ? num_requests : 1]();
+    for (int q = 0; q < num_requests; ++q) {
+      res->requests[q].num_results = requests[q].num_aggregations;
+      res->requests[q].results     = new gbx_column[requests[q].num_aggregations > 0 ? requests[q].num_aggregations : 1]();
+    }
+
+    gb->stats          = gbx_stats{};
+    gb->stats.num_rows = call.n;
+
+    // ---- distinct value columns -> channels
+    std::vector<int> req_chan(num_requests, -1);
+    std::vector<const gbx_column_view*> chan_cols;
+    for (int q = 0; q < num_requests; ++q) {
+      if (requests[q].num_aggregations == 0) continue;
+      int found = -1;
+      for (size_t c = 0; c < chan_cols.size(); ++c)
+        if (same_view(*chan_cols[c], requests[q].values)) found = static_cast<int>(c);
+      if (found < 0) {
+        found = static_cast<int>(chan_cols.size());
+        chan_cols.push_back(&requests[q].values);
+      }
+      req_chan[q] = found;
+    }
+    if (static_cast<int>(chan_cols.size()) > kMaxChannels)
+      fail(GBX_ERR_UNSUPPORTED, "more than %d distinct value columns in one call", kMaxChannels);
+
+    // ---- null counts (one small kernel + one read, merged with the sample read)
+    std::vector<int64_t> key_nulls(nkeys, 0), chan_nulls(chan_cols.size(), 0);
+    MaskSpans ms{};
+    std::vector<std::pair<int, int>> span_owner;  // (0=key,1=chan, index)
+    for (int c = 0; c < nkeys; ++c) {
+      int64_t v = exact_null_count_or_neg(gb->keys[c]);
+      key_nulls[c] = v;
+      if (v < 0) {
+        ms.span[ms.n++] = MaskSpan{gb->keys[c].null_mask, gb->keys[c].offset, gb->keys[c].size};
+        span_owner.push_back({0, c});
+      }
+    }
+    for (size_t c = 0; c < chan_cols.size(); ++c) {
+      int64_t v     = exact_null_count_or_neg(*chan_cols[c]);
+      chan_nulls[c] = v;
+      if (v < 0) {
+        ms.span[ms.n++] = MaskSpan{chan_cols[c]->null_mask, chan_cols[c]->offset, chan_cols[c]->size};
+        span_owner.push_back({1, static_cast<int>(c)});
+      }
+    }
+
+    // ---- empty input: typed empty results (groupby.cu:150-172, 218)
+    if (call.n == 0) {
+      for (int c = 0; c < nkeys; ++c) {
+        alloc_column(call.alloc, res->keys[c], gb->keys[c].type_id, gb->keys[c].scale, 0, false);
+        if (gb->keys[c].type_id == GBX_TYPE_DICTIONARY32) {
+          res->keys[c].view.dict_keys     = gb->keys[c].dict_keys;
+          res->keys[c].view.index_type_id = GBX_TYPE_INT32;
+        }
+      }
+      for (int q = 0; q < num_requests; ++q) {
+        int32_t vt = value_type(requests[q].values);
+        for (int k = 0; k < requests[q].num_aggregations; ++k) {
+          int32_t tt = target_type(vt, requests[q].aggregations[k].kind);
+          alloc_column(call.alloc, res->requests[q].results[k], tt, is_decimal(tt) ? requests[q].values.scale : 0, 0,
+                       false);
+        }
+      }
+      return;
+    }
+
+    Scratch scratch(&call.alloc);
+    // control block: [0..1] sample counters, [2..25] valid counts, [26] status, [27] num_selected
+    constexpr int kCtlWords = 32;
+    auto* ctl = static_cast<unsigned long long*>(scratch.get(kCtlWords * 8));
+    GBX_CUDA(cudaMemsetAsync(ctl, 0, kCtlWords * 8, s));
+    int32_t* d_status        = reinterpret_cast<int32_t*>(ctl + 26);
+    int64_t* d_num_selected  = reinterpret_cast<int64_t*>(ctl + 27);
+    GBX_CUDA(launch_count_valid(ms, ctl + 2, call.dev.num_sms, s));
+
+    bool key_ok       = true;
+    KeyPlan kp_sample = make_key_plan(gb, std::vector<int64_t>(nkeys, -1), key_ok);
+    if (!key_ok)
+      fail(GBX_ERR_UNSUPPORTED, "key columns need more than 128 packed bits; wider composite keys are not supported");
+
+    // ---- sampled distinct count
+    const int64_t nsample = std::min<int64_t>(call.n, 1 << 16);
+    const uint64_t set_cap = 1 << 18;
+    auto* set = static_cast<uint64_t*>(scratch.get(set_cap * 8));
+    GBX_CUDA(launch_sample(kp_sample, call.n, nsample, set, set_cap, ctl, call.dev.num_sms, s));
+
+    unsigned long long h_ctl[kCtlWords];
+    GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
+    GBX_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < span_owner.size(); ++i) {
+      int64_t nulls = static_cast<int64_t>(ms.span[i].size) - static_cast<int64_t>(h_ctl[2 + i]);
+      if (span_owner[i].first == 0) key_nulls[span_owner[i].second] = nulls;
+      else chan_nulls[span_owner[i].second] = nulls;
+    }
+    const double sampled = static_cast<double>(h_ctl[0]);
+    const double distinct = static_cast<double>(h_ctl[1]);
+
+    // Estimate groups: invert the expected distinct count of a uniform draw,
+    // d = C (1 - exp(-m / C)), then G = C (1 - exp(-N / C)).
+    double est;
+    if (nsample >= call.n) {
+      est = distinct;
+    } else if (distinct >= sampled * 0.98) {
+      est = static_cast<double>(call.n);
+    } else {
+      double lo = distinct, hi = 1e12;
+      for (int it = 0; it < 200; ++it) {
+        double mid = 0.5 * (lo + hi);
+        double d   = mid * (1.0 - std::exp(-sampled / mid));
+        if (d < distinct) lo = mid;
+        else hi = mid;
+      }
+      double C = 0.5 * (lo + hi);
+      est      = C * (1.0 - std::exp(-static_cast<double>(call.n) / C));
+    }
+    est = std::max(1.0, std::min(est, static_cast<double>(call.n)));
+    gb->stats.estimated_groups = static_cast<int64_t>(est);
+
+    // ---- plan
+    Plan plan{};
+    plan.key = make_key_plan(gb, key_nulls, key_ok);
+    plan.nchan = static_cast<int32_t>(chan_cols.size());
+    int nacc   = 0;
+    auto add_acc = [&](int kind) -> int8_t {
+      if (nacc >= kMaxAccs) fail(GBX_ERR_UNSUPPORTED, "too many accumulators in one call");
+      plan.acc.kind[nacc] = static_cast<int8_t>(kind);
+      return static_cast<int8_t>(nacc++);
+    };
+    for (int c = 0; c < plan.nchan; ++c) {
+      const gbx_column_view& col = *chan_cols[c];
+      Channel& ch                = plan.chan[c];
+      std::memset(&ch, 0, sizeof(ch));
+      ch.a_cnt = ch.a_sum = ch.a_min = ch.a_max = ch.a_sq = ch.a_k = ch.a_s2 = ch.a_prod = ch.a_amin = ch.a_amax = -1;
+      int32_t vt = value_type(col);
+      ch.data    = col.data;
+      ch.mask    = chan_nulls[c] != 0 ? col.null_mask : nullptr;
+      ch.offset  = col.offset;
+      if (col.type_id == GBX_TYPE_DICTIONARY32) {
+        int32_t it     = col.index_type_id ? col.index_type_id : GBX_TYPE_INT32;
+        ch.dict_data   = col.dict_keys->data;
+        ch.dict_offset = col.dict_keys->offset;
+        ch.dict_size   = col.dict_keys->size;
+        ch.idx_width   = static_cast<int8_t>(type_width(it));
+        ch.idx_signed  = is_unsigned(it) ? 0 : 1;
+      }
+      ch.ptype    = phys_of(vt);
+      ch.is_float = is_floating(vt) ? 1 : 0;
+      uint32_t need = 0;
+      for (int q = 0; q < num_requests; ++q) {
+        if (req_chan[q] != c) continue;
+        for (int k = 0; k < requests[q].num_aggregations; ++k) {
+          switch (requests[q].aggregations[k].kind) {
+            case GBX_AGG_SUM: need |= N_SUM; break;
+            case GBX_AGG_PRODUCT: need |= N_PROD; break;
+            case GBX_AGG_MIN: need |= N_MIN; break;
+            case GBX_AGG_MAX: need |= N_MAX; break;
+            case GBX_AGG_COUNT_VALID: need |= N_CNT; break;
+            case GBX_AGG_COUNT_ALL: break;
+            case GBX_AGG_SUM_OF_SQUARES: need |= N_SQ; break;
+            case GBX_AGG_MEAN: need |= N_SUM | N_CNT; break;
+            case GBX_AGG_VARIANCE:
+            case GBX_AGG_STD: need |= N_SUM | N_CNT | N_VAR; break;
+          }
+        }
+      }
+      ch.need = need;
+      const bool nullable = ch.mask != nullptr;
+      // COUNT_VALID of a column without nulls is the group's row count; a
+      // nullable column needs its own count (also the validity of SUM/MIN/...)
+      if (nullable) ch.a_cnt = add_acc(A_U32_ADD);
+      const bool m64 = ch.ptype == P_I64 || ch.ptype == P_U64 || ch.ptype == P_F64;
+      if (need & N_SUM) ch.a_sum = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
+      if (need & N_MIN) ch.a_min = add_acc(m64 ? A_U64_MIN : A_U32_MIN);
+      if (need & N_MAX) ch.a_max = add_acc(m64 ? A_U64_MAX : A_U32_MAX);
+      if (need & N_SQ) ch.a_sq = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
+      if (need & N_PROD) ch.a_prod = add_acc(ch.is_float ? A_F64_MUL : A_I64_MUL);
+      if (need & N_VAR) {
+        ch.a_k  = add_acc(A_F64_SHIFT);
+        ch.a_s2 = add_acc(A_F64_ADD);
+      }
+    }
+    plan.acc.nacc = nacc;
+
+    // ---- strategy and sizes
+    size_t slot_bytes = static_cast<size_t>(plan.key.nwords) * 8 + 4;
+    for (int a = 0; a < nacc; ++a) slot_bytes += acc_bytes(plan.acc.kind[a]);
+    const size_t smem_budget = std::min<size_t>(call.dev.smem_optin, 100 * 1024);
+    uint32_t s_max           = 1;
+    while (static_cast<size_t>(s_max * 2 + 1) * slot_bytes + 16 * (nacc + 2) <= smem_budget && s_max < (1u << 16))
+      s_max *= 2;
+    int strategy = gb->strategy;
+    if (strategy == GBX_STRATEGY_AUTO)
+      strategy = (est * 2.0 <= static_cast<double>(s_max)) ? GBX_STRATEGY_PRIVATIZED : GBX_STRATEGY_GLOBAL;
+    uint64_t cap = next_pow2(static_cast<uint64_t>(std::max(2.0 * est, 1024.0)));
+    cap          = std::min<uint64_t>(cap, 1ULL << 31);
+
+    gb->stats.strategy = strategy;
+    int launches       = 4;
+    int64_t G          = 0;
+    TableRef t{};
+    uint32_t* map = nullptr;
+    for (int attempt = 0;; ++attempt) {
+      // ---- table
+      t     = TableRef{};
+      t.cap = cap;
+      t.keys = static_cast<uint64_t*>(scratch.get((cap + 1) * plan.key.nwords * 8));
+      t.rows = static_cast<uint32_t*>(scratch.get((cap + 1) * 4));
+      for (int a = 0; a < nacc; ++a) t.acc[a] = scratch.get((cap + 1) * acc_bytes(plan.acc.kind[a]));
+      t.special_used = reinterpret_cast<uint32_t*>(ctl + 28);
+      t.status       = d_status;
+      GBX_CUDA(cudaMemsetAsync(d_status, 0, 4, s));
+      GBX_CUDA(launch_init_table(t, plan.acc, plan.key.nwords, call.dev.num_sms, s));
+      const uint32_t max_probes = static_cast<uint32_t>(std::min<uint64_t>(cap, 1u << 12));
+      if (strategy == GBX_STRATEGY_PRIVATIZED) {
+        uint32_t S = static_cast<uint32_t>(std::min<uint64_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * est, 64.0))), s_max));
+        SmemLayout sl{};
+        sl.slots    = S;
+        uint32_t off = 0;
+        sl.keys_off  = off;
+        off += (S + 1) * plan.key.nwords * 8;
+        for (int a = 0; a < nacc; ++a) {
+          if (acc_bytes(plan.acc.kind[a]) == 8) {
+            off = (off + 7) & ~7u;
+            sl.acc_off[a] = off;
+            off += (S + 1) * 8;
+          }
+        }
+        for (int a = 0; a < nacc; ++a) {
+          if (acc_bytes(plan.acc.kind[a]) == 4) {
+            sl.acc_off[a] = off;
+            off += (S + 1) * 4;
+          }
+        }
+        sl.rows_off = off;
+        off += (S + 1) * 4;
+        sl.total = (off + 15) & ~15u;
+        const int block = 512;
+        int grid        = call.dev.num_sms * std::max<int>(1, std::min<int>(4, static_cast<int>((200 * 1024) / (sl.total + 1024))));
+        int64_t max_grid = (call.n + block * 4 - 1) / (block * 4);
+        grid             = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(grid, max_grid)));
+        GBX_CUDA(launch_agg_privatized(plan, t, sl, call.n, block, grid, std::min<uint32_t>(S, 32), max_probes, s));
+      } else {
+        GBX_CUDA(launch_agg_global(plan, t, call.n, max_probes, call.dev.num_sms, s));
+      }
+      // ---- compaction of occupied slots
+      map               = static_cast<uint32_t*>(scratch.get((cap + 1) * 4));
+      size_t temp_bytes = 0;
+      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, nullptr, &temp_bytes, s));
+      void* temp = scratch.get(temp_bytes);
+      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, temp, &temp_bytes, s));
+      GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
+      GBX_CUDA(cudaStreamSynchronize(s));
+      int32_t status;
+      std::memcpy(&status, reinterpret_cast<char*>(h_ctl) + 26 * 8, 4);
+      std::memcpy(&G, reinterpret_cast<char*>(h_ctl) + 27 * 8, 8);
+      if (status & S_SPIN_LIMIT) fail(GBX_ERR_DEVICE, "a bounded device loop gave up (status 0x%x)", status);
+      if (status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
+      if ((status & S_TABLE_FULL) == 0) break;
+      // table too small for the groups present: grow and redo
+      if (cap >= (1ULL << 31) || attempt >= 2) fail(GBX_ERR_DEVICE, "hash table overflow at capacity %llu", (unsigned long long)cap);
+      gb->stats.retries++;
+      scratch.release_all();
+      ctl = static_cast<unsigned long long*>(scratch.get(kCtlWords * 8));
+      GBX_CUDA(cudaMemsetAsync(ctl, 0, kCtlWords * 8, s));
+      d_status       = reinterpret_cast<int32_t*>(ctl + 26);
+      d_num_selected = reinterpret_cast<int64_t*>(ctl + 27);
+      // the groups present can number at most the rows: size for that bound
+      cap = std::min<uint64_t>(std::max<uint64_t>(cap * 4, next_pow2(2 * static_cast<uint64_t>(call.n) + 2)),
+                               1ULL << 31);
+      if (strategy == GBX_STRATEGY_PRIVATIZED) strategy = GBX_STRATEGY_GLOBAL;
+      est = static_cast<double>(call.n);
+      launches += 4;
+    }
+    gb->stats.strategy        = strategy;
+    gb->stats.table_capacity  = static_cast<int64_t>(cap);
+    gb->stats.num_groups      = G;
+    gb->stats.scratch_bytes   = static_cast<int64_t>(scratch.total());
+    gb->stats.kernel_launches = launches + 1;
+    res->num_groups           = G;
+
+    // ---- outputs
+    OutPlan op{};
+    for (int c = 0; c < nkeys; ++c) {
+      const gbx_column_view& kcv = gb->keys[c];
+      bool with_mask             = plan.key.cols[c].null_bit != 0;
+      int32_t out_type           = kcv.type_id;
+      alloc_column(call.alloc, res->keys[c], out_type, kcv.scale, G, with_mask);
+      if (kcv.type_id == GBX_TYPE_DICTIONARY32) {
+        int32_t it = kcv.index_type_id ? kcv.index_type_id : GBX_TYPE_INT32;
+        res->keys[c].view.index_type_id = it;
+        res->keys[c].view.dict_keys     = kcv.dict_keys;
+        if (type_width(it) != 4) {
+          // re-allocate data at the index width
+          call.alloc.release(res->keys[c].data, res->keys[c].data_bytes);
+          res->keys[c].data_bytes = static_cast<size_t>(G) * type_width(it);
+          res->keys[c].data       = G > 0 ? call.alloc.allocate(res->keys[c].data_bytes) : nullptr;
+          res->keys[c].view.data  = res->keys[c].data;
+        }
+      }
+      if (with_mask) res->keys[c].view.null_count = -1;
+      op.key_data[c] = res->keys[c].data;
+      op.key_mask[c] = res->keys[c].null_mask;
+    }
+    for (int q = 0; q < num_requests; ++q) {
+      const gbx_request& r = requests[q];
+      int32_t vt           = value_type(r.values);
+      for (int k = 0; k < r.num_aggregations; ++k) {
+        int32_t kind = r.aggregations[k].kind;
+        int32_t tt   = target_type(vt, kind);
+        bool has_nulls = chan_nulls[req_chan[q]] != 0;
+        // nullable iff the values have nulls; COUNT never; VAR/STD always (hash/groupby.cu:424-454)
+        bool with_mask = (kind == GBX_AGG_COUNT_VALID || kind == GBX_AGG_COUNT_ALL)
+                           ? false
+                           : (has_nulls || kind == GBX_AGG_VARIANCE || kind == GBX_AGG_STD);
+        int32_t scale = is_decimal(tt) ? (r.values.type_id == GBX_TYPE_DICTIONARY32 ? r.values.dict_keys->scale
+                                                                                    : r.values.scale)
+                                       : 0;
+        gbx_column& oc = res->requests[q].results[k];
+        alloc_column(call.alloc, oc, tt, scale, G, with_mask);
+        if (op.nout >= kMaxOut) fail(GBX_ERR_UNSUPPORTED, "more than %d results in one call", kMaxOut);
+        OutCol& o   = op.out[op.nout++];
+        o.data      = oc.data;
+        o.mask      = oc.null_mask;
+        o.kind      = kind;
+        o.ddof      = r.aggregations[k].ddof;
+        o.chan      = static_cast<int8_t>(req_chan[q]);
+        o.out_ptype = phys_of(tt);
+        o.out_width = static_cast<int8_t>(type_width(tt));
+      }
+    }
+    auto* d_nulls  = static_cast<unsigned long long*>(scratch.get((kMaxKeyCols + kMaxOut) * 8));
+    GBX_CUDA(cudaMemsetAsync(d_nulls, 0, (kMaxKeyCols + kMaxOut) * 8, s));
+    op.null_counts = d_nulls;
+    GBX_CUDA(launch_finalize(plan, t, map, G, op, call.dev.num_sms, s));
+    std::vector<unsigned long long> h_nulls(kMaxKeyCols + kMaxOut, 0);
+    GBX_CUDA(cudaMemcpyAsync(h_nulls.data(), d_nulls, h_nulls.size() * 8, cudaMemcpyDeviceToHost, s));
+    GBX_CUDA(cudaStreamSynchronize(s));
+    for (int c = 0; c < nkeys; ++c)
+      if (res->keys[c].null_mask) res->keys[c].view.null_count = static_cast<int64_t>(h_nulls[c]);
+    {
+      int o = 0;
+      for (int q = 0; q < num_requests; ++q)
+        for (int k = 0; k < requests[q].num_aggregations; ++k, ++o) {
+          gbx_column& oc = res->requests[q].results[k];
+          if (oc.null_mask) oc.view.null_count = static_cast<int64_t>(h_nulls[kMaxKeyCols + o]);
+        }
+    }
+    // scratch is released stream-ordered by ~Scratch
+  });
+  if (st != GBX_OK) {
+    if (res) gbx_result_release(res);
+    return st;
+  }
+  *out = res;
+  return GBX_OK;
+}
+
+}  // extern "C"

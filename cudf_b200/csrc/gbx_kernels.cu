@@ -1,0 +1,673 @@
+// gbx_kernels.cu -- sm_100a kernels of libgbx's hash groupby-aggregation.
+//
+// Replaces the reference's per-row thrust::for_each_n over a cuco::static_set
+// of row indices with row-count-sized "sparse" result columns
+// (cpp/src/groupby/hash/groupby.cu:424-504, groupby_kernels.cuh:98-105) by:
+//   * k_sample_distinct  -- a sampled distinct count that sizes the tables;
+//   * k_init_table       -- identity fill of a capacity-sized global table
+//                           (K2 of the reference writes N-row columns instead);
+//   * k_agg_privatized   -- per-CTA shared-memory tables with inline packed
+//                           keys, spilling to the global table when full and
+//                           flushed into it at the end (K1+K3 fused);
+//   * k_agg_global       -- every row updates the global table directly;
+//   * k_finalize         -- dense outputs: keys decoded from the packed key,
+//                           SUM/COUNT/MIN/MAX/MEAN/VAR/STD finalised and
+//                           validity bitmasks written by warp ballots
+//                           (K4/K6/K7/K8/K9 fused).
+// VAR/STD need no second pass over the rows (the reference's K5,
+// multi_pass_kernels.cuh:35-112): each group keeps a shift K (its first
+// non-NaN value) and the sum of (x - K)^2; partial tables are merged with the
+// shifted-sums identity sum((x-K2)^2) = sum((x-K1)^2) + 2 d S1 + n d^2,
+// d = K1 - K2, S1 = sum(x) - n K1 (Chan, Golub & LeVeque, 1983).
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <cuda_runtime.h>
+
+#include "gbx_device.cuh"
+#include "gbx_kernels.hpp"
+
+namespace gbx {
+namespace dev {
+
+// ------------------------------------------------------------ identities
+
+__device__ __forceinline__ uint64_t identity_bits(int kind)
+{
+  switch (kind) {
+    case A_U32_MIN: return 0xffffffffULL;
+    case A_U64_MIN: return 0xffffffffffffffffULL;
+    case A_F64_SHIFT: return kShiftUnset;
+    case A_I64_MUL: return 1ULL;
+    case A_F64_MUL: return 0x3ff0000000000000ULL;  // 1.0
+    case A_U64_ARGMIN: return 0xffffffffffffffffULL;
+    case A_I32_ARGMIN_CAS:
+    case A_I32_ARGMAX_CAS: return 0xffffffffULL;  // -1 sentinel
+    default: return 0;  // adds, max encodings
+  }
+}
+
+// ---------------------------------------------------- per-row accumulation
+
+// Addressing of one table level: base address of each accumulator array
+// (in the state space of `Space`) and of the row counts.
+template <class Space>
+struct Level {
+  typename Space::addr_t rows;
+  typename Space::addr_t acc[kMaxAccs];
+};
+
+template <class Space>
+__device__ __forceinline__ void mul_cas_i64(typename Space::addr_t a, int64_t x, int32_t* status)
+{
+  uint64_t cur = Space::ld_u64(a);
+  for (int it = 0; it < (1 << 20); ++it) {
+    uint64_t nv  = static_cast<uint64_t>(static_cast<int64_t>(cur) * x);
+    uint64_t old = Space::cas_u64(a, cur, nv);
+    if (old == cur) return;
+    cur = old;
+  }
+  atomicOr(status, S_SPIN_LIMIT);
+}
+
+template <class Space>
+__device__ __forceinline__ void mul_cas_f64(typename Space::addr_t a, double x, int32_t* status)
+{
+  uint64_t cur = Space::ld_u64(a);
+  for (int it = 0; it < (1 << 20); ++it) {
+    double nvd   = __longlong_as_double(static_cast<long long>(cur)) * x;
+    uint64_t nv  = static_cast<uint64_t>(__double_as_longlong(nvd));
+    uint64_t old = Space::cas_u64(a, cur, nv);
+    if (old == cur) return;
+    cur = old;
+  }
+  atomicOr(status, S_SPIN_LIMIT);
+}
+
+// Shift of a VAR accumulator: the recorded K, recording `x` first if unset.
+template <class Space>
+__device__ __forceinline__ double get_shift(typename Space::addr_t a, double x)
+{
+  uint64_t kb = Space::ld_u64(a);
+  if (kb == kShiftUnset && !(x != x)) {
+    uint64_t xb  = static_cast<uint64_t>(__double_as_longlong(x));
+    uint64_t old = Space::cas_u64(a, kShiftUnset, xb);
+    kb           = (old == kShiftUnset) ? xb : old;
+  }
+  return __longlong_as_double(static_cast<long long>(kb));
+}
+
+// Folds row `row` into slot `slot` of a table level (aggregate_row,
+// detail/aggregation/aggregation.cuh:558-573, with update_target_element's
+// null skipping, :116-491).
+template <class Space>
+__device__ __forceinline__ void accumulate_row(const Plan& plan,
+                                               const Level<Space>& L,
+                                               int64_t slot,
+                                               int64_t row,
+                                               int32_t* status)
+{
+  using A = typename Space::addr_t;
+  Space::add_u32(L.rows + static_cast<A>(slot * 4), 1u);
+  for (int c = 0; c < plan.nchan; ++c) {
+    const Channel& ch = plan.chan[c];
+    if (!bit_valid(ch.mask, row + ch.offset)) continue;
+    bool ok;
+    uint64_t b = value_bits(ch, row, ok);
+    if (!ok) {
+      atomicOr(status, S_BAD_INDEX);
+      continue;
+    }
+    if (ch.a_cnt >= 0) Space::add_u32(L.acc[ch.a_cnt] + static_cast<A>(slot * 4), 1u);
+    const bool is64 = minmax_is64(ch.ptype);
+    if (ch.a_min >= 0) {
+      uint64_t e = enc_minmax(b, ch.ptype, true);
+      if (is64) Space::min_u64(L.acc[ch.a_min] + static_cast<A>(slot * 8), e);
+      else Space::min_u32(L.acc[ch.a_min] + static_cast<A>(slot * 4), static_cast<uint32_t>(e));
+    }
+    if (ch.a_max >= 0) {
+      uint64_t e = enc_minmax(b, ch.ptype, false);
+      if (is64) Space::max_u64(L.acc[ch.a_max] + static_cast<A>(slot * 8), e);
+      else Space::max_u32(L.acc[ch.a_max] + static_cast<A>(slot * 4), static_cast<uint32_t>(e));
+    }
+    if (ch.is_float) {
+      double x = as_f64(b, ch.ptype);
+      if (ch.a_sum >= 0) Space::add_f64(L.acc[ch.a_sum] + static_cast<A>(slot * 8), x);
+      if (ch.a_sq >= 0) Space::add_f64(L.acc[ch.a_sq] + static_cast<A>(slot * 8), x * x);
+      if (ch.a_prod >= 0) mul_cas_f64<Space>(L.acc[ch.a_prod] + static_cast<A>(slot * 8), x, status);
+      if (ch.a_k >= 0) {
+        double K = get_shift<Space>(L.acc[ch.a_k] + static_cast<A>(slot * 8), x);
+        double d = x - K;
+        Space::add_f64(L.acc[ch.a_s2] + static_cast<A>(slot * 8), d * d);
+      }
+    } else {
+      int64_t x = as_i64(b, ch.ptype);
+      if (ch.a_sum >= 0) Space::add_u64(L.acc[ch.a_sum] + static_cast<A>(slot * 8), static_cast<uint64_t>(x));
+      if (ch.a_sq >= 0)
+        Space::add_u64(L.acc[ch.a_sq] + static_cast<A>(slot * 8),
+                       static_cast<uint64_t>(x) * static_cast<uint64_t>(x));
+      if (ch.a_prod >= 0) mul_cas_i64<Space>(L.acc[ch.a_prod] + static_cast<A>(slot * 8), x, status);
+      if (ch.a_k >= 0) {
+        double xf = (ch.ptype == P_U64) ? static_cast<double>(static_cast<uint64_t>(x))
+                                        : static_cast<double>(x);
+        double K = get_shift<Space>(L.acc[ch.a_k] + static_cast<A>(slot * 8), xf);
+        double d = xf - K;
+        Space::add_f64(L.acc[ch.a_s2] + static_cast<A>(slot * 8), d * d);
+      }
+    }
+  }
+}
+
+// Merges slot `s` of a (shared-memory) partial level into slot `g` of the
+// global level.
+template <class Src>
+__device__ __forceinline__ void merge_slot(const Plan& plan,
+                                           const Level<Src>& S,
+                                           int64_t s,
+                                           const Level<Global>& G,
+                                           int64_t g,
+                                           int32_t* status)
+{
+  using SA           = typename Src::addr_t;
+  uint32_t rows      = Src::ld_u32(S.rows + static_cast<SA>(s * 4));
+  Global::add_u32(G.rows + static_cast<uint64_t>(g * 4), rows);
+  for (int c = 0; c < plan.nchan; ++c) {
+    const Channel& ch = plan.chan[c];
+    uint32_t n        = rows;
+    if (ch.a_cnt >= 0) {
+      n = Src::ld_u32(S.acc[ch.a_cnt] + static_cast<SA>(s * 4));
+      Global::add_u32(G.acc[ch.a_cnt] + static_cast<uint64_t>(g * 4), n);
+    }
+    if (n == 0) continue;
+    const bool is64 = minmax_is64(ch.ptype);
+    if (ch.a_min >= 0) {
+      if (is64) Global::min_u64(G.acc[ch.a_min] + static_cast<uint64_t>(g * 8), Src::ld_u64(S.acc[ch.a_min] + static_cast<SA>(s * 8)));
+      else Global::min_u32(G.acc[ch.a_min] + static_cast<uint64_t>(g * 4), Src::ld_u32(S.acc[ch.a_min] + static_cast<SA>(s * 4)));
+    }
+    if (ch.a_max >= 0) {
+      if (is64) Global::max_u64(G.acc[ch.a_max] + static_cast<uint64_t>(g * 8), Src::ld_u64(S.acc[ch.a_max] + static_cast<SA>(s * 8)));
+      else Global::max_u32(G.acc[ch.a_max] + static_cast<uint64_t>(g * 4), Src::ld_u32(S.acc[ch.a_max] + static_cast<SA>(s * 4)));
+    }
+    if (ch.is_float) {
+      if (ch.a_sum >= 0)
+        Global::add_f64(G.acc[ch.a_sum] + static_cast<uint64_t>(g * 8),
+                        __longlong_as_double(static_cast<long long>(Src::ld_u64(S.acc[ch.a_sum] + static_cast<SA>(s * 8)))));
+      if (ch.a_sq >= 0)
+        Global::add_f64(G.acc[ch.a_sq] + static_cast<uint64_t>(g * 8),
+                        __longlong_as_double(static_cast<long long>(Src::ld_u64(S.acc[ch.a_sq] + static_cast<SA>(s * 8)))));
+      if (ch.a_prod >= 0)
+        mul_cas_f64<Global>(G.acc[ch.a_prod] + static_cast<uint64_t>(g * 8),
+                            __longlong_as_double(static_cast<long long>(Src::ld_u64(S.acc[ch.a_prod] + static_cast<SA>(s * 8)))),
+                            status);
+    } else {
+      if (ch.a_sum >= 0)
+        Global::add_u64(G.acc[ch.a_sum] + static_cast<uint64_t>(g * 8), Src::ld_u64(S.acc[ch.a_sum] + static_cast<SA>(s * 8)));
+      if (ch.a_sq >= 0)
+        Global::add_u64(G.acc[ch.a_sq] + static_cast<uint64_t>(g * 8), Src::ld_u64(S.acc[ch.a_sq] + static_cast<SA>(s * 8)));
+      if (ch.a_prod >= 0)
+        mul_cas_i64<Global>(G.acc[ch.a_prod] + static_cast<uint64_t>(g * 8),
+                            static_cast<int64_t>(Src::ld_u64(S.acc[ch.a_prod] + static_cast<SA>(s * 8))), status);
+    }
+    if (ch.a_k >= 0) {
+      uint64_t kpb = Src::ld_u64(S.acc[ch.a_k] + static_cast<SA>(s * 8));
+      double s2p   = __longlong_as_double(static_cast<long long>(Src::ld_u64(S.acc[ch.a_s2] + static_cast<SA>(s * 8))));
+      if (kpb == kShiftUnset) {
+        // every valid value was NaN: the partial square sum is NaN already
+        Global::add_f64(G.acc[ch.a_s2] + static_cast<uint64_t>(g * 8), s2p);
+      } else {
+        double Kp   = __longlong_as_double(static_cast<long long>(kpb));
+        double Kg   = get_shift<Global>(G.acc[ch.a_k] + static_cast<uint64_t>(g * 8), Kp);
+        double sump = ch.is_float
+                        ? __longlong_as_double(static_cast<long long>(Src::ld_u64(S.acc[ch.a_sum] + static_cast<SA>(s * 8))))
+                        : (ch.ptype == P_U64 ? static_cast<double>(Src::ld_u64(S.acc[ch.a_sum] + static_cast<SA>(s * 8)))
+                                             : static_cast<double>(static_cast<int64_t>(Src::ld_u64(S.acc[ch.a_sum] + static_cast<SA>(s * 8)))));
+        double S1 = sump - static_cast<double>(n) * Kp;
+        double d  = Kp - Kg;
+        Global::add_f64(G.acc[ch.a_s2] + static_cast<uint64_t>(g * 8), s2p + 2.0 * d * S1 + static_cast<double>(n) * d * d);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ Level<Global> global_level(const TableRef& t, const AccLayout& al)
+{
+  Level<Global> L;
+  L.rows = reinterpret_cast<uint64_t>(t.rows);
+  for (int a = 0; a < al.nacc; ++a) L.acc[a] = reinterpret_cast<uint64_t>(t.acc[a]);
+  return L;
+}
+
+// Global find-or-insert for one key, including the reserved all-ones slot.
+template <int NW>
+__device__ __forceinline__ int64_t global_slot(const TableRef& t,
+                                               const uint64_t (&k)[NW],
+                                               uint32_t max_probes)
+{
+  if (key_is_empty<NW>(k)) {
+    if (Global::ld_u32(reinterpret_cast<uint64_t>(t.special_used)) == 0) atomicExch(t.special_used, 1u);
+    return static_cast<int64_t>(t.cap);
+  }
+  int64_t s = find_or_insert<Global, NW>(reinterpret_cast<uint64_t>(t.keys), t.cap - 1, k, hash_key<NW>(k),
+                                         max_probes);
+  if (s < 0) atomicOr(t.status, S_TABLE_FULL);
+  return s;
+}
+
+}  // namespace dev
+
+using namespace dev;
+
+// ----------------------------------------------------------------- kernels
+
+__global__ void k_init_table(TableRef t, AccLayout al, int nwords)
+{
+  const uint64_t n      = t.cap + 1;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t s = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < n; s += stride) {
+    for (int w = 0; w < nwords; ++w) t.keys[s * nwords + w] = kEmptyWord;
+    t.rows[s] = 0;
+    for (int a = 0; a < al.nacc; ++a) {
+      uint64_t id = identity_bits(al.kind[a]);
+      if (acc_bytes(al.kind[a]) == 4) reinterpret_cast<uint32_t*>(t.acc[a])[s] = static_cast<uint32_t>(id);
+      else reinterpret_cast<uint64_t*>(t.acc[a])[s] = id;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *t.special_used = 0;
+}
+
+template <int NW>
+__global__ void k_agg_global(Plan plan, TableRef t, int64_t n, uint32_t max_probes)
+{
+  const Level<Global> G = global_level(t, plan.acc);
+  const int64_t stride  = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
+    uint64_t k[NW];
+    if (!pack_key<NW>(plan.key, r, k)) continue;
+    int64_t g = global_slot<NW>(t, k, max_probes);
+    if (g < 0) continue;
+    accumulate_row<Global>(plan, G, g, r, t.status);
+  }
+}
+
+// Per-CTA privatised aggregation.  Shared memory holds S+1 slots (slot S is
+// the reserved all-ones key): keys, row counts and every accumulator array.
+template <int NW>
+__global__ void __launch_bounds__(512) k_agg_privatized(Plan plan,
+                                                        TableRef t,
+                                                        SmemLayout sl,
+                                                        int64_t n,
+                                                        int64_t rows_per_block,
+                                                        uint32_t smem_probes,
+                                                        uint32_t max_probes)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t s_special;
+  const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const uint32_t S    = sl.slots;
+  Level<Shared> L;
+  L.rows = base + sl.rows_off;
+  for (int a = 0; a < plan.acc.nacc; ++a) L.acc[a] = base + sl.acc_off[a];
+  const uint32_t keys = base + sl.keys_off;
+
+  // identity fill
+  uint64_t* skeys = reinterpret_cast<uint64_t*>(smem + sl.keys_off);
+  uint32_t* srows = reinterpret_cast<uint32_t*>(smem + sl.rows_off);
+  for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) {
+    for (int w = 0; w < NW; ++w) skeys[s * NW + w] = kEmptyWord;
+    srows[s] = 0;
+    for (int a = 0; a < plan.acc.nacc; ++a) {
+      uint64_t id = identity_bits(plan.acc.kind[a]);
+      if (acc_bytes(plan.acc.kind[a]) == 4) reinterpret_cast<uint32_t*>(smem + sl.acc_off[a])[s] = static_cast<uint32_t>(id);
+      else reinterpret_cast<uint64_t*>(smem + sl.acc_off[a])[s] = id;
+    }
+  }
+  if (threadIdx.x == 0) s_special = 0;
+  __syncthreads();
+
+  const Level<Global> G = global_level(t, plan.acc);
+  const int64_t begin   = static_cast<int64_t>(blockIdx.x) * rows_per_block;
+  const int64_t end     = min(n, begin + rows_per_block);
+  for (int64_t r = begin + threadIdx.x; r < end; r += blockDim.x) {
+    uint64_t k[NW];
+    if (!pack_key<NW>(plan.key, r, k)) continue;
+    int64_t s;
+    if (key_is_empty<NW>(k)) {
+      s = S;
+      if (s_special == 0) s_special = 1;
+    } else {
+      s = find_or_insert<Shared, NW>(keys, S - 1, k, hash_key<NW>(k), smem_probes);
+    }
+    if (s >= 0) {
+      accumulate_row<Shared>(plan, L, s, r, t.status);
+    } else {
+      int64_t g = global_slot<NW>(t, k, max_probes);
+      if (g >= 0) accumulate_row<Global>(plan, G, g, r, t.status);
+    }
+  }
+  __syncthreads();
+
+  // flush the partial table into the global one
+  for (uint32_t s = threadIdx.x; s <= S; s += blockDim.x) {
+    uint64_t k[NW];
+    for (int w = 0; w < NW; ++w) k[w] = skeys[s * NW + w];
+    bool occupied = (s < S) ? !key_is_empty<NW>(k) : (s_special != 0);
+    if (!occupied) continue;
+    int64_t g = global_slot<NW>(t, k, max_probes);
+    if (g >= 0) merge_slot<Shared>(plan, L, s, G, g, t.status);
+  }
+}
+
+// Sampled distinct count: inserts a strided sample of packed keys (folded to
+// 64 bits) into a small global set and counts first insertions.
+template <int NW>
+__global__ void k_sample_distinct(KeyPlan kp,
+                                  int64_t n,
+                                  int64_t nsample,
+                                  uint64_t* set,
+                                  uint64_t set_mask,
+                                  unsigned long long* counters)
+{
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nsample; i += stride) {
+    int64_t r = static_cast<int64_t>((static_cast<double>(i) + 0.5) * static_cast<double>(n) / static_cast<double>(nsample));
+    if (r >= n) r = n - 1;
+    uint64_t k[NW];
+    if (!pack_key<NW>(kp, r, k)) continue;
+    atomicAdd(&counters[0], 1ULL);
+    uint64_t f[1] = {hash_key<NW>(k)};
+    if (f[0] == kEmptyWord) f[0] = 0;
+    uint64_t s = fmix64(f[0] ^ 0x5bd1e995ULL) & set_mask;
+    for (uint64_t p = 0; p <= set_mask; ++p) {
+      uint64_t old = atomicCAS(reinterpret_cast<unsigned long long*>(set + s), kEmptyWord, f[0]);
+      if (old == kEmptyWord) {
+        atomicAdd(&counters[1], 1ULL);
+        break;
+      }
+      if (old == f[0]) break;
+      s = (s + 1) & set_mask;
+    }
+  }
+}
+
+__global__ void k_fill_u64(uint64_t* p, uint64_t n, uint64_t v)
+{
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+
+struct OccupiedPred {
+  const uint64_t* keys;
+  const uint32_t* special_used;
+  uint64_t cap;
+  int nwords;
+  __device__ __forceinline__ bool operator()(const uint32_t& s) const
+  {
+    if (s == cap) return *special_used != 0;
+    if (nwords == 1) return keys[s] != kEmptyWord;
+    return !(keys[2 * (uint64_t)s] == kEmptyWord && keys[2 * (uint64_t)s + 1] == kEmptyWord);
+  }
+};
+
+// ------------------------------------------------------------- finalize
+
+__device__ __forceinline__ void store_bits(void* p, int64_t i, int width, uint64_t v)
+{
+  switch (width) {
+    case 1: reinterpret_cast<uint8_t*>(p)[i] = static_cast<uint8_t>(v); break;
+    case 2: reinterpret_cast<uint16_t*>(p)[i] = static_cast<uint16_t>(v); break;
+    case 4: reinterpret_cast<uint32_t*>(p)[i] = static_cast<uint32_t>(v); break;
+    default: reinterpret_cast<uint64_t*>(p)[i] = v; break;
+  }
+}
+
+__device__ __forceinline__ uint64_t ld_acc(const TableRef& t, int a, uint64_t s, int bytes)
+{
+  if (bytes == 4) return reinterpret_cast<const uint32_t*>(t.acc[a])[s];
+  return reinterpret_cast<const uint64_t*>(t.acc[a])[s];
+}
+
+__global__ void k_finalize(Plan plan, TableRef t, const uint32_t* map, int64_t G, OutPlan op)
+{
+  const int lane        = threadIdx.x & 31;
+  const int64_t wstride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < G;
+       base += wstride) {
+    const int64_t g    = base + lane;
+    const bool active  = g < G;
+    const uint64_t s   = active ? map[g] : 0;
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    uint64_t k[2]      = {0, 0};
+    if (active) {
+      for (int w = 0; w < plan.key.nwords; ++w) k[w] = t.keys[s * plan.key.nwords + w];
+      if (s == t.cap) k[0] = k[1] = kEmptyWord;
+    }
+    // keys
+    for (int c = 0; c < plan.key.ncols; ++c) {
+      const KeyCol& kc = plan.key.cols[c];
+      uint64_t word    = k[kc.word];
+      bool valid       = true;
+      if (kc.null_bit) valid = ((k[kc.null_word] >> kc.null_shift) & 1ULL) == 0;
+      if (active) {
+        int bits   = kc.width * 8;
+        uint64_t v = (bits == 64) ? word : ((word >> kc.shift) & ((1ULL << bits) - 1));
+        store_bits(op.key_data[c], g, kc.width, valid ? v : 0);
+      }
+      if (op.key_mask[c] != nullptr) {
+        uint32_t bal = __ballot_sync(0xffffffffu, active && valid);
+        if (lane == 0) {
+          op.key_mask[c][base >> 5] = bal;
+          uint32_t nulls = __popc(act & ~bal);
+          if (nulls) atomicAdd(op.null_counts + c, static_cast<unsigned long long>(nulls));
+        }
+      }
+    }
+    // results
+    for (int o = 0; o < op.nout; ++o) {
+      const OutCol& oc  = op.out[o];
+      const Channel& ch = plan.chan[oc.chan];
+      bool valid        = false;
+      uint64_t vbits    = 0;
+      if (active) {
+        uint32_t rows = t.rows[s];
+        uint32_t cnt  = (ch.a_cnt >= 0) ? reinterpret_cast<const uint32_t*>(t.acc[ch.a_cnt])[s] : rows;
+        valid         = cnt > 0;
+        switch (oc.kind) {
+          case GBX_AGG_COUNT_VALID: vbits = cnt; valid = true; break;
+          case GBX_AGG_COUNT_ALL: vbits = rows; valid = true; break;
+          case GBX_AGG_SUM:
+          case GBX_AGG_SUM_OF_SQUARES:
+          case GBX_AGG_PRODUCT: {
+            int a = (oc.kind == GBX_AGG_SUM) ? ch.a_sum : (oc.kind == GBX_AGG_PRODUCT ? ch.a_prod : ch.a_sq);
+            uint64_t raw = ld_acc(t, a, s, 8);
+            if (ch.is_float) {
+              double x = __longlong_as_double(static_cast<long long>(raw));
+              vbits    = (oc.out_ptype == P_F32) ? __float_as_uint(static_cast<float>(x))
+                                                 : static_cast<uint64_t>(__double_as_longlong(x));
+            } else {
+              vbits = raw;  // truncated to the output width on store (wraps like the reference)
+            }
+            break;
+          }
+          case GBX_AGG_MIN:
+          case GBX_AGG_MAX: {
+            bool mn      = oc.kind == GBX_AGG_MIN;
+            int a        = mn ? ch.a_min : ch.a_max;
+            uint64_t raw = ld_acc(t, a, s, minmax_is64(ch.ptype) ? 8 : 4);
+            vbits        = dec_minmax(raw, ch.ptype, mn);
+            break;
+          }
+          case GBX_AGG_MEAN: {
+            if (!valid) break;
+            uint64_t raw = ld_acc(t, ch.a_sum, s, 8);
+            if (oc.out_ptype == P_F64) {
+              // integer SUMs are INT64 (target_type), so the mean divides the
+              // signed 64-bit sum, as binary_operation(DIV) does on it
+              double sum = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
+                                       : static_cast<double>(static_cast<int64_t>(raw));
+              vbits = static_cast<uint64_t>(__double_as_longlong(sum / static_cast<double>(cnt)));
+            } else {
+              // duration / decimal MEAN: the SUM wraps to the source width, then
+              // integer division (binary_operation DIV, hash/groupby.cu:298-304)
+              int64_t sw = static_cast<int64_t>(raw);
+              if (oc.out_width == 4) sw = static_cast<int32_t>(static_cast<uint32_t>(raw));
+              vbits = static_cast<uint64_t>(sw / static_cast<int64_t>(cnt));
+            }
+            break;
+          }
+          case GBX_AGG_VARIANCE:
+          case GBX_AGG_STD: {
+            int64_t nn = cnt;
+            if (nn == 0 || nn - oc.ddof <= 0) {
+              valid = false;
+              break;
+            }
+            uint64_t kb = ld_acc(t, ch.a_k, s, 8);
+            double s2   = __longlong_as_double(static_cast<long long>(ld_acc(t, ch.a_s2, s, 8)));
+            double var;
+            if (kb == kShiftUnset) {
+              var = s2;  // NaN inputs only
+            } else {
+              double K      = __longlong_as_double(static_cast<long long>(kb));
+              uint64_t raw  = ld_acc(t, ch.a_sum, s, 8);
+              double sum    = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
+                                          : (ch.ptype == P_U64 ? static_cast<double>(raw)
+                                                               : static_cast<double>(static_cast<int64_t>(raw)));
+              double S1 = sum - static_cast<double>(nn) * K;
+              double M2 = s2 - S1 * S1 / static_cast<double>(nn);
+              if (M2 < 0.0) M2 = 0.0;
+              var = M2 / static_cast<double>(nn - oc.ddof);
+            }
+            if (oc.kind == GBX_AGG_STD) var = sqrt(var);
+            vbits = static_cast<uint64_t>(__double_as_longlong(var));
+            valid = true;
+            break;
+          }
+          default: break;
+        }
+        store_bits(oc.data, g, oc.out_width, valid ? vbits : 0);
+      }
+      if (oc.mask != nullptr) {
+        uint32_t bal = __ballot_sync(0xffffffffu, active && valid);
+        if (lane == 0) {
+          oc.mask[base >> 5] = bal;
+          uint32_t nulls = __popc(act & ~bal);
+          if (nulls) atomicAdd(op.null_counts + kMaxKeyCols + o, static_cast<unsigned long long>(nulls));
+        }
+      }
+    }
+  }
+}
+
+// -------------------------------------------------------------- launchers
+
+namespace {
+inline int grid_for(int64_t work, int block, int max_blocks)
+{
+  int64_t b = (work + block - 1) / block;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return static_cast<int>(b);
+}
+}  // namespace
+
+cudaError_t launch_init_table(const TableRef& t, const AccLayout& al, int nwords, int num_sms, cudaStream_t st)
+{
+  int grid = grid_for(static_cast<int64_t>(t.cap + 1), 256, num_sms * 16);
+  k_init_table<<<grid, 256, 0, st>>>(t, al, nwords);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sample(const KeyPlan& kp, int64_t n, int64_t nsample, uint64_t* set, uint64_t set_cap,
+                          unsigned long long* counters, int num_sms, cudaStream_t st)
+{
+  k_fill_u64<<<grid_for(static_cast<int64_t>(set_cap), 256, num_sms * 8), 256, 0, st>>>(set, set_cap, kEmptyWord);
+  cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st);
+  int grid = grid_for(nsample, 256, num_sms * 8);
+  if (kp.nwords == 1) k_sample_distinct<1><<<grid, 256, 0, st>>>(kp, n, nsample, set, set_cap - 1, counters);
+  else k_sample_distinct<2><<<grid, 256, 0, st>>>(kp, n, nsample, set, set_cap - 1, counters);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_agg_global(const Plan& p, const TableRef& t, int64_t n, uint32_t max_probes, int num_sms,
+                              cudaStream_t st)
+{
+  int grid = grid_for(n, 256, num_sms * 8);
+  if (p.key.nwords == 1) k_agg_global<1><<<grid, 256, 0, st>>>(p, t, n, max_probes);
+  else k_agg_global<2><<<grid, 256, 0, st>>>(p, t, n, max_probes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int block,
+                                  int grid, uint32_t smem_probes, uint32_t max_probes, cudaStream_t st)
+{
+  int64_t rpb = (n + grid - 1) / grid;
+  cudaError_t e;
+  if (p.key.nwords == 1) {
+    e = cudaFuncSetAttribute(k_agg_privatized<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl.total);
+    if (e != cudaSuccess) return e;
+    k_agg_privatized<1><<<grid, block, sl.total, st>>>(p, t, sl, n, rpb, smem_probes, max_probes);
+  } else {
+    e = cudaFuncSetAttribute(k_agg_privatized<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl.total);
+    if (e != cudaSuccess) return e;
+    k_agg_privatized<2><<<grid, block, sl.total, st>>>(p, t, sl, n, rpb, smem_probes, max_probes);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t compact_occupied(const TableRef& t, int nwords, uint32_t* map, int64_t* num_selected, void* temp,
+                             size_t* temp_bytes, cudaStream_t st)
+{
+  OccupiedPred pred{t.keys, t.special_used, t.cap, nwords};
+  thrust::counting_iterator<uint32_t> it(0);
+  return cub::DeviceSelect::If(temp, *temp_bytes, it, map, num_selected, static_cast<int64_t>(t.cap + 1), pred, st);
+}
+
+cudaError_t launch_finalize(const Plan& p, const TableRef& t, const uint32_t* map, int64_t G, const OutPlan& op,
+                            int num_sms, cudaStream_t st)
+{
+  if (G <= 0) return cudaSuccess;
+  int grid = grid_for(G, 256, num_sms * 8);
+  k_finalize<<<grid, 256, 0, st>>>(p, t, map, G, op);
+  return cudaGetLastError();
+}
+
+}  // namespace gbx
+
+namespace gbx {
+
+// Valid-bit counts of several masks (one grid-stride sweep per mask).
+__global__ void k_count_valid(MaskSpans ms, unsigned long long* out)
+{
+  const int64_t tid    = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int c = 0; c < ms.n; ++c) {
+    const MaskSpan sp = ms.span[c];
+    const int64_t b0  = sp.offset;
+    const int64_t b1  = sp.offset + sp.size;
+    const int64_t w0  = b0 >> 5;
+    const int64_t w1  = (b1 + 31) >> 5;
+    unsigned long long local = 0;
+    for (int64_t w = w0 + tid; w < w1; w += stride) {
+      uint32_t word = __ldg(sp.mask + w);
+      int64_t lo    = w << 5;
+      if (lo < b0) word &= 0xffffffffu << (b0 - lo);
+      if (lo + 32 > b1) word &= 0xffffffffu >> (lo + 32 - b1);
+      local += __popc(word);
+    }
+    for (int off = 16; off > 0; off >>= 1) local += __shfl_down_sync(0xffffffffu, local, off);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(out + c, local);
+  }
+}
+
+cudaError_t launch_count_valid(const MaskSpans& ms, unsigned long long* out_valid, int num_sms, cudaStream_t st)
+{
+  if (ms.n == 0) return cudaSuccess;
+  int64_t words = 0;
+  for (int c = 0; c < ms.n; ++c) words = words > (ms.span[c].size / 32 + 2) ? words : (ms.span[c].size / 32 + 2);
+  int64_t b = (words + 255) / 256;
+  if (b < 1) b = 1;
+  if (b > num_sms * 4) b = num_sms * 4;
+  k_count_valid<<<static_cast<int>(b), 256, 0, st>>>(ms, out_valid);
+  return cudaGetLastError();
+}
+
+}  // namespace gbx

@@ -1,0 +1,91 @@
+"""Seeded synthetic inputs with the shapes and distributions of the groupby
+benchmark workloads (plain: 10M / 100M / 200M rows; batched: 4,096
+instances; served: a Poisson request stream).  No public dataset is used.
+
+Every generator takes the row count so the same distribution serves the
+full-size benchmark and the small parity cases.  Seeds are 20241003 + the
+workload number.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+SEED0 = 20241003
+
+
+@dataclass
+class PlainInput:
+    """Key columns and value columns as host numpy arrays (validity optional)."""
+
+    keys: List[np.ndarray]
+    key_valid: List[Optional[np.ndarray]]
+    values: List[np.ndarray]
+    value_valid: List[Optional[np.ndarray]]
+    name: str
+
+    @property
+    def rows(self) -> int:
+        return len(self.keys[0])
+
+    def input_bytes(self) -> int:
+        b = 0
+        for a, m in zip(self.keys + self.values, self.key_valid + self.value_valid):
+            b += a.nbytes + (0 if m is None else (len(m) + 7) // 8)
+        return b
+
+
+def plain_10m(n: int = 10_000_000, seed: int = SEED0 + 1) -> PlainInput:
+    """int32 key uniform over 1,000 values; float64 ~N(0,1); no nulls."""
+    rng = np.random.default_rng(seed)
+    k = rng.integers(0, 1000, size=n, dtype=np.int32)
+    v = rng.standard_normal(n)
+    return PlainInput([k], [None], [v], [None], f"plain int32 key, 1e3 groups, {n} rows")
+
+
+def plain_100m(cardinality: int, n: int = 100_000_000, seed: int = SEED0 + 2) -> PlainInput:
+    """int64 key uniform over `cardinality`; int64 uniform in [-1e6, 1e6];
+    float32 ~N(0,1) with 10% nulls (Bernoulli)."""
+    rng = np.random.default_rng(seed + cardinality)
+    k = rng.integers(0, cardinality, size=n, dtype=np.int64)
+    a = rng.integers(-1_000_000, 1_000_000, size=n, dtype=np.int64, endpoint=True)
+    b = rng.standard_normal(n, dtype=np.float32)
+    bv = rng.random(n) >= 0.10
+    return PlainInput([k], [None], [a, b], [None, bv], f"plain int64 key, C={cardinality:g}, {n} rows")
+
+
+def zipf_ranks(rng, n: int, s: float = 1.2, ranks: int = 100_000) -> np.ndarray:
+    """Inverse-CDF sampling of a Zipf(s) law truncated to `ranks` ranks (0-based)."""
+    w = np.arange(1, ranks + 1, dtype=np.float64) ** (-s)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    u = rng.random(n)
+    return np.minimum(np.searchsorted(cdf, u, side="right"), ranks - 1)
+
+
+def plain_200m(n: int = 200_000_000, seed: int = SEED0 + 3, ranks: int = 100_000) -> PlainInput:
+    """Composite (int32, int16) key, joint index Zipf(1.2) over `ranks` distinct
+    pairs; 2% nulls per key column; float64 ~LogNormal(0, 1)."""
+    rng = np.random.default_rng(seed)
+    # fixed random distinct pairs
+    pairs = set()
+    k1 = np.empty(ranks, np.int32)
+    k2 = np.empty(ranks, np.int16)
+    i = 0
+    while i < ranks:
+        a = int(rng.integers(-2**31, 2**31 - 1))
+        b = int(rng.integers(-2**15, 2**15 - 1))
+        if (a, b) in pairs:
+            continue
+        pairs.add((a, b))
+        k1[i], k2[i] = a, b
+        i += 1
+    j = zipf_ranks(rng, n, 1.2, ranks)
+    c1 = k1[j]
+    c2 = k2[j]
+    v1 = rng.random(n) >= 0.02
+    v2 = rng.random(n) >= 0.02
+    v = rng.lognormal(0.0, 1.0, n)
+    return PlainInput([c1, c2], [v1, v2], [v], [None], f"plain (int32,int16) Zipf(1.2) key, {n} rows")

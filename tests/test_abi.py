@@ -1,0 +1,154 @@
+"""CPU tests of the drop-in boundary: libgbx.so loads and exports every entry
+point include/gbx.h declares, the ctypes mirror matches the C layout, the
+target-type table matches the oracle's restatement, and host-side validation
+(which runs before any CUDA call) behaves like the reference's CUDF_EXPECTS."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from cudf_b200 import _abi, _lib
+from cudf_b200._abi import Kind, TypeId
+from oracle import oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "gbx.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"GBX_API\s+[\w\s\*]+?\b(gbx_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.lib()
+    names = declared_symbols()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), f"{n} missing from libgbx.so"
+        assert n in _abi.SIGNATURES, f"{n} has no ctypes signature"
+    assert lib.gbx_abi_version() == 1
+
+
+STRUCTS = ["gbx_column_view", "gbx_table_view", "gbx_aggregation", "gbx_request", "gbx_allocator",
+           "gbx_column", "gbx_aggregation_result", "gbx_result", "gbx_stats"]
+
+
+def test_ctypes_layout_matches_c_header(tmp_path):
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    for s in STRUCTS:
+        ct = getattr(_abi, s)
+        lines.append(f'printf("{s} %zu\\n", sizeof({s}));')
+        for fname, _ in ct._fields_:
+            lines.append(f'printf("{s}.{fname} %zu\\n", offsetof({s}, {fname}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    c_layout = dict(l.rsplit(" ", 1) for l in out if l)
+    for s in STRUCTS:
+        ct = getattr(_abi, s)
+        assert int(c_layout[s]) == C.sizeof(ct), s
+        for fname, _ in ct._fields_:
+            assert int(c_layout[f"{s}.{fname}"]) == getattr(ct, fname).offset, f"{s}.{fname}"
+
+
+def test_target_types_match_oracle():
+    lib = _lib.lib()
+    hash_kinds = {Kind.SUM, Kind.PRODUCT, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.COUNT_ALL,
+                  Kind.SUM_OF_SQUARES, Kind.MEAN, Kind.VARIANCE, Kind.STD}
+    for t in TypeId:
+        for k in Kind:
+            want = orc.target_type(t, k) if k in hash_kinds else 0
+            assert lib.gbx_target_type(int(t), int(k)) == want, (t.name, k.name)
+
+
+def _keys_view(n=3):
+    arr = np.arange(n, dtype=np.int32)
+    cv = _abi.gbx_column_view()
+    cv.type_id = TypeId.INT32
+    cv.size = n
+    cv.data = arr.ctypes.data  # never dereferenced: validation fails first
+    cols = (_abi.gbx_column_view * 1)(cv)
+    tv = _abi.gbx_table_view(1, 0, C.cast(cols, C.POINTER(_abi.gbx_column_view)))
+    return tv, (arr, cols)
+
+
+def _request(n, kind):
+    r = _abi.gbx_request()
+    r.values.type_id = TypeId.INT32
+    r.values.size = n
+    aggs = (_abi.gbx_aggregation * 1)()
+    aggs[0].kind = int(kind)
+    r.num_aggregations = 1
+    r.aggregations = C.cast(aggs, C.POINTER(_abi.gbx_aggregation))
+    return r, aggs
+
+
+def test_size_mismatch_is_logic_error():
+    """keys_tests.cpp:227-243 / groupby.cu:210-214."""
+    lib = _lib.lib()
+    tv, keep = _keys_view(3)
+    h = C.c_void_p()
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == 0
+    r, keep2 = _request(5, Kind.COUNT_VALID)
+    out = C.POINTER(_abi.gbx_result)()
+    st = lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out))
+    assert st == _abi.Status.ERR_LOGIC
+    assert b"Size mismatch" in lib.gbx_last_error()
+    with pytest.raises(_lib.LogicError):
+        _lib.check(st)
+    lib.gbx_groupby_destroy(h)
+
+
+@pytest.mark.parametrize("kind,status", [(Kind.NTH_ELEMENT, _abi.Status.ERR_UNSUPPORTED),
+                                         (Kind.MEDIAN, _abi.Status.ERR_UNSUPPORTED),
+                                         (Kind.ARGMAX, _abi.Status.ERR_UNSUPPORTED)])
+def test_sort_only_kinds_are_reported(kind, status):
+    lib = _lib.lib()
+    tv, keep = _keys_view(3)
+    h = C.c_void_p()
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == 0
+    r, keep2 = _request(3, kind)
+    out = C.POINTER(_abi.gbx_result)()
+    assert lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out)) == status
+    assert lib.gbx_can_use_hash_groupby(C.byref(r), 1) == 0
+    lib.gbx_groupby_destroy(h)
+
+
+def test_invalid_type_agg_combination_is_logic_error():
+    """VAR of a timestamp column: no target type (aggregation.hpp:1212-1335)."""
+    lib = _lib.lib()
+    tv, keep = _keys_view(3)
+    h = C.c_void_p()
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == 0
+    r, keep2 = _request(3, Kind.VARIANCE)
+    r.values.type_id = TypeId.TIMESTAMP_DAYS
+    out = C.POINTER(_abi.gbx_result)()
+    assert lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out)) == _abi.Status.ERR_LOGIC
+    assert lib.gbx_can_use_hash_groupby(C.byref(r), 1) == 0
+    lib.gbx_groupby_destroy(h)
+
+
+def test_create_rejects_string_keys_and_bad_policy():
+    lib = _lib.lib()
+    tv, keep = _keys_view(3)
+    h = C.c_void_p()
+    assert lib.gbx_groupby_create(C.byref(tv), 7, 0, C.byref(h)) == _abi.Status.ERR_LOGIC
+    keep[1][0].type_id = TypeId.STRING
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == _abi.Status.ERR_UNSUPPORTED
+
+
+def test_can_use_hash_groupby_for_hash_kinds():
+    lib = _lib.lib()
+    for k in (Kind.SUM, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.MEAN, Kind.VARIANCE, Kind.STD):
+        r, keep = _request(3, k)
+        assert lib.gbx_can_use_hash_groupby(C.byref(r), 1) == 1
