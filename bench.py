@@ -1,0 +1,498 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 hash groupby (libgbx) on the 100M-row workload.
+
+Workload (one "step"): four plain groupbys of 100,000,000 rows each, one per
+key cardinality C in {1e2, 1e4, 1e6, 1e8}: int64 key uniform over C values;
+value `a` int64 uniform in [-1e6, 1e6]; value `b` float32 ~N(0,1) with 10%
+nulls; SUM, COUNT, MIN, MAX, MEAN, VAR on both values.  Inputs are seeded
+synthetic data (no public dataset), generated on the device.  Inputs (2.01 GB
+per groupby) are larger than L2 (126 MB), so no L2 flush is needed.
+
+  value  -- rows/s over the whole job with inputs resident in HBM, through the
+            public API (cudf_b200.GroupBy.aggregate), CUDA events on the stream
+  e2e    -- same metric with host (pinned) inputs: every step copies inputs
+            host->device and reads all results back device->host
+  roofline -- the aggregation kernel: algorithmic input bytes / its
+            CUDA-event duration, against the measured HBM copy bandwidth
+
+`--impl reference` times the reference's CPU algorithm (the oracle
+restatement, all host threads) on a bounded sample of the same workload.
+Multi-GPU (torchrun): N independent replicas ("replicas only": a hash groupby
+of one input does not shard without an exchange step); value sums all ranks'
+rows over the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+CARDS = [100, 10_000, 1_000_000, 100_000_000]
+ROWS = 100_000_000
+BYTES_PER_ROW_IN = 8 + 8 + 4 + 1.0 / 8  # key + a + b + b's validity bit
+# output bytes per group: key 8; a: sum 8, count 4, min 8, max 8, mean 8, var 8;
+# b: sum 4, count 4, min 4, max 4, mean 8, var 8; validity bits
+BYTES_PER_GROUP_OUT = 8 + (8 + 4 + 8 + 8 + 8 + 8) + (4 + 4 + 4 + 4 + 8 + 8) + 6.0 / 8
+METRIC = "groupby rows/s (plain hash groupby, 100M rows, int64 key, cardinality 1e2/1e4/1e6/1e8)"
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--rows", type=int, default=ROWS)
+    p.add_argument("--cards", type=str, default=",".join(str(c) for c in CARDS))
+    p.add_argument("--cpu-sample-rows", type=int, default=2_000_000)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args(argv)
+
+
+# --------------------------------------------------------------- distributed
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Max of a per-rank float over all ranks (identity when world == 1)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm_sorted = sorted(sm)
+        return {"sm_mhz": sm_sorted[len(sm_sorted) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# -------------------------------------------------------------------- data
+
+def device_inputs(card: int, n: int, seed: int, device):
+    """The 100M-row workload's columns generated on the device (seeded)."""
+    import torch
+
+    from cudf_b200 import Column, TypeId
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed * 1_000_003 + card)
+    k = torch.randint(0, card, (n,), generator=g, device=device, dtype=torch.int64)
+    a = torch.randint(-1_000_000, 1_000_001, (n,), generator=g, device=device, dtype=torch.int64)
+    b = torch.randn(n, generator=g, device=device, dtype=torch.float32)
+    bvalid = torch.rand(n, generator=g, device=device) >= 0.10
+    words = pack_mask_torch(bvalid)
+    nulls = int(n - int(bvalid.sum().item()))
+    return (Column(TypeId.INT64, n, k), Column(TypeId.INT64, n, a),
+            Column(TypeId.FLOAT32, n, b, words, 0, nulls))
+
+
+def pack_mask_torch(valid):
+    """Bool tensor -> cudf bitmask words (int32, LSB-first) padded to 64 bytes."""
+    import torch
+
+    n = valid.numel()
+    nbits = ((n + 511) // 512) * 512
+    v = torch.zeros(nbits, dtype=torch.int64, device=valid.device)
+    v[:n] = valid.to(torch.int64)
+    w = (v.view(-1, 32) << torch.arange(32, device=valid.device, dtype=torch.int64)).sum(dim=1)
+    return torch.where(w >= (1 << 31), w - (1 << 32), w).to(torch.int32)
+
+
+def aggs():
+    from cudf_b200 import aggregation as agg
+
+    return [agg.sum(), agg.count(), agg.min(), agg.max(), agg.mean(), agg.variance()]
+
+
+# --------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from cudf_b200 import Column, GroupBy, GroupByRequest, Table, TorchAllocator
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+    cards = [int(c) for c in args.cards.split(",")]
+    n = args.rows
+    stream = torch.cuda.current_stream()
+    alloc = TorchAllocator(device)
+
+    data = {c: device_inputs(c, n, 20241003 + 2 + rank, device) for c in cards}
+    gbs = {}
+    reqs = {}
+    for c in cards:
+        k, a, b = data[c]
+        gb = GroupBy(Table([k]))
+        gb.set_timing(True)
+        gbs[c] = gb
+        reqs[c] = [GroupByRequest(a, aggs()), GroupByRequest(b, aggs())]
+    torch.cuda.synchronize()
+
+    def step(record=None):
+        for c in cards:
+            kt, res = gbs[c].aggregate(reqs[c], stream=stream, allocator=alloc)
+            if record is not None:
+                record.append((c, gbs[c].last_stats(), kt.num_rows()))
+            del kt, res
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    rec = []
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(rec)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_local = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms_local, world, device)
+    rows_per_step = n * len(cards)
+    value = world * rows_per_step * args.steps / (ms / 1e3)
+
+    # per-cardinality breakdown and the aggregation kernel's roofline
+    import json as _json
+
+    peaks = _load_peaks()
+    per = {}
+    agg_ms_total = 0.0
+    agg_bytes_total = 0.0
+    launches = 0
+    for c, st, g in rec:
+        d = per.setdefault(c, {"calls": 0, "total_ms": 0.0, "aggregate_ms": 0.0, "groups": g,
+                               "strategy": st["strategy"], "phases_ms": {}})
+        d["calls"] += 1
+        d["total_ms"] += st["total_ms"]
+        d["aggregate_ms"] += st["aggregate_ms"]
+        for ph in ("sample_ms", "init_ms", "aggregate_ms", "compact_ms", "finalize_ms"):
+            d["phases_ms"][ph] = d["phases_ms"].get(ph, 0.0) + st[ph]
+        agg_ms_total += st["aggregate_ms"]
+        agg_bytes_total += n * BYTES_PER_ROW_IN
+        launches += st["kernel_launches"]
+    per_out = {}
+    for c, d in per.items():
+        calls = d["calls"]
+        call_ms = d["total_ms"] / calls
+        groups = d["groups"]
+        alg = n * BYTES_PER_ROW_IN + groups * BYTES_PER_GROUP_OUT
+        per_out[f"{c:g}"] = {
+            "groups": groups, "strategy": d["strategy"],
+            "ms_per_call": round(call_ms, 4),
+            "rows_per_s": n / (call_ms / 1e3),
+            "hbm_frac_whole_call": (alg / (call_ms / 1e3)) / 1e9 / peaks["hbm_gbs"],
+            "phases_ms": {k: round(v / calls, 4) for k, v in d["phases_ms"].items()},
+        }
+    achieved = (agg_bytes_total / (agg_ms_total / 1e3)) / 1e9 if agg_ms_total > 0 else None
+    traffic = _load_traffic()
+    roofline = {
+        "bound": "hbm", "kernel": "aggregation pass (k_agg_*)",
+        "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
+        "peak_source": peaks["source"],
+        "traffic": traffic,
+        "algorithmic_bytes_per_launch": n * BYTES_PER_ROW_IN,
+    }
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, cards)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64+f32 (f64 accumulation)",
+        "data": "synthetic (seeded, generated on device)",
+        "config": {"workload": "plain groupby, 100M rows x 4 cardinalities", "rows": n, "cardinalities": cards,
+                   "key": "int64", "values": ["int64 U[-1e6,1e6]", "float32 N(0,1) 10% nulls"],
+                   "aggregations": ["SUM", "COUNT", "MIN", "MAX", "MEAN", "VAR"],
+                   "l2": "inputs (2.01 GB per groupby) larger than L2; no flush",
+                   "parallelism": f"replicas x{world}"},
+        "per_cardinality": per_out,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
+    """Host-resident inputs: H2D copies and D2H result reads inside the timed region."""
+    import torch
+
+    from cudf_b200 import Column, GroupBy, GroupByRequest, Table
+
+    host = {}
+    dev = {}
+    for c in cards:
+        k, a, b = data[c]
+        host[c] = [k.data.cpu().pin_memory(), a.data.cpu().pin_memory(), b.data.cpu().pin_memory(),
+                   b.mask.cpu().pin_memory()]
+        dev[c] = [torch.empty_like(t, device=device) for t in host[c]]
+    h2d = sum(t.numel() * t.element_size() for c in cards for t in host[c])
+    d2h_bytes = [0]
+
+    def step():
+        for c in cards:
+            hk, ha, hb, hm = host[c]
+            dk, da, db, dm = dev[c]
+            for s_, d_ in zip(host[c], dev[c]):
+                d_.copy_(s_, non_blocking=True)
+            n = dk.numel()
+            kc = Column(data[c][0].type_id, n, dk)
+            ac = Column(data[c][1].type_id, n, da)
+            bc = Column(data[c][2].type_id, n, db, dm, 0, data[c][2]._null_count)
+            gb = GroupBy(Table([kc]))
+            kt, res = gb.aggregate([GroupByRequest(ac, aggs()), GroupByRequest(bc, aggs())], stream=stream,
+                                   allocator=alloc)
+            outs = [col for col in kt.columns()] + [col for t in res for col in t.columns()]
+            got = 0
+            for col in outs:
+                if col.data is not None:
+                    got += col.data.numel() * col.data.element_size()
+                    col.data.cpu()
+                if col.mask is not None:
+                    got += col.mask.numel() * col.mask.element_size()
+                    col.mask.cpu()
+            d2h_bytes[0] = got if c == cards[0] else d2h_bytes[0] + got
+
+    step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = max(1, min(args.steps, 2))
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, device)
+    rows = args.rows * len(cards) * steps * world
+    return {"value": rows / (ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h_bytes[0],
+            "steps": steps, "ms_per_step": ms / steps}
+
+
+# ----------------------------------------------------------- CPU baselines
+
+def _sample_inputs(cards, rows):
+    from cudf_b200 import workloads as W
+
+    return {c: W.plain_100m(c, n=rows) for c in cards}
+
+
+def _oracle_requests(d):
+    from cudf_b200._abi import Kind
+    from oracle.oracle import HostCol
+
+    a6 = [(Kind.SUM, 0), (Kind.COUNT_VALID, 0), (Kind.MIN, 0), (Kind.MAX, 0), (Kind.MEAN, 0), (Kind.VARIANCE, 1)]
+    return [HostCol(d.keys[0])], [(HostCol(d.values[0]), a6), (HostCol(d.values[1], d.value_valid[1]), a6)]
+
+
+def cpu_baseline(args, cards):
+    """The oracle (a C restatement of the reference's hash groupby) on a bounded
+    sample of the workload, single-threaded; pandas on the same sample."""
+    from oracle import oracle as orc
+
+    rows = args.cpu_sample_rows
+    samples = _sample_inputs(cards, rows)
+    t_total = 0.0
+    for c in cards:
+        keys, reqs = _oracle_requests(samples[c])
+        t0 = time.perf_counter()
+        orc.groupby(keys, reqs, 0, threads=1)
+        t_total += time.perf_counter() - t0
+    out = {"value": rows * len(cards) / t_total, "unit": "rows/s", "cores": 1, "kind": "port",
+           "sample": f"{rows} rows of each of the {len(cards)} cardinalities (same distributions, numpy seed)"}
+    try:
+        import numpy as np
+        import pandas as pd
+
+        tp = 0.0
+        for c in cards:
+            d = samples[c]
+            df = pd.DataFrame({"k": d.keys[0], "a": d.values[0],
+                               "b": np.where(d.value_valid[1], d.values[1], np.nan).astype(np.float32)})
+            t0 = time.perf_counter()
+            df.groupby("k", sort=False).agg({"a": ["sum", "count", "min", "max", "mean", "var"],
+                                              "b": ["sum", "count", "min", "max", "mean", "var"]})
+            tp += time.perf_counter() - t0
+        out["pandas_rows_per_s"] = rows * len(cards) / tp
+        out["pandas_version"] = pd.__version__
+    except Exception as e:  # pragma: no cover
+        out["pandas_error"] = str(e)
+    out["host_cpu_count"] = os.cpu_count()
+    return out
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's CPU algorithm (the oracle restatement)
+    with all host threads, on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+
+    cards = [int(c) for c in args.cards.split(",")]
+    rows = args.cpu_sample_rows
+    samples = _sample_inputs(cards, rows)
+    threads = os.cpu_count() or 1
+    prepared = {c: _oracle_requests(samples[c]) for c in cards}
+
+    def step():
+        for c in cards:
+            keys, reqs = prepared[c]
+            orc.groupby(keys, reqs, 0, threads=threads)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = rows * len(cards) * args.steps / dt
+    out = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "int64+f32 (long double accumulation)",
+           "data": "synthetic (seeded numpy)", "impl": "reference",
+           "config": {"workload": "plain groupby, 100M rows x 4 cardinalities (bounded CPU sample)",
+                      "rows": rows, "cardinalities": cards},
+           "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
+                            "sample": f"{rows} rows per cardinality per step"},
+           "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------- peaks
+
+def _load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return {"hbm_gbs": float(p["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
+
+
+def _load_traffic():
+    """DRAM bytes per aggregation launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("aggregate_dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

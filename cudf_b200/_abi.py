@@ -196,7 +196,13 @@ class gbx_stats(C.Structure):
         ("retries", C.c_int32),
         ("scratch_bytes", C.c_int64),
         ("kernel_launches", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("timed", C.c_int32),
+        ("sample_ms", C.c_float),
+        ("init_ms", C.c_float),
+        ("aggregate_ms", C.c_float),
+        ("compact_ms", C.c_float),
+        ("finalize_ms", C.c_float),
+        ("total_ms", C.c_float),
     ]
 
 
@@ -216,4 +222,5 @@ SIGNATURES = {
     "gbx_abi_version": (C.c_int32, []),
     "gbx_groupby_set_strategy": (C.c_int, [C.c_void_p, C.c_int32]),
     "gbx_groupby_last_stats": (C.c_int, [C.c_void_p, C.POINTER(gbx_stats)]),
+    "gbx_groupby_set_timing": (C.c_int, [C.c_void_p, C.c_int32]),
 }

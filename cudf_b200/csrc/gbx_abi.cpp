@@ -280,8 +280,57 @@ struct gbx_groupby {
   int32_t null_policy = GBX_NULL_EXCLUDE;
   int32_t keys_are_sorted = 0;
   int32_t strategy = GBX_STRATEGY_AUTO;
+  int32_t timing = 0;
+  cudaEvent_t events[6] = {};  // phase boundaries when timing is on
+  int events_device = -1;
   gbx_stats stats{};
+  ~gbx_groupby()
+  {
+    for (auto& e : events)
+      if (e) cudaEventDestroy(e);
+  }
 };
+
+namespace gbx {
+namespace {
+
+// Records the phase boundaries of one aggregate() call on its stream.
+struct PhaseTimer {
+  gbx_groupby* gb;
+  cudaStream_t st;
+  bool on;
+  PhaseTimer(gbx_groupby* g, cudaStream_t s, int device) : gb(g), st(s), on(g->timing != 0)
+  {
+    if (!on) return;
+    if (gb->events_device != device) {
+      for (auto& e : gb->events)
+        if (e) cudaEventDestroy(e);
+      for (auto& e : gb->events) GBX_CUDA(cudaEventCreate(&e));
+      gb->events_device = device;
+    }
+  }
+  void mark(int i)
+  {
+    if (on) GBX_CUDA(cudaEventRecord(gb->events[i], st));
+  }
+  // after the stream has been synchronised past mark(5)
+  void read(gbx_stats& s)
+  {
+    if (!on) return;
+    float t[5];
+    for (int i = 0; i < 5; ++i) GBX_CUDA(cudaEventElapsedTime(&t[i], gb->events[i], gb->events[i + 1]));
+    s.timed        = 1;
+    s.sample_ms    = t[0];
+    s.init_ms      = t[1];
+    s.aggregate_ms = t[2];
+    s.compact_ms   = t[3];
+    s.finalize_ms  = t[4];
+    GBX_CUDA(cudaEventElapsedTime(&s.total_ms, gb->events[0], gb->events[5]));
+  }
+};
+
+}  // namespace
+}  // namespace gbx
 
 struct ResultInternal {
   Alloc alloc;
@@ -489,6 +538,14 @@ int gbx_groupby_set_strategy(gbx_groupby* gb, int32_t strategy)
   });
 }
 
+int gbx_groupby_set_timing(gbx_groupby* gb, int32_t enable)
+{
+  return guarded([&] {
+    GBX_EXPECTS(gb != nullptr, "null groupby");
+    gb->timing = enable ? 1 : 0;
+  });
+}
+
 int gbx_groupby_last_stats(const gbx_groupby* gb, gbx_stats* out)
 {
   return guarded([&] {
@@ -634,6 +691,9 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     }
 
     Scratch scratch(&call.alloc);
+    PhaseTimer timer(gb, s, call.dev.device);
+    int launches = 0;
+    timer.mark(0);
     // control block: [0..1] sample counters, [2..25] valid counts, [26] status, [27] num_selected
     constexpr int kCtlWords = 32;
     auto* ctl = static_cast<unsigned long long*>(scratch.get(kCtlWords * 8));
@@ -641,6 +701,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     int32_t* d_status        = reinterpret_cast<int32_t*>(ctl + 26);
     int64_t* d_num_selected  = reinterpret_cast<int64_t*>(ctl + 27);
     GBX_CUDA(launch_count_valid(ms, ctl + 2, call.dev.num_sms, s));
+    launches += ms.n > 0 ? 1 : 0;
 
     bool key_ok       = true;
     KeyPlan kp_sample = make_key_plan(gb, std::vector<int64_t>(nkeys, -1), key_ok);
@@ -652,6 +713,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     const uint64_t set_cap = 1 << 18;
     auto* set = static_cast<uint64_t*>(scratch.get(set_cap * 8));
     GBX_CUDA(launch_sample(kp_sample, call.n, nsample, set, set_cap, ctl, call.dev.num_sms, s));
+    launches += 2;
+    timer.mark(1);
 
     unsigned long long h_ctl[kCtlWords];
     GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
@@ -764,7 +827,6 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     cap          = std::min<uint64_t>(cap, 1ULL << 31);
 
     gb->stats.strategy = strategy;
-    int launches       = 4;
     int64_t G          = 0;
     TableRef t{};
     uint32_t* map = nullptr;
@@ -779,6 +841,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       t.status       = d_status;
       GBX_CUDA(cudaMemsetAsync(d_status, 0, 4, s));
       GBX_CUDA(launch_init_table(t, plan.acc, plan.key.nwords, call.dev.num_sms, s));
+      launches += 1;
+      timer.mark(2);
       const uint32_t max_probes = static_cast<uint32_t>(std::min<uint64_t>(cap, 1u << 12));
       if (strategy == GBX_STRATEGY_PRIVATIZED) {
         uint32_t S = static_cast<uint32_t>(std::min<uint64_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * est, 64.0))), s_max));
@@ -811,12 +875,16 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       } else {
         GBX_CUDA(launch_agg_global(plan, t, call.n, max_probes, call.dev.num_sms, s));
       }
+      launches += 1;
+      timer.mark(3);
       // ---- compaction of occupied slots
       map               = static_cast<uint32_t*>(scratch.get((cap + 1) * 4));
       size_t temp_bytes = 0;
       GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, nullptr, &temp_bytes, s));
       void* temp = scratch.get(temp_bytes);
       GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, temp, &temp_bytes, s));
+      launches += 2;  // cub select: tile-state init + sweep
+      timer.mark(4);
       GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
       GBX_CUDA(cudaStreamSynchronize(s));
       int32_t status;
@@ -838,13 +906,12 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
                                1ULL << 31);
       if (strategy == GBX_STRATEGY_PRIVATIZED) strategy = GBX_STRATEGY_GLOBAL;
       est = static_cast<double>(call.n);
-      launches += 4;
     }
     gb->stats.strategy        = strategy;
     gb->stats.table_capacity  = static_cast<int64_t>(cap);
     gb->stats.num_groups      = G;
     gb->stats.scratch_bytes   = static_cast<int64_t>(scratch.total());
-    gb->stats.kernel_launches = launches + 1;
+    gb->stats.kernel_launches = launches + (G > 0 ? 1 : 0);  // + finalize
     res->num_groups           = G;
 
     // ---- outputs
@@ -901,6 +968,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     GBX_CUDA(cudaMemsetAsync(d_nulls, 0, (kMaxKeyCols + kMaxOut) * 8, s));
     op.null_counts = d_nulls;
     GBX_CUDA(launch_finalize(plan, t, map, G, op, call.dev.num_sms, s));
+    timer.mark(5);
     std::vector<unsigned long long> h_nulls(kMaxKeyCols + kMaxOut, 0);
     GBX_CUDA(cudaMemcpyAsync(h_nulls.data(), d_nulls, h_nulls.size() * 8, cudaMemcpyDeviceToHost, s));
     GBX_CUDA(cudaStreamSynchronize(s));
@@ -914,6 +982,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
           if (oc.null_mask) oc.view.null_count = static_cast<int64_t>(h_nulls[kMaxKeyCols + o]);
         }
     }
+    timer.read(gb->stats);
     // scratch is released stream-ordered by ~Scratch
   });
   if (st != GBX_OK) {

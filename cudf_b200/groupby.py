@@ -97,10 +97,14 @@ class GroupBy:
     def set_strategy(self, strategy: _abi.Strategy) -> None:
         _lib.check(_lib.lib().gbx_groupby_set_strategy(self._h, int(strategy)))
 
+    def set_timing(self, enable: bool = True) -> None:
+        """Record per-phase CUDA-event times (see last_stats())."""
+        _lib.check(_lib.lib().gbx_groupby_set_timing(self._h, 1 if enable else 0))
+
     def last_stats(self) -> dict:
         st = _abi.gbx_stats()
         _lib.check(_lib.lib().gbx_groupby_last_stats(self._h, C.byref(st)))
-        return {name: getattr(st, name) for name, _ in _abi.gbx_stats._fields_ if name != "reserved0"}
+        return {name: getattr(st, name) for name, _ in _abi.gbx_stats._fields_}
 
     def aggregate(self, requests: List[GroupByRequest], stream: Optional[torch.cuda.Stream] = None,
                   allocator: Optional[TorchAllocator] = None) -> Tuple[Table, List[Table]]:

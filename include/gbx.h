@@ -260,10 +260,21 @@ typedef struct gbx_stats {
   int32_t retries;       /* table re-sizes after an overflow */
   int64_t scratch_bytes; /* device scratch held during the call */
   int32_t kernel_launches;
-  int32_t reserved0;
+  int32_t timed;         /* 1 when the phase times below were recorded */
+  /* CUDA-event times on the call's stream (gbx_groupby_set_timing) in ms */
+  float sample_ms;       /* null counts + sampled distinct count */
+  float init_ms;         /* table identity fill */
+  float aggregate_ms;    /* the aggregation pass over the rows */
+  float compact_ms;      /* occupied-slot compaction */
+  float finalize_ms;     /* output keys/results + null counts */
+  float total_ms;        /* first to last event of the call */
 } gbx_stats;
 
 GBX_API int gbx_groupby_last_stats(const gbx_groupby* gb, gbx_stats* out);
+
+/* Record per-phase CUDA-event times into gbx_stats on subsequent calls
+ * (enable = 1) or stop (0).  Adds a few event records per call. */
+GBX_API int gbx_groupby_set_timing(gbx_groupby* gb, int32_t enable);
 
 #ifdef __cplusplus
 }

@@ -73,14 +73,28 @@ def test_two_word_keys(strategy):
 
 
 def test_two_word_keys_with_nulls_include():
+    """(int64, int32) keys with a null bit each: 96 value bits + 2 null bits."""
     rng = np.random.default_rng(9)
     n = 100_000
     a = rng.integers(0, 30, size=n).astype(np.int64)
-    b = rng.integers(0, 30, size=n).astype(np.int64)
+    b = rng.integers(0, 30, size=n).astype(np.int32)
     va = rng.random(n) > 0.1
     vb = rng.random(n) > 0.1
     v = rng.integers(0, 1000, size=n).astype(np.int32)
     T.assert_parity([hc(a, va), hc(b, vb)], [(hc(v), ALL6)], NullPolicy.INCLUDE)
+    T.assert_parity([hc(a, va), hc(b, vb)], [(hc(v), ALL6)], NullPolicy.EXCLUDE)
+
+
+def test_keys_wider_than_128_bits_are_reported():
+    """Two int64 keys plus their null bits need 130 packed bits: a clear
+    UNSUPPORTED error, not a wrong answer."""
+    from cudf_b200 import UnsupportedError
+
+    n = 1000
+    a = np.arange(n, dtype=np.int64)
+    va = np.arange(n) % 3 > 0
+    with pytest.raises(UnsupportedError, match="128 packed bits"):
+        T.run_gpu([hc(a, va), hc(a, va)], [(hc(a), [(Kind.SUM, 0)])], NullPolicy.INCLUDE)
 
 
 def test_all_distinct_and_all_equal_keys():
