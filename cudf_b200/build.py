@@ -63,3 +63,19 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build_library(force="--force" in sys.argv, verbose=True))
+
+
+FACADE_TEST_SRC = os.path.join(os.path.dirname(HERE), "tests", "cpp", "groupby_facade_test.cpp")
+FACADE_TEST_BIN = os.path.join(os.path.dirname(HERE), "tests", "cpp", "_build", "groupby_facade_test")
+
+
+def build_facade_test(verbose: bool = False) -> str:
+    """Compiles the C++ facade test (reference-style gtests against include/cudf)."""
+    os.makedirs(os.path.dirname(FACADE_TEST_BIN), exist_ok=True)
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O2", "-x", "cu", "-I", inc, FACADE_TEST_SRC, "-L", HERE, "-lgbx",
+           "-Xlinker", "-rpath," + HERE, "-Xlinker", "-rpath,$ORIGIN/../../../cudf_b200", "-o", FACADE_TEST_BIN]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return FACADE_TEST_BIN

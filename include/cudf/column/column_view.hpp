@@ -1,0 +1,71 @@
+// cudf/column/column_view.hpp -- a non-owning column description with the
+// reference's accessors (cpp/include/cudf/column/column_view.hpp).  A
+// DICTIONARY32 view has two children: 0 = indices, 1 = keys.
+#pragma once
+
+#include <vector>
+
+#include "../types.hpp"
+
+namespace cudf {
+
+class column_view {
+ public:
+  column_view() = default;
+  column_view(data_type type, size_type size, void const* data, bitmask_type const* null_mask = nullptr,
+              size_type null_count = 0, size_type offset = 0, std::vector<column_view> const& children = {})
+    : _type(type), _size(size), _data(data), _null_mask(null_mask), _null_count(null_count), _offset(offset),
+      _children(children)
+  {
+  }
+  [[nodiscard]] data_type type() const noexcept { return _type; }
+  [[nodiscard]] size_type size() const noexcept { return _size; }
+  [[nodiscard]] bool is_empty() const noexcept { return _size == 0; }
+  [[nodiscard]] size_type offset() const noexcept { return _offset; }
+  [[nodiscard]] bitmask_type const* null_mask() const noexcept { return _null_mask; }
+  [[nodiscard]] bool nullable() const noexcept { return _null_mask != nullptr; }
+  [[nodiscard]] size_type null_count() const noexcept { return _null_count; }
+  [[nodiscard]] bool has_nulls() const noexcept { return null_count() > 0; }
+  [[nodiscard]] void const* head() const noexcept { return _data; }
+  template <typename T>
+  [[nodiscard]] T const* data() const noexcept
+  {
+    return static_cast<T const*>(_data) + _offset;
+  }
+  [[nodiscard]] size_type num_children() const noexcept { return static_cast<size_type>(_children.size()); }
+  [[nodiscard]] column_view child(size_type i) const { return _children.at(i); }
+
+  // The C-ABI descriptor of this view; `keys_storage` receives the dictionary
+  // keys' descriptor and must outlive the returned value.
+  gbx_column_view to_gbx(gbx_column_view* keys_storage) const
+  {
+    gbx_column_view v{};
+    v.type_id    = static_cast<int32_t>(_type.id());
+    v.scale      = _type.scale();
+    v.size       = _size;
+    v.offset     = _offset;
+    v.data       = _data;
+    v.null_mask  = _null_mask;
+    v.null_count = _null_mask ? _null_count : 0;
+    if (_type.id() == type_id::DICTIONARY32 && _children.size() == 2) {
+      column_view const& idx = _children[0];
+      v.data                 = idx.head();
+      v.offset               = _offset + idx.offset();
+      v.index_type_id        = static_cast<int32_t>(idx.type().id());
+      *keys_storage          = _children[1].to_gbx(nullptr);
+      v.dict_keys            = keys_storage;
+    }
+    return v;
+  }
+
+ private:
+  data_type _type{type_id::EMPTY};
+  size_type _size{};
+  void const* _data{};
+  bitmask_type const* _null_mask{};
+  size_type _null_count{};
+  size_type _offset{};
+  std::vector<column_view> _children{};
+};
+
+}  // namespace cudf
