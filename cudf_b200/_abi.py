@@ -223,4 +223,12 @@ SIGNATURES = {
     "gbx_groupby_set_strategy": (C.c_int, [C.c_void_p, C.c_int32]),
     "gbx_groupby_last_stats": (C.c_int, [C.c_void_p, C.POINTER(gbx_stats)]),
     "gbx_groupby_set_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "gbx_groupby_aggregate_noalloc": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(gbx_request), C.c_int32, C.c_void_p, C.POINTER(gbx_column), C.POINTER(gbx_column),
+         C.c_int64, C.POINTER(C.c_int64)],
+    ),
 }
+
+NOALLOC_SCRATCH_BYTES = 16 << 20
+NOALLOC_MAX_GROUPS = 32768

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgbx.so")
 
-SOURCES = ["gbx_kernels.cu", "gbx_abi.cpp"]
+SOURCES = ["gbx_kernels.cu", "gbx_abi.cpp", "gbx_noalloc.cu"]
 HEADERS = ["gbx_plan.hpp", "gbx_device.cuh", "gbx_kernels.hpp", os.path.join("..", "..", "include", "gbx.h")]
 
 NVCC_FLAGS = [

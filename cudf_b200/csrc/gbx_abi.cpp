@@ -994,3 +994,267 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
 }
 
 }  // extern "C"
+
+// ============================================= groupby without allocation
+
+namespace gbx {
+cudaError_t noalloc_scratch(int device, void** ptr, size_t* bytes);  // gbx_noalloc.cu
+}
+
+extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
+                                             const gbx_request* requests,
+                                             int32_t num_requests,
+                                             void* stream,
+                                             gbx_column* out_keys,
+                                             gbx_column* out_results,
+                                             int64_t capacity,
+                                             int64_t* num_groups)
+{
+  return guarded([&] {
+    GBX_EXPECTS(gb != nullptr && num_groups != nullptr, "null argument");
+    *num_groups = 0;
+    validate(gb, requests, num_requests);
+    const int nkeys = static_cast<int>(gb->keys.size());
+    int nout        = 0;
+    for (int q = 0; q < num_requests; ++q) nout += requests[q].num_aggregations;
+    GBX_EXPECTS(nkeys == 0 || out_keys != nullptr, "out_keys is null");
+    GBX_EXPECTS(nout == 0 || out_results != nullptr, "out_results is null");
+    GBX_EXPECTS(capacity >= 0, "negative capacity");
+    cudaStream_t s  = static_cast<cudaStream_t>(stream);
+    DeviceInfo dev  = current_device();
+    const int64_t n = gb->keys.empty() ? 0 : gb->keys[0].size;
+
+    // ---- the fixed scratch array of this device (looked up once per device)
+    void* base        = nullptr;
+    size_t base_bytes = 0;
+    GBX_CUDA(noalloc_scratch(dev.device, &base, &base_bytes));
+    size_t off = 0;
+    auto carve = [&](size_t bytes) -> void* {
+      off       = (off + 255) & ~size_t(255);
+      void* p   = static_cast<char*>(base) + off;
+      off      += bytes;
+      if (off > base_bytes)
+        fail(GBX_ERR_LOGIC,
+             "the aggregations' per-group state exceeds the %u-byte scratch of the no-allocation groupby; "
+             "use gbx_groupby_aggregate",
+             GBX_NOALLOC_SCRATCH_BYTES);
+      return p;
+    };
+    constexpr int kCtlWords = 32;
+    auto* ctl               = static_cast<unsigned long long*>(carve(kCtlWords * 8));
+    auto* d_nulls           = static_cast<unsigned long long*>(carve((kMaxKeyCols + kMaxOut) * 8));
+
+    // ---- distinct value columns -> channels
+    std::vector<int> req_chan(num_requests, -1);
+    std::vector<const gbx_column_view*> chan_cols;
+    for (int q = 0; q < num_requests; ++q) {
+      if (requests[q].num_aggregations == 0) continue;
+      int found = -1;
+      for (size_t c = 0; c < chan_cols.size(); ++c)
+        if (same_view(*chan_cols[c], requests[q].values)) found = static_cast<int>(c);
+      if (found < 0) {
+        found = static_cast<int>(chan_cols.size());
+        chan_cols.push_back(&requests[q].values);
+      }
+      req_chan[q] = found;
+    }
+    if (static_cast<int>(chan_cols.size()) > kMaxChannels)
+      fail(GBX_ERR_UNSUPPORTED, "more than %d distinct value columns in one call", kMaxChannels);
+    if (nout > kMaxOut) fail(GBX_ERR_UNSUPPORTED, "more than %d results in one call", kMaxOut);
+
+    // ---- null counts of masks with an unknown count
+    std::vector<int64_t> key_nulls(nkeys, 0), chan_nulls(chan_cols.size(), 0);
+    MaskSpans ms{};
+    std::vector<std::pair<int, int>> span_owner;
+    for (int c = 0; c < nkeys; ++c) {
+      key_nulls[c] = exact_null_count_or_neg(gb->keys[c]);
+      if (key_nulls[c] < 0) {
+        ms.span[ms.n++] = MaskSpan{gb->keys[c].null_mask, gb->keys[c].offset, gb->keys[c].size};
+        span_owner.push_back({0, c});
+      }
+    }
+    for (size_t c = 0; c < chan_cols.size(); ++c) {
+      chan_nulls[c] = exact_null_count_or_neg(*chan_cols[c]);
+      if (chan_nulls[c] < 0) {
+        ms.span[ms.n++] = MaskSpan{chan_cols[c]->null_mask, chan_cols[c]->offset, chan_cols[c]->size};
+        span_owner.push_back({1, static_cast<int>(c)});
+      }
+    }
+    unsigned long long h_ctl[kCtlWords];
+    GBX_CUDA(cudaMemsetAsync(ctl, 0, kCtlWords * 8, s));
+    if (ms.n > 0 && n > 0) {
+      GBX_CUDA(launch_count_valid(ms, ctl + 2, dev.num_sms, s));
+      GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
+      GBX_CUDA(cudaStreamSynchronize(s));
+      for (size_t i = 0; i < span_owner.size(); ++i) {
+        int64_t nulls = ms.span[i].size - static_cast<int64_t>(h_ctl[2 + i]);
+        if (span_owner[i].first == 0) key_nulls[span_owner[i].second] = nulls;
+        else chan_nulls[span_owner[i].second] = nulls;
+      }
+    } else {
+      for (int c = 0; c < nkeys; ++c) key_nulls[c] = std::max<int64_t>(key_nulls[c], 0);
+      for (auto& v : chan_nulls) v = std::max<int64_t>(v, 0);
+    }
+
+    // ---- plan: packed keys and one accumulator set per channel
+    bool key_ok = true;
+    Plan plan{};
+    plan.key = make_key_plan(gb, key_nulls, key_ok);
+    if (!key_ok)
+      fail(GBX_ERR_UNSUPPORTED, "key columns need more than 128 packed bits; wider composite keys are not supported");
+    plan.nchan = static_cast<int32_t>(chan_cols.size());
+    int nacc   = 0;
+    auto add_acc = [&](int kind) -> int8_t {
+      if (nacc >= kMaxAccs) fail(GBX_ERR_UNSUPPORTED, "too many accumulators in one call");
+      plan.acc.kind[nacc] = static_cast<int8_t>(kind);
+      return static_cast<int8_t>(nacc++);
+    };
+    for (int c = 0; c < plan.nchan; ++c) {
+      const gbx_column_view& col = *chan_cols[c];
+      Channel& ch                = plan.chan[c];
+      std::memset(&ch, 0, sizeof(ch));
+      ch.a_cnt = ch.a_sum = ch.a_min = ch.a_max = ch.a_sq = ch.a_k = ch.a_s2 = ch.a_prod = ch.a_amin = ch.a_amax = -1;
+      int32_t vt = value_type(col);
+      ch.data    = col.data;
+      ch.mask    = chan_nulls[c] != 0 ? col.null_mask : nullptr;
+      ch.offset  = col.offset;
+      if (col.type_id == GBX_TYPE_DICTIONARY32) {
+        int32_t it     = col.index_type_id ? col.index_type_id : GBX_TYPE_INT32;
+        ch.dict_data   = col.dict_keys->data;
+        ch.dict_offset = col.dict_keys->offset;
+        ch.dict_size   = col.dict_keys->size;
+        ch.idx_width   = static_cast<int8_t>(type_width(it));
+        ch.idx_signed  = is_unsigned(it) ? 0 : 1;
+      }
+      ch.ptype      = phys_of(vt);
+      ch.is_float   = is_floating(vt) ? 1 : 0;
+      uint32_t need = 0;
+      for (int q = 0; q < num_requests; ++q) {
+        if (req_chan[q] != c) continue;
+        for (int k = 0; k < requests[q].num_aggregations; ++k) {
+          switch (requests[q].aggregations[k].kind) {
+            case GBX_AGG_SUM: need |= N_SUM; break;
+            case GBX_AGG_PRODUCT: need |= N_PROD; break;
+            case GBX_AGG_MIN: need |= N_MIN; break;
+            case GBX_AGG_MAX: need |= N_MAX; break;
+            case GBX_AGG_COUNT_VALID: need |= N_CNT; break;
+            case GBX_AGG_SUM_OF_SQUARES: need |= N_SQ; break;
+            case GBX_AGG_MEAN: need |= N_SUM | N_CNT; break;
+            case GBX_AGG_VARIANCE:
+            case GBX_AGG_STD: need |= N_SUM | N_CNT | N_VAR; break;
+            default: break;
+          }
+        }
+      }
+      ch.need        = need;
+      const bool m64 = ch.ptype == P_I64 || ch.ptype == P_U64 || ch.ptype == P_F64;
+      if (ch.mask != nullptr) ch.a_cnt = add_acc(A_U32_ADD);
+      if (need & N_SUM) ch.a_sum = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
+      if (need & N_MIN) ch.a_min = add_acc(m64 ? A_U64_MIN : A_U32_MIN);
+      if (need & N_MAX) ch.a_max = add_acc(m64 ? A_U64_MAX : A_U32_MAX);
+      if (need & N_SQ) ch.a_sq = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
+      if (need & N_PROD) ch.a_prod = add_acc(ch.is_float ? A_F64_MUL : A_I64_MUL);
+      if (need & N_VAR) {
+        ch.a_k  = add_acc(A_F64_SHIFT);
+        ch.a_s2 = add_acc(A_F64_ADD);
+      }
+    }
+    plan.acc.nacc = nacc;
+
+    // ---- fixed-capacity global table carved from the scratch array
+    const uint64_t cap = 2ull * GBX_NOALLOC_MAX_GROUPS;
+    TableRef t{};
+    t.cap          = cap;
+    t.keys         = static_cast<uint64_t*>(carve((cap + 1) * plan.key.nwords * 8));
+    t.rows         = static_cast<uint32_t*>(carve((cap + 1) * 4));
+    for (int a = 0; a < nacc; ++a) t.acc[a] = carve((cap + 1) * acc_bytes(plan.acc.kind[a]));
+    t.special_used = reinterpret_cast<uint32_t*>(ctl + 28);
+    t.status       = reinterpret_cast<int32_t*>(ctl + 26);
+    auto* map      = static_cast<uint32_t*>(carve((cap + 1) * 4));
+    auto* d_num_selected = reinterpret_cast<int64_t*>(ctl + 27);
+    size_t temp_bytes    = 0;
+    GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, nullptr, &temp_bytes, s));
+    void* temp = carve(temp_bytes);
+
+    int64_t G = 0;
+    if (n > 0) {
+      GBX_CUDA(launch_init_table(t, plan.acc, plan.key.nwords, dev.num_sms, s));
+      GBX_CUDA(launch_agg_global(plan, t, n, static_cast<uint32_t>(std::min<uint64_t>(cap, 1u << 12)), dev.num_sms, s));
+      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, temp, &temp_bytes, s));
+      GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
+      GBX_CUDA(cudaStreamSynchronize(s));
+      int32_t status;
+      std::memcpy(&status, reinterpret_cast<char*>(h_ctl) + 26 * 8, 4);
+      std::memcpy(&G, reinterpret_cast<char*>(h_ctl) + 27 * 8, 8);
+      if (status & S_SPIN_LIMIT) fail(GBX_ERR_DEVICE, "a bounded device loop gave up (status 0x%x)", status);
+      if (status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
+      if ((status & S_TABLE_FULL) || G > GBX_NOALLOC_MAX_GROUPS)
+        fail(GBX_ERR_LOGIC, "the input has more than %d groups, the limit of the no-allocation groupby",
+             GBX_NOALLOC_MAX_GROUPS);
+    }
+    GBX_EXPECTS(G <= capacity, "the input has %lld groups but the outputs hold %lld rows", (long long)G,
+                (long long)capacity);
+
+    // ---- describe the caller's output columns
+    OutPlan op{};
+    auto describe = [&](gbx_column& c, int32_t type_id, int32_t scale, bool with_mask) {
+      GBX_EXPECTS(G == 0 || c.data != nullptr, "an output column has no data buffer");
+      GBX_EXPECTS(!with_mask || G == 0 || c.null_mask != nullptr, "a nullable output column has no null_mask buffer");
+      c.view            = gbx_column_view{};
+      c.view.type_id    = type_id;
+      c.view.scale      = scale;
+      c.view.size       = G;
+      c.view.data       = c.data;
+      c.view.null_mask  = with_mask ? c.null_mask : nullptr;
+      c.view.null_count = 0;
+    };
+    for (int c = 0; c < nkeys; ++c) {
+      const gbx_column_view& kcv = gb->keys[c];
+      bool with_mask             = plan.key.cols[c].null_bit != 0;
+      describe(out_keys[c], kcv.type_id, kcv.scale, with_mask);
+      if (kcv.type_id == GBX_TYPE_DICTIONARY32) {
+        out_keys[c].view.index_type_id = kcv.index_type_id ? kcv.index_type_id : GBX_TYPE_INT32;
+        out_keys[c].view.dict_keys     = kcv.dict_keys;
+      }
+      op.key_data[c] = out_keys[c].data;
+      op.key_mask[c] = with_mask ? out_keys[c].null_mask : nullptr;
+    }
+    int o = 0;
+    for (int q = 0; q < num_requests; ++q) {
+      const gbx_request& r = requests[q];
+      int32_t vt           = value_type(r.values);
+      for (int k = 0; k < r.num_aggregations; ++k, ++o) {
+        int32_t kind   = r.aggregations[k].kind;
+        int32_t tt     = target_type(vt, kind);
+        bool with_mask = (kind == GBX_AGG_COUNT_VALID || kind == GBX_AGG_COUNT_ALL)
+                           ? false
+                           : (chan_nulls[req_chan[q]] != 0 || kind == GBX_AGG_VARIANCE || kind == GBX_AGG_STD);
+        int32_t scale  = is_decimal(tt) ? (r.values.type_id == GBX_TYPE_DICTIONARY32 ? r.values.dict_keys->scale
+                                                                                     : r.values.scale)
+                                        : 0;
+        describe(out_results[o], tt, scale, with_mask);
+        OutCol& oc   = op.out[op.nout++];
+        oc.data      = out_results[o].data;
+        oc.mask      = with_mask ? out_results[o].null_mask : nullptr;
+        oc.kind      = kind;
+        oc.ddof      = r.aggregations[k].ddof;
+        oc.chan      = static_cast<int8_t>(req_chan[q]);
+        oc.out_ptype = phys_of(tt);
+        oc.out_width = static_cast<int8_t>(type_width(tt));
+      }
+    }
+    if (G > 0) {
+      GBX_CUDA(cudaMemsetAsync(d_nulls, 0, (kMaxKeyCols + kMaxOut) * 8, s));
+      op.null_counts = d_nulls;
+      GBX_CUDA(launch_finalize(plan, t, map, G, op, dev.num_sms, s));
+      unsigned long long h_nulls[kMaxKeyCols + kMaxOut];
+      GBX_CUDA(cudaMemcpyAsync(h_nulls, d_nulls, sizeof(h_nulls), cudaMemcpyDeviceToHost, s));
+      GBX_CUDA(cudaStreamSynchronize(s));
+      for (int c = 0; c < nkeys; ++c)
+        if (op.key_mask[c]) out_keys[c].view.null_count = static_cast<int64_t>(h_nulls[c]);
+      for (int i = 0; i < op.nout; ++i)
+        if (op.out[i].mask) out_results[i].view.null_count = static_cast<int64_t>(h_nulls[kMaxKeyCols + i]);
+    }
+    *num_groups = G;
+  });
+}

@@ -276,6 +276,48 @@ GBX_API int gbx_groupby_last_stats(const gbx_groupby* gb, gbx_stats* out);
  * (enable = 1) or stop (0).  Adds a few event records per call. */
 GBX_API int gbx_groupby_set_timing(gbx_groupby* gb, int32_t enable);
 
+/* ---- groupby without device allocation -----------------------------------
+ * No counterpart in the reference (libcudf always allocates its hash set and
+ * results from an rmm resource).
+ *
+ * For callers that cannot allocate device memory during the call: an engine
+ * that gives its whole GPU budget to its own pool and forbids other
+ * allocations, or a latency-critical thread on which cudaMalloc / cudaFree
+ * would block or synchronise the device.  This call computes the same result
+ * as gbx_groupby_aggregate but allocates nothing: the hash table, compaction
+ * map and control words live in a fixed device array of
+ * GBX_NOALLOC_SCRATCH_BYTES inside libgbx (every GPU that loads the library
+ * holds it until the process exits), and the caller passes every output
+ * buffer.
+ *
+ * Limits: at most GBX_NOALLOC_MAX_GROUPS groups (more is rejected with
+ * GBX_ERR_LOGIC after the aggregation pass, outputs untouched), and the
+ * aggregations' per-group state must fit the array (else GBX_ERR_LOGIC).
+ *
+ * Outputs: `out_keys` has one gbx_column per key column and `out_results` one
+ * per aggregation of every request, in request order.  The caller sets each
+ * column's `data` (room for `capacity` rows of the output type, see
+ * gbx_target_type) and `null_mask` (room for `capacity` bits in 32-bit words;
+ * required where the output can hold nulls, ignored otherwise); the call
+ * fills each `view` and `*num_groups`.
+ *
+ * Every call shares the one array: calls whose work overlaps on the GPU (on
+ * different streams or threads) race and corrupt each other's results, so
+ * serialise them.  The array keeps the last call's contents; each call clears
+ * what must start at zero itself.  The first call on a device looks up the
+ * array's device address (once per device); it synchronises `stream` twice,
+ * as gbx_groupby_aggregate does. */
+#define GBX_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define GBX_NOALLOC_MAX_GROUPS 32768
+GBX_API int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
+                                          const gbx_request* requests,
+                                          int32_t num_requests,
+                                          void* stream,
+                                          gbx_column* out_keys,
+                                          gbx_column* out_results,
+                                          int64_t capacity,
+                                          int64_t* num_groups);
+
 #ifdef __cplusplus
 }
 #endif
