@@ -53,6 +53,8 @@ def parse_args(argv=None):
     p.add_argument("--rows", type=int, default=ROWS)
     p.add_argument("--cards", type=str, default=",".join(str(c) for c in CARDS))
     p.add_argument("--cpu-sample-rows", type=int, default=2_000_000)
+    p.add_argument("--strategy", choices=["auto", "warp", "privatized", "global", "partitioned"], default="auto",
+                   help="force one aggregation strategy (default: chosen per call)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args(argv)
@@ -210,6 +212,10 @@ def run_ours(args, rank, world, local):
         k, a, b = data[c]
         gb = GroupBy(Table([k]))
         gb.set_timing(True)
+        if args.strategy != "auto":
+            from cudf_b200 import Strategy
+
+            gb.set_strategy(Strategy[args.strategy.upper()])
         gbs[c] = gb
         reqs[c] = [GroupByRequest(a, aggs()), GroupByRequest(b, aggs())]
     torch.cuda.synchronize()
@@ -332,6 +338,28 @@ def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
         dev[c] = [torch.empty_like(t, device=device) for t in host[c]]
     h2d = sum(t.numel() * t.element_size() for c in cards for t in host[c])
     d2h_bytes = [0]
+    from cudf_b200.column import storage_dtype
+
+    # one pinned host buffer receives every result column of a step
+    max_groups = max(args.rows, 1)
+    out_host = torch.empty(int(max_groups * BYTES_PER_GROUP_OUT * 1.1) + (1 << 20), dtype=torch.uint8,
+                           pin_memory=True)
+
+    def read_back(outs):
+        """D2H of each column's rows (data and mask) into the pinned buffer."""
+        off = 0
+        for col in outs:
+            if col.size == 0:
+                continue
+            if col.data is not None:
+                nb = col.size * storage_dtype(col.type_id).itemsize
+                out_host[off:off + nb].copy_(col.data.view(torch.uint8)[:nb], non_blocking=True)
+                off += nb
+            if col.mask is not None:
+                nb = ((col.size + 31) // 32) * 4
+                out_host[off:off + nb].copy_(col.mask.view(torch.uint8)[:nb], non_blocking=True)
+                off += nb
+        return off
 
     def step():
         for c in cards:
@@ -347,14 +375,8 @@ def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
             kt, res = gb.aggregate([GroupByRequest(ac, aggs()), GroupByRequest(bc, aggs())], stream=stream,
                                    allocator=alloc)
             outs = [col for col in kt.columns()] + [col for t in res for col in t.columns()]
-            got = 0
-            for col in outs:
-                if col.data is not None:
-                    got += col.data.numel() * col.data.element_size()
-                    col.data.cpu()
-                if col.mask is not None:
-                    got += col.mask.numel() * col.mask.element_size()
-                    col.mask.cpu()
+            got = read_back(outs)
+            stream.synchronize()
             d2h_bytes[0] = got if c == cards[0] else d2h_bytes[0] + got
 
     step()

@@ -95,6 +95,7 @@ class Strategy(enum.IntEnum):
     PRIVATIZED = 1
     GLOBAL = 2
     PARTITIONED = 3
+    WARP = 4
 
 
 # element width in bytes of each fixed-width type (0: not fixed width)

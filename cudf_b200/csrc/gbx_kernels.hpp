@@ -47,6 +47,57 @@ cudaError_t launch_agg_global(const Plan& p, const TableRef& t, int64_t n, uint3
                               cudaStream_t st);
 cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int block,
                                   int grid, uint32_t smem_probes, uint32_t max_probes, cudaStream_t st);
+// ---- radix-partitioned path
+// Row-partitioned copies of the inputs: packed key words (SoA), each
+// channel's resolved value bits, and a validity byte per row for channels
+// with nulls (valid == nullptr otherwise).
+struct PartCol {
+  const void* vals;
+  const uint8_t* valid;
+  int32_t width;
+  int32_t pad;
+};
+struct PartBufs {
+  const uint64_t* keys[2];
+  PartCol col[kMaxChannels];
+};
+
+struct PartPlan {
+  int32_t bits;              // P = 2^bits buckets, bucket = top bits of the key hash
+  int32_t shard_bits;        // each bucket's counter is split over 2^shard_bits warps' shards
+  uint32_t slice_rows;       // rows per work item of a large bucket
+  uint32_t* counts;          // [(P << shard_bits) + 1] rows per (bucket, shard) (last entry 0)
+  uint32_t* offsets;         // [(P << shard_bits) + 1] exclusive scan of counts
+  uint32_t* cursor;          // [P << shard_bits] scatter cursors (copy of offsets)
+  uint32_t* nslices;         // [P + 1] work items per bucket (last entry 0)
+  uint32_t* item_start;      // [P + 1] exclusive scan of nslices
+  uint32_t* multi;           // [P + 1] 1 when a bucket has several items (last entry 0)
+  uint32_t* region;          // [P + 1] exclusive scan of multi: region table of the bucket
+  uint32_t* item_bucket;     // [items] bucket of each work item
+  unsigned long long* item_counter;  // work-item dispenser
+  unsigned long long* out_counter;   // output rows written so far
+  uint32_t region_slots;     // slots per region table (= the warp table size)
+  int32_t* status;           // device status word
+};
+
+cudaError_t launch_part_hist(const KeyPlan& kp, int64_t n, const PartPlan& pp, int num_sms, cudaStream_t st);
+// counts -> offsets, nslices, item_start, multi, region (device scans)
+cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_bytes, int num_sms, cudaStream_t st);
+// item_bucket[item_start[b] + j] = b for every slice j of every bucket b
+cudaError_t launch_part_items(const PartPlan& pp, int64_t n, int num_sms, cudaStream_t st);
+cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, const PartBufs& out, int num_sms,
+                                cudaStream_t st);
+// Aggregates every bucket: single-item buckets write their groups to `op`
+// directly; multi-item buckets merge into region tables of `t` (t.cap =
+// regions * region_slots) that launch_part_region_finalize then writes out.
+cudaError_t launch_part_agg(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
+                            const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st);
+cudaError_t launch_part_region_finalize(const Plan& p, const PartPlan& pp, const TableRef& t, const OutPlan& op,
+                                       int num_sms, cudaStream_t st);
+
+// Warp-private shared-memory tables (sl describes one warp's table).
+cudaError_t launch_agg_warp(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int num_sms,
+                            uint32_t max_probes, cudaStream_t st);
 // cub select of occupied slot ids; call once with temp == nullptr to size `temp_bytes`.
 cudaError_t compact_occupied(const TableRef& t, int nwords, uint32_t* map, int64_t* num_selected, void* temp,
                              size_t* temp_bytes, cudaStream_t st);

@@ -1,0 +1,401 @@
+// gbx_part.cu -- radix-partitioned aggregation for high cardinality.
+//
+// When the groups do not fit per-warp tables, rows are first partitioned by
+// the top bits of their key hash into P = 2^bits buckets of ~50-100 groups
+// each (histogram, scans, scatter).  A warp then owns a bucket -- or, for a
+// large bucket, a slice of it -- with a private shared-memory table
+// (gbx_warpcore.cuh): no atomics on the row path.  A bucket handled by one
+// warp is finalised straight into the output columns (dense rows reserved with
+// one atomic per 32 groups); slices of a large bucket merge into a compact
+// per-bucket region table that a last kernel writes out.  The reference keeps
+// one global set of row indices sized by rows and updates N-row sparse columns
+// with per-row atomics (hash/groupby.cu:424-504, 571-580); here every group's
+// state lives in shared memory until it is final.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+
+#include "gbx_warpcore.cuh"
+
+namespace gbx {
+
+using namespace dev;
+
+namespace {
+__device__ __forceinline__ uint32_t bucket_of(uint64_t h, int bits)
+{
+  return bits == 0 ? 0u : static_cast<uint32_t>(h >> (64 - bits));
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+// Counter of bucket b for row r: with few buckets each bucket's counter is
+// split into shards (by the row's 32-row batch, the same in the histogram and
+// the scatter) so that warps do not all update the same address.
+__device__ __forceinline__ uint32_t counter_of(uint32_t b, int64_t r, const PartPlan& pp)
+{
+  return (b << pp.shard_bits) | (static_cast<uint32_t>(r >> 5) & ((1u << pp.shard_bits) - 1u));
+}
+}  // namespace
+
+// Rows per bucket (warp-aggregated: one atomic per bucket present in a warp).
+template <int NW>
+__global__ void k_part_hist(const __grid_constant__ KeyPlan kp, int64_t n, const __grid_constant__ PartPlan pp)
+{
+  const int lane       = threadIdx.x & 31;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < n;
+       base += stride) {
+    const int64_t r = base + lane;
+    uint64_t k[NW];
+    const bool act    = r < n && pack_key<NW>(kp, r, k);
+    const uint32_t b  = act ? bucket_of(hash_key<NW>(k), pp.bits) : 0xffffffffu;
+    const uint32_t pe = __match_any_sync(kFull, b);
+    if (act && (__ffs(pe) - 1) == lane) atomicAdd(pp.counts + counter_of(b, r, pp), static_cast<uint32_t>(__popc(pe)));
+  }
+}
+
+__global__ void k_part_slices(const __grid_constant__ PartPlan pp)
+{
+  const uint32_t P = 1u << pp.bits;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b <= P; b += gridDim.x * blockDim.x) {
+    if (b == P) {
+      pp.nslices[b] = 0;
+      pp.multi[b]   = 0;
+    } else {
+      const uint32_t c  = pp.offsets[(b + 1) << pp.shard_bits] - pp.offsets[b << pp.shard_bits];
+      const uint32_t ns = c == 0 ? 1u : (c + pp.slice_rows - 1) / pp.slice_rows;
+      pp.nslices[b]     = ns;
+      pp.multi[b]       = ns > 1 ? 1u : 0u;
+    }
+  }
+}
+
+// Bucket of every work item (one thread per bucket writes its slices).
+__global__ void k_part_items(const __grid_constant__ PartPlan pp)
+{
+  const uint32_t P = 1u << pp.bits;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < P; b += gridDim.x * blockDim.x) {
+    const uint32_t i0 = pp.item_start[b];
+    const uint32_t ns = pp.nslices[b];
+    for (uint32_t j = 0; j < ns; ++j) pp.item_bucket[i0 + j] = b;
+  }
+}
+
+// Writes each row's packed key, resolved values and validity to its bucket.
+// Each warp takes 4 batches of 32 rows at a time so that the 4 batches'
+// cursor atomics (whose results the writes need) are in flight together.
+template <int NW>
+__global__ void k_part_scatter(const __grid_constant__ Plan plan, int64_t n, const __grid_constant__ PartPlan pp,
+                               const __grid_constant__ PartBufs out)
+{
+  constexpr int U         = 4;
+  const int lane          = threadIdx.x & 31;
+  const int64_t warp      = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps    = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const RowSource src{&plan};
+  for (int64_t base = warp * 32 * U; base < n; base += nwarps * 32 * U) {
+    uint64_t k[U][NW];
+    bool act[U];
+    uint32_t pe[U], pos[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t r  = base + u * 32 + lane;
+      act[u]           = r < n && src.key<NW>(r, k[u]);
+      const uint32_t b = act[u] ? bucket_of(hash_key<NW>(k[u]), pp.bits) : 0xffffffffu;
+      pe[u]            = __match_any_sync(kFull, b);
+      pos[u]           = 0;
+      if (act[u] && lane == __ffs(pe[u]) - 1)
+        pos[u] = atomicAdd(pp.cursor + counter_of(b, base + u * 32 + lane, pp), static_cast<uint32_t>(__popc(pe[u])));
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint32_t p0 = __shfl_sync(kFull, pos[u], __ffs(pe[u]) - 1);
+      if (!act[u]) continue;
+      const int64_t r   = base + u * 32 + lane;
+      const uint32_t at = p0 + __popc(pe[u] & lanemask_lt(lane));
+#pragma unroll
+      for (int w = 0; w < NW; ++w) const_cast<uint64_t*>(out.keys[w])[at] = k[u][w];
+      for (int c = 0; c < plan.nchan; ++c) {
+        uint64_t bits = 0;
+        const bool v  = src.value(c, r, bits, pp.status);
+        store_bits(const_cast<void*>(out.col[c].vals), at, out.col[c].width, v ? bits : 0);
+        if (out.col[c].valid != nullptr) const_cast<uint8_t*>(out.col[c].valid)[at] = v ? 1 : 0;
+      }
+    }
+  }
+}
+
+// Bucket / slice aggregation (see the file comment).  blockDim.x / 32 warp
+// tables of sl.total bytes, then 32 u32 of compaction scratch per warp.
+template <int NW, int NCH>
+__global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Plan plan, const __grid_constant__ PartPlan pp, const __grid_constant__ PartBufs in, const __grid_constant__ TableRef t, const __grid_constant__ SmemLayout sl,
+                                                  const __grid_constant__ OutPlan op)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane   = threadIdx.x & 31;
+  const int warp   = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  WarpTable<NW> T{smem + static_cast<size_t>(warp) * sl.total, &sl, sl.slots};
+  uint32_t* scratch = reinterpret_cast<uint32_t*>(smem + static_cast<size_t>(nwarps) * sl.total) + warp * 32;
+  const PartSource src{&in};
+  const uint32_t P          = 1u << pp.bits;
+  const uint64_t items      = pp.item_start[P];
+  const Level<Global> Gl    = global_level(t);
+  const uint64_t* keys      = T.keys();
+
+  constexpr int kClaim = 4;  // work items claimed per atomic
+  unsigned long long claimed = 0, claim_end = 0;
+  for (;;) {
+    if (claimed == claim_end) {
+      unsigned long long c0 = 0;
+      if (lane == 0) c0 = atomicAdd(pp.item_counter, static_cast<unsigned long long>(kClaim));
+      claimed   = __shfl_sync(kFull, c0, 0);
+      claim_end = claimed + kClaim;
+    }
+    const unsigned long long item = claimed++;
+    if (item >= items) break;
+    const uint32_t b   = pp.item_bucket[item];
+    const uint32_t ns  = pp.nslices[b];
+    const uint64_t j   = item - pp.item_start[b];
+    const uint64_t b0  = pp.offsets[b << pp.shard_bits];
+    const uint64_t len = pp.offsets[(b + 1) << pp.shard_bits] - b0;
+    const int64_t r0   = static_cast<int64_t>(b0 + len * j / ns);
+    const int64_t r1   = static_cast<int64_t>(b0 + len * (j + 1) / ns);
+
+    T.reset(plan.acc, lane);
+    bool special = false;
+    int64_t r = r0 + lane;
+    uint64_t k[NW];
+    bool act  = r < r1 && src.key<NW>(r, k);
+    RowVals<NCH> v;
+    load_row_values(plan, src, act, r, v, t.status);
+    for (int64_t base = r0; base < r1; base += 32) {
+      const int64_t rn = base + 32 + lane;
+      uint64_t kn[NW];
+      const bool actn = rn < r1 && src.key<NW>(rn, kn);
+      RowVals<NCH> vn;
+      load_row_values(plan, src, actn, rn, vn, t.status);
+
+      uint32_t slot;
+      const int state = warp_find_or_insert<NW>(T, plan.acc, act, k, lane, slot);
+      if (__any_sync(kFull, state == ST_FOUND && slot == T.S)) special = true;
+      if (state == ST_SPILL) atomicOr(t.status, S_TABLE_FULL);  // bucket larger than its table: host retries
+      warp_accumulate(plan, T.tb, sl, state == ST_FOUND, slot, v, lane);
+
+      r   = rn;
+      act = actn;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) k[w] = kn[w];
+      v = vn;
+    }
+
+    if (ns == 1) {
+      // the whole bucket is here: write its groups out
+      const SmemAccs A{T.tb, &sl};
+      for (uint32_t s0 = 0; s0 <= T.S; s0 += 32) {
+        const uint32_t s = s0 + lane;
+        bool occ         = false;
+        uint64_t kw[NW];
+        if (s < T.S) {
+#pragma unroll
+          for (int w = 0; w < NW; ++w) kw[w] = keys[s * NW + w];
+          occ = !key_is_empty<NW>(kw);
+        } else if (s == T.S) {
+          occ = special;
+        }
+        const uint32_t bal = __ballot_sync(kFull, occ);
+        if (bal == 0) continue;
+        const int cnt = __popc(bal);
+        if (occ) scratch[__popc(bal & lanemask_lt(lane))] = s;
+        __syncwarp();
+        unsigned long long ob = 0;
+        if (lane == 0) ob = atomicAdd(pp.out_counter, static_cast<unsigned long long>(cnt));
+        ob                = __shfl_sync(kFull, ob, 0);
+        const bool active = lane < cnt;
+        const uint32_t ss = active ? scratch[lane] : 0;
+        uint64_t k2[2]    = {0, 0};
+        if (active) {
+          if (ss == T.S) {
+            k2[0] = k2[1] = kEmptyWord;
+          } else {
+#pragma unroll
+            for (int w = 0; w < NW; ++w) k2[w] = keys[ss * NW + w];
+          }
+        }
+        warp_write_groups(plan, op, A, active, ss, k2, static_cast<int64_t>(ob), lane);
+        __syncwarp();
+      }
+    } else {
+      // a slice of a large bucket: merge into the bucket's region table
+      const Level<Shared> L{static_cast<uint32_t>(__cvta_generic_to_shared(T.tb)), &sl};
+      const uint64_t rbase = static_cast<uint64_t>(pp.region[b]) * pp.region_slots;
+      for (uint32_t s = lane; s <= T.S; s += 32) {
+        uint64_t kw[NW];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) kw[w] = keys[s * NW + w];
+        const bool occ = (s < T.S) ? !key_is_empty<NW>(kw) : special;
+        if (!occ) continue;
+        int64_t g;
+        if (s == T.S) {
+          g = global_slot<NW>(t, kw, 1);
+        } else {
+          g = find_or_insert<Global, NW>(reinterpret_cast<uint64_t>(t.keys + rbase * NW), pp.region_slots - 1, kw,
+                                         hash_key<NW>(kw), pp.region_slots);
+          if (g < 0) atomicOr(t.status, S_TABLE_FULL);
+          else g += static_cast<int64_t>(rbase);
+        }
+        if (g >= 0) merge_slot<Shared>(plan, L, s, Gl, g, t.status);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Writes out the groups of the region tables (and the reserved all-ones slot).
+template <int NW>
+__global__ void k_part_region_finalize(const __grid_constant__ Plan plan, const __grid_constant__ PartPlan pp, const __grid_constant__ TableRef t, const __grid_constant__ OutPlan op)
+{
+  __shared__ uint32_t scratch_all[8][32];
+  const int lane         = threadIdx.x & 31;
+  uint32_t* scratch      = scratch_all[(threadIdx.x >> 5) & 7];
+  const uint64_t nslots  = t.cap + 1;
+  const uint64_t stride  = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const GlobalAccs A{&t};
+  for (uint64_t s0 = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~uint64_t(31); s0 < nslots;
+       s0 += stride) {
+    const uint64_t s = s0 + lane;
+    bool occ         = false;
+    if (s < t.cap) {
+      uint64_t kw[NW];
+#pragma unroll
+      for (int w = 0; w < NW; ++w) kw[w] = t.keys[s * NW + w];
+      occ = !key_is_empty<NW>(kw);
+    } else if (s == t.cap) {
+      occ = *t.special_used != 0;
+    }
+    const uint32_t bal = __ballot_sync(kFull, occ);
+    if (bal == 0) continue;
+    const int cnt = __popc(bal);
+    if (occ) scratch[__popc(bal & lanemask_lt(lane))] = static_cast<uint32_t>(s - s0);
+    __syncwarp();
+    unsigned long long ob = 0;
+    if (lane == 0) ob = atomicAdd(pp.out_counter, static_cast<unsigned long long>(cnt));
+    ob                = __shfl_sync(kFull, ob, 0);
+    const bool active = lane < cnt;
+    const uint64_t ss = active ? s0 + scratch[lane] : 0;
+    uint64_t k2[2]    = {0, 0};
+    if (active) {
+      if (ss == t.cap) {
+        k2[0] = k2[1] = kEmptyWord;
+      } else {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) k2[w] = t.keys[ss * NW + w];
+      }
+    }
+    warp_write_groups(plan, op, A, active, ss, k2, static_cast<int64_t>(ob), lane);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+
+namespace {
+inline int grid_rows(int64_t n, int block, int max_blocks)
+{
+  int64_t b = (n + block - 1) / block;
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, max_blocks)));
+}
+}  // namespace
+
+cudaError_t launch_part_hist(const KeyPlan& kp, int64_t n, const PartPlan& pp, int num_sms, cudaStream_t st)
+{
+  const size_t counters = (size_t(1) << (pp.bits + pp.shard_bits)) + 1;
+  cudaError_t e         = cudaMemsetAsync(pp.counts, 0, counters * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  const int grid = grid_rows(n, 256, num_sms * 8);
+  if (kp.nwords == 1) k_part_hist<1><<<grid, 256, 0, st>>>(kp, n, pp);
+  else k_part_hist<2><<<grid, 256, 0, st>>>(kp, n, pp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_bytes, int num_sms, cudaStream_t st)
+{
+  const int items    = (1 << pp.bits) + 1;
+  const int counters = (1 << (pp.bits + pp.shard_bits)) + 1;
+  if (temp == nullptr) {
+    return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, pp.counts, pp.offsets, counters, st);
+  }
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.counts, pp.offsets, counters, st);
+  if (e != cudaSuccess) return e;
+  k_part_slices<<<grid_rows(items, 256, num_sms * 4), 256, 0, st>>>(pp);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.nslices, pp.item_start, items, st)) != cudaSuccess)
+    return e;
+  if ((e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.multi, pp.region, items, st)) != cudaSuccess)
+    return e;
+  return cudaMemcpyAsync(pp.cursor, pp.offsets, (counters - 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+}
+
+cudaError_t launch_part_items(const PartPlan& pp, int64_t n, int num_sms, cudaStream_t st)
+{
+  (void)n;
+  k_part_items<<<grid_rows(int64_t(1) << pp.bits, 256, num_sms * 8), 256, 0, st>>>(pp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, const PartBufs& out, int num_sms,
+                                cudaStream_t st)
+{
+  const int grid = grid_rows(n, 256, num_sms * 8);
+  if (p.key.nwords == 1) k_part_scatter<1><<<grid, 256, 0, st>>>(p, n, pp, out);
+  else k_part_scatter<2><<<grid, 256, 0, st>>>(p, n, pp, out);
+  return cudaGetLastError();
+}
+
+namespace {
+template <int NW, int NCH>
+cudaError_t launch_part_agg_impl(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
+                                 const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st)
+{
+  const int block   = 256;
+  const int warps   = block / 32;
+  const size_t smem = static_cast<size_t>(sl.total) * warps + warps * 32 * sizeof(uint32_t);
+  cudaError_t e =
+    cudaFuncSetAttribute(k_part_agg<NW, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_agg<NW, NCH>, block, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  k_part_agg<NW, NCH><<<num_sms * per_sm, block, smem, st>>>(p, pp, in, t, sl, op);
+  return cudaGetLastError();
+}
+
+template <int NW>
+cudaError_t launch_part_agg_nw(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
+                               const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st)
+{
+  if (p.nchan <= 2) return launch_part_agg_impl<NW, 2>(p, pp, in, t, sl, op, num_sms, st);
+  if (p.nchan <= 4) return launch_part_agg_impl<NW, 4>(p, pp, in, t, sl, op, num_sms, st);
+  return launch_part_agg_impl<NW, kMaxChannels>(p, pp, in, t, sl, op, num_sms, st);
+}
+}  // namespace
+
+cudaError_t launch_part_agg(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
+                            const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st)
+{
+  return p.key.nwords == 1 ? launch_part_agg_nw<1>(p, pp, in, t, sl, op, num_sms, st)
+                           : launch_part_agg_nw<2>(p, pp, in, t, sl, op, num_sms, st);
+}
+
+cudaError_t launch_part_region_finalize(const Plan& p, const PartPlan& pp, const TableRef& t, const OutPlan& op,
+                                       int num_sms, cudaStream_t st)
+{
+  const int grid = grid_rows(static_cast<int64_t>(t.cap + 1), 256, num_sms * 8);
+  if (p.key.nwords == 1) k_part_region_finalize<1><<<grid, 256, 0, st>>>(p, pp, t, op);
+  else k_part_region_finalize<2><<<grid, 256, 0, st>>>(p, pp, t, op);
+  return cudaGetLastError();
+}
+
+}  // namespace gbx

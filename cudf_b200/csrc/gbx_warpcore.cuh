@@ -1,0 +1,504 @@
+// gbx_warpcore.cuh -- the warp-exclusive table core shared by the warp-private
+// kernel (gbx_warp.cu) and the partitioned kernel (gbx_part.cu).
+//
+// A warp owns a shared-memory table nobody else touches.  For each batch of
+// up to 32 rows it
+//   1. finds or inserts each key: lanes probe in parallel; missing keys are
+//      inserted in rounds where, for every contended empty slot, one lane
+//      (__match_any_sync on the target slot) writes its key and the others
+//      re-probe -- so distinct keys with distinct targets insert together;
+//   2. ranks lanes that hit the same slot (__match_any_sync) and applies the
+//      rows in rounds, one row per slot per round, with plain loads and
+//      stores (no atomics).
+#pragma once
+
+#include "gbx_kernels.hpp"
+#include "gbx_table.cuh"
+
+namespace gbx {
+namespace dev {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+// ------------------------------------------------------------- row sources
+
+// Rows of the caller's columns.
+struct RowSource {
+  const Plan* plan;
+  template <int NW>
+  __device__ __forceinline__ bool key(int64_t r, uint64_t (&k)[NW]) const
+  {
+    return pack_key<NW>(plan->key, r, k);
+  }
+  __device__ __forceinline__ bool value(int c, int64_t r, uint64_t& b, int32_t* status) const
+  {
+    const Channel& ch = plan->chan[c];
+    if (!bit_valid(ch.mask, r + ch.offset)) return false;
+    bool ok;
+    b = value_bits(ch, r, ok);
+    if (!ok) {
+      atomicOr(status, S_BAD_INDEX);
+      return false;
+    }
+    return true;
+  }
+};
+
+// Rows of the radix-partitioned copies (keys already packed, dictionary
+// values resolved, validity as one byte per row).
+struct PartSource {
+  const PartBufs* pb;
+  template <int NW>
+  __device__ __forceinline__ bool key(int64_t r, uint64_t (&k)[NW]) const
+  {
+#pragma unroll
+    for (int w = 0; w < NW; ++w) k[w] = __ldg(pb->keys[w] + r);
+    return true;
+  }
+  __device__ __forceinline__ bool value(int c, int64_t r, uint64_t& b, int32_t*) const
+  {
+    const PartCol& pc = pb->col[c];
+    if (pc.valid != nullptr && __ldg(pc.valid + r) == 0) return false;
+    b = load_bits(pc.vals, r, pc.width);
+    return true;
+  }
+};
+
+// ------------------------------------------------------- per-row values
+
+// One lane's row: the raw value bits of each of up to NCH channels
+// (dictionary resolved) and a validity bit per channel.  Loaded for a whole batch before probing so
+// that the loads of all columns are in flight together.
+template <int NCH>
+struct RowVals {
+  uint64_t bits[NCH];
+  uint32_t valid;
+};
+
+template <int NCH, class Src>
+__device__ __forceinline__ void load_row_values(const Plan& plan, const Src& src, bool act, int64_t r,
+                                                RowVals<NCH>& v, int32_t* status)
+{
+  v.valid = 0;
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) {
+    v.bits[c] = 0;
+    if (c < plan.nchan && act && src.value(c, r, v.bits[c], status)) v.valid |= 1u << c;
+  }
+}
+
+// Applies one row to an exclusively owned shared-memory slot with plain
+// loads and stores (aggregate_row, detail/aggregation/aggregation.cuh:558-573,
+// with update_target_element's null skipping, :116-491).
+template <int NCH>
+__device__ __forceinline__ void apply_row(const Plan& plan, unsigned char* tb, const SmemLayout& sl, uint32_t s,
+                                          const RowVals<NCH>& v)
+{
+  reinterpret_cast<uint32_t*>(tb + sl.rows_off)[s] += 1;
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) {
+    if (c >= plan.nchan) break;
+    if (!((v.valid >> c) & 1u)) continue;
+    const Channel& ch = plan.chan[c];
+    const uint64_t b  = v.bits[c];
+    if (ch.a_cnt >= 0) reinterpret_cast<uint32_t*>(tb + sl.acc_off[ch.a_cnt])[s] += 1;
+    const bool m64 = minmax_is64(ch.ptype);
+    if (ch.a_min >= 0) {
+      const uint64_t e = enc_minmax(b, ch.ptype, true);
+      if (m64) {
+        uint64_t* p = reinterpret_cast<uint64_t*>(tb + sl.acc_off[ch.a_min]) + s;
+        *p          = min(*p, e);
+      } else {
+        uint32_t* p = reinterpret_cast<uint32_t*>(tb + sl.acc_off[ch.a_min]) + s;
+        *p          = min(*p, static_cast<uint32_t>(e));
+      }
+    }
+    if (ch.a_max >= 0) {
+      const uint64_t e = enc_minmax(b, ch.ptype, false);
+      if (m64) {
+        uint64_t* p = reinterpret_cast<uint64_t*>(tb + sl.acc_off[ch.a_max]) + s;
+        *p          = max(*p, e);
+      } else {
+        uint32_t* p = reinterpret_cast<uint32_t*>(tb + sl.acc_off[ch.a_max]) + s;
+        *p          = max(*p, static_cast<uint32_t>(e));
+      }
+    }
+    double xf;
+    if (ch.is_float) {
+      xf = as_f64(b, ch.ptype);
+      if (ch.a_sum >= 0) reinterpret_cast<double*>(tb + sl.acc_off[ch.a_sum])[s] += xf;
+      if (ch.a_sq >= 0) reinterpret_cast<double*>(tb + sl.acc_off[ch.a_sq])[s] += xf * xf;
+      if (ch.a_prod >= 0) reinterpret_cast<double*>(tb + sl.acc_off[ch.a_prod])[s] *= xf;
+    } else {
+      const int64_t x = as_i64(b, ch.ptype);
+      if (ch.a_sum >= 0) reinterpret_cast<uint64_t*>(tb + sl.acc_off[ch.a_sum])[s] += static_cast<uint64_t>(x);
+      if (ch.a_sq >= 0)
+        reinterpret_cast<uint64_t*>(tb + sl.acc_off[ch.a_sq])[s] +=
+          static_cast<uint64_t>(x) * static_cast<uint64_t>(x);
+      if (ch.a_prod >= 0) {
+        int64_t* p = reinterpret_cast<int64_t*>(tb + sl.acc_off[ch.a_prod]) + s;
+        *p         = static_cast<int64_t>(static_cast<uint64_t>(*p) * static_cast<uint64_t>(x));
+      }
+      xf = (ch.ptype == P_U64) ? static_cast<double>(static_cast<uint64_t>(x)) : static_cast<double>(x);
+    }
+    if (ch.a_k >= 0) {
+      // first non-NaN value becomes the shift; with no shift yet K is a NaN
+      // pattern, so an all-NaN group's square sum is NaN
+      uint64_t* kp = reinterpret_cast<uint64_t*>(tb + sl.acc_off[ch.a_k]) + s;
+      if (*kp == kShiftUnset && !(xf != xf)) *kp = static_cast<uint64_t>(__double_as_longlong(xf));
+      const double d = xf - __longlong_as_double(static_cast<long long>(*kp));
+      reinterpret_cast<double*>(tb + sl.acc_off[ch.a_s2])[s] += d * d;
+    }
+  }
+}
+
+// ------------------------------------------------------ the warp's table
+
+// One warp's table in shared memory: S slots plus the reserved slot S.
+template <int NW>
+struct WarpTable {
+  unsigned char* tb;
+  const SmemLayout* sl;
+  uint32_t S;
+  __device__ __forceinline__ uint64_t* keys() const { return reinterpret_cast<uint64_t*>(tb + sl->keys_off); }
+  __device__ __forceinline__ uint32_t* rows() const { return reinterpret_cast<uint32_t*>(tb + sl->rows_off); }
+
+  // Identity of one slot's row count and accumulators.
+  __device__ __forceinline__ void init_slot(const AccLayout& al, uint32_t s) const
+  {
+    rows()[s] = 0;
+    for (int a = 0; a < al.nacc; ++a) {
+      uint64_t id = identity_bits(al.kind[a]);
+      if (acc_bytes(al.kind[a]) == 4) reinterpret_cast<uint32_t*>(tb + sl->acc_off[a])[s] = static_cast<uint32_t>(id);
+      else reinterpret_cast<uint64_t*>(tb + sl->acc_off[a])[s] = id;
+    }
+  }
+
+  // Empties the table: keys only (a slot's accumulators are set when a key
+  // is inserted), plus the reserved slot S in full.
+  __device__ __forceinline__ void reset(const AccLayout& al, int lane) const
+  {
+    uint64_t* kk = keys();
+    for (uint32_t s = lane; s <= S; s += 32) {  // slot S keeps the all-ones key it stands for
+#pragma unroll
+      for (int w = 0; w < NW; ++w) kk[s * NW + w] = kEmptyWord;
+    }
+    if (lane == 0) init_slot(al, S);
+    __syncwarp();
+  }
+
+  __device__ __forceinline__ void init(const AccLayout& al, int lane) const
+  {
+    uint64_t* kk = keys();
+    uint32_t* rr = rows();
+    for (uint32_t s = lane; s <= S; s += 32) {
+#pragma unroll
+      for (int w = 0; w < NW; ++w) kk[s * NW + w] = kEmptyWord;
+      rr[s] = 0;
+      for (int a = 0; a < al.nacc; ++a) {
+        uint64_t id = identity_bits(al.kind[a]);
+        if (acc_bytes(al.kind[a]) == 4) reinterpret_cast<uint32_t*>(tb + sl->acc_off[a])[s] = static_cast<uint32_t>(id);
+        else reinterpret_cast<uint64_t*>(tb + sl->acc_off[a])[s] = id;
+      }
+    }
+    __syncwarp();
+  }
+};
+
+enum RowState { ST_DONE = 0, ST_PROBING = 1, ST_INSERT = 2, ST_FOUND = 3, ST_SPILL = 4 };
+
+// Finds or inserts each active lane's key (warp-synchronous; all 32 lanes
+// call it).  On return state is ST_FOUND (slot set; S for the all-ones key),
+// ST_SPILL (the table is full around the key) or ST_DONE (inactive lane).
+template <int NW>
+__device__ __forceinline__ int warp_find_or_insert(const WarpTable<NW>& T, const AccLayout& al, bool act,
+                                                   const uint64_t (&k)[NW], int lane, uint32_t& slot)
+{
+  uint64_t* keys       = T.keys();
+  const uint32_t S     = T.S;
+  const uint32_t smask = S - 1;
+  int state            = ST_DONE;
+  slot                 = 0;
+  if (act) {
+    if (key_is_empty<NW>(k)) {
+      state = ST_FOUND;
+      slot  = S;
+    } else {
+      state = ST_PROBING;
+      slot  = static_cast<uint32_t>(hash_key<NW>(k)) & smask;
+    }
+  }
+  // probe (the table only changes in the insertion rounds below)
+  for (uint32_t p = 0; p <= S && __any_sync(kFull, state == ST_PROBING); ++p) {
+    if (state == ST_PROBING) {
+      bool eq = true, empty = true;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        uint64_t cur = keys[slot * NW + w];
+        eq           = eq && (cur == k[w]);
+        empty        = empty && (cur == kEmptyWord);
+      }
+      if (eq) state = ST_FOUND;
+      else if (empty) state = ST_INSERT;
+      else if (p == S) state = ST_SPILL;
+      else slot = (slot + 1) & smask;
+    }
+  }
+  if (state == ST_PROBING) state = ST_SPILL;
+  // insertion rounds: one writer per contended empty slot
+  for (int round = 0; round < 33 && __any_sync(kFull, state == ST_INSERT); ++round) {
+    const uint32_t im = __ballot_sync(kFull, state == ST_INSERT);
+    if (state == ST_INSERT) {
+      const uint32_t grp = __match_any_sync(im, slot);
+      if ((__ffs(grp) - 1) == lane) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) keys[slot * NW + w] = k[w];
+        T.init_slot(al, slot);
+      }
+    }
+    __syncwarp();
+    if (state == ST_INSERT) {
+      bool eq = true;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) eq = eq && (keys[slot * NW + w] == k[w]);
+      if (eq) {
+        state = ST_FOUND;
+      } else {
+        state = ST_SPILL;
+        for (uint32_t p = 1; p < S; ++p) {
+          slot     = (slot + 1) & smask;
+          bool e2  = true, em = true;
+#pragma unroll
+          for (int w = 0; w < NW; ++w) {
+            uint64_t cur = keys[slot * NW + w];
+            e2           = e2 && (cur == k[w]);
+            em           = em && (cur == kEmptyWord);
+          }
+          if (e2) {
+            state = ST_FOUND;
+            break;
+          }
+          if (em) {
+            state = ST_INSERT;
+            break;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (state == ST_INSERT) state = ST_SPILL;
+  return state;
+}
+
+// Applies the batch's rows to the warp's table.  Lanes on the same slot are
+// ranked (__match_any_sync); in round r the lanes of rank r apply their row,
+// so every slot has one writer per round and needs no atomics.
+template <int NCH>
+__device__ __forceinline__ void warp_accumulate(const Plan& plan, unsigned char* tb, const SmemLayout& sl, bool has,
+                                                uint32_t slot, const RowVals<NCH>& v, int lane)
+{
+  const uint32_t m     = __ballot_sync(kFull, has);
+  const uint32_t peers = has ? __match_any_sync(m, slot) : 0u;
+  const int rank       = __popc(peers & ((1u << lane) - 1u));
+  const int rounds     = static_cast<int>(__reduce_max_sync(kFull, has ? static_cast<unsigned>(rank + 1) : 0u));
+  for (int rd = 0; rd < rounds; ++rd) {
+    if (has && rank == rd) apply_row(plan, tb, sl, slot, v);
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------ finalisation
+
+// Accumulator reads of one slot from a global table or a warp's table.
+struct GlobalAccs {
+  const TableRef* t;
+  __device__ __forceinline__ uint32_t rows(uint64_t s) const { return t->rows[s]; }
+  __device__ __forceinline__ uint64_t acc(int a, uint64_t s, int bytes) const
+  {
+    if (bytes == 4) return reinterpret_cast<const uint32_t*>(t->acc[a])[s];
+    return reinterpret_cast<const uint64_t*>(t->acc[a])[s];
+  }
+};
+
+struct SmemAccs {
+  const unsigned char* tb;
+  const SmemLayout* sl;
+  __device__ __forceinline__ uint32_t rows(uint64_t s) const
+  {
+    return reinterpret_cast<const uint32_t*>(tb + sl->rows_off)[s];
+  }
+  __device__ __forceinline__ uint64_t acc(int a, uint64_t s, int bytes) const
+  {
+    if (bytes == 4) return reinterpret_cast<const uint32_t*>(tb + sl->acc_off[a])[s];
+    return reinterpret_cast<const uint64_t*>(tb + sl->acc_off[a])[s];
+  }
+};
+
+__device__ __forceinline__ void store_bits(void* p, int64_t i, int width, uint64_t v)
+{
+  switch (width) {
+    case 1: reinterpret_cast<uint8_t*>(p)[i] = static_cast<uint8_t>(v); break;
+    case 2: reinterpret_cast<uint16_t*>(p)[i] = static_cast<uint16_t>(v); break;
+    case 4: reinterpret_cast<uint32_t*>(p)[i] = static_cast<uint32_t>(v); break;
+    default: reinterpret_cast<uint64_t*>(p)[i] = v; break;
+  }
+}
+
+// Final value and validity of output column `oc` for one group
+// (hash_compound_agg_finalizer, hash/groupby.cu:183-349).
+template <class Accs>
+__device__ __forceinline__ uint64_t finalize_value(const Plan& plan, const OutCol& oc, const Accs& A, uint64_t s,
+                                                   bool& valid)
+{
+  const Channel& ch = plan.chan[oc.chan];
+  const uint32_t rows = A.rows(s);
+  const uint32_t cnt  = (ch.a_cnt >= 0) ? static_cast<uint32_t>(A.acc(ch.a_cnt, s, 4)) : rows;
+  valid               = cnt > 0;
+  uint64_t vbits      = 0;
+  switch (oc.kind) {
+    case GBX_AGG_COUNT_VALID: vbits = cnt; valid = true; break;
+    case GBX_AGG_COUNT_ALL: vbits = rows; valid = true; break;
+    case GBX_AGG_SUM:
+    case GBX_AGG_SUM_OF_SQUARES:
+    case GBX_AGG_PRODUCT: {
+      int a        = (oc.kind == GBX_AGG_SUM) ? ch.a_sum : (oc.kind == GBX_AGG_PRODUCT ? ch.a_prod : ch.a_sq);
+      uint64_t raw = A.acc(a, s, 8);
+      if (ch.is_float) {
+        double x = __longlong_as_double(static_cast<long long>(raw));
+        vbits    = (oc.out_ptype == P_F32) ? __float_as_uint(static_cast<float>(x))
+                                           : static_cast<uint64_t>(__double_as_longlong(x));
+      } else {
+        vbits = raw;  // truncated to the output width on store (wraps like the reference)
+      }
+      break;
+    }
+    case GBX_AGG_MIN:
+    case GBX_AGG_MAX: {
+      bool mn      = oc.kind == GBX_AGG_MIN;
+      int a        = mn ? ch.a_min : ch.a_max;
+      uint64_t raw = A.acc(a, s, minmax_is64(ch.ptype) ? 8 : 4);
+      vbits        = dec_minmax(raw, ch.ptype, mn);
+      break;
+    }
+    case GBX_AGG_MEAN: {
+      if (!valid) break;
+      uint64_t raw = A.acc(ch.a_sum, s, 8);
+      if (oc.out_ptype == P_F64) {
+        // integer SUMs are INT64 (target_type): the mean divides the signed sum,
+        // as binary_operation(DIV) does on it (hash/groupby.cu:298-304)
+        double sum = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
+                                 : static_cast<double>(static_cast<int64_t>(raw));
+        vbits = static_cast<uint64_t>(__double_as_longlong(sum / static_cast<double>(cnt)));
+      } else {
+        // duration / decimal MEAN: the SUM wraps to the source width, then
+        // integer division of the representation
+        int64_t sw = static_cast<int64_t>(raw);
+        if (oc.out_width == 4) sw = static_cast<int32_t>(static_cast<uint32_t>(raw));
+        vbits = static_cast<uint64_t>(sw / static_cast<int64_t>(cnt));
+      }
+      break;
+    }
+    case GBX_AGG_VARIANCE:
+    case GBX_AGG_STD: {
+      int64_t nn = cnt;
+      if (nn == 0 || nn - oc.ddof <= 0) {
+        valid = false;
+        break;
+      }
+      uint64_t kb = A.acc(ch.a_k, s, 8);
+      double s2   = __longlong_as_double(static_cast<long long>(A.acc(ch.a_s2, s, 8)));
+      double var;
+      if (kb == kShiftUnset) {
+        var = s2;  // NaN inputs only
+      } else {
+        double K     = __longlong_as_double(static_cast<long long>(kb));
+        uint64_t raw = A.acc(ch.a_sum, s, 8);
+        double sum   = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
+                                   : (ch.ptype == P_U64 ? static_cast<double>(raw)
+                                                        : static_cast<double>(static_cast<int64_t>(raw)));
+        double S1 = sum - static_cast<double>(nn) * K;
+        double M2 = s2 - S1 * S1 / static_cast<double>(nn);
+        if (M2 < 0.0) M2 = 0.0;
+        var = M2 / static_cast<double>(nn - oc.ddof);
+      }
+      if (oc.kind == GBX_AGG_STD) var = sqrt(var);
+      vbits = static_cast<uint64_t>(__double_as_longlong(var));
+      valid = true;
+      break;
+    }
+    default: break;
+  }
+  return valid ? vbits : 0;
+}
+
+// Decoded key column `c` of a packed key; `valid` false for a null key.
+__device__ __forceinline__ uint64_t decode_key(const KeyCol& kc, const uint64_t (&k)[2], bool& valid)
+{
+  valid = true;
+  if (kc.null_bit) valid = ((k[kc.null_word] >> kc.null_shift) & 1ULL) == 0;
+  const int bits      = kc.width * 8;
+  const uint64_t word = k[kc.word];
+  uint64_t v          = (bits == 64) ? word : ((word >> kc.shift) & ((1ULL << bits) - 1));
+  return valid ? v : 0;
+}
+
+// Or-s a warp's 32 validity bits for rows [base, base + 32) into a bitmask
+// whose words the caller zeroed (other warps may own the neighbouring bits).
+__device__ __forceinline__ void or_mask_bits(uint32_t* mask, int64_t base, uint32_t bits)
+{
+  if (bits == 0) return;
+  const int64_t w = base >> 5;
+  const int sh    = static_cast<int>(base & 31);
+  if (sh == 0) {
+    atomicOr(mask + w, bits);
+  } else {
+    const uint32_t lo = bits << sh;
+    const uint32_t hi = bits >> (32 - sh);
+    if (lo) atomicOr(mask + w, lo);
+    if (hi) atomicOr(mask + w + 1, hi);
+  }
+}
+
+// Warp-cooperative output of up to 32 groups: lane i writes output row
+// base + i from slot `s` when `active` (active lanes form a prefix).  Keys
+// are decoded, every result finalised; validity bits are or-ed in one word
+// operation per warp and null counts added once per warp.
+template <class Accs>
+__device__ __forceinline__ void warp_write_groups(const Plan& plan, const OutPlan& op, const Accs& A, bool active,
+                                                  uint64_t s, const uint64_t (&k)[2], int64_t base, int lane)
+{
+  const uint32_t act = __ballot_sync(kFull, active);
+  const int64_t g    = base + lane;
+  for (int c = 0; c < plan.key.ncols; ++c) {
+    const KeyCol& kc = plan.key.cols[c];
+    bool valid       = false;
+    uint64_t v       = active ? decode_key(kc, k, valid) : 0;
+    if (active) store_bits(op.key_data[c], g, kc.width, v);
+    if (op.key_mask[c] != nullptr) {
+      const uint32_t bits = __ballot_sync(kFull, active && valid);
+      if (lane == 0) {
+        or_mask_bits(op.key_mask[c], base, bits);
+        const uint32_t nulls = __popc(act & ~bits);
+        if (nulls) atomicAdd(op.null_counts + c, static_cast<unsigned long long>(nulls));
+      }
+    }
+  }
+  for (int o = 0; o < op.nout; ++o) {
+    const OutCol& oc = op.out[o];
+    bool valid       = false;
+    uint64_t v       = active ? finalize_value(plan, oc, A, s, valid) : 0;
+    if (active) store_bits(oc.data, g, oc.out_width, v);
+    if (oc.mask != nullptr) {
+      const uint32_t bits = __ballot_sync(kFull, active && valid);
+      if (lane == 0) {
+        or_mask_bits(oc.mask, base, bits);
+        const uint32_t nulls = __popc(act & ~bits);
+        if (nulls) atomicAdd(op.null_counts + kMaxKeyCols + o, static_cast<unsigned long long>(nulls));
+      }
+    }
+  }
+}
+
+}  // namespace dev
+}  // namespace gbx

@@ -244,7 +244,8 @@ typedef enum gbx_strategy {
   GBX_STRATEGY_AUTO       = 0, /* chosen from a sampled cardinality estimate */
   GBX_STRATEGY_PRIVATIZED = 1, /* per-CTA shared-memory tables, flushed to a global table */
   GBX_STRATEGY_GLOBAL     = 2, /* every row updates the global open-addressing table */
-  GBX_STRATEGY_PARTITIONED = 3 /* radix-partition rows by key hash, then per-partition smem tables */
+  GBX_STRATEGY_PARTITIONED = 3, /* radix-partition rows by key hash, then per-partition smem tables */
+  GBX_STRATEGY_WARP       = 4  /* per-warp private shared-memory tables, no atomics on the hot path */
 } gbx_strategy;
 
 /* Force a strategy for subsequent calls on this gb object (AUTO restores). */

@@ -17,7 +17,7 @@ from tests import gbx_testing as T
 pytestmark = pytest.mark.gpu
 
 ALL6 = [(Kind.SUM, 0), (Kind.COUNT_VALID, 0), (Kind.MIN, 0), (Kind.MAX, 0), (Kind.MEAN, 0), (Kind.VARIANCE, 1)]
-STRATS = [Strategy.AUTO, Strategy.PRIVATIZED, Strategy.GLOBAL]
+STRATS = [Strategy.AUTO, Strategy.PRIVATIZED, Strategy.GLOBAL, Strategy.WARP, Strategy.PARTITIONED]
 
 
 def hc(a, v=None, **kw):
@@ -37,6 +37,8 @@ def test_plain_100m_shape(card, strategy):
     d = W.plain_100m(card, n=1_000_000)
     reqs = [(hc(d.values[0]), ALL6), (hc(d.values[1], d.value_valid[1]), ALL6)]
     got, want = T.assert_parity([hc(d.keys[0])], reqs, strategy=strategy)
+    if strategy == Strategy.WARP and card == 100:
+        assert got["stats"]["strategy"] == Strategy.WARP
     if strategy == Strategy.AUTO and card == 100:
         assert got["stats"]["strategy"] == Strategy.PRIVATIZED
 
@@ -258,3 +260,28 @@ def test_empty_input_types():
     assert got["num_groups"] == 0
     types = [r[0] for r in got["results"][0]]
     assert types == [TypeId.FLOAT32, TypeId.INT32, TypeId.FLOAT32, TypeId.FLOAT32, TypeId.FLOAT64, TypeId.FLOAT64]
+
+
+@pytest.mark.parametrize("card", [1_000, 100_000, 3_000_000])
+def test_partitioned_bucket_and_slice_modes(card):
+    """Partitioned strategy: few large buckets (split across warps, merged in
+    region tables) and many small buckets (written out directly)."""
+    rng = np.random.default_rng(card)
+    n = 2_000_000
+    k = rng.integers(0, card, size=n).astype(np.int64)
+    k[::101] = -1
+    a = rng.integers(-1000, 1000, size=n).astype(np.int32)
+    b = rng.standard_normal(n)
+    bv = rng.random(n) > 0.2
+    reqs = [(hc(a), ALL6), (hc(b, bv), ALL6)]
+    got, _ = T.assert_parity([hc(k)], reqs, strategy=Strategy.PARTITIONED)
+    assert got["stats"]["strategy"] == Strategy.PARTITIONED
+
+
+def test_partitioned_skewed_keys():
+    """Zipf-skewed composite keys: one bucket holds a large share of the rows."""
+    d = W.plain_200m(n=1_500_000, ranks=50_000)
+    keys = [hc(d.keys[0], d.key_valid[0]), hc(d.keys[1], d.key_valid[1])]
+    for policy in (NullPolicy.EXCLUDE, NullPolicy.INCLUDE):
+        T.assert_parity(keys, [(hc(d.values[0]), [(Kind.SUM, 0), (Kind.MEAN, 0), (Kind.VARIANCE, 1)])], policy,
+                        Strategy.PARTITIONED)
