@@ -13,7 +13,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgbx.so")
 
 SOURCES = ["gbx_kernels.cu", "gbx_warp.cu", "gbx_part.cu", "gbx_abi.cpp", "gbx_noalloc.cu"]
-HEADERS = ["gbx_plan.hpp", "gbx_device.cuh", "gbx_table.cuh", "gbx_warpcore.cuh", "gbx_kernels.hpp", os.path.join("..", "..", "include", "gbx.h")]
+HEADERS = ["gbx_plan.hpp", "gbx_host.hpp", "gbx_device.cuh", "gbx_table.cuh", "gbx_warpcore.cuh", "gbx_kernels.hpp",
+           os.path.join("..", "..", "include", "gbx.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -43,17 +44,23 @@ def _stale() -> bool:
 def build_library(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
-    objs = []
+    from concurrent.futures import ThreadPoolExecutor
+
+    cmds, objs = [], []
     for src in SOURCES:
         obj = os.path.join(CSRC, "_build", src + ".o")
         os.makedirs(os.path.dirname(obj), exist_ok=True)
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        if src.endswith(".cpp"):
-            cmd = [nvcc(), "-x", "cu", *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        lang = ["-x", "cu"] if src.endswith(".cpp") else []
+        cmds.append([nvcc(), *lang, *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj])
+        objs.append(obj)
+
+    def compile_one(cmd):
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(compile_one, cmds))
     tmp = LIB + ".tmp"
     cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs]
     subprocess.run(cmd, check=True)

@@ -16,17 +16,12 @@
 #include <vector>
 
 #include "../../include/gbx.h"
+#include "gbx_host.hpp"
 #include "gbx_kernels.hpp"
 
 namespace gbx {
-namespace {
 
 thread_local std::string g_last_error;
-
-struct Failure {
-  int code;
-  std::string msg;
-};
 
 [[noreturn]] void fail(int code, const char* fmt, ...)
 {
@@ -36,38 +31,6 @@ struct Failure {
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
   throw Failure{code, buf};
-}
-
-#define GBX_CUDA(call)                                                                      \
-  do {                                                                                      \
-    cudaError_t e_ = (call);                                                                \
-    if (e_ != cudaSuccess) {                                                                \
-      if (e_ == cudaErrorMemoryAllocation)                                                  \
-        fail(GBX_ERR_ALLOC, "CUDA error at %s:%d: %s", __FILE__, __LINE__,                  \
-             cudaGetErrorString(e_));                                                       \
-      fail(GBX_ERR_CUDA, "CUDA error at %s:%d: %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
-    }                                                                                       \
-  } while (0)
-
-#define GBX_EXPECTS(cond, ...)               \
-  do {                                       \
-    if (!(cond)) fail(GBX_ERR_LOGIC, __VA_ARGS__); \
-  } while (0)
-
-template <class F>
-int guarded(F&& f)
-{
-  try {
-    f();
-    g_last_error.clear();
-    return GBX_OK;
-  } catch (Failure& e) {
-    g_last_error = e.msg;
-    return e.code;
-  } catch (std::bad_alloc&) {
-    g_last_error = "host allocation failed";
-    return GBX_ERR_ALLOC;
-  }
 }
 
 // ------------------------------------------------------------------- types
@@ -186,68 +149,32 @@ bool same_view(const gbx_column_view& a, const gbx_column_view& b)
 
 // -------------------------------------------------------------- allocation
 
-struct Alloc {
-  gbx_allocator user{};
-  bool has_user = false;
-  cudaStream_t st = nullptr;
-
-  void* allocate(size_t bytes)
-  {
-    if (bytes == 0) bytes = 8;
-    bytes = (bytes + 255) & ~size_t(255);
-    void* p = nullptr;
-    if (has_user) {
-      p = user.allocate(user.ctx, bytes, st);
-      if (!p) fail(GBX_ERR_ALLOC, "allocator returned null for %zu bytes", bytes);
-      return p;
-    }
-    cudaError_t e = cudaMallocAsync(&p, bytes, st);
-    if (e != cudaSuccess) {
-      (void)cudaGetLastError();
-      fail(GBX_ERR_ALLOC, "cudaMallocAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));
-    }
+void* Alloc::allocate(size_t bytes)
+{
+  if (bytes == 0) bytes = 8;
+  bytes   = (bytes + 255) & ~size_t(255);
+  void* p = nullptr;
+  if (has_user) {
+    p = user.allocate(user.ctx, bytes, st);
+    if (!p) fail(GBX_ERR_ALLOC, "allocator returned null for %zu bytes", bytes);
     return p;
   }
-  void release(void* p, size_t bytes)
-  {
-    if (!p) return;
-    if (bytes == 0) bytes = 8;
-    bytes = (bytes + 255) & ~size_t(255);
-    if (has_user) user.deallocate(user.ctx, p, bytes, st);
-    else cudaFreeAsync(p, st);
+  cudaError_t e = cudaMallocAsync(&p, bytes, st);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    fail(GBX_ERR_ALLOC, "cudaMallocAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));
   }
-};
+  return p;
+}
 
-// Scratch buffers released (stream-ordered) when the call ends.
-struct Scratch {
-  Alloc* a;
-  std::vector<std::pair<void*, size_t>> bufs;
-  explicit Scratch(Alloc* al) : a(al) {}
-  void* get(size_t bytes)
-  {
-    void* p = a->allocate(bytes);
-    bufs.emplace_back(p, bytes);
-    return p;
-  }
-  size_t total() const
-  {
-    size_t s = 0;
-    for (auto& b : bufs) s += b.second;
-    return s;
-  }
-  void release_all()
-  {
-    for (auto& b : bufs) a->release(b.first, b.second);
-    bufs.clear();
-  }
-  ~Scratch() { release_all(); }
-};
-
-struct DeviceInfo {
-  int device = -1;
-  int num_sms = 0;
-  size_t smem_optin = 0;
-};
+void Alloc::release(void* p, size_t bytes)
+{
+  if (!p) return;
+  if (bytes == 0) bytes = 8;
+  bytes = (bytes + 255) & ~size_t(255);
+  if (has_user) user.deallocate(user.ctx, p, bytes, st);
+  else cudaFreeAsync(p, st);
+}
 
 DeviceInfo current_device()
 {
@@ -267,7 +194,6 @@ uint64_t next_pow2(uint64_t v)
   return p;
 }
 
-}  // namespace
 }  // namespace gbx
 
 using namespace gbx;
@@ -332,12 +258,7 @@ struct PhaseTimer {
 }  // namespace
 }  // namespace gbx
 
-struct ResultInternal {
-  Alloc alloc;
-};
-
 namespace gbx {
-namespace {
 
 // Output column allocation helper.
 void alloc_column(Alloc& a, gbx_column& c, int32_t type_id, int32_t scale, int64_t n, bool with_mask)
@@ -360,14 +281,9 @@ void alloc_column(Alloc& a, gbx_column& c, int32_t type_id, int32_t scale, int64
   c.view.null_count = with_mask ? -1 : 0;
 }
 
-struct ReqMap {
-  int chan;
-};
-
-void validate(const gbx_groupby* gb, const gbx_request* reqs, int32_t nreq)
+void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n)
 {
   GBX_EXPECTS(nreq >= 0 && (nreq == 0 || reqs != nullptr), "invalid request array");
-  const int64_t n = gb->keys.empty() ? 0 : gb->keys[0].size;
   for (int32_t q = 0; q < nreq; ++q) {
     const gbx_request& r = reqs[q];
     // groupby.cu:210-214
@@ -432,30 +348,29 @@ SmemLayout make_smem_layout(const Plan& plan, uint32_t S)
   return sl;
 }
 
-struct Call {
-  gbx_groupby* gb;
-  const gbx_request* reqs;
-  int32_t nreq;
-  Alloc alloc;
-  DeviceInfo dev;
-  int64_t n = 0;
-};
+size_t slot_bytes(const Plan& plan)
+{
+  size_t b = static_cast<size_t>(plan.key.nwords) * 8 + 4;
+  for (int a = 0; a < plan.acc.nacc; ++a) b += acc_bytes(plan.acc.kind[a]);
+  return b;
+}
 
 // Builds the key plan.  `key_nulls[c]` is the null count of key column c.
-KeyPlan make_key_plan(const gbx_groupby* gb, const std::vector<int64_t>& key_nulls, bool& ok)
+KeyPlan make_key_plan(const gbx_column_view* keys, int nkeys, int32_t null_policy,
+                      const std::vector<int64_t>& key_nulls, bool& ok)
 {
   KeyPlan kp{};
   ok                   = true;
-  kp.ncols             = static_cast<int32_t>(gb->keys.size());
+  kp.ncols             = nkeys;
   bool any_nulls       = false;
   for (auto v : key_nulls) any_nulls |= (v != 0);
-  const bool include   = gb->null_policy == GBX_NULL_INCLUDE;
+  const bool include   = null_policy == GBX_NULL_INCLUDE;
   kp.skip_null_rows    = (!include && any_nulls) ? 1 : 0;
   // value fields first (never split across a word), then the null bits in
   // the first free bits of either word
   int word = 0, bit = 0;
   for (int c = 0; c < kp.ncols; ++c) {
-    const gbx_column_view& col = gb->keys[c];
+    const gbx_column_view& col = keys[c];
     KeyCol& kc                 = kp.cols[c];
     int32_t phys_type          = col.type_id == GBX_TYPE_DICTIONARY32
                                    ? (col.index_type_id ? col.index_type_id : GBX_TYPE_INT32)
@@ -501,8 +416,135 @@ KeyPlan make_key_plan(const gbx_groupby* gb, const std::vector<int64_t>& key_nul
   return kp;
 }
 
-}  // namespace
+std::vector<const gbx_column_view*> collect_channels(const gbx_request* reqs, int32_t nreq,
+                                                     std::vector<int>& req_chan)
+{
+  req_chan.assign(nreq, -1);
+  std::vector<const gbx_column_view*> chan_cols;
+  for (int q = 0; q < nreq; ++q) {
+    if (reqs[q].num_aggregations == 0) continue;
+    int found = -1;
+    for (size_t c = 0; c < chan_cols.size(); ++c)
+      if (same_view(*chan_cols[c], reqs[q].values)) found = static_cast<int>(c);
+    if (found < 0) {
+      found = static_cast<int>(chan_cols.size());
+      chan_cols.push_back(&reqs[q].values);
+    }
+    req_chan[q] = found;
+  }
+  if (static_cast<int>(chan_cols.size()) > kMaxChannels)
+    fail(GBX_ERR_UNSUPPORTED, "more than %d distinct value columns in one call", kMaxChannels);
+  return chan_cols;
+}
+
+void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_cols,
+                   const std::vector<int64_t>& chan_nulls, const gbx_request* reqs, int32_t nreq,
+                   const std::vector<int>& req_chan)
+{
+  plan.nchan = static_cast<int32_t>(chan_cols.size());
+  int nacc   = 0;
+  auto add_acc = [&](int kind) -> int8_t {
+    if (nacc >= kMaxAccs) fail(GBX_ERR_UNSUPPORTED, "too many accumulators in one call");
+    plan.acc.kind[nacc] = static_cast<int8_t>(kind);
+    return static_cast<int8_t>(nacc++);
+  };
+  for (int c = 0; c < plan.nchan; ++c) {
+    const gbx_column_view& col = *chan_cols[c];
+    Channel& ch                = plan.chan[c];
+    std::memset(&ch, 0, sizeof(ch));
+    ch.a_cnt = ch.a_sum = ch.a_min = ch.a_max = ch.a_sq = ch.a_k = ch.a_s2 = ch.a_prod = ch.a_amin = ch.a_amax = -1;
+    int32_t vt = value_type(col);
+    ch.data    = col.data;
+    ch.mask    = chan_nulls[c] != 0 ? col.null_mask : nullptr;
+    ch.offset  = col.offset;
+    if (col.type_id == GBX_TYPE_DICTIONARY32) {
+      int32_t it     = col.index_type_id ? col.index_type_id : GBX_TYPE_INT32;
+      ch.dict_data   = col.dict_keys->data;
+      ch.dict_offset = col.dict_keys->offset;
+      ch.dict_size   = col.dict_keys->size;
+      ch.idx_width   = static_cast<int8_t>(type_width(it));
+      ch.idx_signed  = is_unsigned(it) ? 0 : 1;
+    }
+    ch.ptype      = phys_of(vt);
+    ch.is_float   = is_floating(vt) ? 1 : 0;
+    uint32_t need = 0;
+    for (int q = 0; q < nreq; ++q) {
+      if (req_chan[q] != c) continue;
+      for (int k = 0; k < reqs[q].num_aggregations; ++k) {
+        switch (reqs[q].aggregations[k].kind) {
+          case GBX_AGG_SUM: need |= N_SUM; break;
+          case GBX_AGG_PRODUCT: need |= N_PROD; break;
+          case GBX_AGG_MIN: need |= N_MIN; break;
+          case GBX_AGG_MAX: need |= N_MAX; break;
+          case GBX_AGG_COUNT_VALID: need |= N_CNT; break;
+          case GBX_AGG_SUM_OF_SQUARES: need |= N_SQ; break;
+          case GBX_AGG_MEAN: need |= N_SUM | N_CNT; break;
+          case GBX_AGG_VARIANCE:
+          case GBX_AGG_STD: need |= N_SUM | N_CNT | N_VAR; break;
+          default: break;  // COUNT_ALL uses the row count
+        }
+      }
+    }
+    ch.need        = need;
+    const bool m64 = ch.ptype == P_I64 || ch.ptype == P_U64 || ch.ptype == P_F64;
+    // COUNT_VALID of a column without nulls is the group's row count; a
+    // nullable column needs its own count (also the validity of SUM/MIN/...)
+    if (chan_nulls[c] != 0) ch.a_cnt = add_acc(A_U32_ADD);
+    if (need & N_SUM) ch.a_sum = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
+    if (need & N_MIN) ch.a_min = add_acc(m64 ? A_U64_MIN : A_U32_MIN);
+    if (need & N_MAX) ch.a_max = add_acc(m64 ? A_U64_MAX : A_U32_MAX);
+    if (need & N_SQ) ch.a_sq = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
+    if (need & N_PROD) ch.a_prod = add_acc(ch.is_float ? A_F64_MUL : A_I64_MUL);
+    if (need & N_VAR) {
+      ch.a_k  = add_acc(A_F64_SHIFT);
+      ch.a_s2 = add_acc(A_F64_ADD);
+    }
+  }
+  plan.acc.nacc = nacc;
+}
+
+// Invert the expected distinct count of a uniform draw, d = C (1 - exp(-m / C)),
+// then G = C (1 - exp(-N / C)).
+double estimate_groups(double sampled, double distinct, int64_t n, int64_t nsample)
+{
+  double est;
+  if (nsample >= n) {
+    est = distinct;
+  } else if (distinct >= sampled) {
+    est = static_cast<double>(n);
+  } else {
+    double lo = distinct, hi = 1e12;
+    for (int it = 0; it < 200; ++it) {
+      double mid = 0.5 * (lo + hi);
+      double d   = mid * (1.0 - std::exp(-sampled / mid));
+      if (d < distinct) lo = mid;
+      else hi = mid;
+    }
+    double C = 0.5 * (lo + hi);
+    est      = C * (1.0 - std::exp(-static_cast<double>(n) / C));
+  }
+  return std::max(1.0, std::min(est, static_cast<double>(n)));
+}
+
 }  // namespace gbx
+
+namespace {
+
+struct Call {
+  gbx_groupby* gb;
+  const gbx_request* reqs;
+  int32_t nreq;
+  gbx::Alloc alloc;
+  gbx::DeviceInfo dev;
+  int64_t n = 0;
+};
+
+void validate(const gbx_groupby* gb, const gbx_request* reqs, int32_t nreq)
+{
+  gbx::validate_requests(reqs, nreq, gb->keys.empty() ? 0 : gb->keys[0].size);
+}
+
+}  // namespace
 
 // ================================================================== C ABI
 
@@ -663,21 +705,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     gb->stats.num_rows = call.n;
 
     // ---- distinct value columns -> channels
-    std::vector<int> req_chan(num_requests, -1);
-    std::vector<const gbx_column_view*> chan_cols;
-    for (int q = 0; q < num_requests; ++q) {
-      if (requests[q].num_aggregations == 0) continue;
-      int found = -1;
-      for (size_t c = 0; c < chan_cols.size(); ++c)
-        if (same_view(*chan_cols[c], requests[q].values)) found = static_cast<int>(c);
-      if (found < 0) {
-        found = static_cast<int>(chan_cols.size());
-        chan_cols.push_back(&requests[q].values);
-      }
-      req_chan[q] = found;
-    }
-    if (static_cast<int>(chan_cols.size()) > kMaxChannels)
-      fail(GBX_ERR_UNSUPPORTED, "more than %d distinct value columns in one call", kMaxChannels);
+    std::vector<int> req_chan;
+    std::vector<const gbx_column_view*> chan_cols = collect_channels(requests, num_requests, req_chan);
 
     // ---- null counts (one small kernel + one read, merged with the sample read)
     std::vector<int64_t> key_nulls(nkeys, 0), chan_nulls(chan_cols.size(), 0);
@@ -734,7 +763,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     launches += ms.n > 0 ? 1 : 0;
 
     bool key_ok       = true;
-    KeyPlan kp_sample = make_key_plan(gb, std::vector<int64_t>(nkeys, -1), key_ok);
+    KeyPlan kp_sample =
+      make_key_plan(gb->keys.data(), nkeys, gb->null_policy, std::vector<int64_t>(nkeys, -1), key_ok);
     if (!key_ok)
       fail(GBX_ERR_UNSUPPORTED, "key columns need more than 128 packed bits; wider composite keys are not supported");
 
@@ -754,98 +784,17 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       if (span_owner[i].first == 0) key_nulls[span_owner[i].second] = nulls;
       else chan_nulls[span_owner[i].second] = nulls;
     }
-    const double sampled = static_cast<double>(h_ctl[0]);
-    const double distinct = static_cast<double>(h_ctl[1]);
-
-    // Estimate groups: invert the expected distinct count of a uniform draw,
-    // d = C (1 - exp(-m / C)), then G = C (1 - exp(-N / C)).
-    double est;
-    if (nsample >= call.n) {
-      est = distinct;
-    } else if (distinct >= sampled) {
-      est = static_cast<double>(call.n);
-    } else {
-      double lo = distinct, hi = 1e12;
-      for (int it = 0; it < 200; ++it) {
-        double mid = 0.5 * (lo + hi);
-        double d   = mid * (1.0 - std::exp(-sampled / mid));
-        if (d < distinct) lo = mid;
-        else hi = mid;
-      }
-      double C = 0.5 * (lo + hi);
-      est      = C * (1.0 - std::exp(-static_cast<double>(call.n) / C));
-    }
-    est = std::max(1.0, std::min(est, static_cast<double>(call.n)));
+    double est = estimate_groups(static_cast<double>(h_ctl[0]), static_cast<double>(h_ctl[1]), call.n, nsample);
     gb->stats.estimated_groups = static_cast<int64_t>(est);
 
     // ---- plan
     Plan plan{};
-    plan.key = make_key_plan(gb, key_nulls, key_ok);
-    plan.nchan = static_cast<int32_t>(chan_cols.size());
-    int nacc   = 0;
-    auto add_acc = [&](int kind) -> int8_t {
-      if (nacc >= kMaxAccs) fail(GBX_ERR_UNSUPPORTED, "too many accumulators in one call");
-      plan.acc.kind[nacc] = static_cast<int8_t>(kind);
-      return static_cast<int8_t>(nacc++);
-    };
-    for (int c = 0; c < plan.nchan; ++c) {
-      const gbx_column_view& col = *chan_cols[c];
-      Channel& ch                = plan.chan[c];
-      std::memset(&ch, 0, sizeof(ch));
-      ch.a_cnt = ch.a_sum = ch.a_min = ch.a_max = ch.a_sq = ch.a_k = ch.a_s2 = ch.a_prod = ch.a_amin = ch.a_amax = -1;
-      int32_t vt = value_type(col);
-      ch.data    = col.data;
-      ch.mask    = chan_nulls[c] != 0 ? col.null_mask : nullptr;
-      ch.offset  = col.offset;
-      if (col.type_id == GBX_TYPE_DICTIONARY32) {
-        int32_t it     = col.index_type_id ? col.index_type_id : GBX_TYPE_INT32;
-        ch.dict_data   = col.dict_keys->data;
-        ch.dict_offset = col.dict_keys->offset;
-        ch.dict_size   = col.dict_keys->size;
-        ch.idx_width   = static_cast<int8_t>(type_width(it));
-        ch.idx_signed  = is_unsigned(it) ? 0 : 1;
-      }
-      ch.ptype    = phys_of(vt);
-      ch.is_float = is_floating(vt) ? 1 : 0;
-      uint32_t need = 0;
-      for (int q = 0; q < num_requests; ++q) {
-        if (req_chan[q] != c) continue;
-        for (int k = 0; k < requests[q].num_aggregations; ++k) {
-          switch (requests[q].aggregations[k].kind) {
-            case GBX_AGG_SUM: need |= N_SUM; break;
-            case GBX_AGG_PRODUCT: need |= N_PROD; break;
-            case GBX_AGG_MIN: need |= N_MIN; break;
-            case GBX_AGG_MAX: need |= N_MAX; break;
-            case GBX_AGG_COUNT_VALID: need |= N_CNT; break;
-            case GBX_AGG_COUNT_ALL: break;
-            case GBX_AGG_SUM_OF_SQUARES: need |= N_SQ; break;
-            case GBX_AGG_MEAN: need |= N_SUM | N_CNT; break;
-            case GBX_AGG_VARIANCE:
-            case GBX_AGG_STD: need |= N_SUM | N_CNT | N_VAR; break;
-          }
-        }
-      }
-      ch.need = need;
-      const bool nullable = ch.mask != nullptr;
-      // COUNT_VALID of a column without nulls is the group's row count; a
-      // nullable column needs its own count (also the validity of SUM/MIN/...)
-      if (nullable) ch.a_cnt = add_acc(A_U32_ADD);
-      const bool m64 = ch.ptype == P_I64 || ch.ptype == P_U64 || ch.ptype == P_F64;
-      if (need & N_SUM) ch.a_sum = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
-      if (need & N_MIN) ch.a_min = add_acc(m64 ? A_U64_MIN : A_U32_MIN);
-      if (need & N_MAX) ch.a_max = add_acc(m64 ? A_U64_MAX : A_U32_MAX);
-      if (need & N_SQ) ch.a_sq = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
-      if (need & N_PROD) ch.a_prod = add_acc(ch.is_float ? A_F64_MUL : A_I64_MUL);
-      if (need & N_VAR) {
-        ch.a_k  = add_acc(A_F64_SHIFT);
-        ch.a_s2 = add_acc(A_F64_ADD);
-      }
-    }
-    plan.acc.nacc = nacc;
+    plan.key = make_key_plan(gb->keys.data(), nkeys, gb->null_policy, key_nulls, key_ok);
+    fill_channels(plan, chan_cols, chan_nulls, requests, num_requests, req_chan);
+    const int nacc = plan.acc.nacc;
 
     // ---- strategy and sizes
-    size_t slot_bytes = static_cast<size_t>(plan.key.nwords) * 8 + 4;
-    for (int a = 0; a < nacc; ++a) slot_bytes += acc_bytes(plan.acc.kind[a]);
+    const size_t slot_bytes  = gbx::slot_bytes(plan);
     const size_t smem_budget = std::min<size_t>(call.dev.smem_optin, 100 * 1024);
     uint32_t s_max           = 1;
     while (static_cast<size_t>(s_max * 2 + 1) * slot_bytes + 16 * (nacc + 2) <= smem_budget && s_max < (1u << 16))
@@ -936,7 +885,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       int bits          = 0;
       while (static_cast<double>(1ull << bits) * gpb < est && bits < 22) ++bits;
       const SmemLayout sl = make_smem_layout(plan, S);
-      if (sl.total * 8 + 8 * 32 * 4 > call.dev.smem_optin)
+      if (static_cast<size_t>(sl.total) * 8 + 8 * (S + 32) * 4 > call.dev.smem_optin)
         fail(GBX_ERR_UNSUPPORTED, "per-group state too large for the partitioned path");
       PartBufs pbufs{};
       for (int w = 0; w < plan.key.nwords; ++w)
@@ -1067,27 +1016,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         GBX_CUDA(launch_agg_warp(plan, t, make_smem_layout(plan, s_warp), call.n, call.dev.num_sms, max_probes, s));
       } else if (strategy == GBX_STRATEGY_PRIVATIZED) {
         uint32_t S = static_cast<uint32_t>(std::min<uint64_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * est, 64.0))), s_max));
-        SmemLayout sl{};
-        sl.slots    = S;
-        uint32_t off = 0;
-        sl.keys_off  = off;
-        off += (S + 1) * plan.key.nwords * 8;
-        for (int a = 0; a < nacc; ++a) {
-          if (acc_bytes(plan.acc.kind[a]) == 8) {
-            off = (off + 7) & ~7u;
-            sl.acc_off[a] = off;
-            off += (S + 1) * 8;
-          }
-        }
-        for (int a = 0; a < nacc; ++a) {
-          if (acc_bytes(plan.acc.kind[a]) == 4) {
-            sl.acc_off[a] = off;
-            off += (S + 1) * 4;
-          }
-        }
-        sl.rows_off = off;
-        off += (S + 1) * 4;
-        sl.total = (off + 15) & ~15u;
+        const SmemLayout sl = make_smem_layout(plan, S);
         const int block = 512;
         int grid        = call.dev.num_sms * std::max<int>(1, std::min<int>(4, static_cast<int>((200 * 1024) / (sl.total + 1024))));
         int64_t max_grid = (call.n + block * 4 - 1) / (block * 4);
@@ -1218,21 +1147,8 @@ extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
     auto* d_nulls           = static_cast<unsigned long long*>(carve((kMaxKeyCols + kMaxOut) * 8));
 
     // ---- distinct value columns -> channels
-    std::vector<int> req_chan(num_requests, -1);
-    std::vector<const gbx_column_view*> chan_cols;
-    for (int q = 0; q < num_requests; ++q) {
-      if (requests[q].num_aggregations == 0) continue;
-      int found = -1;
-      for (size_t c = 0; c < chan_cols.size(); ++c)
-        if (same_view(*chan_cols[c], requests[q].values)) found = static_cast<int>(c);
-      if (found < 0) {
-        found = static_cast<int>(chan_cols.size());
-        chan_cols.push_back(&requests[q].values);
-      }
-      req_chan[q] = found;
-    }
-    if (static_cast<int>(chan_cols.size()) > kMaxChannels)
-      fail(GBX_ERR_UNSUPPORTED, "more than %d distinct value columns in one call", kMaxChannels);
+    std::vector<int> req_chan;
+    std::vector<const gbx_column_view*> chan_cols = collect_channels(requests, num_requests, req_chan);
     if (nout > kMaxOut) fail(GBX_ERR_UNSUPPORTED, "more than %d results in one call", kMaxOut);
 
     // ---- null counts of masks with an unknown count
@@ -1272,67 +1188,11 @@ extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
     // ---- plan: packed keys and one accumulator set per channel
     bool key_ok = true;
     Plan plan{};
-    plan.key = make_key_plan(gb, key_nulls, key_ok);
+    plan.key = make_key_plan(gb->keys.data(), nkeys, gb->null_policy, key_nulls, key_ok);
     if (!key_ok)
       fail(GBX_ERR_UNSUPPORTED, "key columns need more than 128 packed bits; wider composite keys are not supported");
-    plan.nchan = static_cast<int32_t>(chan_cols.size());
-    int nacc   = 0;
-    auto add_acc = [&](int kind) -> int8_t {
-      if (nacc >= kMaxAccs) fail(GBX_ERR_UNSUPPORTED, "too many accumulators in one call");
-      plan.acc.kind[nacc] = static_cast<int8_t>(kind);
-      return static_cast<int8_t>(nacc++);
-    };
-    for (int c = 0; c < plan.nchan; ++c) {
-      const gbx_column_view& col = *chan_cols[c];
-      Channel& ch                = plan.chan[c];
-      std::memset(&ch, 0, sizeof(ch));
-      ch.a_cnt = ch.a_sum = ch.a_min = ch.a_max = ch.a_sq = ch.a_k = ch.a_s2 = ch.a_prod = ch.a_amin = ch.a_amax = -1;
-      int32_t vt = value_type(col);
-      ch.data    = col.data;
-      ch.mask    = chan_nulls[c] != 0 ? col.null_mask : nullptr;
-      ch.offset  = col.offset;
-      if (col.type_id == GBX_TYPE_DICTIONARY32) {
-        int32_t it     = col.index_type_id ? col.index_type_id : GBX_TYPE_INT32;
-        ch.dict_data   = col.dict_keys->data;
-        ch.dict_offset = col.dict_keys->offset;
-        ch.dict_size   = col.dict_keys->size;
-        ch.idx_width   = static_cast<int8_t>(type_width(it));
-        ch.idx_signed  = is_unsigned(it) ? 0 : 1;
-      }
-      ch.ptype      = phys_of(vt);
-      ch.is_float   = is_floating(vt) ? 1 : 0;
-      uint32_t need = 0;
-      for (int q = 0; q < num_requests; ++q) {
-        if (req_chan[q] != c) continue;
-        for (int k = 0; k < requests[q].num_aggregations; ++k) {
-          switch (requests[q].aggregations[k].kind) {
-            case GBX_AGG_SUM: need |= N_SUM; break;
-            case GBX_AGG_PRODUCT: need |= N_PROD; break;
-            case GBX_AGG_MIN: need |= N_MIN; break;
-            case GBX_AGG_MAX: need |= N_MAX; break;
-            case GBX_AGG_COUNT_VALID: need |= N_CNT; break;
-            case GBX_AGG_SUM_OF_SQUARES: need |= N_SQ; break;
-            case GBX_AGG_MEAN: need |= N_SUM | N_CNT; break;
-            case GBX_AGG_VARIANCE:
-            case GBX_AGG_STD: need |= N_SUM | N_CNT | N_VAR; break;
-            default: break;
-          }
-        }
-      }
-      ch.need        = need;
-      const bool m64 = ch.ptype == P_I64 || ch.ptype == P_U64 || ch.ptype == P_F64;
-      if (ch.mask != nullptr) ch.a_cnt = add_acc(A_U32_ADD);
-      if (need & N_SUM) ch.a_sum = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
-      if (need & N_MIN) ch.a_min = add_acc(m64 ? A_U64_MIN : A_U32_MIN);
-      if (need & N_MAX) ch.a_max = add_acc(m64 ? A_U64_MAX : A_U32_MAX);
-      if (need & N_SQ) ch.a_sq = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
-      if (need & N_PROD) ch.a_prod = add_acc(ch.is_float ? A_F64_MUL : A_I64_MUL);
-      if (need & N_VAR) {
-        ch.a_k  = add_acc(A_F64_SHIFT);
-        ch.a_s2 = add_acc(A_F64_ADD);
-      }
-    }
-    plan.acc.nacc = nacc;
+    fill_channels(plan, chan_cols, chan_nulls, requests, num_requests, req_chan);
+    const int nacc = plan.acc.nacc;
 
     // ---- fixed-capacity global table carved from the scratch array
     const uint64_t cap = 2ull * GBX_NOALLOC_MAX_GROUPS;

@@ -68,20 +68,30 @@ __device__ __forceinline__ uint64_t load_bits(const void* p, int64_t i, int widt
   }
 }
 
-// Packs row `row`'s key into NW words.  Returns false when the row must be
-// skipped (a null key under null_policy::EXCLUDE).  Float keys are normalised
-// so that -0.0 == +0.0 and every NaN is one key, matching the reference's
-// nan-equal comparator and hash normalisation (row_operators.cuh:1285-1312,
+// Buffers of the key columns as a KeyPlan names them.
+struct PlanKeyBufs {
+  const KeyPlan* kp;
+  __device__ __forceinline__ const void* data(int c) const { return kp->cols[c].data; }
+  __device__ __forceinline__ const uint32_t* mask(int c) const { return kp->cols[c].mask; }
+  __device__ __forceinline__ int64_t offset(int c) const { return kp->cols[c].offset; }
+};
+
+// Packs row `row`'s key into NW words, reading column c from bufs.data(c)
+// (validity bufs.mask(c), row offset bufs.offset(c)) with the layout of
+// kp.cols[c].  Returns false when the row must be skipped (a null key under
+// null_policy::EXCLUDE).  Float keys are normalised so that -0.0 == +0.0 and
+// every NaN is one key, matching the reference's nan-equal comparator and
+// hash normalisation (row_operators.cuh:1285-1312,
 // hashing/detail/hash_functions.cuh:41-47).
-template <int NW>
-__device__ __forceinline__ bool pack_key(const KeyPlan& kp, int64_t row, uint64_t (&k)[NW])
+template <int NW, class Bufs>
+__device__ __forceinline__ bool pack_key_from(const KeyPlan& kp, const Bufs& bufs, int64_t row, uint64_t (&k)[NW])
 {
 #pragma unroll
   for (int w = 0; w < NW; ++w) k[w] = 0;
   for (int c = 0; c < kp.ncols; ++c) {
     const KeyCol& kc = kp.cols[c];
-    int64_t i        = row + kc.offset;
-    bool valid       = bit_valid(kc.mask, i);
+    int64_t i        = row + bufs.offset(c);
+    bool valid       = bit_valid(bufs.mask(c), i);
     if (!valid) {
       if (kp.skip_null_rows) return false;
       if (kc.null_bit) {
@@ -89,7 +99,7 @@ __device__ __forceinline__ bool pack_key(const KeyPlan& kp, int64_t row, uint64_
         continue;
       }
     }
-    uint64_t v = load_bits(kc.data, i, kc.width);
+    uint64_t v = load_bits(bufs.data(c), i, kc.width);
     if (kc.is_float) {
       if (kc.width == 4) {
         float f = __uint_as_float(static_cast<uint32_t>(v));
@@ -108,11 +118,17 @@ __device__ __forceinline__ bool pack_key(const KeyPlan& kp, int64_t row, uint64_
   return true;
 }
 
+template <int NW>
+__device__ __forceinline__ bool pack_key(const KeyPlan& kp, int64_t row, uint64_t (&k)[NW])
+{
+  return pack_key_from<NW>(kp, PlanKeyBufs{&kp}, row, k);
+}
+
 // ------------------------------------------------------------ value loads
 
-__device__ __forceinline__ int64_t dict_index(const Channel& ch, int64_t i)
+__device__ __forceinline__ int64_t dict_index(const Channel& ch, const void* data, int64_t i)
 {
-  uint64_t b = load_bits(ch.data, i, ch.idx_width);
+  uint64_t b = load_bits(data, i, ch.idx_width);
   if (ch.idx_signed) {
     switch (ch.idx_width) {
       case 1: return static_cast<int8_t>(b);
@@ -124,20 +140,24 @@ __device__ __forceinline__ int64_t dict_index(const Channel& ch, int64_t i)
   return static_cast<int64_t>(b);
 }
 
-// Raw element of the value (dictionary resolved).  `ok` false on an
-// out-of-range dictionary index (the row is then ignored and a status bit set).
-__device__ __forceinline__ uint64_t value_bits(const Channel& ch, int64_t row, bool& ok)
+// Raw element of a value column with the element layout of `ch` read from
+// `data` at row + offset (dictionary resolved through dict_data when it is
+// set).  `ok` false on an out-of-range dictionary index (the row is then
+// ignored and a status bit set).
+__device__ __forceinline__ uint64_t value_bits_at(const Channel& ch, const void* data, int64_t offset,
+                                                  const void* dict_data, int64_t dict_offset, int64_t dict_size,
+                                                  int64_t row, bool& ok)
 {
-  const void* base = ch.data;
-  int64_t i        = row + ch.offset;
-  if (ch.dict_data != nullptr) {
-    int64_t k = dict_index(ch, i);
-    if (k < 0 || k >= ch.dict_size) {
+  const void* base = data;
+  int64_t i        = row + offset;
+  if (dict_data != nullptr) {
+    int64_t k = dict_index(ch, data, i);
+    if (k < 0 || k >= dict_size) {
       ok = false;
       return 0;
     }
-    base = ch.dict_data;
-    i    = k + ch.dict_offset;
+    base = dict_data;
+    i    = k + dict_offset;
   }
   ok = true;
   switch (ch.ptype) {
@@ -151,6 +171,11 @@ __device__ __forceinline__ uint64_t value_bits(const Channel& ch, int64_t row, b
     case P_F32: return load_bits(base, i, 4);
     default: return load_bits(base, i, 8);
   }
+}
+
+__device__ __forceinline__ uint64_t value_bits(const Channel& ch, int64_t row, bool& ok)
+{
+  return value_bits_at(ch, ch.data, ch.offset, ch.dict_data, ch.dict_offset, ch.dict_size, row, ok);
 }
 
 __device__ __forceinline__ int64_t as_i64(uint64_t b, int ptype)

@@ -23,6 +23,10 @@
 #include <thrust/iterator/counting_iterator.h>
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "gbx_kernels.hpp"
 #include "gbx_table.cuh"
 
@@ -374,11 +378,11 @@ cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLa
   int64_t rpb = (n + grid - 1) / grid;
   cudaError_t e;
   if (p.key.nwords == 1) {
-    e = cudaFuncSetAttribute(k_agg_privatized<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl.total);
+    e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_agg_privatized<1>), sl.total);
     if (e != cudaSuccess) return e;
     k_agg_privatized<1><<<grid, block, sl.total, st>>>(p, t, sl, n, rpb, smem_probes, max_probes);
   } else {
-    e = cudaFuncSetAttribute(k_agg_privatized<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl.total);
+    e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_agg_privatized<2>), sl.total);
     if (e != cudaSuccess) return e;
     k_agg_privatized<2><<<grid, block, sl.total, st>>>(p, t, sl, n, rpb, smem_probes, max_probes);
   }
@@ -428,6 +432,50 @@ __global__ void k_count_valid(const __grid_constant__ MaskSpans ms, unsigned lon
     for (int off = 16; off > 0; off >>= 1) local += __shfl_down_sync(0xffffffffu, local, off);
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(out + c, local);
   }
+}
+
+// dst bits [0, n) = src bits [src_bit, src_bit + n); every dst word of the
+// range is written (bits past n cleared); src words are read only where
+// their bits are needed.
+__global__ void k_copy_bits(const uint32_t* __restrict__ src, int64_t src_bit, uint32_t* __restrict__ dst, int64_t n)
+{
+  const int64_t words  = (n + 31) >> 5;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t w = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; w < words; w += stride) {
+    const int64_t b   = src_bit + (w << 5);
+    const int64_t sw  = b >> 5;
+    const int sh      = static_cast<int>(b & 31);
+    const int64_t rem = n - (w << 5);
+    uint32_t v        = __ldg(src + sw) >> sh;
+    if (sh != 0 && rem > 32 - sh) v |= __ldg(src + sw + 1) << (32 - sh);
+    if (rem < 32) v &= (1u << rem) - 1u;
+    dst[w] = v;
+  }
+}
+
+cudaError_t ensure_dynamic_smem(const void* func, size_t bytes)
+{
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limit;
+  int device    = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limit[{device, func}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
+
+cudaError_t launch_copy_bits(const uint32_t* src, int64_t src_bit, uint32_t* dst, int64_t n, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  const int64_t words = (n + 31) >> 5;
+  int64_t b           = (words + 255) / 256;
+  if (b > 4096) b = 4096;
+  k_copy_bits<<<static_cast<int>(b), 256, 0, st>>>(src, src_bit, dst, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_count_valid(const MaskSpans& ms, unsigned long long* out_valid, int num_sms, cudaStream_t st)

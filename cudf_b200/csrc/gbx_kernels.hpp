@@ -120,4 +120,12 @@ struct MaskSpans {
   MaskSpan span[kMaxMaskSpans];
 };
 cudaError_t launch_count_valid(const MaskSpans& ms, unsigned long long* out_valid, int num_sms, cudaStream_t st);
+
+// dst bits [0, n) = src bits [src_bit, src_bit + n) (a bitmask slice).
+cudaError_t launch_copy_bits(const uint32_t* src, int64_t src_bit, uint32_t* dst, int64_t n, cudaStream_t st);
+
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`.  It never lowers it, so a launch on another thread that was
+// sized against the current limit stays valid.
+cudaError_t ensure_dynamic_smem(const void* func, size_t bytes);
 }  // namespace gbx

@@ -127,7 +127,8 @@ __global__ void k_part_scatter(const __grid_constant__ Plan plan, int64_t n, con
 }
 
 // Bucket / slice aggregation (see the file comment).  blockDim.x / 32 warp
-// tables of sl.total bytes, then 32 u32 of compaction scratch per warp.
+// tables of sl.total bytes, then sl.slots + 32 u32 of compaction scratch per
+// warp (the occupied slots of a bucket, listed before its rows are reserved).
 template <int NW, int NCH>
 __global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Plan plan, const __grid_constant__ PartPlan pp, const __grid_constant__ PartBufs in, const __grid_constant__ TableRef t, const __grid_constant__ SmemLayout sl,
                                                   const __grid_constant__ OutPlan op)
@@ -137,7 +138,8 @@ __global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Pla
   const int warp   = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
   WarpTable<NW> T{smem + static_cast<size_t>(warp) * sl.total, &sl, sl.slots};
-  uint32_t* scratch = reinterpret_cast<uint32_t*>(smem + static_cast<size_t>(nwarps) * sl.total) + warp * 32;
+  uint32_t* scratch = reinterpret_cast<uint32_t*>(smem + static_cast<size_t>(nwarps) * sl.total) +
+                      static_cast<size_t>(warp) * (sl.slots + 32);
   const PartSource src{&in};
   const uint32_t P          = 1u << pp.bits;
   const uint64_t items      = pp.item_start[P];
@@ -191,8 +193,10 @@ __global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Pla
     }
 
     if (ns == 1) {
-      // the whole bucket is here: write its groups out
+      // the whole bucket is here: list its occupied slots, reserve their
+      // output rows with one atomic, then write them 32 at a time
       const SmemAccs A{T.tb, &sl};
+      uint32_t total = 0;
       for (uint32_t s0 = 0; s0 <= T.S; s0 += 32) {
         const uint32_t s = s0 + lane;
         bool occ         = false;
@@ -205,27 +209,30 @@ __global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Pla
           occ = special;
         }
         const uint32_t bal = __ballot_sync(kFull, occ);
-        if (bal == 0) continue;
-        const int cnt = __popc(bal);
-        if (occ) scratch[__popc(bal & lanemask_lt(lane))] = s;
-        __syncwarp();
-        unsigned long long ob = 0;
-        if (lane == 0) ob = atomicAdd(pp.out_counter, static_cast<unsigned long long>(cnt));
-        ob                = __shfl_sync(kFull, ob, 0);
-        const bool active = lane < cnt;
-        const uint32_t ss = active ? scratch[lane] : 0;
-        uint64_t k2[2]    = {0, 0};
-        if (active) {
-          if (ss == T.S) {
-            k2[0] = k2[1] = kEmptyWord;
-          } else {
-#pragma unroll
-            for (int w = 0; w < NW; ++w) k2[w] = keys[ss * NW + w];
-          }
-        }
-        warp_write_groups(plan, op, A, active, ss, k2, static_cast<int64_t>(ob), lane);
-        __syncwarp();
+        if (occ) scratch[total + __popc(bal & lanemask_lt(lane))] = s;
+        total += __popc(bal);
       }
+      __syncwarp();
+      if (total > 0) {
+        unsigned long long ob = 0;
+        if (lane == 0) ob = atomicAdd(pp.out_counter, static_cast<unsigned long long>(total));
+        ob = __shfl_sync(kFull, ob, 0);
+        for (uint32_t g0 = 0; g0 < total; g0 += 32) {
+          const bool active = g0 + lane < total;
+          const uint32_t ss = active ? scratch[g0 + lane] : 0;
+          uint64_t k2[2]    = {0, 0};
+          if (active) {
+            if (ss == T.S) {
+              k2[0] = k2[1] = kEmptyWord;
+            } else {
+#pragma unroll
+              for (int w = 0; w < NW; ++w) k2[w] = keys[ss * NW + w];
+            }
+          }
+          warp_write_groups(plan, op, A, active, ss, k2, static_cast<int64_t>(ob + g0), lane);
+        }
+      }
+      __syncwarp();
     } else {
       // a slice of a large bucket: merge into the bucket's region table
       const Level<Shared> L{static_cast<uint32_t>(__cvta_generic_to_shared(T.tb)), &sl};
@@ -360,9 +367,8 @@ cudaError_t launch_part_agg_impl(const Plan& p, const PartPlan& pp, const PartBu
 {
   const int block   = 256;
   const int warps   = block / 32;
-  const size_t smem = static_cast<size_t>(sl.total) * warps + warps * 32 * sizeof(uint32_t);
-  cudaError_t e =
-    cudaFuncSetAttribute(k_part_agg<NW, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  const size_t smem = static_cast<size_t>(sl.total) * warps + warps * (sl.slots + 32) * sizeof(uint32_t);
+  cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_part_agg<NW, NCH>), smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_agg<NW, NCH>, block, smem);

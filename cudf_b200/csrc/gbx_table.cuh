@@ -91,27 +91,49 @@ __device__ __forceinline__ double get_shift(typename Space::addr_t a, double x)
   return __longlong_as_double(static_cast<long long>(kb));
 }
 
-// Folds row `row` into slot `slot` of a table level (aggregate_row,
+// ------------------------------------------------------------- row sources
+
+// Rows of the caller's columns as the plan names them.
+struct RowSource {
+  const Plan* plan;
+  template <int NW>
+  __device__ __forceinline__ bool key(int64_t r, uint64_t (&k)[NW]) const
+  {
+    return pack_key<NW>(plan->key, r, k);
+  }
+  // Raw bits of channel c at row r; false for a null value (or an
+  // out-of-range dictionary index, which also sets S_BAD_INDEX).
+  __device__ __forceinline__ bool value(int c, int64_t r, uint64_t& b, int32_t* status) const
+  {
+    const Channel& ch = plan->chan[c];
+    if (!bit_valid(ch.mask, r + ch.offset)) return false;
+    bool ok;
+    b = value_bits(ch, r, ok);
+    if (!ok) {
+      atomicOr(status, S_BAD_INDEX);
+      return false;
+    }
+    return true;
+  }
+};
+
+// Folds row `row` of `src` into slot `slot` of a table level (aggregate_row,
 // detail/aggregation/aggregation.cuh:558-573, with update_target_element's
 // null skipping, :116-491).
-template <class Space>
-__device__ __forceinline__ void accumulate_row(const Plan& plan,
-                                               const Level<Space>& L,
-                                               int64_t slot,
-                                               int64_t row,
-                                               int32_t* status)
+template <class Space, class Src>
+__device__ __forceinline__ void accumulate_row_from(const Plan& plan,
+                                                    const Src& src,
+                                                    const Level<Space>& L,
+                                                    int64_t slot,
+                                                    int64_t row,
+                                                    int32_t* status)
 {
   using A = typename Space::addr_t;
   Space::add_u32(L.rows() + static_cast<A>(slot * 4), 1u);
   for (int c = 0; c < plan.nchan; ++c) {
     const Channel& ch = plan.chan[c];
-    if (!bit_valid(ch.mask, row + ch.offset)) continue;
-    bool ok;
-    uint64_t b = value_bits(ch, row, ok);
-    if (!ok) {
-      atomicOr(status, S_BAD_INDEX);
-      continue;
-    }
+    uint64_t b;
+    if (!src.value(c, row, b, status)) continue;
     if (ch.a_cnt >= 0) Space::add_u32(L.acc(ch.a_cnt) + static_cast<A>(slot * 4), 1u);
     const bool is64 = minmax_is64(ch.ptype);
     if (ch.a_min >= 0) {
@@ -150,6 +172,16 @@ __device__ __forceinline__ void accumulate_row(const Plan& plan,
       }
     }
   }
+}
+
+template <class Space>
+__device__ __forceinline__ void accumulate_row(const Plan& plan,
+                                               const Level<Space>& L,
+                                               int64_t slot,
+                                               int64_t row,
+                                               int32_t* status)
+{
+  accumulate_row_from<Space>(plan, RowSource{&plan}, L, slot, row, status);
 }
 
 // Merges slot `s` of a (shared-memory) partial level into slot `g` of the

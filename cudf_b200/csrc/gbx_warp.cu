@@ -92,8 +92,7 @@ cudaError_t launch_agg_warp_impl(const Plan& p, const TableRef& t, const SmemLay
   const int block   = 256;
   const int warps   = block / 32;
   const size_t smem = static_cast<size_t>(sl.total) * warps;
-  cudaError_t e =
-    cudaFuncSetAttribute(k_agg_warp<NW, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_agg_warp<NW, NCH>), smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_agg_warp<NW, NCH>, block, smem);

@@ -22,27 +22,7 @@ constexpr uint32_t kFull = 0xffffffffu;
 
 // ------------------------------------------------------------- row sources
 
-// Rows of the caller's columns.
-struct RowSource {
-  const Plan* plan;
-  template <int NW>
-  __device__ __forceinline__ bool key(int64_t r, uint64_t (&k)[NW]) const
-  {
-    return pack_key<NW>(plan->key, r, k);
-  }
-  __device__ __forceinline__ bool value(int c, int64_t r, uint64_t& b, int32_t* status) const
-  {
-    const Channel& ch = plan->chan[c];
-    if (!bit_valid(ch.mask, r + ch.offset)) return false;
-    bool ok;
-    b = value_bits(ch, r, ok);
-    if (!ok) {
-      atomicOr(status, S_BAD_INDEX);
-      return false;
-    }
-    return true;
-  }
-};
+// (RowSource, the caller's columns, is in gbx_table.cuh.)
 
 // Rows of the radix-partitioned copies (keys already packed, dictionary
 // values resolved, validity as one byte per row).
