@@ -207,8 +207,135 @@ class gbx_stats(C.Structure):
     ]
 
 
+class BatchMode(enum.IntEnum):
+    """gbx_batch_mode."""
+
+    AUTO = 0
+    SHARED = 1
+    WARP = 2
+    GLOBAL = 3
+
+
+class Tune(enum.IntEnum):
+    """gbx_batch_tune."""
+
+    OFF = 0
+    CACHED = 1
+    MISSING = 2
+    ALL = 3
+
+
+class gbx_batch_instance(C.Structure):
+    _fields_ = [("keys", gbx_table_view), ("requests", C.POINTER(gbx_request))]
+
+
+class gbx_batch_options(C.Structure):
+    _fields_ = [
+        ("null_policy", C.c_int32),
+        ("tune", C.c_int32),
+        ("tune_file", C.c_char_p),
+        ("force_mode", C.c_int32),
+        ("block_threads", C.c_int32),
+        ("one_shot", C.c_int32),
+        ("tile_rows", C.c_int64),
+    ]
+
+
+class gbx_batch_output(C.Structure):
+    _fields_ = [
+        ("num_instances", C.c_int32),
+        ("reserved", C.c_int32),
+        ("group_offsets", C.POINTER(C.c_int64)),
+        ("device_group_offsets", C.c_void_p),
+        ("columns", gbx_result),
+    ]
+
+
+class gbx_batch_stats(C.Structure):
+    _fields_ = [
+        ("num_instances", C.c_int32),
+        ("block_threads", C.c_int32),
+        ("grid", C.c_int32),
+        ("work_items", C.c_int32),
+        ("num_rows", C.c_int64),
+        ("num_groups", C.c_int64),
+        ("dynamic_smem", C.c_int64),
+        ("arena_bytes", C.c_int64),
+        ("output_rows", C.c_int64),
+        ("mode_count", C.c_int32 * 4),
+        ("classes", C.c_int32),
+        ("classes_measured", C.c_int32),
+        ("classes_cached", C.c_int32),
+        ("retries", C.c_int32),
+        ("graph_nodes", C.c_int32),
+        ("kernels_per_execute", C.c_int32),
+        ("create_ms", C.c_float),
+        ("tune_ms", C.c_float),
+        ("execute_ms", C.c_float),
+        ("init_ms", C.c_float),
+        ("aggregate_ms", C.c_float),
+        ("output_ms", C.c_float),
+    ]
+
+
+class gbx_server_options(C.Structure):
+    _fields_ = [
+        ("workers", C.c_int32),
+        ("null_policy", C.c_int32),
+        ("hbm_budget_bytes", C.c_int64),
+        ("batch_max_rows", C.c_int64),
+        ("batch_max_requests", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class gbx_server_timing(C.Structure):
+    _fields_ = [
+        ("submitted_s", C.c_double),
+        ("admitted_s", C.c_double),
+        ("done_s", C.c_double),
+        ("reserved_bytes", C.c_int64),
+        ("batched", C.c_int32),
+        ("worker", C.c_int32),
+    ]
+
+
+class gbx_server_stats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("batches", C.c_int64),
+        ("batched_requests", C.c_int64),
+        ("peak_reserved_bytes", C.c_int64),
+        ("rows", C.c_int64),
+        ("max_in_flight", C.c_int32),
+        ("workers", C.c_int32),
+        ("busy_s", C.c_double),
+    ]
+
+
 # Every entry point include/gbx.h declares, with (restype, argtypes).
 SIGNATURES = {
+    "gbx_batch_create": (
+        C.c_int,
+        [C.POINTER(gbx_batch_instance), C.c_int32, C.c_int32, C.POINTER(gbx_batch_options), C.c_void_p,
+         C.POINTER(gbx_allocator), C.POINTER(C.c_void_p)],
+    ),
+    "gbx_batch_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.POINTER(gbx_batch_output))]),
+    "gbx_batch_rebind": (C.c_int, [C.c_void_p, C.POINTER(gbx_batch_instance), C.c_int32]),
+    "gbx_batch_instance_plan": (
+        C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "gbx_batch_last_stats": (C.c_int, [C.c_void_p, C.POINTER(gbx_batch_stats)]),
+    "gbx_batch_destroy": (None, [C.c_void_p]),
+    "gbx_server_create": (C.c_int, [C.POINTER(gbx_server_options), C.POINTER(C.c_void_p)]),
+    "gbx_server_submit": (
+        C.c_int, [C.c_void_p, C.POINTER(gbx_table_view), C.POINTER(gbx_request), C.c_int32, C.POINTER(C.c_uint64)]),
+    "gbx_server_wait": (
+        C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.POINTER(gbx_result)), C.POINTER(gbx_server_timing)]),
+    "gbx_server_now": (C.c_double, [C.c_void_p]),
+    "gbx_server_last_stats": (C.c_int, [C.c_void_p, C.POINTER(gbx_server_stats)]),
+    "gbx_server_destroy": (None, [C.c_void_p]),
     "gbx_groupby_create": (C.c_int, [C.POINTER(gbx_table_view), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
     "gbx_groupby_aggregate": (
         C.c_int,

@@ -65,6 +65,45 @@ def zipf_ranks(rng, n: int, s: float = 1.2, ranks: int = 100_000) -> np.ndarray:
     return np.minimum(np.searchsorted(cdf, u, side="right"), ranks - 1)
 
 
+@dataclass
+class BatchSpec:
+    """Per-instance row counts and key cardinalities of a batched workload."""
+
+    rows: np.ndarray
+    cards: np.ndarray
+    seed: int
+
+    @property
+    def num_instances(self) -> int:
+        return len(self.rows)
+
+    @property
+    def total_rows(self) -> int:
+        return int(self.rows.sum())
+
+
+def batched_spec(num_instances: int = 4096, rows_range=(1e3, 1e6), card_range=(10, 1e4),
+                 seed: int = SEED0 + 4) -> BatchSpec:
+    """Row counts log-uniform in rows_range, cardinalities log-uniform in
+    card_range (floored), one draw per instance."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log10(rows_range[0]), np.log10(rows_range[1])
+    rows = np.floor(10.0 ** rng.uniform(lo, hi, num_instances)).astype(np.int64)
+    clo, chi = np.log10(card_range[0]), np.log10(card_range[1])
+    cards = np.maximum(1, np.floor(10.0 ** rng.uniform(clo, chi, num_instances))).astype(np.int64)
+    return BatchSpec(rows, cards, seed)
+
+
+def batched_instance(spec: BatchSpec, i: int):
+    """Instance i on the host: int32 key uniform in [0, C_i), int64 value
+    uniform in [0, 1e9]."""
+    rng = np.random.default_rng([spec.seed, i])
+    n = int(spec.rows[i])
+    k = rng.integers(0, int(spec.cards[i]), size=n, dtype=np.int32)
+    v = rng.integers(0, 1_000_000_000, size=n, dtype=np.int64, endpoint=True)
+    return k, v
+
+
 def plain_200m(n: int = 200_000_000, seed: int = SEED0 + 3, ranks: int = 100_000) -> PlainInput:
     """Composite (int32, int16) key, joint index Zipf(1.2) over `ranks` distinct
     pairs; 2% nulls per key column; float64 ~LogNormal(0, 1)."""

@@ -319,6 +319,196 @@ GBX_API int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
                                           int64_t capacity,
                                           int64_t* num_groups);
 
+/* ---- batched groupby ------------------------------------------------------
+ * No counterpart in the reference: a libcudf caller with many tables loops
+ * over cudf::groupby::groupby(keys_i).aggregate(requests_i), one call (with
+ * its own launches, allocations and result-size synchronisation) per table.
+ *
+ * A batch holds many independent groupby instances that share one schema:
+ * the same number and types of key columns, and the same requests (value
+ * types, aggregation kinds and ddof) over each instance's own columns and row
+ * count.  gbx_batch_create samples every instance's distinct count, lets the
+ * autotuner choose per instance a table mode (shared-memory table per CTA,
+ * per warp, or the global table), its table sizes and tile size, and the
+ * block shape of the batch; it then allocates one table arena and the
+ * outputs and captures the whole batch -- table fill, one persistent
+ * aggregation kernel over all instances' tiles, group counting, offsets and
+ * output writing -- as one CUDA graph.  gbx_batch_execute launches that
+ * graph (one launch) and waits for it.
+ *
+ * Inputs are read at execute time from the buffers given at create (or the
+ * last gbx_batch_rebind): the caller may refill them in place between
+ * executes.  Results are the concatenation of every instance's groups:
+ * instance i's groups are rows [group_offsets[i], group_offsets[i+1]) of the
+ * output columns, in unspecified order within the run, with the same values
+ * (and the same dtypes) as gbx_groupby_aggregate on that instance alone.  A
+ * result column carries a null mask when any instance's output can hold
+ * nulls.  The output columns belong to the batch and stay valid until the
+ * next execute, rebind or destroy. */
+typedef struct gbx_batch gbx_batch;
+
+typedef struct gbx_batch_instance {
+  gbx_table_view keys;          /* this instance's key columns */
+  const gbx_request* requests;  /* num_requests requests over this instance's rows */
+} gbx_batch_instance;
+
+typedef enum gbx_batch_mode {
+  GBX_BATCH_MODE_AUTO   = 0, /* the autotuner's choice per instance */
+  GBX_BATCH_MODE_SHARED = 1, /* one shared-memory table per CTA, merged into the global table */
+  GBX_BATCH_MODE_WARP   = 2, /* one shared-memory table per warp, updated without atomics */
+  GBX_BATCH_MODE_GLOBAL = 3  /* every row updates the instance's global table */
+} gbx_batch_mode;
+
+typedef enum gbx_batch_tune {
+  GBX_TUNE_OFF     = 0, /* built-in defaults; the tuning file is not read */
+  GBX_TUNE_CACHED  = 1, /* choices from the tuning file where present, defaults elsewhere */
+  GBX_TUNE_MISSING = 2, /* as CACHED, and measure + append the classes the file lacks */
+  GBX_TUNE_ALL     = 3  /* re-measure every class present in the batch and append */
+} gbx_batch_tune;
+
+typedef struct gbx_batch_options {
+  int32_t null_policy;         /* GBX_NULL_EXCLUDE or GBX_NULL_INCLUDE, for every instance */
+  int32_t tune;                /* gbx_batch_tune */
+  const char* tune_file;       /* the persisted tuning table (NULL: none) */
+  int32_t force_mode;          /* gbx_batch_mode for every instance (AUTO: per instance) */
+  int32_t block_threads;       /* 0: tuner's choice; else 256 or 512 */
+  int32_t one_shot;            /* 1: launch the kernels directly at execute instead of capturing a
+                                  graph (cheaper for a batch that runs once) */
+  int64_t tile_rows;           /* 0: tuner's choice; else rows per work item */
+} gbx_batch_options;
+
+typedef struct gbx_batch_output {
+  int32_t num_instances;
+  int32_t reserved;
+  const int64_t* group_offsets;        /* host memory, num_instances + 1 entries */
+  const int64_t* device_group_offsets; /* the same offsets in device memory */
+  gbx_result columns;                  /* concatenated keys and results (owned by the batch) */
+} gbx_batch_output;
+
+typedef struct gbx_batch_stats {
+  int32_t num_instances;
+  int32_t block_threads;       /* threads per CTA of the aggregation kernel */
+  int32_t grid;                /* persistent CTAs */
+  int32_t work_items;
+  int64_t num_rows;            /* all instances */
+  int64_t num_groups;          /* last execute */
+  int64_t dynamic_smem;        /* bytes per CTA */
+  int64_t arena_bytes;         /* global tables */
+  int64_t output_rows;         /* capacity of the concatenated outputs */
+  int32_t mode_count[4];       /* instances per gbx_batch_mode (index 0 unused) */
+  int32_t classes;             /* tuning classes present */
+  int32_t classes_measured;    /* measured by this create */
+  int32_t classes_cached;      /* read from the tuning file */
+  int32_t retries;             /* re-plans after a table overflow */
+  int32_t graph_nodes;
+  int32_t kernels_per_execute; /* kernel launches per execute */
+  float create_ms;             /* host wall time of gbx_batch_create */
+  float tune_ms;               /* of which measuring candidates */
+  float execute_ms;            /* CUDA-event time of the last execute's launch */
+  float init_ms;               /* of which: table fill (events recorded by the execution) */
+  float aggregate_ms;          /*   the persistent aggregation kernel */
+  float output_ms;             /*   counting, offsets and output writing */
+} gbx_batch_stats;
+
+GBX_API int gbx_batch_create(const gbx_batch_instance* instances,
+                             int32_t num_instances,
+                             int32_t num_requests,
+                             const gbx_batch_options* options,
+                             void* stream,
+                             const gbx_allocator* mr,
+                             gbx_batch** out);
+
+/* Runs the batch on `stream` and waits for it; *out stays valid until the
+ * next execute, rebind or destroy. */
+GBX_API int gbx_batch_execute(gbx_batch* batch, void* stream, const gbx_batch_output** out);
+
+/* Points the batch at new input buffers of the same schema and the same row
+ * count per instance (tables, tuning and graph are kept). */
+GBX_API int gbx_batch_rebind(gbx_batch* batch, const gbx_batch_instance* instances, int32_t num_instances);
+
+/* The tuner's choice for each instance (mode and table slots) and its
+ * estimated group count; arrays of num_instances entries, any may be NULL. */
+GBX_API int gbx_batch_instance_plan(const gbx_batch* batch, int32_t* modes, int64_t* table_slots,
+                                    int64_t* estimated_groups);
+
+GBX_API int gbx_batch_last_stats(const gbx_batch* batch, gbx_batch_stats* out);
+GBX_API void gbx_batch_destroy(gbx_batch* batch);
+
+/* ---- served groupby -------------------------------------------------------
+ * No counterpart in the reference (a libcudf service calls groupby::aggregate
+ * per request on its own threads and streams).
+ *
+ * A server accepts groupby requests over device-resident columns as they
+ * arrive and runs them with continuous batching: `workers` requests (or
+ * merged batches) are on the GPU at once, each on its own stream, so their
+ * kernels overlap; a request is admitted when a worker is free and the
+ * device memory it may need fits the HBM budget beside the requests already
+ * admitted (requests are considered in arrival order, and a later one that
+ * fits may go ahead of one that does not); small requests of one schema that
+ * are waiting together are merged into one batched launch (gbx_batch, one
+ * shot).  Every result is the same as gbx_groupby_aggregate on that request
+ * alone: same groups and dtypes, integer results bit-identical, floating
+ * results within the stated summation bound (the accumulation order of
+ * atomics is not fixed, as in the reference).
+ *
+ * gbx_server_submit copies the request's descriptors (the caller keeps the
+ * column buffers alive until the request completes) and returns at once;
+ * gbx_server_wait blocks until that request is done and hands over its
+ * result (released with gbx_result_release).  Times are taken on the host's
+ * steady clock, in seconds since the server was created. */
+typedef struct gbx_server gbx_server;
+
+typedef struct gbx_server_options {
+  int32_t workers;              /* requests on the GPU at once (streams); 0: 8 */
+  int32_t null_policy;          /* GBX_NULL_EXCLUDE / INCLUDE for every request */
+  int64_t hbm_budget_bytes;     /* device memory admitted requests may hold; 0: 150 GB */
+  int64_t batch_max_rows;       /* requests of at most this many rows may be merged (0: never) */
+  int32_t batch_max_requests;   /* at most this many requests per merged launch; 0: 64 */
+  int32_t reserved;
+} gbx_server_options;
+
+typedef struct gbx_server_timing {
+  double submitted_s;      /* gbx_server_submit */
+  double admitted_s;       /* given a worker and memory */
+  double done_s;           /* result ready on the host side */
+  int64_t reserved_bytes;  /* admission charge */
+  int32_t batched;         /* number of requests in its launch (1: alone) */
+  int32_t worker;
+} gbx_server_timing;
+
+typedef struct gbx_server_stats {
+  int64_t submitted;
+  int64_t completed;
+  int64_t failed;
+  int64_t batches;            /* merged launches */
+  int64_t batched_requests;   /* requests served inside merged launches */
+  int64_t peak_reserved_bytes;
+  int64_t rows;               /* rows of completed requests */
+  int32_t max_in_flight;
+  int32_t workers;
+  double busy_s;              /* time with at least one request on the GPU */
+} gbx_server_stats;
+
+GBX_API int gbx_server_create(const gbx_server_options* options, gbx_server** out);
+
+/* Queues a request: `keys` and `requests` as for gbx_groupby_create /
+ * gbx_groupby_aggregate.  Validation errors are returned here. */
+GBX_API int gbx_server_submit(gbx_server* server, const gbx_table_view* keys, const gbx_request* requests,
+                              int32_t num_requests, uint64_t* ticket);
+
+/* Waits up to timeout_s seconds (< 0: no limit) for the request; returns
+ * GBX_ERR_LOGIC with a message starting "timeout" if it is not done by then
+ * (the ticket stays valid).  On completion *out receives the result (or the
+ * request's error code is returned) and the ticket is retired. */
+GBX_API int gbx_server_wait(gbx_server* server, uint64_t ticket, double timeout_s, gbx_result** out,
+                            gbx_server_timing* timing);
+
+GBX_API double gbx_server_now(const gbx_server* server);
+GBX_API int gbx_server_last_stats(const gbx_server* server, gbx_server_stats* out);
+
+/* Finishes the admitted requests, fails the waiting ones, and frees the server. */
+GBX_API void gbx_server_destroy(gbx_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,7 +37,9 @@ def test_library_exports_every_declared_symbol():
 
 
 STRUCTS = ["gbx_column_view", "gbx_table_view", "gbx_aggregation", "gbx_request", "gbx_allocator",
-           "gbx_column", "gbx_aggregation_result", "gbx_result", "gbx_stats"]
+           "gbx_column", "gbx_aggregation_result", "gbx_result", "gbx_stats", "gbx_batch_instance",
+           "gbx_batch_options", "gbx_batch_output", "gbx_batch_stats", "gbx_server_options", "gbx_server_timing",
+           "gbx_server_stats"]
 
 
 def test_ctypes_layout_matches_c_header(tmp_path):
@@ -152,3 +154,62 @@ def test_can_use_hash_groupby_for_hash_kinds():
     for k in (Kind.SUM, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.MEAN, Kind.VARIANCE, Kind.STD):
         r, keep = _request(3, k)
         assert lib.gbx_can_use_hash_groupby(C.byref(r), 1) == 1
+
+
+# ---- batched form: schema checks run on the host before any CUDA call
+
+def _batch_instance(n, key_type=TypeId.INT32, kind=Kind.SUM, value_type=TypeId.INT32):
+    tv, keep = _keys_view(n)
+    keep[1][0].type_id = key_type
+    r, aggs = _request(n, kind)
+    r.values.type_id = value_type
+    reqs = (_abi.gbx_request * 1)(r)
+    inst = _abi.gbx_batch_instance(tv, C.cast(reqs, C.POINTER(_abi.gbx_request)))
+    return inst, (tv, keep, r, aggs, reqs)
+
+
+def _create_batch(insts, nreq=1, opts=None):
+    arr = (_abi.gbx_batch_instance * max(1, len(insts)))(*insts)
+    h = C.c_void_p()
+    o = opts if opts is not None else _abi.gbx_batch_options()
+    st = _lib.lib().gbx_batch_create(arr, len(insts), nreq, C.byref(o), None, None, C.byref(h))
+    return st, _lib.lib().gbx_last_error()
+
+
+def test_batch_needs_instances_of_one_schema():
+    a, ka = _batch_instance(4)
+    b, kb = _batch_instance(9, key_type=TypeId.INT64)
+    st, msg = _create_batch([a, b])
+    assert st == _abi.Status.ERR_LOGIC and b"key column 0 differs" in msg
+    c, kc = _batch_instance(9, kind=Kind.MAX)
+    st, msg = _create_batch([a, c])
+    assert st == _abi.Status.ERR_LOGIC and b"differs in aggregations" in msg
+    d, kd = _batch_instance(9, value_type=TypeId.INT64)
+    st, msg = _create_batch([a, d])
+    assert st == _abi.Status.ERR_LOGIC and b"values differ in type" in msg
+
+
+def test_batch_rejects_bad_arguments():
+    a, ka = _batch_instance(4)
+    st, _ = _create_batch([])
+    assert st == _abi.Status.ERR_LOGIC
+    st, _ = _create_batch([a], opts=_abi.gbx_batch_options(block_threads=300))
+    assert st == _abi.Status.ERR_LOGIC
+    st, _ = _create_batch([a], opts=_abi.gbx_batch_options(null_policy=5))
+    assert st == _abi.Status.ERR_LOGIC
+    st, _ = _create_batch([a], opts=_abi.gbx_batch_options(force_mode=9))
+    assert st == _abi.Status.ERR_LOGIC
+    # a request whose values are shorter than the keys (groupby.cu:210-214)
+    b, kb = _batch_instance(4)
+    kb[4][0].values.size = 3
+    st, msg = _create_batch([a, b])
+    assert st == _abi.Status.ERR_LOGIC and b"Size mismatch" in msg
+
+
+def test_batch_rejects_dictionary_keys_and_sort_kinds():
+    a, ka = _batch_instance(4, key_type=TypeId.DICTIONARY32)
+    st, _ = _create_batch([a])
+    assert st == _abi.Status.ERR_UNSUPPORTED
+    b, kb = _batch_instance(4, kind=Kind.MEDIAN)
+    st, _ = _create_batch([b])
+    assert st == _abi.Status.ERR_UNSUPPORTED
