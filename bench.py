@@ -57,6 +57,16 @@ def parse_args(argv=None):
                    help="force one aggregation strategy (default: chosen per call)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--sections", type=str, default="plain,batched,served",
+                   help="comma list of: plain (the headline line), batched (4,096-instance batch), "
+                        "served (Poisson request stream)")
+    p.add_argument("--batch-instances", type=int, default=4096)
+    p.add_argument("--batch-tune", choices=["off", "cached", "missing", "all"], default="missing")
+    p.add_argument("--batch-tune-save", type=str, default=None,
+                   help="write the tuning table the batch used (and extended) to this path")
+    p.add_argument("--served-requests", type=int, default=200)
+    p.add_argument("--served-workers", type=int, default=8)
+    p.add_argument("--served-batch-rows", type=int, default=1_000_000)
     return p.parse_args(argv)
 
 
@@ -298,6 +308,22 @@ def run_ours(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, cards)
 
+    # release the plain workload before the batched and served ones
+    del gbs, reqs, data
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    sections = args.sections.split(",")
+    batched = None
+    if "batched" in sections:
+        batched = run_batched(args, rank, world, device, stream, alloc)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    served = None
+    if "served" in sections:
+        served = run_served(args, rank, device, stream)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
     out = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -314,6 +340,8 @@ def run_ours(args, rank, world, local):
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
+        "batched": batched,
+        "served": served,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -394,6 +422,362 @@ def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
     rows = args.rows * len(cards) * steps * world
     return {"value": rows / (ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h_bytes[0],
             "steps": steps, "ms_per_step": ms / steps}
+
+
+# ------------------------------------------------------------- batched form
+
+BATCH_BYTES_PER_ROW = 4 + 8            # int32 key + int64 value
+BATCH_BYTES_PER_GROUP = 4 + 8 + 4 + 8  # key, SUM (int64), COUNT (int32), MAX (int64)
+TUNE_TABLE = os.path.join(ROOT, "cudf_b200", "tuning", "batch_tune.txt")
+
+
+def _segmented_inputs(spec, device, seed, key_dtype, value_kind):
+    """Every instance's columns in two device buffers (instance i at rows
+    [start_i, start_i + rows_i)): key uniform in [0, C_i); value int64
+    uniform in [0, 1e9] ("int") or float64 N(0, 1) ("normal")."""
+    import numpy as np
+    import torch
+
+    rows = torch.from_numpy(spec.rows).to(device)
+    total = int(spec.rows.sum())
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    cards = torch.repeat_interleave(torch.from_numpy(spec.cards.astype(np.float64)).to(device), rows)
+    k = (torch.rand(total, generator=g, device=device, dtype=torch.float64) * cards).floor_().to(key_dtype)
+    del cards
+    if value_kind == "int":
+        v = torch.randint(0, 1_000_000_001, (total,), generator=g, device=device, dtype=torch.int64)
+    else:
+        v = torch.randn(total, generator=g, device=device, dtype=torch.float64)
+    starts = np.concatenate([[0], np.cumsum(spec.rows)[:-1]]).astype(np.int64)
+    return k, v, starts
+
+
+def _percentiles(xs):
+    import numpy as np
+
+    a = np.asarray(xs, dtype=np.float64)
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "max": float(a.max())}
+
+
+def run_batched(args, rank, world, device, stream, alloc):
+    """4,096 independent groupbys (rows log-uniform in [1e3, 1e6], cardinality
+    log-uniform in [10, 1e4], int32 key, int64 value, SUM/COUNT/MAX) as one
+    graph launch, against a loop of the plain form over the same instances."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    from cudf_b200 import BatchGroupBy, BatchInstance, Column, GroupBy, GroupByRequest, Table, Tune, TypeId
+    from cudf_b200 import aggregation as agg
+    from cudf_b200 import workloads as W
+    from cudf_b200.column import storage_dtype
+
+    spec = W.batched_spec(args.batch_instances)
+    k, v, starts = _segmented_inputs(spec, device, 20241003 + 4 + rank, torch.int32, "int")
+    total = spec.total_rows
+    insts = []
+    for i in range(spec.num_instances):
+        n, s = int(spec.rows[i]), int(starts[i])
+        insts.append(BatchInstance(Table([Column(TypeId.INT32, n, k, None, s)]),
+                                   [GroupByRequest(Column(TypeId.INT64, n, v, None, s),
+                                                   [agg.sum(), agg.count(), agg.max()])]))
+    tune = {"off": Tune.OFF, "cached": Tune.CACHED, "missing": Tune.MISSING, "all": Tune.ALL}[args.batch_tune]
+    tune_copy = None
+    if tune != Tune.OFF:
+        fd, tune_copy = tempfile.mkstemp(suffix=".txt")
+        os.close(fd)
+        if os.path.exists(TUNE_TABLE):
+            shutil.copyfile(TUNE_TABLE, tune_copy)
+    t0 = time.perf_counter()
+    b = BatchGroupBy(insts, tune=tune, tune_file=tune_copy, stream=stream, allocator=alloc)
+    create_s = time.perf_counter() - t0
+    st0 = b.stats()
+    if args.batch_tune_save and tune_copy:
+        shutil.copyfile(tune_copy, args.batch_tune_save)
+
+    for _ in range(args.warmup):
+        b.execute(stream)
+    torch.cuda.synchronize()
+    lat_ms, agg_ms = [], []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = max(args.steps, 5)
+    with ClockSampler(device.index) as clk:
+        e0.record(stream)
+        for _ in range(steps):
+            res = b.execute(stream)
+            s = b.stats()
+            lat_ms.append(s["execute_ms"])
+            agg_ms.append(s["aggregate_ms"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    stats = b.stats()
+    groups = res.num_groups
+    peaks = _load_peaks()
+    agg_avg = sum(agg_ms) / len(agg_ms)
+    achieved = total * BATCH_BYTES_PER_ROW / (agg_avg / 1e3) / 1e9
+    batch_rows_s = total / (ms / 1e3)
+
+    # e2e: host (pinned) inputs copied in place each step, results read back
+    hk = k.cpu().pin_memory()
+    hv = v.cpu().pin_memory()
+    out_host = torch.empty(int(groups * BATCH_BYTES_PER_GROUP * 1.05) + (1 << 20), dtype=torch.uint8,
+                           pin_memory=True)
+
+    def e2e_step():
+        k.copy_(hk, non_blocking=True)
+        v.copy_(hv, non_blocking=True)
+        r = b.execute(stream)
+        off = 0
+        for col in list(r.keys.columns()) + [c for t in r.results for c in t.columns()]:
+            nb = col.size * storage_dtype(col.type_id).itemsize
+            out_host[off:off + nb].copy_(col.data.view(torch.uint8)[:nb], non_blocking=True)
+            off += nb
+        stream.synchronize()
+        return off
+
+    e2e_step()
+    e2e_steps = 3
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        d2h = e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    h2d = hk.numel() * hk.element_size() + hv.numel() * hv.element_size()
+    del hk, hv
+
+    # the plain form, one aggregate() per instance, on the same GPU
+    gbs = [GroupBy(x.keys) for x in insts]
+
+    def loop_pass(record):
+        t_start = time.perf_counter()
+        for gb, x in zip(gbs, insts):
+            kt, rs = gb.aggregate(x.requests, stream=stream, allocator=alloc)
+            if record is not None:
+                record.append((time.perf_counter() - t_start) * 1e3)
+            del kt, rs
+        return (time.perf_counter() - t_start) * 1e3
+
+    loop_pass(None)
+    torch.cuda.synchronize()
+    done_ms = []
+    loop_ms = loop_pass(done_ms)
+    loop_rows_s = total / (loop_ms / 1e3)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = _batched_cpu(spec)
+    b.close()
+    if tune_copy:
+        os.unlink(tune_copy)
+    return {
+        "metric": "batched groupby rows/s (4,096 instances, one graph launch)",
+        "config": {"instances": spec.num_instances, "total_rows": total, "rows": "log-uniform [1e3, 1e6]",
+                   "cardinality": "log-uniform [10, 1e4]", "key": "int32", "value": "int64 U[0, 1e9]",
+                   "aggregations": ["SUM", "COUNT", "MAX"], "tune": args.batch_tune,
+                   "l2": "inputs (%.1f GB) larger than L2; no flush" % (total * BATCH_BYTES_PER_ROW / 1e9)},
+        "value": batch_rows_s, "unit": "rows/s", "ms_per_step": ms, "steps": steps, "groups": groups,
+        "latency_ms": {"batched": {"p50": float(_percentiles(lat_ms)["p50"]), "p99": _percentiles(lat_ms)["p99"],
+                                   "note": "every instance completes when the launch does"},
+                       "plain_loop": dict(_percentiles(done_ms),
+                                          note="completion time of instance i when all arrive at once")},
+        "plain_loop": {"value": loop_rows_s, "unit": "rows/s", "ms_per_pass": loop_ms, "calls": spec.num_instances},
+        "speedup_vs_plain_loop": batch_rows_s / loop_rows_s,
+        "phases_ms": {"init": stats["init_ms"], "aggregate": agg_avg, "output": stats["output_ms"],
+                      "launch": stats["execute_ms"]},
+        "roofline": {"bound": "hbm", "kernel": "k_batch_agg", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_launch": total * BATCH_BYTES_PER_ROW},
+        "e2e": {"value": total / (e2e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "tuner": {"create_s": create_s, "tune_ms": st0["tune_ms"], "classes": st0["classes"],
+                  "classes_measured": st0["classes_measured"], "classes_cached": st0["classes_cached"],
+                  "block_threads": stats["block_threads"], "grid": stats["grid"],
+                  "mode_count": {"shared": stats["mode_count"][1], "warp": stats["mode_count"][2],
+                                 "global": stats["mode_count"][3]},
+                  "work_items": stats["work_items"], "dynamic_smem": stats["dynamic_smem"]},
+        "gpu_launches": stats["kernels_per_execute"] * steps,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+
+
+def _batched_cpu(spec, sample_instances=48):
+    """Oracle (single thread) and pandas on the first instances of the batch."""
+    from cudf_b200 import workloads as W
+    from cudf_b200._abi import Kind
+    from oracle import oracle as orc
+    from oracle.oracle import HostCol
+
+    data = [W.batched_instance(spec, i) for i in range(min(sample_instances, spec.num_instances))]
+    rows = sum(len(kk) for kk, _ in data)
+    t0 = time.perf_counter()
+    for kk, vv in data:
+        orc.groupby([HostCol(kk)], [(HostCol(vv), [(Kind.SUM, 0), (Kind.COUNT_VALID, 0), (Kind.MAX, 0)])], 0,
+                    threads=1)
+    out = {"value": rows / (time.perf_counter() - t0), "unit": "rows/s", "cores": 1, "kind": "port",
+           "sample": f"the first {len(data)} instances ({rows} rows)"}
+    try:
+        import pandas as pd
+
+        frames = [pd.DataFrame({"k": kk, "v": vv}) for kk, vv in data]
+        t0 = time.perf_counter()
+        for df in frames:
+            df.groupby("k", sort=False).agg({"v": ["sum", "count", "max"]})
+        out["pandas_rows_per_s"] = rows / (time.perf_counter() - t0)
+    except Exception as e:  # pragma: no cover
+        out["pandas_error"] = str(e)
+    out["host_cpu_count"] = os.cpu_count()
+    return out
+
+
+# -------------------------------------------------------------- served form
+
+def _serve_run(lib, srv, prepared, arrivals):
+    """Submits request i at arrivals[i] (seconds from the run's start) from one
+    thread, waits for every result in another; returns per-request latency in
+    ms (done - scheduled arrival), the run's span in s and merged requests."""
+    import ctypes as C
+    import threading
+
+    from cudf_b200 import _abi
+
+    n = len(prepared)
+    tickets = [0] * n
+    done = [0.0] * n
+    batched = [1] * n
+    ready = [threading.Event() for _ in range(n)]
+    errors = []
+    start = lib.gbx_server_now(srv) + 0.002
+
+    def submitter():
+        for i, (tv, reqs, nreq, _) in enumerate(prepared):
+            t_arr = start + arrivals[i]
+            while True:
+                d = t_arr - lib.gbx_server_now(srv)
+                if d <= 0:
+                    break
+                time.sleep(d if d > 0.002 else 0)
+            t = C.c_uint64()
+            if lib.gbx_server_submit(srv, C.byref(tv), reqs, nreq, C.byref(t)) != 0:
+                errors.append(lib.gbx_last_error())
+            tickets[i] = t.value
+            ready[i].set()
+
+    def waiter():
+        for i in range(n):
+            ready[i].wait()
+            if not tickets[i]:
+                continue
+            out = C.POINTER(_abi.gbx_result)()
+            tm = _abi.gbx_server_timing()
+            if lib.gbx_server_wait(srv, tickets[i], -1.0, C.byref(out), C.byref(tm)) != 0:
+                errors.append(lib.gbx_last_error())
+                continue
+            done[i] = tm.done_s
+            batched[i] = tm.batched
+            lib.gbx_result_release(out)
+
+    ts = [threading.Thread(target=submitter), threading.Thread(target=waiter)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if errors:
+        raise RuntimeError(f"served run failed: {errors[0]}")
+    lat = [(done[i] - (start + arrivals[i])) * 1e3 for i in range(n)]
+    return lat, max(done) - start, sum(1 for b in batched if b > 1)
+
+
+def run_served(args, rank, device, stream):
+    """A Poisson stream of groupby requests (rows log-uniform in [1e4, 5e7],
+    cardinality log-uniform in [1e2, 1e7], int64 key, float64 N(0,1) value,
+    SUM/COUNT/MEAN) over device-resident columns, at 0.5x, 0.9x and 1.2x of
+    the plain loop's capacity: the served form (continuous batching, HBM
+    admission) against a per-request loop of the plain form (one worker, no
+    merging) on the same arrivals."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from cudf_b200 import Column, GroupByRequest, Table, TypeId, _abi, _lib
+    from cudf_b200 import aggregation as agg
+    from cudf_b200 import workloads as W
+    from cudf_b200.server import request_array
+
+    spec = W.batched_spec(args.served_requests, rows_range=(1e4, 5e7), card_range=(1e2, 1e7), seed=20241003 + 5)
+    k, v, starts = _segmented_inputs(spec, device, 20241003 + 5 + rank, torch.int64, "normal")
+    torch.cuda.synchronize()
+    lib = _lib.lib()
+    prepared = []
+    for i in range(spec.num_instances):
+        n, s = int(spec.rows[i]), int(starts[i])
+        kt = Table([Column(TypeId.INT64, n, k, None, s)])
+        rq = [GroupByRequest(Column(TypeId.FLOAT64, n, v, None, s), [agg.sum(), agg.count(), agg.mean()])]
+        tv, cols = kt.view()
+        reqs, keep = request_array(rq)
+        prepared.append((tv, reqs, len(rq), (kt, rq, cols, keep)))
+    total_rows = spec.total_rows
+
+    def server(workers, batch_rows):
+        opts = _abi.gbx_server_options(workers=workers, null_policy=0, hbm_budget_bytes=150 << 30,
+                                       batch_max_rows=batch_rows, batch_max_requests=64)
+        h = C.c_void_p()
+        _lib.check(lib.gbx_server_create(C.byref(opts), C.byref(h)))
+        return h
+
+    served_cfg = (args.served_workers, args.served_batch_rows)
+    loop_cfg = (1, 0)
+    warm = min(20, len(prepared))
+    for cfg in (served_cfg, loop_cfg):  # pools, modules, first-touch
+        h = server(*cfg)
+        _serve_run(lib, h, prepared[:warm], [0.0] * warm)
+        lib.gbx_server_destroy(h)
+    # the plain loop's capacity: every request queued at t = 0
+    h = server(*loop_cfg)
+    _, span0, _ = _serve_run(lib, h, prepared, [0.0] * len(prepared))
+    lib.gbx_server_destroy(h)
+    capacity_rps = len(prepared) / span0
+    rng = np.random.default_rng(20241003 + 5)
+    gaps = rng.exponential(1.0, len(prepared))
+    rates = {}
+    with ClockSampler(device.index) as clk:
+        for mult in (0.5, 0.9, 1.2):
+            lam = mult * capacity_rps
+            arrivals = np.cumsum(gaps / lam) - gaps[0] / lam
+            res = {"arrival_rate_per_s": lam}
+            for name, cfg in (("served", served_cfg), ("plain_loop", loop_cfg)):
+                h = server(*cfg)
+                lat, span, merged = _serve_run(lib, h, prepared, arrivals)
+                st = _abi.gbx_server_stats()
+                lib.gbx_server_last_stats(h, C.byref(st))
+                lib.gbx_server_destroy(h)
+                p = _percentiles(lat)
+                res[name] = {"p50_ms": p["p50"], "p99_ms": p["p99"], "rows_per_s": total_rows / span,
+                             "max_in_flight": st.max_in_flight, "merged_requests": merged,
+                             "batched_launches": st.batches, "peak_reserved_gb": st.peak_reserved_bytes / 1e9}
+            res["p99_speedup"] = res["plain_loop"]["p99_ms"] / res["served"]["p99_ms"]
+            res["rows_per_s_speedup"] = res["served"]["rows_per_s"] / res["plain_loop"]["rows_per_s"]
+            rates[f"{mult}x"] = res
+    del prepared
+    return {
+        "metric": "served groupby p50/p99 latency and rows/s at 3 Poisson arrival rates",
+        "config": {"requests": spec.num_instances, "total_rows": total_rows, "rows": "log-uniform [1e4, 5e7]",
+                   "cardinality": "log-uniform [1e2, 1e7]", "key": "int64", "value": "float64 N(0,1)",
+                   "aggregations": ["SUM", "COUNT", "MEAN"], "hbm_budget_gb": 150,
+                   "served": {"workers": served_cfg[0], "merge_rows_max": served_cfg[1]},
+                   "plain_loop": "one worker, one request at a time, arrival order",
+                   "rates": "0.5x, 0.9x, 1.2x of the plain loop's capacity (requests/s with all queued at t=0)"},
+        "plain_loop_capacity_requests_per_s": capacity_rps,
+        "plain_loop_capacity_rows_per_s": total_rows / span0,
+        "rates": rates,
+        "clocks": clk.summary(),
+    }
 
 
 # ----------------------------------------------------------- CPU baselines
