@@ -733,10 +733,11 @@ def run_served(args, rank, device, stream):
 
     served_cfg = (args.served_workers, args.served_batch_rows)
     loop_cfg = (1, 0)
-    warm = min(20, len(prepared))
-    for cfg in (served_cfg, loop_cfg):  # pools, modules, first-touch
+    # warm-up: every request once per configuration, so that the stream-ordered
+    # pool has grown to what concurrent requests hold and modules are loaded
+    for cfg in (served_cfg, loop_cfg):
         h = server(*cfg)
-        _serve_run(lib, h, prepared[:warm], [0.0] * warm)
+        _serve_run(lib, h, prepared, [0.0] * len(prepared))
         lib.gbx_server_destroy(h)
     # the plain loop's capacity: every request queued at t = 0
     h = server(*loop_cfg)
