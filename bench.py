@@ -42,6 +42,10 @@ BYTES_PER_ROW_IN = 8 + 8 + 4 + 1.0 / 8  # key + a + b + b's validity bit
 # b: sum 4, count 4, min 4, max 4, mean 8, var 8; validity bits
 BYTES_PER_GROUP_OUT = 8 + (8 + 4 + 8 + 8 + 8 + 8) + (4 + 4 + 4 + 4 + 8 + 8) + 6.0 / 8
 METRIC = "groupby rows/s (plain hash groupby, 100M rows, int64 key, cardinality 1e2/1e4/1e6/1e8)"
+PARTITIONED = 3  # gbx_strategy of the radix-partitioned path
+# DRAM bytes per row of one k_part_agg launch measured by ncu (20M rows,
+# cardinality 2e7: 0.436 GB read + 1.017 GB written)
+K_PART_AGG_DRAM_BYTES_PER_ROW = (0.435927e9 + 1.016502e9) / 20_000_000
 
 
 def parse_args(argv=None):
@@ -262,8 +266,12 @@ def run_ours(args, rank, world, local):
 
     peaks = _load_peaks()
     per = {}
+    # the dominant kernel is k_part_agg (the partitioned strategy's aggregation
+    # pass, which also writes the outputs): its algorithmic bytes per launch
+    # are the rows read and the groups written
     agg_ms_total = 0.0
     agg_bytes_total = 0.0
+    agg_launches = 0
     launches = 0
     for c, st, g in rec:
         d = per.setdefault(c, {"calls": 0, "total_ms": 0.0, "aggregate_ms": 0.0, "groups": g,
@@ -273,8 +281,10 @@ def run_ours(args, rank, world, local):
         d["aggregate_ms"] += st["aggregate_ms"]
         for ph in ("sample_ms", "init_ms", "aggregate_ms", "compact_ms", "finalize_ms"):
             d["phases_ms"][ph] = d["phases_ms"].get(ph, 0.0) + st[ph]
-        agg_ms_total += st["aggregate_ms"]
-        agg_bytes_total += n * BYTES_PER_ROW_IN
+        if st["strategy"] == PARTITIONED:
+            agg_ms_total += st["aggregate_ms"]
+            agg_bytes_total += n * BYTES_PER_ROW_IN + g * BYTES_PER_GROUP_OUT
+            agg_launches += 1
         launches += st["kernel_launches"]
     per_out = {}
     for c, d in per.items():
@@ -290,14 +300,19 @@ def run_ours(args, rank, world, local):
             "phases_ms": {k: round(v / calls, 4) for k, v in d["phases_ms"].items()},
         }
     achieved = (agg_bytes_total / (agg_ms_total / 1e3)) / 1e9 if agg_ms_total > 0 else None
-    traffic = _load_traffic()
     roofline = {
-        "bound": "hbm", "kernel": "aggregation pass (k_agg_*)",
+        "bound": "hbm", "kernel": "k_part_agg (cardinality 1e4 / 1e6 / 1e8 launches)",
         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
         "peak_source": peaks["source"],
-        "traffic": traffic,
-        "algorithmic_bytes_per_launch": n * BYTES_PER_ROW_IN,
+        "algorithmic_bytes_per_launch": agg_bytes_total / agg_launches if agg_launches else None,
+        "launches_per_step": agg_launches // max(1, args.steps),
+        # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_part_agg
+        # launch on 20M rows of cardinality 2e7 (1.452 GB), scaled by rows to
+        # the 100M-row cardinality-1e8 launch; that launch's algorithmic bytes
+        # are 100M x 20.125 + 63.2M x 85 = 7.39 GB
+        "traffic": K_PART_AGG_DRAM_BYTES_PER_ROW * n,
+        "traffic_launch": "cardinality 1e8",
     }
 
     e2e = None
@@ -880,16 +895,6 @@ def _load_peaks():
         return {"hbm_gbs": float(p["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
     except (OSError, KeyError, ValueError):
         return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
-
-
-def _load_traffic():
-    """DRAM bytes per aggregation launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
-    try:
-        with open(path) as f:
-            return json.load(f).get("aggregate_dram_bytes_per_launch")
-    except (OSError, ValueError):
-        return None
 
 
 def main(argv=None):
