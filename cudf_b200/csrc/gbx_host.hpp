@@ -126,6 +126,7 @@ struct DeviceInfo {
   int device        = -1;
   int num_sms       = 0;
   size_t smem_optin = 0;
+  size_t l2_bytes   = 0;
 };
 
 DeviceInfo current_device();
