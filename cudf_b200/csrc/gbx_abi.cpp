@@ -898,20 +898,32 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       const SmemLayout sl = make_smem_layout(plan, S);
       if (static_cast<size_t>(sl.total) * 8 + 8 * (S + 32) * 4 > call.dev.smem_optin)
         fail(GBX_ERR_UNSUPPORTED, "per-group state too large for the partitioned path");
-      PartBufs pbufs{};
-      for (int w = 0; w < plan.key.nwords; ++w)
-        pbufs.keys[w] = static_cast<const uint64_t*>(scratch.get(static_cast<size_t>(call.n) * 8));
-      for (int c = 0; c < plan.nchan; ++c) {
-        const int8_t pt = plan.chan[c].ptype;
-        const int width = (pt == P_I8 || pt == P_U8 || pt == P_BOOL) ? 1
-                          : (pt == P_I16 || pt == P_U16)             ? 2
-                          : (pt == P_I32 || pt == P_U32 || pt == P_F32) ? 4
-                                                                        : 8;
-        pbufs.col[c].width = width;
-        pbufs.col[c].vals  = scratch.get(static_cast<size_t>(call.n) * width);
-        pbufs.col[c].valid =
-          plan.chan[c].mask ? static_cast<const uint8_t*>(scratch.get(static_cast<size_t>(call.n))) : nullptr;
-      }
+      // bucket-ordered copies of the rows: packed key words, resolved value
+      // bits, a validity byte per row of a nullable channel
+      auto part_bufs = [&]() {
+        PartBufs pb{};
+        for (int w = 0; w < plan.key.nwords; ++w)
+          pb.keys[w] = static_cast<const uint64_t*>(scratch.get(static_cast<size_t>(call.n) * 8));
+        for (int c = 0; c < plan.nchan; ++c) {
+          const int8_t pt = plan.chan[c].ptype;
+          const int width = (pt == P_I8 || pt == P_U8 || pt == P_BOOL) ? 1
+                            : (pt == P_I16 || pt == P_U16)             ? 2
+                            : (pt == P_I32 || pt == P_U32 || pt == P_F32) ? 4
+                                                                          : 8;
+          pb.col[c].width = width;
+          pb.col[c].vals  = scratch.get(static_cast<size_t>(call.n) * width);
+          pb.col[c].valid =
+            plan.chan[c].a_cnt >= 0 ? static_cast<const uint8_t*>(scratch.get(static_cast<size_t>(call.n))) : nullptr;
+        }
+        return pb;
+      };
+      PartBufs pbufs = part_bufs();
+      // the radix passes' second set of copies and their counters
+      PartBufs tbufs{};
+      uint32_t* rcounts  = nullptr;
+      uint32_t* roffsets = nullptr;
+      void* rtemp        = nullptr;
+      size_t rtemp_bytes = 0;
       // outputs sized for the upper bound (every row its own group): the group
       // count is only known once the buckets have been written out
       OutPlan pop    = build_outputs(call.n);
@@ -966,7 +978,21 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         t2.special_used = reinterpret_cast<uint32_t*>(ctl + 28);
         t2.status       = d_status;
         GBX_CUDA(launch_init_table(t2, plan.acc, plan.key.nwords, call.dev.num_sms, s));
-        GBX_CUDA(launch_part_scatter(plan, call.n, pp, pbufs, call.dev.num_sms, s));
+        if (pp.shard_bits == 0 && bits >= 9) {
+          // many buckets: coalesced radix passes (gbx_radix.cu)
+          if (rcounts == nullptr) {
+            tbufs    = part_bufs();
+            rcounts  = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
+            roffsets = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
+            GBX_CUDA(part_radix_temp_bytes(call.n, &rtemp_bytes));
+            rtemp = scratch.get(rtemp_bytes);
+          }
+          GBX_CUDA(launch_part_radix(plan, call.n, bits, pp.offsets + P, pbufs, tbufs, rcounts, roffsets, rtemp,
+                                     rtemp_bytes, d_status, s));
+          launches += 3 * ((bits + 7) / 8) - 1;
+        } else {
+          GBX_CUDA(launch_part_scatter(plan, call.n, pp, pbufs, call.dev.num_sms, s));
+        }
         timer.mark(2);
         GBX_CUDA(launch_part_agg(plan, pp, pbufs, t2, sl, pop, call.dev.num_sms, s));
         timer.mark(3);

@@ -87,6 +87,17 @@ cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_byte
 cudaError_t launch_part_items(const PartPlan& pp, int64_t n, int num_sms, cudaStream_t st);
 cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, const PartBufs& out, int num_sms,
                                 cudaStream_t st);
+// Radix partitioning into bucket order (gbx_radix.cu): the same result as
+// launch_part_scatter for 2^bits buckets with unsharded counters, in
+// ceil(bits / 8) coalesced passes that alternate between `dst` and `tmp`
+// (same layout) and end in `dst`.  *n_active (device) is the number of rows
+// kept (the bucket histogram's total); `counts` and `offsets` hold
+// part_radix_count_bytes(n) bytes each, `temp` part_radix_temp_bytes(n).
+size_t part_radix_count_bytes(int64_t n);
+cudaError_t part_radix_temp_bytes(int64_t n, size_t* temp_bytes);
+cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
+                              const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
+                              size_t temp_bytes, int32_t* status, cudaStream_t st);
 // Aggregates every bucket: single-item buckets write their groups to `op`
 // directly; multi-item buckets merge into region tables of `t` (t.cap =
 // regions * region_slots) that launch_part_region_finalize then writes out.

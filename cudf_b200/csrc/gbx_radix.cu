@@ -1,0 +1,378 @@
+// gbx_radix.cu -- coalesced radix partitioning of the rows into hash buckets
+// (the partitioned path's scatter for many buckets).
+//
+// A one-pass scatter into 2^bits buckets sends each warp's 32 rows to 32
+// far-apart places once bits is large, so every 32-byte sector it writes is
+// partial and is filled from DRAM before the write lands (3.3x the
+// algorithmic traffic measured with ncu at 2^18 buckets), and every row waits
+// for a global cursor atomic.  Here the bucket id is instead split into
+// digits of at most 8 bits and the rows are moved once per digit, least
+// significant digit first, by a stable counting sort: per 4,096-row tile a
+// histogram of the digit, one exclusive scan over (digit, tile), and a
+// scatter in which each row's position is its tile's offset for the digit
+// plus its rank among the tile's rows of that digit.  A tile's rows of one
+// digit land next to each other, so sectors are written whole while they sit
+// in L2, and no global atomics are used.  After the last pass the rows are in
+// bucket order, stable within a bucket, exactly where the bucket offsets of
+// the histogram (k_part_hist) place them.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+
+#include "gbx_warpcore.cuh"
+
+namespace gbx {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kRadixBlock  = 256;
+constexpr int kRadixWarps  = kRadixBlock / 32;
+constexpr int kRowsPerWarp = 512;  // 16 batches of 32
+constexpr int kTileRows    = kRadixWarps * kRowsPerWarp;
+constexpr int kMaxRadix    = 256;
+constexpr int kLoadGroup   = 4;  // 32-row batches whose loads a warp has in flight together
+
+struct Digit {
+  int bits;   // bucket id = top `bits` bits of the key hash
+  int shift;  // this pass's digit = (bucket >> shift) & (radix - 1)
+  int width;  // digit bits (<= 8)
+};
+
+template <int NW>
+__device__ __forceinline__ uint32_t digit_of(const uint64_t (&k)[NW], const Digit& dg)
+{
+  const uint64_t h = hash_key<NW>(k);
+  const uint32_t b = dg.bits == 0 ? 0u : static_cast<uint32_t>(h >> (64 - dg.bits));
+  return (b >> dg.shift) & ((1u << dg.width) - 1u);
+}
+
+// Row r of the pass's source: the caller's columns (first pass: rows with a
+// null key under EXCLUDE are dropped, values resolved) or the previous pass's
+// bucket copies.
+template <int NW, bool FROM_COLUMNS>
+struct PassSource {
+  const Plan* plan;
+  const PartBufs* in;
+  __device__ __forceinline__ bool key(int64_t r, uint64_t (&k)[NW]) const
+  {
+    if constexpr (FROM_COLUMNS) {
+      return pack_key<NW>(plan->key, r, k);
+    } else {
+#pragma unroll
+      for (int w = 0; w < NW; ++w) k[w] = __ldg(in->keys[w] + r);
+      return true;
+    }
+  }
+  __device__ __forceinline__ bool value(int c, int64_t r, uint64_t& b, int32_t* status) const
+  {
+    if constexpr (FROM_COLUMNS) {
+      return RowSource{plan}.value(c, r, b, status);
+    } else {
+      const PartCol& pc = in->col[c];
+      b                 = load_bits(pc.vals, r, pc.width);
+      return pc.valid == nullptr || __ldg(pc.valid + r) != 0;
+    }
+  }
+};
+
+__device__ __forceinline__ int64_t source_rows(int64_t n, const uint32_t* n_active, bool from_columns)
+{
+  return from_columns ? n : static_cast<int64_t>(*n_active);
+}
+
+// counts[d * ntiles + t] = rows of tile t whose digit is d.
+template <int NW, bool FROM_COLUMNS>
+__global__ void __launch_bounds__(kRadixBlock) k_radix_hist(const __grid_constant__ Plan plan,
+                                                            const __grid_constant__ PartBufs in, int64_t n,
+                                                            const uint32_t* n_active, const Digit dg, int ntiles,
+                                                            uint32_t* counts)
+{
+  __shared__ uint32_t hist[kMaxRadix];
+  const int radix = 1 << dg.width;
+  for (int i = threadIdx.x; i < radix; i += kRadixBlock) hist[i] = 0;
+  __syncthreads();
+  const PassSource<NW, FROM_COLUMNS> src{&plan, &in};
+  const int64_t rows = source_rows(n, n_active, FROM_COLUMNS);
+  const int lane     = threadIdx.x & 31;
+  const int warp     = threadIdx.x >> 5;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kTileRows + warp * kRowsPerWarp;
+  for (int j0 = 0; j0 < kRowsPerWarp / 32; j0 += kLoadGroup) {
+    // the group's loads are issued before any of them is used
+    uint64_t k[kLoadGroup][NW];
+    bool act[kLoadGroup];
+#pragma unroll
+    for (int u = 0; u < kLoadGroup; ++u) {
+      const int64_t r = base + (j0 + u) * 32 + lane;
+      act[u]          = r < rows && src.key(r, k[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadGroup; ++u) {
+      const uint32_t d  = act[u] ? digit_of<NW>(k[u], dg) : 0xffffffffu;
+      const uint32_t pe = __match_any_sync(kFull, d);
+      if (act[u] && lane == __ffs(pe) - 1) atomicAdd(&hist[d], static_cast<uint32_t>(__popc(pe)));
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < radix; i += kRadixBlock)
+    counts[static_cast<size_t>(i) * ntiles + blockIdx.x] = hist[i];
+}
+
+// Shared memory of k_radix_scatter (dynamic: more than the 48 KB static limit).
+struct ScatterSmem {
+  uint64_t stage[kTileRows];              // one column of the tile, in digit order
+  uint32_t cnt[kRadixWarps][kMaxRadix];   // per warp: rows of each digit, then its first local position
+  uint32_t tstart[kMaxRadix];             // first local position of each digit in the tile
+  uint32_t goff[kMaxRadix];               // first global position of the tile's rows of each digit
+  uint16_t lpos[kTileRows];               // local position of tile row (warp, batch, lane); 0xffff: dropped
+  uint8_t dig[kTileRows];                 // digit of each local position
+  uint8_t vstage[kTileRows];              // validity of the staged values
+  uint32_t active;                        // rows of the tile kept
+};
+constexpr size_t kScatterSmem = sizeof(ScatterSmem);
+
+// Moves the rows of tile blockIdx.x to offsets[d * ntiles + t] + their rank
+// among the tile's rows of digit d (tile order: warp, then batch, then lane).
+// Rows are first ranked in digit order inside the tile (local positions);
+// each column is then staged in shared memory at those positions and written
+// out by consecutive threads, so a digit's run of rows is stored by
+// consecutive lanes into consecutive addresses.
+template <int NW, bool FROM_COLUMNS>
+__global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_constant__ Plan plan,
+                                                               const __grid_constant__ PartBufs in, int64_t n,
+                                                               const uint32_t* n_active, const Digit dg, int ntiles,
+                                                               const uint32_t* __restrict__ offsets,
+                                                               const __grid_constant__ PartBufs out, int32_t* status)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScatterSmem& sm = *reinterpret_cast<ScatterSmem*>(smem_raw);
+  const int radix = 1 << dg.width;
+  for (int i = threadIdx.x; i < kRadixWarps * kMaxRadix; i += kRadixBlock) (&sm.cnt[0][0])[i] = 0;
+  __syncthreads();
+  const PassSource<NW, FROM_COLUMNS> src{&plan, &in};
+  const int64_t rows = source_rows(n, n_active, FROM_COLUMNS);
+  const int lane     = threadIdx.x & 31;
+  const int warp     = threadIdx.x >> 5;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kTileRows + warp * kRowsPerWarp;
+  const uint32_t lt  = (1u << lane) - 1u;
+
+  // rows of each digit per warp (each warp owns its row of cnt); each row's
+  // digit is kept in lpos (0xffff: row dropped) until its position is known
+  for (int j0 = 0; j0 < kRowsPerWarp / 32; j0 += kLoadGroup) {
+    uint64_t k[kLoadGroup][NW];
+    bool act[kLoadGroup];
+#pragma unroll
+    for (int u = 0; u < kLoadGroup; ++u) {
+      const int64_t r = base + (j0 + u) * 32 + lane;
+      act[u]          = r < rows && src.key(r, k[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadGroup; ++u) {
+      const uint32_t d  = act[u] ? digit_of<NW>(k[u], dg) : 0xffffffffu;
+      const uint32_t pe = __match_any_sync(kFull, d);
+      if (act[u] && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
+      sm.lpos[warp * kRowsPerWarp + (j0 + u) * 32 + lane] = static_cast<uint16_t>(act[u] ? d : 0xffffu);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // digit totals of the tile -> first local position of each digit (warp 0
+  // scans 8 digits per lane); global offsets of the tile's runs
+  if (warp == 0) {
+    uint32_t tot[kMaxRadix / 32];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int q = 0; q < kMaxRadix / 32; ++q) {
+      const int d = lane * (kMaxRadix / 32) + q;
+      uint32_t c  = 0;
+      if (d < radix)
+        for (int w = 0; w < kRadixWarps; ++w) c += sm.cnt[w][d];
+      tot[q] = c;
+      sum += c;
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, incl, off);
+      if (lane >= off) incl += v;
+    }
+    uint32_t run = incl - sum;
+#pragma unroll
+    for (int q = 0; q < kMaxRadix / 32; ++q) {
+      const int d = lane * (kMaxRadix / 32) + q;
+      if (d < radix) sm.tstart[d] = run;
+      run += tot[q];
+    }
+    if (lane == 31) sm.active = incl;
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < radix; d += kRadixBlock) {
+    sm.goff[d]   = offsets[static_cast<size_t>(d) * ntiles + blockIdx.x];
+    uint32_t run = sm.tstart[d];
+    for (int w = 0; w < kRadixWarps; ++w) {
+      const uint32_t c = sm.cnt[w][d];
+      sm.cnt[w][d]     = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  // local positions (the digits come back from lpos, which then takes the
+  // position); key word 0 staged on the way
+  for (int j0 = 0; j0 < kRowsPerWarp / 32; j0 += kLoadGroup) {
+    uint64_t k0[kLoadGroup];
+    uint32_t dd[kLoadGroup];
+#pragma unroll
+    for (int u = 0; u < kLoadGroup; ++u) {
+      const int row = warp * kRowsPerWarp + (j0 + u) * 32 + lane;
+      dd[u]         = sm.lpos[row];
+      k0[u]         = 0;
+      if (dd[u] != 0xffffu) {
+        uint64_t k[NW];
+        src.key(base + (j0 + u) * 32 + lane, k);
+        k0[u] = k[0];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadGroup; ++u) {
+      const bool act    = dd[u] != 0xffffu;
+      const uint32_t d  = act ? dd[u] : 0xffffffffu;
+      const uint32_t pe = __match_any_sync(kFull, d);
+      const uint32_t lp = act ? sm.cnt[warp][d] + static_cast<uint32_t>(__popc(pe & lt)) : 0xffffu;
+      __syncwarp();
+      if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
+      sm.lpos[warp * kRowsPerWarp + (j0 + u) * 32 + lane] = static_cast<uint16_t>(lp);
+      if (act) {
+        sm.dig[lp]   = static_cast<uint8_t>(d);
+        sm.stage[lp] = k0[u];
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  const uint32_t active = sm.active;
+  auto global_pos = [&](uint32_t i) -> uint32_t {
+    const uint32_t d = sm.dig[i];
+    return sm.goff[d] + (i - sm.tstart[d]);
+  };
+  for (uint32_t i = threadIdx.x; i < active; i += kRadixBlock)
+    const_cast<uint64_t*>(out.keys[0])[global_pos(i)] = sm.stage[i];
+  __syncthreads();
+  // remaining key word, then every channel's values and validity
+  for (int col = 1; col < NW + plan.nchan; ++col) {
+    const int c = col - NW;
+    for (int j0 = 0; j0 < kRowsPerWarp / 32; j0 += kLoadGroup) {
+      uint32_t lp[kLoadGroup];
+      uint64_t val[kLoadGroup];
+      bool v[kLoadGroup];
+#pragma unroll
+      for (int u = 0; u < kLoadGroup; ++u) {
+        lp[u]  = sm.lpos[warp * kRowsPerWarp + (j0 + u) * 32 + lane];
+        val[u] = 0;
+        v[u]   = false;
+        if (lp[u] == 0xffffu) continue;
+        const int64_t r = base + (j0 + u) * 32 + lane;
+        if (col < NW) {
+          uint64_t k[NW];
+          src.key(r, k);
+          val[u] = k[col & (NW - 1)];
+          v[u]   = true;
+        } else {
+          v[u] = src.value(c, r, val[u], status);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kLoadGroup; ++u) {
+        if (lp[u] == 0xffffu) continue;
+        sm.stage[lp[u]]  = v[u] ? val[u] : 0;
+        sm.vstage[lp[u]] = v[u] ? 1 : 0;
+      }
+    }
+    __syncthreads();
+    if (col < NW) {
+      for (uint32_t i = threadIdx.x; i < active; i += kRadixBlock)
+        const_cast<uint64_t*>(out.keys[col & (NW - 1)])[global_pos(i)] = sm.stage[i];
+    } else {
+      const PartCol& pc = out.col[c];
+      for (uint32_t i = threadIdx.x; i < active; i += kRadixBlock) {
+        const uint32_t at = global_pos(i);
+        store_bits(const_cast<void*>(pc.vals), at, pc.width, sm.stage[i]);
+        if (pc.valid != nullptr) const_cast<uint8_t*>(pc.valid)[at] = sm.vstage[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+size_t part_radix_count_bytes(int64_t n)
+{
+  const int64_t ntiles = (n + kTileRows - 1) / kTileRows;
+  return static_cast<size_t>(std::max<int64_t>(ntiles, 1)) * kMaxRadix * sizeof(uint32_t);
+}
+
+cudaError_t part_radix_temp_bytes(int64_t n, size_t* temp_bytes)
+{
+  const int64_t ntiles = (n + kTileRows - 1) / kTileRows;
+  const int items      = static_cast<int>(std::max<int64_t>(ntiles, 1) * kMaxRadix);
+  return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, static_cast<uint32_t*>(nullptr),
+                                       static_cast<uint32_t*>(nullptr), items, cudaStream_t(nullptr));
+}
+
+namespace {
+template <int NW, bool FROM_COLUMNS>
+cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint32_t* n_active, const Digit& dg,
+                       int ntiles, uint32_t* counts, uint32_t* offsets, void* temp, size_t temp_bytes,
+                       const PartBufs& out, int32_t* status, cudaStream_t st)
+{
+  k_radix_hist<NW, FROM_COLUMNS><<<ntiles, kRadixBlock, 0, st>>>(p, in, n, n_active, dg, ntiles, counts);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int items = ntiles << dg.width;
+  e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offsets, items, st);
+  if (e != cudaSuccess) return e;
+  e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter<NW, FROM_COLUMNS>), kScatterSmem);
+  if (e != cudaSuccess) return e;
+  k_radix_scatter<NW, FROM_COLUMNS>
+    <<<ntiles, kRadixBlock, kScatterSmem, st>>>(p, in, n, n_active, dg, ntiles, offsets, out, status);
+  return cudaGetLastError();
+}
+
+template <int NW>
+cudaError_t radix_all(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
+                      const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp, size_t temp_bytes,
+                      int32_t* status, cudaStream_t st)
+{
+  const int passes     = (bits + 7) / 8;
+  const int ntiles     = static_cast<int>(std::max<int64_t>((n + kTileRows - 1) / kTileRows, 1));
+  int shift            = 0;
+  const PartBufs* prev = nullptr;
+  for (int i = 0; i < passes; ++i) {
+    Digit dg;
+    dg.bits  = bits;
+    dg.shift = shift;
+    dg.width = bits / passes + (i < bits % passes ? 1 : 0);
+    shift += dg.width;
+    // the last pass writes `dst`; earlier ones alternate so that it does
+    const PartBufs& out = ((passes - 1 - i) % 2 == 0) ? dst : tmp;
+    cudaError_t e;
+    if (i == 0) e = radix_pass<NW, true>(p, out, n, n_active, dg, ntiles, counts, offsets, temp, temp_bytes, out, status, st);
+    else e = radix_pass<NW, false>(p, *prev, n, n_active, dg, ntiles, counts, offsets, temp, temp_bytes, out, status, st);
+    if (e != cudaSuccess) return e;
+    prev = &out;
+  }
+  return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
+                              const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
+                              size_t temp_bytes, int32_t* status, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  return p.key.nwords == 1 ? radix_all<1>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, st)
+                           : radix_all<2>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, st);
+}
+
+}  // namespace gbx

@@ -143,46 +143,32 @@ struct WarpTable {
   __device__ __forceinline__ uint64_t* keys() const { return reinterpret_cast<uint64_t*>(tb + sl->keys_off); }
   __device__ __forceinline__ uint32_t* rows() const { return reinterpret_cast<uint32_t*>(tb + sl->rows_off); }
 
-  // Identity of one slot's row count and accumulators.
-  __device__ __forceinline__ void init_slot(const AccLayout& al, uint32_t s) const
-  {
-    rows()[s] = 0;
-    for (int a = 0; a < al.nacc; ++a) {
-      uint64_t id = identity_bits(al.kind[a]);
-      if (acc_bytes(al.kind[a]) == 4) reinterpret_cast<uint32_t*>(tb + sl->acc_off[a])[s] = static_cast<uint32_t>(id);
-      else reinterpret_cast<uint64_t*>(tb + sl->acc_off[a])[s] = id;
-    }
-  }
-
-  // Empties the table: keys only (a slot's accumulators are set when a key
-  // is inserted), plus the reserved slot S in full.
-  __device__ __forceinline__ void reset(const AccLayout& al, int lane) const
-  {
-    uint64_t* kk = keys();
-    for (uint32_t s = lane; s <= S; s += 32) {  // slot S keeps the all-ones key it stands for
-#pragma unroll
-      for (int w = 0; w < NW; ++w) kk[s * NW + w] = kEmptyWord;
-    }
-    if (lane == 0) init_slot(al, S);
-    __syncwarp();
-  }
-
+  // Empties the table: every key word empty and every accumulator of every
+  // slot (the reserved slot S included) at its identity, so that inserting a
+  // key only writes the key.  One accumulator array at a time, the lanes
+  // taking consecutive slots.
   __device__ __forceinline__ void init(const AccLayout& al, int lane) const
   {
     uint64_t* kk = keys();
     uint32_t* rr = rows();
-    for (uint32_t s = lane; s <= S; s += 32) {
+    for (uint32_t s = lane; s <= S; s += 32) {  // slot S keeps the all-ones key it stands for
 #pragma unroll
       for (int w = 0; w < NW; ++w) kk[s * NW + w] = kEmptyWord;
       rr[s] = 0;
-      for (int a = 0; a < al.nacc; ++a) {
-        uint64_t id = identity_bits(al.kind[a]);
-        if (acc_bytes(al.kind[a]) == 4) reinterpret_cast<uint32_t*>(tb + sl->acc_off[a])[s] = static_cast<uint32_t>(id);
-        else reinterpret_cast<uint64_t*>(tb + sl->acc_off[a])[s] = id;
+    }
+    for (int a = 0; a < al.nacc; ++a) {
+      const uint64_t id = identity_bits(al.kind[a]);
+      if (acc_bytes(al.kind[a]) == 4) {
+        uint32_t* p = reinterpret_cast<uint32_t*>(tb + sl->acc_off[a]);
+        for (uint32_t s = lane; s <= S; s += 32) p[s] = static_cast<uint32_t>(id);
+      } else {
+        uint64_t* p = reinterpret_cast<uint64_t*>(tb + sl->acc_off[a]);
+        for (uint32_t s = lane; s <= S; s += 32) p[s] = id;
       }
     }
     __syncwarp();
   }
+  __device__ __forceinline__ void reset(const AccLayout& al, int lane) const { init(al, lane); }
 };
 
 enum RowState { ST_DONE = 0, ST_PROBING = 1, ST_INSERT = 2, ST_FOUND = 3, ST_SPILL = 4 };
@@ -231,9 +217,9 @@ __device__ __forceinline__ int warp_find_or_insert(const WarpTable<NW>& T, const
     if (state == ST_INSERT) {
       const uint32_t grp = __match_any_sync(im, slot);
       if ((__ffs(grp) - 1) == lane) {
+        // the slot's accumulators are at their identities since init()
 #pragma unroll
         for (int w = 0; w < NW; ++w) keys[slot * NW + w] = k[w];
-        T.init_slot(al, slot);
       }
     }
     __syncwarp();
