@@ -892,7 +892,9 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     if (strategy == GBX_STRATEGY_PARTITIONED) {
       // ---- radix-partitioned path (gbx_part.cu)
       const uint32_t S  = slot_bytes >= 48 ? 128u : 256u;  // warp table slots (two CTAs per SM)
-      const double gpb  = S * 0.4;                         // target groups per bucket
+      // target groups per bucket: half the table, so that the fullest of ~1M
+      // buckets (mean + 5 sigma of a Poisson count) still fits
+      const double gpb  = S * 0.5;
       int bits          = 0;
       while (static_cast<double>(1ull << bits) * gpb < est && bits < 22) ++bits;
       const SmemLayout sl = make_smem_layout(plan, S);

@@ -32,7 +32,7 @@ constexpr int kRadixWarps  = kRadixBlock / 32;
 constexpr int kRowsPerWarp = 512;  // 16 batches of 32
 constexpr int kTileRows    = kRadixWarps * kRowsPerWarp;
 constexpr int kMaxRadix    = 256;
-constexpr int kLoadGroup   = 4;  // 32-row batches whose loads a warp has in flight together
+constexpr int kLoadGroup   = 8;  // 32-row batches whose loads a warp has in flight together
 
 struct Digit {
   int bits;   // bucket id = top `bits` bits of the key hash
