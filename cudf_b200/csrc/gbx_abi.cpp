@@ -957,7 +957,22 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
           if (c.null_mask) GBX_CUDA(cudaMemsetAsync(c.null_mask, 0, c.mask_bytes, s));
         });
         GBX_CUDA(cudaMemsetAsync(p_nulls, 0, (kMaxKeyCols + kMaxOut) * 8, s));
-        GBX_CUDA(launch_part_hist(plan.key, call.n, pp, call.dev.num_sms, s));
+        // many buckets: coalesced radix passes (gbx_radix.cu), whose first
+        // histogram also counts the rows per bucket
+        const bool use_radix = pp.shard_bits == 0 && bits >= 9;
+        if (use_radix) {
+          if (rcounts == nullptr) {
+            tbufs    = part_bufs();
+            rcounts  = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
+            roffsets = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
+            GBX_CUDA(part_radix_temp_bytes(call.n, &rtemp_bytes));
+            rtemp = scratch.get(rtemp_bytes);
+          }
+          GBX_CUDA(cudaMemsetAsync(pp.counts, 0, nctr * sizeof(uint32_t), s));
+          GBX_CUDA(launch_part_radix_hist0(plan, call.n, bits, rcounts, pp.counts, s));
+        } else {
+          GBX_CUDA(launch_part_hist(plan.key, call.n, pp, call.dev.num_sms, s));
+        }
         size_t temp_bytes = 0;
         GBX_CUDA(launch_part_layout(pp, nullptr, &temp_bytes, call.dev.num_sms, s));
         void* temp = scratch.get(temp_bytes);
@@ -980,18 +995,10 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         t2.special_used = reinterpret_cast<uint32_t*>(ctl + 28);
         t2.status       = d_status;
         GBX_CUDA(launch_init_table(t2, plan.acc, plan.key.nwords, call.dev.num_sms, s));
-        if (pp.shard_bits == 0 && bits >= 9) {
-          // many buckets: coalesced radix passes (gbx_radix.cu)
-          if (rcounts == nullptr) {
-            tbufs    = part_bufs();
-            rcounts  = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
-            roffsets = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
-            GBX_CUDA(part_radix_temp_bytes(call.n, &rtemp_bytes));
-            rtemp = scratch.get(rtemp_bytes);
-          }
+        if (use_radix) {
           GBX_CUDA(launch_part_radix(plan, call.n, bits, pp.offsets + P, pbufs, tbufs, rcounts, roffsets, rtemp,
-                                     rtemp_bytes, d_status, s));
-          launches += 3 * ((bits + 7) / 8) - 1;
+                                     rtemp_bytes, d_status, /*hist0_done=*/true, s));
+          launches += 3 * ((bits + 7) / 8) - 2;
         } else {
           GBX_CUDA(launch_part_scatter(plan, call.n, pp, pbufs, call.dev.num_sms, s));
         }

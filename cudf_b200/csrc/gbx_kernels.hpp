@@ -93,11 +93,17 @@ cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, co
 // (same layout) and end in `dst`.  *n_active (device) is the number of rows
 // kept (the bucket histogram's total); `counts` and `offsets` hold
 // part_radix_count_bytes(n) bytes each, `temp` part_radix_temp_bytes(n).
+// launch_part_radix_hist0 runs the first pass's tile histogram early and
+// adds every kept row to bucket_counts[its bucket] (zeroed by the caller),
+// which then stands in for launch_part_hist; launch_part_radix is told so
+// with hist0_done.
 size_t part_radix_count_bytes(int64_t n);
 cudaError_t part_radix_temp_bytes(int64_t n, size_t* temp_bytes);
+cudaError_t launch_part_radix_hist0(const Plan& p, int64_t n, int bits, uint32_t* counts, uint32_t* bucket_counts,
+                                    cudaStream_t st);
 cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
                               const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
-                              size_t temp_bytes, int32_t* status, cudaStream_t st);
+                              size_t temp_bytes, int32_t* status, bool hist0_done, cudaStream_t st);
 // Aggregates every bucket: single-item buckets write their groups to `op`
 // directly; multi-item buckets merge into region tables of `t` (t.cap =
 // regions * region_slots) that launch_part_region_finalize then writes out.

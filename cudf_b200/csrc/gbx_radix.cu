@@ -82,12 +82,14 @@ __device__ __forceinline__ int64_t source_rows(int64_t n, const uint32_t* n_acti
   return from_columns ? n : static_cast<int64_t>(*n_active);
 }
 
-// counts[d * ntiles + t] = rows of tile t whose digit is d.
+// counts[d * ntiles + t] = rows of tile t whose digit is d; when
+// bucket_counts is set, also adds every row to its bucket's count there
+// (the bucket histogram of the partitioned path, warp-aggregated).
 template <int NW, bool FROM_COLUMNS>
 __global__ void __launch_bounds__(kRadixBlock) k_radix_hist(const __grid_constant__ Plan plan,
                                                             const __grid_constant__ PartBufs in, int64_t n,
                                                             const uint32_t* n_active, const Digit dg, int ntiles,
-                                                            uint32_t* counts)
+                                                            uint32_t* counts, uint32_t* bucket_counts)
 {
   __shared__ uint32_t hist[kMaxRadix];
   const int radix = 1 << dg.width;
@@ -109,9 +111,15 @@ __global__ void __launch_bounds__(kRadixBlock) k_radix_hist(const __grid_constan
     }
 #pragma unroll
     for (int u = 0; u < kLoadGroup; ++u) {
-      const uint32_t d  = act[u] ? digit_of<NW>(k[u], dg) : 0xffffffffu;
-      const uint32_t pe = __match_any_sync(kFull, d);
+      const uint64_t h   = act[u] ? hash_key<NW>(k[u]) : 0;
+      const uint32_t bkt = dg.bits == 0 ? 0u : static_cast<uint32_t>(h >> (64 - dg.bits));
+      const uint32_t d   = act[u] ? ((bkt >> dg.shift) & ((1u << dg.width) - 1u)) : 0xffffffffu;
+      const uint32_t pe  = __match_any_sync(kFull, d);
       if (act[u] && lane == __ffs(pe) - 1) atomicAdd(&hist[d], static_cast<uint32_t>(__popc(pe)));
+      if (bucket_counts != nullptr) {
+        const uint32_t pb = __match_any_sync(kFull, act[u] ? bkt : 0xffffffffu);
+        if (act[u] && lane == __ffs(pb) - 1) atomicAdd(bucket_counts + bkt, static_cast<uint32_t>(__popc(pb)));
+      }
     }
   }
   __syncthreads();
@@ -321,14 +329,30 @@ cudaError_t part_radix_temp_bytes(int64_t n, size_t* temp_bytes)
 }
 
 namespace {
+// Digit of pass i (least significant first) of a `bits`-bit bucket id.
+Digit pass_digit(int bits, int i)
+{
+  const int passes = (bits + 7) / 8;
+  Digit dg;
+  dg.bits  = bits;
+  dg.shift = 0;
+  for (int j = 0; j < i; ++j) dg.shift += bits / passes + (j < bits % passes ? 1 : 0);
+  dg.width = bits / passes + (i < bits % passes ? 1 : 0);
+  return dg;
+}
+
+int tiles_of(int64_t n) { return static_cast<int>(std::max<int64_t>((n + kTileRows - 1) / kTileRows, 1)); }
+
 template <int NW, bool FROM_COLUMNS>
 cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint32_t* n_active, const Digit& dg,
                        int ntiles, uint32_t* counts, uint32_t* offsets, void* temp, size_t temp_bytes,
-                       const PartBufs& out, int32_t* status, cudaStream_t st)
+                       const PartBufs& out, int32_t* status, bool hist_done, cudaStream_t st)
 {
-  k_radix_hist<NW, FROM_COLUMNS><<<ntiles, kRadixBlock, 0, st>>>(p, in, n, n_active, dg, ntiles, counts);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  if (!hist_done) {
+    k_radix_hist<NW, FROM_COLUMNS><<<ntiles, kRadixBlock, 0, st>>>(p, in, n, n_active, dg, ntiles, counts, nullptr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   const int items = ntiles << dg.width;
   e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offsets, items, st);
   if (e != cudaSuccess) return e;
@@ -342,23 +366,22 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint3
 template <int NW>
 cudaError_t radix_all(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
                       const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp, size_t temp_bytes,
-                      int32_t* status, cudaStream_t st)
+                      int32_t* status, bool hist0_done, cudaStream_t st)
 {
   const int passes     = (bits + 7) / 8;
-  const int ntiles     = static_cast<int>(std::max<int64_t>((n + kTileRows - 1) / kTileRows, 1));
-  int shift            = 0;
+  const int ntiles     = tiles_of(n);
   const PartBufs* prev = nullptr;
   for (int i = 0; i < passes; ++i) {
-    Digit dg;
-    dg.bits  = bits;
-    dg.shift = shift;
-    dg.width = bits / passes + (i < bits % passes ? 1 : 0);
-    shift += dg.width;
+    const Digit dg = pass_digit(bits, i);
     // the last pass writes `dst`; earlier ones alternate so that it does
     const PartBufs& out = ((passes - 1 - i) % 2 == 0) ? dst : tmp;
     cudaError_t e;
-    if (i == 0) e = radix_pass<NW, true>(p, out, n, n_active, dg, ntiles, counts, offsets, temp, temp_bytes, out, status, st);
-    else e = radix_pass<NW, false>(p, *prev, n, n_active, dg, ntiles, counts, offsets, temp, temp_bytes, out, status, st);
+    if (i == 0)
+      e = radix_pass<NW, true>(p, out, n, n_active, dg, ntiles, counts, offsets, temp, temp_bytes, out, status,
+                               hist0_done, st);
+    else
+      e = radix_pass<NW, false>(p, *prev, n, n_active, dg, ntiles, counts, offsets, temp, temp_bytes, out, status,
+                                false, st);
     if (e != cudaSuccess) return e;
     prev = &out;
   }
@@ -366,13 +389,28 @@ cudaError_t radix_all(const Plan& p, int64_t n, int bits, const uint32_t* n_acti
 }
 }  // namespace
 
-cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
-                              const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
-                              size_t temp_bytes, int32_t* status, cudaStream_t st)
+cudaError_t launch_part_radix_hist0(const Plan& p, int64_t n, int bits, uint32_t* counts, uint32_t* bucket_counts,
+                                    cudaStream_t st)
 {
   if (n <= 0) return cudaSuccess;
-  return p.key.nwords == 1 ? radix_all<1>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, st)
-                           : radix_all<2>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, st);
+  const Digit dg   = pass_digit(bits, 0);
+  const int ntiles = tiles_of(n);
+  const PartBufs none{};
+  if (p.key.nwords == 1)
+    k_radix_hist<1, true><<<ntiles, kRadixBlock, 0, st>>>(p, none, n, nullptr, dg, ntiles, counts, bucket_counts);
+  else
+    k_radix_hist<2, true><<<ntiles, kRadixBlock, 0, st>>>(p, none, n, nullptr, dg, ntiles, counts, bucket_counts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
+                              const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
+                              size_t temp_bytes, int32_t* status, bool hist0_done, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  return p.key.nwords == 1
+           ? radix_all<1>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, hist0_done, st)
+           : radix_all<2>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, hist0_done, st);
 }
 
 }  // namespace gbx
