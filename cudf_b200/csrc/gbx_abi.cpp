@@ -891,15 +891,22 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
 
     if (strategy == GBX_STRATEGY_PARTITIONED) {
       // ---- radix-partitioned path (gbx_part.cu)
-      const uint32_t S  = slot_bytes >= 48 ? 128u : 256u;  // warp table slots (two CTAs per SM)
+      // warp table slots (two CTAs per SM), halved until eight warps' tables
+      // and scratch fit one CTA's shared memory (wide schemas)
+      uint32_t S    = slot_bytes >= 48 ? 128u : 256u;
+      SmemLayout sl = make_smem_layout(plan, S);
+      auto part_smem = [&]() { return static_cast<size_t>(sl.total) * 8 + 8 * (S + 32) * 4; };
+      while (S > 32 && part_smem() > call.dev.smem_optin) {
+        S >>= 1;
+        sl = make_smem_layout(plan, S);
+      }
+      if (part_smem() > call.dev.smem_optin)
+        fail(GBX_ERR_UNSUPPORTED, "per-group state too large for the partitioned path");
       // target groups per bucket: half the table, so that the fullest of ~1M
       // buckets (mean + 5 sigma of a Poisson count) still fits
       const double gpb  = S * 0.5;
       int bits          = 0;
       while (static_cast<double>(1ull << bits) * gpb < est && bits < 22) ++bits;
-      const SmemLayout sl = make_smem_layout(plan, S);
-      if (static_cast<size_t>(sl.total) * 8 + 8 * (S + 32) * 4 > call.dev.smem_optin)
-        fail(GBX_ERR_UNSUPPORTED, "per-group state too large for the partitioned path");
       // bucket-ordered copies of the rows: packed key words, resolved value
       // bits, a validity byte per row of a nullable channel
       auto part_bufs = [&]() {
@@ -937,7 +944,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         PartPlan pp{};
         pp.bits         = bits;
         pp.shard_bits   = std::max(0, std::min(5, 12 - bits));
-        pp.slice_rows   = 16384;
+        pp.slice_rows   = 16384;  // < 65536: ranks and counts of a whole bucket fit 16 bits
         pp.region_slots = S;
         pp.status       = d_status;
         auto arr        = [&]() { return static_cast<uint32_t*>(scratch.get((static_cast<size_t>(P) + 1) * 4)); };
@@ -982,32 +989,48 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         GBX_CUDA(cudaMemcpyAsync(&h_counts[0], pp.region + P, 4, cudaMemcpyDeviceToHost, s));
         GBX_CUDA(cudaMemcpyAsync(&h_counts[1], pp.item_start + P, 4, cudaMemcpyDeviceToHost, s));
         GBX_CUDA(cudaStreamSynchronize(s));
-        const uint32_t h_regions = h_counts[0];
-        pp.item_bucket = static_cast<uint32_t*>(scratch.get((static_cast<size_t>(h_counts[1]) + 1) * 4));
-        GBX_CUDA(launch_part_items(pp, call.n, call.dev.num_sms, s));
-        launches += 1;
+        const uint32_t h_regions = h_counts[0];  // buckets larger than slice_rows
+        const uint32_t h_items   = h_counts[1];  // their slices
         // region tables of the buckets split over several warps
         TableRef t2{};
-        t2.cap  = static_cast<uint64_t>(h_regions) * S;
-        t2.keys = static_cast<uint64_t*>(scratch.get((t2.cap + 1) * plan.key.nwords * 8));
-        t2.rows = static_cast<uint32_t*>(scratch.get((t2.cap + 1) * 4));
-        for (int a = 0; a < nacc; ++a) t2.acc[a] = scratch.get((t2.cap + 1) * acc_bytes(plan.acc.kind[a]));
-        t2.special_used = reinterpret_cast<uint32_t*>(ctl + 28);
-        t2.status       = d_status;
-        GBX_CUDA(launch_init_table(t2, plan.acc, plan.key.nwords, call.dev.num_sms, s));
+        if (h_items > 0) {
+          pp.item_bucket = static_cast<uint32_t*>(scratch.get((static_cast<size_t>(h_items) + 1) * 4));
+          GBX_CUDA(launch_part_items(pp, call.n, call.dev.num_sms, s));
+          t2.cap  = static_cast<uint64_t>(h_regions) * S;
+          t2.keys = static_cast<uint64_t*>(scratch.get((t2.cap + 1) * plan.key.nwords * 8));
+          t2.rows = static_cast<uint32_t*>(scratch.get((t2.cap + 1) * 4));
+          for (int a = 0; a < nacc; ++a) t2.acc[a] = scratch.get((t2.cap + 1) * acc_bytes(plan.acc.kind[a]));
+          t2.special_used = reinterpret_cast<uint32_t*>(ctl + 28);
+          t2.status       = d_status;
+          GBX_CUDA(launch_init_table(t2, plan.acc, plan.key.nwords, call.dev.num_sms, s));
+          launches += 2;
+        }
         if (use_radix) {
           GBX_CUDA(launch_part_radix(plan, call.n, bits, pp.offsets + P, pbufs, tbufs, rcounts, roffsets, rtemp,
                                      rtemp_bytes, d_status, /*hist0_done=*/true, s));
           launches += 3 * ((bits + 7) / 8) - 2;
         } else {
           GBX_CUDA(launch_part_scatter(plan, call.n, pp, pbufs, call.dev.num_sms, s));
+          launches += 1;
+          if (tbufs.keys[0] == nullptr) tbufs = part_bufs();
         }
+        // the second set of copies (free again after the radix passes) takes
+        // the whole buckets' rows in group order; its key words hold the rank
+        // records of buckets too large for shared memory
+        pp.rank_rec       = const_cast<uint32_t*>(reinterpret_cast<const uint32_t*>(tbufs.keys[0]));
+        pp.bucket_counter = ctl + 31;
         timer.mark(2);
-        GBX_CUDA(launch_part_agg(plan, pp, pbufs, t2, sl, pop, call.dev.num_sms, s));
-        timer.mark(3);
-        GBX_CUDA(launch_part_region_finalize(plan, pp, t2, pop, call.dev.num_sms, s));
+        GBX_CUDA(launch_part_ranked(plan, pp, pbufs, tbufs, S, pop, call.dev.num_sms, s));
+        launches += 1;
+        if (h_items > 0) {
+          GBX_CUDA(launch_part_agg(plan, pp, pbufs, t2, sl, call.dev.num_sms, s));
+          timer.mark(3);
+          GBX_CUDA(launch_part_region_finalize(plan, pp, t2, pop, call.dev.num_sms, s));
+          launches += 2;
+        } else {
+          timer.mark(3);
+        }
         timer.mark(4);
-        launches += 4;
         GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
         GBX_CUDA(cudaStreamSynchronize(s));
         int32_t status;

@@ -69,15 +69,20 @@ struct PartPlan {
   uint32_t* counts;          // [(P << shard_bits) + 1] rows per (bucket, shard) (last entry 0)
   uint32_t* offsets;         // [(P << shard_bits) + 1] exclusive scan of counts
   uint32_t* cursor;          // [P << shard_bits] scatter cursors (copy of offsets)
-  uint32_t* nslices;         // [P + 1] work items per bucket (last entry 0)
+  uint32_t* nslices;         // [P + 1] slices of a bucket larger than slice_rows, else 0 (last entry 0)
   uint32_t* item_start;      // [P + 1] exclusive scan of nslices
   uint32_t* multi;           // [P + 1] 1 when a bucket has several items (last entry 0)
   uint32_t* region;          // [P + 1] exclusive scan of multi: region table of the bucket
   uint32_t* item_bucket;     // [items] bucket of each work item
-  unsigned long long* item_counter;  // work-item dispenser
+  unsigned long long* item_counter;  // work-item dispenser (slices)
+  unsigned long long* bucket_counter;  // bucket dispenser (whole buckets)
   unsigned long long* out_counter;   // output rows written so far
   uint32_t region_slots;     // slots per region table (= the warp table size)
   int32_t* status;           // device status word
+  // [n], indexed by partitioned row: a bucket handled by one warp whose rows
+  // do not fit the warp's shared memory ranks them here (slot << 16 | rank
+  // within the slot; slice_rows < 65536)
+  uint32_t* rank_rec;
 };
 
 cudaError_t launch_part_hist(const KeyPlan& kp, int64_t n, const PartPlan& pp, int num_sms, cudaStream_t st);
@@ -104,11 +109,16 @@ cudaError_t launch_part_radix_hist0(const Plan& p, int64_t n, int bits, uint32_t
 cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
                               const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
                               size_t temp_bytes, int32_t* status, bool hist0_done, cudaStream_t st);
-// Aggregates every bucket: single-item buckets write their groups to `op`
-// directly; multi-item buckets merge into region tables of `t` (t.cap =
-// regions * region_slots) that launch_part_region_finalize then writes out.
+// Aggregates every bucket of at most slice_rows rows (S-slot warp tables)
+// and writes its groups to `op`, the rows permuted into group order in
+// `sorted` (the layout of `in`, overwritten; its key words hold rank records).
+cudaError_t launch_part_ranked(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
+                               uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st);
+// Aggregates the slices of the larger buckets (item_start[P] of them, > 0)
+// into region tables of `t` (t.cap = regions * region_slots) that
+// launch_part_region_finalize then writes out.
 cudaError_t launch_part_agg(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
-                            const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st);
+                            const SmemLayout& sl, int num_sms, cudaStream_t st);
 cudaError_t launch_part_region_finalize(const Plan& p, const PartPlan& pp, const TableRef& t, const OutPlan& op,
                                        int num_sms, cudaStream_t st);
 

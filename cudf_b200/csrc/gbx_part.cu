@@ -5,9 +5,10 @@
 // each (histogram, scans, scatter).  A warp then owns a bucket -- or, for a
 // large bucket, a slice of it -- with a private shared-memory table
 // (gbx_warpcore.cuh): no atomics on the row path.  A bucket handled by one
-// warp is finalised straight into the output columns (dense rows reserved with
-// one atomic per 32 groups); slices of a large bucket merge into a compact
-// per-bucket region table that a last kernel writes out.  The reference keeps
+// warp has its rows ranked by group and each group folded in one lane's
+// registers, then written straight into the output columns (dense rows
+// reserved with one atomic per bucket); slices of a large bucket merge into a
+// compact per-bucket region table that a last kernel writes out.  The reference keeps
 // one global set of row indices sized by rows and updates N-row sparse columns
 // with per-row atomics (hash/groupby.cu:424-504, 571-580); here every group's
 // state lives in shared memory until it is final.
@@ -36,6 +37,147 @@ __device__ __forceinline__ uint32_t counter_of(uint32_t b, int64_t r, const Part
 {
   return (b << pp.shard_bits) | (static_cast<uint32_t>(r >> 5) & ((1u << pp.shard_bits) - 1u));
 }
+
+constexpr uint32_t kNoRank = 0xffffffffu;
+
+// Element i of a buffer that this kernel also writes (a plain load: the
+// read-only path is not coherent with the kernel's own stores).
+__device__ __forceinline__ uint64_t load_bits_rw(const void* p, int64_t i, int width)
+{
+  switch (width) {
+    case 1: return reinterpret_cast<const uint8_t*>(p)[i];
+    case 2: return reinterpret_cast<const uint16_t*>(p)[i];
+    case 4: return reinterpret_cast<const uint32_t*>(p)[i];
+    default: return reinterpret_cast<const uint64_t*>(p)[i];
+  }
+}
+
+// One whole bucket, rows [r0, r1), aggregated by one warp in four steps:
+//   1. rank: each row finds or inserts its key in the warp's table (keys and
+//      row counts only) and takes the next rank of its slot, lanes of a batch
+//      in lane order, so that a group's rows keep their partitioned order;
+//   2. scan: an exclusive scan of the slot counts gives each slot's first
+//      position, and the occupied slots are listed with their counts;
+//   3. permute: each row's values move to r0 + position + rank of `sorted`
+//      (the same rows of a second set of copies), so that every group's rows
+//      are contiguous;
+//   4. fold: lane i takes the i-th listed group of a batch of 32 and folds
+//      its run of rows into registers (ChanAcc), one channel at a time, then
+//      writes that channel's outputs; the keys come from the table.
+// No accumulator is read or written in shared memory and no slot has more
+// than one writer.  Folding one channel at a time keeps a single copy of the
+// accumulate and finalise code in the loop, so the kernel's hot code stays
+// within the instruction cache.  The rank records live in the warp's
+// shared memory (rec_smem, rec_rows entries) when the bucket fits, else in
+// pp.rank_rec.
+template <int NW>
+__device__ __forceinline__ void part_bucket_ranked(const Plan& plan, const PartPlan& pp, const PartBufs& in,
+                                                   const PartBufs& sorted, const WarpTable<NW>& T,
+                                                   uint32_t* rec_smem, uint32_t rec_rows, const OutPlan& op,
+                                                   int64_t r0, int64_t r1, uint32_t* scratch, int lane,
+                                                   uint32_t* cta_nulls, int32_t* status)
+{
+  const PartSource src{&in};
+  T.reset_keys(lane);
+  uint32_t* cnt      = T.rows();
+  const uint32_t len = static_cast<uint32_t>(r1 - r0);
+  uint32_t* rec      = len <= rec_rows ? rec_smem : pp.rank_rec + r0;
+
+  // 1. rank
+  int64_t r = r0 + lane;
+  uint64_t k[NW];
+  bool act = r < r1 && src.key<NW>(r, k);
+  for (int64_t base = r0; base < r1; base += 32) {
+    const int64_t rn = base + 32 + lane;
+    uint64_t kn[NW];
+    const bool actn = rn < r1 && src.key<NW>(rn, kn);
+    uint32_t slot;
+    const int state = warp_find_or_insert<NW>(T, plan.acc, act, k, lane, slot);
+    if (state == ST_SPILL) atomicOr(status, S_TABLE_FULL);  // bucket larger than its table: host retries
+    const bool found      = state == ST_FOUND;
+    const uint32_t fm     = __ballot_sync(kFull, found);
+    const uint32_t peers  = found ? __match_any_sync(fm, slot) : 0u;
+    const uint32_t before = __popc(peers & lanemask_lt(lane));
+    const uint32_t rank   = found ? cnt[slot] + before : 0u;
+    __syncwarp();
+    if (found && before == 0) cnt[slot] += __popc(peers);
+    if (act) rec[r - r0] = found ? ((slot << 16) | rank) : kNoRank;
+    __syncwarp();
+    r   = rn;
+    act = actn;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) k[w] = kn[w];
+  }
+
+  // 2. scan: slot counts -> first positions (in place); occupied slots with
+  // their counts (count << 16 | slot) into scratch
+  uint32_t run = 0, ngroups = 0;
+  for (uint32_t s0 = 0; s0 <= T.S; s0 += 32) {
+    const uint32_t s = s0 + lane;
+    const uint32_t c = s <= T.S ? cnt[s] : 0u;
+    uint32_t incl    = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, incl, d);
+      if (lane >= d) incl += y;
+    }
+    if (s <= T.S) cnt[s] = run + incl - c;
+    const uint32_t bal = __ballot_sync(kFull, c > 0);
+    if (c > 0) scratch[ngroups + __popc(bal & lanemask_lt(lane))] = (c << 16) | s;
+    run += __shfl_sync(kFull, incl, 31);
+    ngroups += __popc(bal);
+  }
+  __syncwarp();
+
+  // 3. permute
+  for (uint32_t i = lane; i < len; i += 32) {
+    const uint32_t v = rec[i];
+    if (v == kNoRank) continue;
+    const int64_t from = r0 + i;
+    const int64_t to   = r0 + cnt[v >> 16] + (v & 0xffffu);
+    for (int c = 0; c < plan.nchan; ++c) {
+      const PartCol& a = in.col[c];
+      const PartCol& b = sorted.col[c];
+      store_bits(const_cast<void*>(b.vals), to, a.width, load_bits(a.vals, from, a.width));
+      if (a.valid != nullptr) const_cast<uint8_t*>(b.valid)[to] = __ldg(a.valid + from);
+    }
+  }
+  __syncwarp();  // orders the warp's stores before its loads below
+  if (ngroups == 0) return;
+
+  // 4. fold and write
+  unsigned long long ob = 0;
+  if (lane == 0) ob = atomicAdd(pp.out_counter, static_cast<unsigned long long>(ngroups));
+  ob                   = __shfl_sync(kFull, ob, 0);
+  const uint64_t* keys = T.keys();
+  const NullSink sink{op.null_counts, cta_nulls};
+  for (uint32_t g0 = 0; g0 < ngroups; g0 += 32) {
+    const bool active   = g0 + lane < ngroups;
+    const uint32_t ent  = active ? scratch[g0 + lane] : 0u;
+    const uint32_t ss   = ent & 0xffffu;
+    const uint32_t gc   = ent >> 16;
+    const int64_t first = r0 + (active ? cnt[ss] : 0u);
+    const int64_t base  = static_cast<int64_t>(ob + g0);
+    const uint32_t act  = __ballot_sync(kFull, active);
+    uint64_t k2[2]      = {0, 0};
+    if (active) {
+#pragma unroll
+      for (int w = 0; w < NW; ++w) k2[w] = keys[ss * NW + w];
+      if (ss == T.S) k2[0] = k2[1] = kEmptyWord;
+    }
+    warp_write_keys(plan, op, active, k2, base, lane, act, sink);
+    for (int c = 0; c < plan.nchan; ++c) {
+      const PartCol& pc = sorted.col[c];
+      ChanAcc A;
+      chan_acc_init(A);
+      for (uint32_t j = 0; j < gc; ++j) {
+        const uint64_t b = load_bits_rw(pc.vals, first + j, pc.width);
+        if (pc.valid == nullptr || pc.valid[first + j] != 0) chan_acc_add(plan.chan[c], A, b);
+      }
+      warp_write_chan(plan, op, active, gc, A, c, base, lane, act, sink);
+    }
+  }
+}
 }  // namespace
 
 // Rows per bucket (warp-aggregated: one atomic per bucket present in a warp).
@@ -63,9 +205,11 @@ __global__ void k_part_slices(const __grid_constant__ PartPlan pp)
       pp.nslices[b] = 0;
       pp.multi[b]   = 0;
     } else {
+      // a bucket of at most slice_rows rows is a whole-bucket item of
+      // k_part_ranked, not a slice
       const uint32_t c  = pp.offsets[(b + 1) << pp.shard_bits] - pp.offsets[b << pp.shard_bits];
-      const uint32_t ns = c == 0 ? 1u : (c + pp.slice_rows - 1) / pp.slice_rows;
-      pp.nslices[b]     = ns;
+      const uint32_t ns = (c + pp.slice_rows - 1) / pp.slice_rows;
+      pp.nslices[b]     = ns > 1 ? ns : 0u;
       pp.multi[b]       = ns > 1 ? 1u : 0u;
     }
   }
@@ -126,20 +270,69 @@ __global__ void k_part_scatter(const __grid_constant__ Plan plan, int64_t n, con
   }
 }
 
-// Bucket / slice aggregation (see the file comment).  blockDim.x / 32 warp
-// tables of sl.total bytes, then sl.slots + 32 u32 of compaction scratch per
-// warp (the occupied slots of a bucket, listed before its rows are reserved).
+// Per-warp shared memory of k_part_ranked: a keys-and-counts table
+// (sl.slots + 1 slots), the occupied-slot list and the rank records.
+struct RankedLayout {
+  uint32_t stride;       // bytes per warp
+  uint32_t scratch_off;  // sl.slots + 32 u32
+  uint32_t rec_off;      // rec_rows u32
+  uint32_t rec_rows;
+};
+
+// Whole buckets, claimed a few at a time, each through part_bucket_ranked.
+// `sl` describes the table part of each warp's shared memory (keys_off,
+// rows_off); it has no accumulator arrays.
+template <int NW>
+__global__ void __launch_bounds__(256, 4) k_part_ranked(const __grid_constant__ Plan plan,
+                                                       const __grid_constant__ PartPlan pp,
+                                                       const __grid_constant__ PartBufs in,
+                                                       const __grid_constant__ PartBufs sorted,
+                                                       const __grid_constant__ SmemLayout sl,
+                                                       const __grid_constant__ RankedLayout rl,
+                                                       const __grid_constant__ OutPlan op)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane         = threadIdx.x & 31;
+  unsigned char* wmem    = smem + static_cast<size_t>(threadIdx.x >> 5) * rl.stride;
+  const WarpTable<NW> T{wmem, &sl, sl.slots};
+  uint32_t* scratch      = reinterpret_cast<uint32_t*>(wmem + rl.scratch_off);
+  uint32_t* rec          = reinterpret_cast<uint32_t*>(wmem + rl.rec_off);
+  const uint32_t P       = 1u << pp.bits;
+  __shared__ uint32_t s_nulls[kNullSlots];
+  cta_nulls_zero(s_nulls);
+
+  constexpr int kClaim = 4;  // buckets claimed per atomic
+  unsigned long long claimed = 0, claim_end = 0;
+  for (;;) {
+    if (claimed == claim_end) {
+      unsigned long long c0 = 0;
+      if (lane == 0) c0 = atomicAdd(pp.bucket_counter, static_cast<unsigned long long>(kClaim));
+      claimed   = __shfl_sync(kFull, c0, 0);
+      claim_end = claimed + kClaim;
+    }
+    const unsigned long long b = claimed++;
+    if (b >= P) break;
+    if (pp.multi[b] != 0) continue;  // sliced: k_part_agg
+    const int64_t r0 = pp.offsets[b << pp.shard_bits];
+    const int64_t r1 = pp.offsets[(b + 1) << pp.shard_bits];
+    if (r1 == r0) continue;
+    part_bucket_ranked<NW>(plan, pp, in, sorted, T, rec, rl.rec_rows, op, r0, r1, scratch, lane, s_nulls,
+                           pp.status);
+    __syncwarp();
+  }
+  cta_nulls_flush(s_nulls, op.null_counts);
+}
+
+// Slices of the buckets larger than slice_rows (see the file comment):
+// blockDim.x / 32 warp tables of sl.total bytes with accumulators, merged
+// into the bucket's region table.
 template <int NW, int NCH>
-__global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Plan plan, const __grid_constant__ PartPlan pp, const __grid_constant__ PartBufs in, const __grid_constant__ TableRef t, const __grid_constant__ SmemLayout sl,
-                                                  const __grid_constant__ OutPlan op)
+__global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Plan plan, const __grid_constant__ PartPlan pp, const __grid_constant__ PartBufs in, const __grid_constant__ TableRef t, const __grid_constant__ SmemLayout sl)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane   = threadIdx.x & 31;
   const int warp   = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
   WarpTable<NW> T{smem + static_cast<size_t>(warp) * sl.total, &sl, sl.slots};
-  uint32_t* scratch = reinterpret_cast<uint32_t*>(smem + static_cast<size_t>(nwarps) * sl.total) +
-                      static_cast<size_t>(warp) * (sl.slots + 32);
   const PartSource src{&in};
   const uint32_t P          = 1u << pp.bits;
   const uint64_t items      = pp.item_start[P];
@@ -192,49 +385,7 @@ __global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Pla
       v = vn;
     }
 
-    if (ns == 1) {
-      // the whole bucket is here: list its occupied slots, reserve their
-      // output rows with one atomic, then write them 32 at a time
-      const SmemAccs A{T.tb, &sl};
-      uint32_t total = 0;
-      for (uint32_t s0 = 0; s0 <= T.S; s0 += 32) {
-        const uint32_t s = s0 + lane;
-        bool occ         = false;
-        uint64_t kw[NW];
-        if (s < T.S) {
-#pragma unroll
-          for (int w = 0; w < NW; ++w) kw[w] = keys[s * NW + w];
-          occ = !key_is_empty<NW>(kw);
-        } else if (s == T.S) {
-          occ = special;
-        }
-        const uint32_t bal = __ballot_sync(kFull, occ);
-        if (occ) scratch[total + __popc(bal & lanemask_lt(lane))] = s;
-        total += __popc(bal);
-      }
-      __syncwarp();
-      if (total > 0) {
-        unsigned long long ob = 0;
-        if (lane == 0) ob = atomicAdd(pp.out_counter, static_cast<unsigned long long>(total));
-        ob = __shfl_sync(kFull, ob, 0);
-        for (uint32_t g0 = 0; g0 < total; g0 += 32) {
-          const bool active = g0 + lane < total;
-          const uint32_t ss = active ? scratch[g0 + lane] : 0;
-          uint64_t k2[2]    = {0, 0};
-          if (active) {
-            if (ss == T.S) {
-              k2[0] = k2[1] = kEmptyWord;
-            } else {
-#pragma unroll
-              for (int w = 0; w < NW; ++w) k2[w] = keys[ss * NW + w];
-            }
-          }
-          warp_write_groups(plan, op, A, active, ss, k2, static_cast<int64_t>(ob + g0), lane);
-        }
-      }
-      __syncwarp();
-    } else {
-      // a slice of a large bucket: merge into the bucket's region table
+    {
       const Level<Shared> L{static_cast<uint32_t>(__cvta_generic_to_shared(T.tb)), &sl};
       const uint64_t rbase = static_cast<uint64_t>(pp.region[b]) * pp.region_slots;
       for (uint32_t s = lane; s <= T.S; s += 32) {
@@ -264,6 +415,8 @@ template <int NW>
 __global__ void k_part_region_finalize(const __grid_constant__ Plan plan, const __grid_constant__ PartPlan pp, const __grid_constant__ TableRef t, const __grid_constant__ OutPlan op)
 {
   __shared__ uint32_t scratch_all[8][32];
+  __shared__ uint32_t s_nulls[kNullSlots];
+  cta_nulls_zero(s_nulls);
   const int lane         = threadIdx.x & 31;
   uint32_t* scratch      = scratch_all[(threadIdx.x >> 5) & 7];
   const uint64_t nslots  = t.cap + 1;
@@ -300,9 +453,10 @@ __global__ void k_part_region_finalize(const __grid_constant__ Plan plan, const 
         for (int w = 0; w < NW; ++w) k2[w] = t.keys[ss * NW + w];
       }
     }
-    warp_write_groups(plan, op, A, active, ss, k2, static_cast<int64_t>(ob), lane);
+    warp_write_groups(plan, op, A, active, ss, k2, static_cast<int64_t>(ob), lane, s_nulls);
     __syncwarp();
   }
+  cta_nulls_flush(s_nulls, op.null_counts);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -363,36 +517,81 @@ cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, co
 namespace {
 template <int NW, int NCH>
 cudaError_t launch_part_agg_impl(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
-                                 const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st)
+                                 const SmemLayout& sl, int num_sms, cudaStream_t st)
 {
   const int block   = 256;
   const int warps   = block / 32;
-  const size_t smem = static_cast<size_t>(sl.total) * warps + warps * (sl.slots + 32) * sizeof(uint32_t);
+  const size_t smem = static_cast<size_t>(sl.total) * warps;
   cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_part_agg<NW, NCH>), smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_agg<NW, NCH>, block, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  k_part_agg<NW, NCH><<<num_sms * per_sm, block, smem, st>>>(p, pp, in, t, sl, op);
+  k_part_agg<NW, NCH><<<num_sms * per_sm, block, smem, st>>>(p, pp, in, t, sl);
   return cudaGetLastError();
 }
 
 template <int NW>
 cudaError_t launch_part_agg_nw(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
-                               const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st)
+                               const SmemLayout& sl, int num_sms, cudaStream_t st)
 {
-  if (p.nchan <= 2) return launch_part_agg_impl<NW, 2>(p, pp, in, t, sl, op, num_sms, st);
-  if (p.nchan <= 4) return launch_part_agg_impl<NW, 4>(p, pp, in, t, sl, op, num_sms, st);
-  return launch_part_agg_impl<NW, kMaxChannels>(p, pp, in, t, sl, op, num_sms, st);
+  if (p.nchan <= 2) return launch_part_agg_impl<NW, 2>(p, pp, in, t, sl, num_sms, st);
+  if (p.nchan <= 4) return launch_part_agg_impl<NW, 4>(p, pp, in, t, sl, num_sms, st);
+  return launch_part_agg_impl<NW, kMaxChannels>(p, pp, in, t, sl, num_sms, st);
+}
+
+// Shared memory of k_part_ranked: eight warps per CTA, each with its table,
+// list and as many rank records as fit a quarter of the SM's shared memory
+// per CTA (four CTAs per SM); buckets with more rows keep their records in
+// global memory.
+template <int NW>
+cudaError_t launch_part_ranked_nw(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
+                                  uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st)
+{
+  const int block = 256;
+  const int warps = block / 32;
+  int dev = 0, per_sm_bytes = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&per_sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+    return e;
+  SmemLayout sl{};
+  sl.slots    = S;
+  sl.keys_off = 0;
+  sl.rows_off = (S + 1) * NW * 8;
+  sl.total    = (sl.rows_off + (S + 1) * 4 + 15) & ~15u;
+  RankedLayout rl{};
+  rl.scratch_off = sl.total;
+  rl.rec_off     = (rl.scratch_off + (S + 32) * 4 + 15) & ~15u;
+  // per CTA: a quarter of the SM less 1 KB of reserved and static memory
+  const int64_t cta_bytes = per_sm_bytes / 4 - 2048;
+  const int64_t rec_bytes = cta_bytes / warps - rl.rec_off;
+  rl.rec_rows = rec_bytes > 0 ? static_cast<uint32_t>(std::min<int64_t>(rec_bytes / 4, pp.slice_rows)) & ~31u : 0u;
+  rl.stride   = (rl.rec_off + rl.rec_rows * 4 + 15) & ~15u;
+  const size_t smem = static_cast<size_t>(rl.stride) * warps;
+  if ((e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_part_ranked<NW>), smem)) != cudaSuccess) return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_ranked<NW>, block, smem)) != cudaSuccess)
+    return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  k_part_ranked<NW><<<num_sms * per_sm, block, smem, st>>>(p, pp, in, sorted, sl, rl, op);
+  return cudaGetLastError();
 }
 }  // namespace
 
-cudaError_t launch_part_agg(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
-                            const SmemLayout& sl, const OutPlan& op, int num_sms, cudaStream_t st)
+cudaError_t launch_part_ranked(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
+                               uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st)
 {
-  return p.key.nwords == 1 ? launch_part_agg_nw<1>(p, pp, in, t, sl, op, num_sms, st)
-                           : launch_part_agg_nw<2>(p, pp, in, t, sl, op, num_sms, st);
+  return p.key.nwords == 1 ? launch_part_ranked_nw<1>(p, pp, in, sorted, S, op, num_sms, st)
+                           : launch_part_ranked_nw<2>(p, pp, in, sorted, S, op, num_sms, st);
+}
+
+cudaError_t launch_part_agg(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
+                            const SmemLayout& sl, int num_sms, cudaStream_t st)
+{
+  return p.key.nwords == 1 ? launch_part_agg_nw<1>(p, pp, in, t, sl, num_sms, st)
+                           : launch_part_agg_nw<2>(p, pp, in, t, sl, num_sms, st);
 }
 
 cudaError_t launch_part_region_finalize(const Plan& p, const PartPlan& pp, const TableRef& t, const OutPlan& op,

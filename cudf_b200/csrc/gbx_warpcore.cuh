@@ -169,6 +169,19 @@ struct WarpTable {
     __syncwarp();
   }
   __device__ __forceinline__ void reset(const AccLayout& al, int lane) const { init(al, lane); }
+  // Empties the keys and zeroes the row counts only (a table used to rank
+  // rows by group, whose accumulators are not read).
+  __device__ __forceinline__ void reset_keys(int lane) const
+  {
+    uint64_t* kk = keys();
+    uint32_t* rr = rows();
+    for (uint32_t s = lane; s <= S; s += 32) {
+#pragma unroll
+      for (int w = 0; w < NW; ++w) kk[s * NW + w] = kEmptyWord;
+      rr[s] = 0;
+    }
+    __syncwarp();
+  }
 };
 
 enum RowState { ST_DONE = 0, ST_PROBING = 1, ST_INSERT = 2, ST_FOUND = 3, ST_SPILL = 4 };
@@ -311,15 +324,105 @@ __device__ __forceinline__ void store_bits(void* p, int64_t i, int width, uint64
   }
 }
 
-// Final value and validity of output column `oc` for one group
-// (hash_compound_agg_finalizer, hash/groupby.cu:183-349).
+// One group's accumulators of one channel as finalize_from reads them:
+// a slot of a table level ...
 template <class Accs>
-__device__ __forceinline__ uint64_t finalize_value(const Plan& plan, const OutCol& oc, const Accs& A, uint64_t s,
-                                                   bool& valid)
+struct SlotView {
+  const Accs& A;
+  const Channel& ch;
+  uint64_t s;
+  __device__ __forceinline__ uint32_t rows() const { return A.rows(s); }
+  __device__ __forceinline__ uint32_t cnt() const
+  {
+    return (ch.a_cnt >= 0) ? static_cast<uint32_t>(A.acc(ch.a_cnt, s, 4)) : rows();
+  }
+  __device__ __forceinline__ uint64_t sum() const { return A.acc(ch.a_sum, s, 8); }
+  __device__ __forceinline__ uint64_t sq() const { return A.acc(ch.a_sq, s, 8); }
+  __device__ __forceinline__ uint64_t prod() const { return A.acc(ch.a_prod, s, 8); }
+  __device__ __forceinline__ uint64_t minmax(bool mn) const
+  {
+    return A.acc(mn ? ch.a_min : ch.a_max, s, minmax_is64(ch.ptype) ? 8 : 4);
+  }
+  __device__ __forceinline__ uint64_t shift() const { return A.acc(ch.a_k, s, 8); }
+  __device__ __forceinline__ uint64_t s2() const { return A.acc(ch.a_s2, s, 8); }
+};
+
+// ... or one thread's registers (a group folded by a single lane).  Every
+// field holds the same encoding as the table accumulator of that role.
+struct ChanAcc {
+  uint32_t cnt;   // valid values
+  uint64_t mn;    // enc_minmax(., true) of the least value
+  uint64_t mx;    // enc_minmax(., false) of the greatest value
+  uint64_t sum;   // wrapping integer sum or double bits
+  uint64_t sq;    // sum of squares, same encoding as sum
+  uint64_t prod;  // product, same encoding as sum
+  uint64_t k;     // VAR shift (first non-NaN value) or kShiftUnset
+  double s2;      // sum of (x - K)^2
+};
+
+struct RegView {
+  const ChanAcc& a;
+  uint32_t nrows;
+  __device__ __forceinline__ uint32_t rows() const { return nrows; }
+  __device__ __forceinline__ uint32_t cnt() const { return a.cnt; }
+  __device__ __forceinline__ uint64_t sum() const { return a.sum; }
+  __device__ __forceinline__ uint64_t sq() const { return a.sq; }
+  __device__ __forceinline__ uint64_t prod() const { return a.prod; }
+  __device__ __forceinline__ uint64_t minmax(bool mn) const { return mn ? a.mn : a.mx; }
+  __device__ __forceinline__ uint64_t shift() const { return a.k; }
+  __device__ __forceinline__ uint64_t s2() const { return static_cast<uint64_t>(__double_as_longlong(a.s2)); }
+};
+
+__device__ __forceinline__ void chan_acc_init(ChanAcc& a)
 {
-  const Channel& ch = plan.chan[oc.chan];
-  const uint32_t rows = A.rows(s);
-  const uint32_t cnt  = (ch.a_cnt >= 0) ? static_cast<uint32_t>(A.acc(ch.a_cnt, s, 4)) : rows;
+  a.cnt  = 0;
+  a.mn   = ~0ULL;
+  a.mx   = 0;
+  a.sum  = 0;
+  a.sq   = 0;
+  a.prod = 0;
+  a.k    = kShiftUnset;
+  a.s2   = 0.0;
+}
+
+// Folds one valid value (raw bits) into a channel's registers, with the
+// arithmetic of apply_row (integers wrap, floats in double, the shift K is
+// the first non-NaN value).  Products start from 1 on the first value.
+__device__ __forceinline__ void chan_acc_add(const Channel& ch, ChanAcc& a, uint64_t b)
+{
+  const bool first = a.cnt == 0;
+  a.cnt += 1;
+  if (ch.a_min >= 0) a.mn = min(a.mn, enc_minmax(b, ch.ptype, true));
+  if (ch.a_max >= 0) a.mx = max(a.mx, enc_minmax(b, ch.ptype, false));
+  double xf;
+  if (ch.is_float) {
+    xf = as_f64(b, ch.ptype);
+    if (ch.a_sum >= 0) a.sum = static_cast<uint64_t>(__double_as_longlong(__longlong_as_double(static_cast<long long>(a.sum)) + xf));
+    if (ch.a_sq >= 0) a.sq = static_cast<uint64_t>(__double_as_longlong(__longlong_as_double(static_cast<long long>(a.sq)) + xf * xf));
+    if (ch.a_prod >= 0)
+      a.prod = static_cast<uint64_t>(__double_as_longlong(first ? xf : __longlong_as_double(static_cast<long long>(a.prod)) * xf));
+  } else {
+    const int64_t x = as_i64(b, ch.ptype);
+    if (ch.a_sum >= 0) a.sum += static_cast<uint64_t>(x);
+    if (ch.a_sq >= 0) a.sq += static_cast<uint64_t>(x) * static_cast<uint64_t>(x);
+    if (ch.a_prod >= 0) a.prod = first ? static_cast<uint64_t>(x) : a.prod * static_cast<uint64_t>(x);
+    xf = (ch.ptype == P_U64) ? static_cast<double>(static_cast<uint64_t>(x)) : static_cast<double>(x);
+  }
+  if (ch.a_k >= 0) {
+    if (a.k == kShiftUnset && !(xf != xf)) a.k = static_cast<uint64_t>(__double_as_longlong(xf));
+    const double d = xf - __longlong_as_double(static_cast<long long>(a.k));
+    a.s2 += d * d;
+  }
+}
+
+// Final value and validity of output column `oc` of one group from its
+// channel's accumulators (hash_compound_agg_finalizer,
+// hash/groupby.cu:183-349).
+template <class View>
+__device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCol& oc, const View& V, bool& valid)
+{
+  const uint32_t rows = V.rows();
+  const uint32_t cnt  = V.cnt();
   valid               = cnt > 0;
   uint64_t vbits      = 0;
   switch (oc.kind) {
@@ -328,8 +431,7 @@ __device__ __forceinline__ uint64_t finalize_value(const Plan& plan, const OutCo
     case GBX_AGG_SUM:
     case GBX_AGG_SUM_OF_SQUARES:
     case GBX_AGG_PRODUCT: {
-      int a        = (oc.kind == GBX_AGG_SUM) ? ch.a_sum : (oc.kind == GBX_AGG_PRODUCT ? ch.a_prod : ch.a_sq);
-      uint64_t raw = A.acc(a, s, 8);
+      uint64_t raw = (oc.kind == GBX_AGG_SUM) ? V.sum() : (oc.kind == GBX_AGG_PRODUCT ? V.prod() : V.sq());
       if (ch.is_float) {
         double x = __longlong_as_double(static_cast<long long>(raw));
         vbits    = (oc.out_ptype == P_F32) ? __float_as_uint(static_cast<float>(x))
@@ -341,15 +443,13 @@ __device__ __forceinline__ uint64_t finalize_value(const Plan& plan, const OutCo
     }
     case GBX_AGG_MIN:
     case GBX_AGG_MAX: {
-      bool mn      = oc.kind == GBX_AGG_MIN;
-      int a        = mn ? ch.a_min : ch.a_max;
-      uint64_t raw = A.acc(a, s, minmax_is64(ch.ptype) ? 8 : 4);
-      vbits        = dec_minmax(raw, ch.ptype, mn);
+      bool mn = oc.kind == GBX_AGG_MIN;
+      vbits   = dec_minmax(V.minmax(mn), ch.ptype, mn);
       break;
     }
     case GBX_AGG_MEAN: {
       if (!valid) break;
-      uint64_t raw = A.acc(ch.a_sum, s, 8);
+      uint64_t raw = V.sum();
       if (oc.out_ptype == P_F64) {
         // integer SUMs are INT64 (target_type): the mean divides the signed sum,
         // as binary_operation(DIV) does on it (hash/groupby.cu:298-304)
@@ -372,14 +472,14 @@ __device__ __forceinline__ uint64_t finalize_value(const Plan& plan, const OutCo
         valid = false;
         break;
       }
-      uint64_t kb = A.acc(ch.a_k, s, 8);
-      double s2   = __longlong_as_double(static_cast<long long>(A.acc(ch.a_s2, s, 8)));
+      uint64_t kb = V.shift();
+      double s2   = __longlong_as_double(static_cast<long long>(V.s2()));
       double var;
       if (kb == kShiftUnset) {
         var = s2;  // NaN inputs only
       } else {
         double K     = __longlong_as_double(static_cast<long long>(kb));
-        uint64_t raw = A.acc(ch.a_sum, s, 8);
+        uint64_t raw = V.sum();
         double sum   = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
                                    : (ch.ptype == P_U64 ? static_cast<double>(raw)
                                                         : static_cast<double>(static_cast<int64_t>(raw)));
@@ -396,6 +496,15 @@ __device__ __forceinline__ uint64_t finalize_value(const Plan& plan, const OutCo
     default: break;
   }
   return valid ? vbits : 0;
+}
+
+// finalize_from on slot `s` of a table level.
+template <class Accs>
+__device__ __forceinline__ uint64_t finalize_value(const Plan& plan, const OutCol& oc, const Accs& A, uint64_t s,
+                                                   bool& valid)
+{
+  const Channel& ch = plan.chan[oc.chan];
+  return finalize_from(ch, oc, SlotView<Accs>{A, ch, s}, valid);
 }
 
 // Decoded key column `c` of a packed key; `valid` false for a null key.
@@ -426,16 +535,46 @@ __device__ __forceinline__ void or_mask_bits(uint32_t* mask, int64_t base, uint3
   }
 }
 
+// Null counts of the output columns, indexed like OutPlan::null_counts:
+// either straight into the global counters or into per-CTA shared-memory
+// counters that the kernel adds to them once at its end (many warps adding
+// to the same few global words serialise on them).
+struct NullSink {
+  unsigned long long* global;
+  uint32_t* cta;  // shared memory, or nullptr
+  __device__ __forceinline__ void add(int i, uint32_t v) const
+  {
+    if (cta != nullptr) atomicAdd(cta + i, v);
+    else atomicAdd(global + i, static_cast<unsigned long long>(v));
+  }
+};
+
+constexpr int kNullSlots = kMaxKeyCols + kMaxOut;
+
+// Per-CTA null counters: zeroed before the CTA's first output, flushed by
+// every thread of the block after its last (both include __syncthreads).
+__device__ __forceinline__ void cta_nulls_zero(uint32_t* c)
+{
+  for (int i = threadIdx.x; i < kNullSlots; i += blockDim.x) c[i] = 0;
+  __syncthreads();
+}
+__device__ __forceinline__ void cta_nulls_flush(const uint32_t* c, unsigned long long* global)
+{
+  __syncthreads();
+  for (int i = threadIdx.x; i < kNullSlots; i += blockDim.x)
+    if (c[i] != 0) atomicAdd(global + i, static_cast<unsigned long long>(c[i]));
+}
+
 // Warp-cooperative output of up to 32 groups: lane i writes output row
 // base + i from slot `s` when `active` (active lanes form a prefix).  Keys
 // are decoded, every result finalised; validity bits are or-ed in one word
 // operation per warp and null counts added once per warp.
-template <class Accs>
-__device__ __forceinline__ void warp_write_groups(const Plan& plan, const OutPlan& op, const Accs& A, bool active,
-                                                  uint64_t s, const uint64_t (&k)[2], int64_t base, int lane)
+// The key columns of such a batch of output rows.
+__device__ __forceinline__ void warp_write_keys(const Plan& plan, const OutPlan& op, bool active,
+                                                const uint64_t (&k)[2], int64_t base, int lane, uint32_t act,
+                                                const NullSink& sink)
 {
-  const uint32_t act = __ballot_sync(kFull, active);
-  const int64_t g    = base + lane;
+  const int64_t g = base + lane;
   for (int c = 0; c < plan.key.ncols; ++c) {
     const KeyCol& kc = plan.key.cols[c];
     bool valid       = false;
@@ -446,10 +585,21 @@ __device__ __forceinline__ void warp_write_groups(const Plan& plan, const OutPla
       if (lane == 0) {
         or_mask_bits(op.key_mask[c], base, bits);
         const uint32_t nulls = __popc(act & ~bits);
-        if (nulls) atomicAdd(op.null_counts + c, static_cast<unsigned long long>(nulls));
+        if (nulls) sink.add(c, nulls);
       }
     }
   }
+}
+
+template <class Accs>
+__device__ __forceinline__ void warp_write_groups(const Plan& plan, const OutPlan& op, const Accs& A, bool active,
+                                                  uint64_t s, const uint64_t (&k)[2], int64_t base, int lane,
+                                                  uint32_t* cta_nulls = nullptr)
+{
+  const NullSink sink{op.null_counts, cta_nulls};
+  const uint32_t act = __ballot_sync(kFull, active);
+  const int64_t g    = base + lane;
+  warp_write_keys(plan, op, active, k, base, lane, act, sink);
   for (int o = 0; o < op.nout; ++o) {
     const OutCol& oc = op.out[o];
     bool valid       = false;
@@ -460,7 +610,34 @@ __device__ __forceinline__ void warp_write_groups(const Plan& plan, const OutPla
       if (lane == 0) {
         or_mask_bits(oc.mask, base, bits);
         const uint32_t nulls = __popc(act & ~bits);
-        if (nulls) atomicAdd(op.null_counts + kMaxKeyCols + o, static_cast<unsigned long long>(nulls));
+        if (nulls) sink.add(kMaxKeyCols + o, nulls);
+      }
+    }
+  }
+}
+
+// The outputs of channel c for a batch of groups folded in registers: lane
+// i's group (output row base + i when `active`) has `nrows` rows and channel
+// accumulators A.
+__device__ __forceinline__ void warp_write_chan(const Plan& plan, const OutPlan& op, bool active, uint32_t nrows,
+                                                const ChanAcc& A, int c, int64_t base, int lane, uint32_t act,
+                                                const NullSink& sink)
+{
+  const Channel& ch = plan.chan[c];
+  const RegView V{A, nrows};
+  const int64_t g   = base + lane;
+  for (int o = 0; o < op.nout; ++o) {
+    const OutCol& oc = op.out[o];
+    if (oc.chan != c) continue;
+    bool valid = false;
+    uint64_t v = active ? finalize_from(ch, oc, V, valid) : 0;
+    if (active) store_bits(oc.data, g, oc.out_width, v);
+    if (oc.mask != nullptr) {
+      const uint32_t bits = __ballot_sync(kFull, active && valid);
+      if (lane == 0) {
+        or_mask_bits(oc.mask, base, bits);
+        const uint32_t nulls = __popc(act & ~bits);
+        if (nulls) sink.add(kMaxKeyCols + o, nulls);
       }
     }
   }

@@ -278,6 +278,35 @@ def test_partitioned_bucket_and_slice_modes(card):
     assert got["stats"]["strategy"] == Strategy.PARTITIONED
 
 
+@pytest.mark.parametrize("card", [3_000, 200_000])
+def test_partitioned_every_kind_and_type(card):
+    """Partitioned strategy on every aggregation kind and value type, eight
+    channels (several register-fold passes per group), a dictionary value
+    column and durations, with ~1.5 and ~100 rows per group."""
+    rng = np.random.default_rng(24 + card)
+    n = 300_000
+    k = rng.integers(0, card, size=n).astype(np.int64)
+    k[::97] = -1  # the all-ones key
+    every = ALL6 + [(Kind.SUM_OF_SQUARES, 0), (Kind.COUNT_ALL, 0), (Kind.STD, 0), (Kind.VARIANCE, 0)]
+    reqs = []
+    for tid, dt in [(TypeId.INT8, np.int8), (TypeId.UINT16, np.uint16), (TypeId.UINT64, np.uint64)]:
+        info = np.iinfo(dt)
+        v = rng.integers(info.min, info.max, size=n, endpoint=True, dtype=dt)
+        if tid == TypeId.UINT64:
+            v = v >> np.uint64(24)  # per-group sums below 2^63, as in test_value_types
+        reqs.append((hc(v, rng.random(n) > 0.2, type_id=tid), every))
+    reqs.append((hc(rng.standard_normal(n).astype(np.float32), rng.random(n) > 0.1), every))
+    reqs.append((hc(rng.integers(-3, 4, size=n).astype(np.int64)), [(Kind.PRODUCT, 0), (Kind.SUM, 0)]))
+    reqs.append((hc(rng.uniform(0.9, 1.1, size=n)), [(Kind.PRODUCT, 0), (Kind.MIN, 0), (Kind.MAX, 0)]))
+    dict_vals = np.array([5, -3, 17, 1 << 40, 0, -9], dtype=np.int64)
+    idx = rng.integers(0, len(dict_vals), size=n).astype(np.int32)
+    reqs.append((hc(idx, rng.random(n) > 0.05, dict_keys=hc(dict_vals)), ALL6))
+    d = rng.integers(-10**6, 10**6, size=n).astype(np.int64)
+    reqs.append((hc(d, type_id=TypeId.DURATION_SECONDS), [(Kind.SUM, 0), (Kind.MEAN, 0), (Kind.MAX, 0)]))
+    got, _ = T.assert_parity([hc(k)], reqs, strategy=Strategy.PARTITIONED)
+    assert got["stats"]["strategy"] == Strategy.PARTITIONED
+
+
 def test_partitioned_skewed_keys():
     """Zipf-skewed composite keys: one bucket holds a large share of the rows."""
     d = W.plain_200m(n=1_500_000, ranks=50_000)
