@@ -933,6 +933,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       uint32_t* roffsets = nullptr;
       void* rtemp        = nullptr;
       size_t rtemp_bytes = 0;
+      uint2* group_runs  = nullptr;  // (first sorted row, rows) per output row
       // outputs sized for the upper bound (every row its own group): the group
       // count is only known once the buckets have been written out
       OutPlan pop    = build_outputs(call.n);
@@ -1019,9 +1020,11 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         // records of buckets too large for shared memory
         pp.rank_rec       = const_cast<uint32_t*>(reinterpret_cast<const uint32_t*>(tbufs.keys[0]));
         pp.bucket_counter = ctl + 31;
+        if (group_runs == nullptr) group_runs = static_cast<uint2*>(scratch.get(static_cast<size_t>(call.n) * 8));
+        pp.group_run = group_runs;
         timer.mark(2);
         GBX_CUDA(launch_part_ranked(plan, pp, pbufs, tbufs, S, pop, call.dev.num_sms, s));
-        launches += 1;
+        launches += 2;
         if (h_items > 0) {
           GBX_CUDA(launch_part_agg(plan, pp, pbufs, t2, sl, call.dev.num_sms, s));
           timer.mark(3);

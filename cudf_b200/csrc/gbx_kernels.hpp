@@ -83,6 +83,9 @@ struct PartPlan {
   // do not fit the warp's shared memory ranks them here (slot << 16 | rank
   // within the slot; slice_rows < 65536)
   uint32_t* rank_rec;
+  // [n], indexed by output row: (first row, row count) of a whole bucket's
+  // group in the group-ordered copies
+  uint2* group_run;
 };
 
 cudaError_t launch_part_hist(const KeyPlan& kp, int64_t n, const PartPlan& pp, int num_sms, cudaStream_t st);
@@ -111,7 +114,9 @@ cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t
                               size_t temp_bytes, int32_t* status, bool hist0_done, cudaStream_t st);
 // Aggregates every bucket of at most slice_rows rows (S-slot warp tables)
 // and writes its groups to `op`, the rows permuted into group order in
-// `sorted` (the layout of `in`, overwritten; its key words hold rank records).
+// `sorted` (the layout of `in`, overwritten; its key words hold rank
+// records) and each group's run listed in pp.group_run (two launches:
+// grouping, then one thread per group).
 cudaError_t launch_part_ranked(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
                                uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st);
 // Aggregates the slices of the larger buckets (item_start[P] of them, > 0)

@@ -40,18 +40,6 @@ __device__ __forceinline__ uint32_t counter_of(uint32_t b, int64_t r, const Part
 
 constexpr uint32_t kNoRank = 0xffffffffu;
 
-// Element i of a buffer that this kernel also writes (a plain load: the
-// read-only path is not coherent with the kernel's own stores).
-__device__ __forceinline__ uint64_t load_bits_rw(const void* p, int64_t i, int width)
-{
-  switch (width) {
-    case 1: return reinterpret_cast<const uint8_t*>(p)[i];
-    case 2: return reinterpret_cast<const uint16_t*>(p)[i];
-    case 4: return reinterpret_cast<const uint32_t*>(p)[i];
-    default: return reinterpret_cast<const uint64_t*>(p)[i];
-  }
-}
-
 // One whole bucket, rows [r0, r1), aggregated by one warp in four steps:
 //   1. rank: each row finds or inserts its key in the warp's table (keys and
 //      row counts only) and takes the next rank of its slot, lanes of a batch
@@ -61,15 +49,16 @@ __device__ __forceinline__ uint64_t load_bits_rw(const void* p, int64_t i, int w
 //   3. permute: each row's values move to r0 + position + rank of `sorted`
 //      (the same rows of a second set of copies), so that every group's rows
 //      are contiguous;
-//   4. fold: lane i takes the i-th listed group of a batch of 32 and folds
-//      its run of rows into registers (ChanAcc), one channel at a time, then
-//      writes that channel's outputs; the keys come from the table.
-// No accumulator is read or written in shared memory and no slot has more
-// than one writer.  Folding one channel at a time keeps a single copy of the
-// accumulate and finalise code in the loop, so the kernel's hot code stays
-// within the instruction cache.  The rank records live in the warp's
-// shared memory (rec_smem, rec_rows entries) when the bucket fits, else in
-// pp.rank_rec.
+//   4. emit: the bucket's groups get consecutive output rows; each group's
+//      key columns and its run (first sorted row, row count) are written
+//      there.
+// The values are folded afterwards by k_part_fold, one thread per output
+// row.  No accumulator lives in shared memory and no slot has more than one
+// writer.  Keeping the generic accumulate/finalise code out of this kernel
+// keeps its hot code within the instruction cache (a single kernel that also
+// folded ran 2-2.5x slower from instruction-cache misses on B200).  The rank
+// records live in the warp's shared memory (rec_smem, rec_rows entries) when
+// the bucket fits, else in pp.rank_rec.
 template <int NW>
 __device__ __forceinline__ void part_bucket_ranked(const Plan& plan, const PartPlan& pp, const PartBufs& in,
                                                    const PartBufs& sorted, const WarpTable<NW>& T,
@@ -145,36 +134,72 @@ __device__ __forceinline__ void part_bucket_ranked(const Plan& plan, const PartP
   __syncwarp();  // orders the warp's stores before its loads below
   if (ngroups == 0) return;
 
-  // 4. fold and write
+  // 4. emit: output rows reserved with one atomic; each group's key columns
+  // and (first sorted row, row count) at its output row
   unsigned long long ob = 0;
   if (lane == 0) ob = atomicAdd(pp.out_counter, static_cast<unsigned long long>(ngroups));
   ob                   = __shfl_sync(kFull, ob, 0);
   const uint64_t* keys = T.keys();
   const NullSink sink{op.null_counts, cta_nulls};
   for (uint32_t g0 = 0; g0 < ngroups; g0 += 32) {
-    const bool active   = g0 + lane < ngroups;
-    const uint32_t ent  = active ? scratch[g0 + lane] : 0u;
-    const uint32_t ss   = ent & 0xffffu;
-    const uint32_t gc   = ent >> 16;
-    const int64_t first = r0 + (active ? cnt[ss] : 0u);
-    const int64_t base  = static_cast<int64_t>(ob + g0);
-    const uint32_t act  = __ballot_sync(kFull, active);
-    uint64_t k2[2]      = {0, 0};
+    const int64_t base = static_cast<int64_t>(ob + g0);
+    const bool active  = g0 + lane < ngroups;
+    const uint32_t ent = active ? scratch[g0 + lane] : 0u;
+    const uint32_t ss  = ent & 0xffffu;
+    const uint32_t act = __ballot_sync(kFull, active);
+    uint64_t k2[2]     = {0, 0};
     if (active) {
 #pragma unroll
       for (int w = 0; w < NW; ++w) k2[w] = keys[ss * NW + w];
       if (ss == T.S) k2[0] = k2[1] = kEmptyWord;
+      pp.group_run[base + lane] = make_uint2(static_cast<uint32_t>(r0) + cnt[ss], ent >> 16);
     }
     warp_write_keys(plan, op, active, k2, base, lane, act, sink);
+  }
+}
+
+// The value columns of the groups that part_bucket_ranked emitted (output
+// rows [0, *pp.out_counter) when it ran first): one thread per output row
+// folds its group's run of sorted rows into registers (ChanAcc), one channel
+// at a time, and writes that channel's outputs.  Warps own aligned 32-row
+// runs of output rows, so validity words are stored whole.
+__device__ __forceinline__ void fold_group_rows(const Plan& plan, const PartPlan& pp, const PartBufs& sorted,
+                                                const OutPlan& op, int64_t G, uint32_t* cta_nulls)
+{
+  const int lane         = threadIdx.x & 31;
+  const int64_t wstride  = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < G;
+       base += wstride) {
+    const int64_t g     = base + lane;
+    const bool active   = g < G;
+    const uint2 run     = active ? pp.group_run[g] : make_uint2(0u, 0u);
+    const uint32_t act  = __ballot_sync(kFull, active);
     for (int c = 0; c < plan.nchan; ++c) {
+      const Channel& ch = plan.chan[c];
       const PartCol& pc = sorted.col[c];
       ChanAcc A;
       chan_acc_init(A);
-      for (uint32_t j = 0; j < gc; ++j) {
-        const uint64_t b = load_bits_rw(pc.vals, first + j, pc.width);
-        if (pc.valid == nullptr || pc.valid[first + j] != 0) chan_acc_add(plan.chan[c], A, b);
+      for (uint32_t j = 0; j < run.y; ++j) {
+        const int64_t r  = static_cast<int64_t>(run.x) + j;
+        const uint64_t b = load_bits(pc.vals, r, pc.width);
+        if (pc.valid == nullptr || __ldg(pc.valid + r) != 0) chan_acc_add(ch, A, b);
       }
-      warp_write_chan(plan, op, active, gc, A, c, base, lane, act, sink);
+      const RegView V{A, run.y};
+      for (int o = 0; o < op.nout; ++o) {
+        const OutCol& oc = op.out[o];
+        if (oc.chan != c) continue;
+        bool valid = false;
+        const uint64_t v = active ? finalize_from(ch, oc, V, valid) : 0;
+        if (active) store_bits(oc.data, g, oc.out_width, v);
+        if (oc.mask != nullptr) {
+          const uint32_t bits = __ballot_sync(kFull, active && valid);
+          if (lane == 0) {
+            oc.mask[base >> 5] = bits;
+            const uint32_t nulls = __popc(act & ~bits);
+            if (nulls != 0) atomicAdd(cta_nulls + kMaxKeyCols + o, nulls);
+          }
+        }
+      }
     }
   }
 }
@@ -282,8 +307,10 @@ struct RankedLayout {
 // Whole buckets, claimed a few at a time, each through part_bucket_ranked.
 // `sl` describes the table part of each warp's shared memory (keys_off,
 // rows_off); it has no accumulator arrays.
+constexpr int kRankedCtasPerSm = 4;
+
 template <int NW>
-__global__ void __launch_bounds__(256, 4) k_part_ranked(const __grid_constant__ Plan plan,
+__global__ void __launch_bounds__(256, kRankedCtasPerSm) k_part_ranked(const __grid_constant__ Plan plan,
                                                        const __grid_constant__ PartPlan pp,
                                                        const __grid_constant__ PartBufs in,
                                                        const __grid_constant__ PartBufs sorted,
@@ -320,6 +347,19 @@ __global__ void __launch_bounds__(256, 4) k_part_ranked(const __grid_constant__ 
                            pp.status);
     __syncwarp();
   }
+  cta_nulls_flush(s_nulls, op.null_counts);
+}
+
+// Value outputs of the groups k_part_ranked emitted (fold_group_rows);
+// launched right after it, before any slice adds output rows.
+__global__ void __launch_bounds__(256) k_part_fold(const __grid_constant__ Plan plan,
+                                                   const __grid_constant__ PartPlan pp,
+                                                   const __grid_constant__ PartBufs sorted,
+                                                   const __grid_constant__ OutPlan op)
+{
+  __shared__ uint32_t s_nulls[kNullSlots];
+  cta_nulls_zero(s_nulls);
+  fold_group_rows(plan, pp, sorted, op, static_cast<int64_t>(*pp.out_counter), s_nulls);
   cta_nulls_flush(s_nulls, op.null_counts);
 }
 
@@ -542,9 +582,9 @@ cudaError_t launch_part_agg_nw(const Plan& p, const PartPlan& pp, const PartBufs
 }
 
 // Shared memory of k_part_ranked: eight warps per CTA, each with its table,
-// list and as many rank records as fit a quarter of the SM's shared memory
-// per CTA (four CTAs per SM); buckets with more rows keep their records in
-// global memory.
+// list and as many rank records as fit the CTA's share of the SM's shared
+// memory (kRankedCtasPerSm CTAs per SM); buckets with more rows keep their
+// records in global memory.
 template <int NW>
 cudaError_t launch_part_ranked_nw(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
                                   uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st)
@@ -564,8 +604,8 @@ cudaError_t launch_part_ranked_nw(const Plan& p, const PartPlan& pp, const PartB
   RankedLayout rl{};
   rl.scratch_off = sl.total;
   rl.rec_off     = (rl.scratch_off + (S + 32) * 4 + 15) & ~15u;
-  // per CTA: a quarter of the SM less 1 KB of reserved and static memory
-  const int64_t cta_bytes = per_sm_bytes / 4 - 2048;
+  // per CTA: its share of the SM less reserved and static memory
+  const int64_t cta_bytes = per_sm_bytes / kRankedCtasPerSm - 2048;
   const int64_t rec_bytes = cta_bytes / warps - rl.rec_off;
   rl.rec_rows = rec_bytes > 0 ? static_cast<uint32_t>(std::min<int64_t>(rec_bytes / 4, pp.slice_rows)) & ~31u : 0u;
   rl.stride   = (rl.rec_off + rl.rec_rows * 4 + 15) & ~15u;
@@ -576,6 +616,9 @@ cudaError_t launch_part_ranked_nw(const Plan& p, const PartPlan& pp, const PartB
     return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   k_part_ranked<NW><<<num_sms * per_sm, block, smem, st>>>(p, pp, in, sorted, sl, rl, op);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_fold, block, 0)) != cudaSuccess) return e;
+  k_part_fold<<<num_sms * std::max(per_sm, 1), block, 0, st>>>(p, pp, sorted, op);
   return cudaGetLastError();
 }
 }  // namespace

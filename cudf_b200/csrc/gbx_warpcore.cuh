@@ -616,32 +616,5 @@ __device__ __forceinline__ void warp_write_groups(const Plan& plan, const OutPla
   }
 }
 
-// The outputs of channel c for a batch of groups folded in registers: lane
-// i's group (output row base + i when `active`) has `nrows` rows and channel
-// accumulators A.
-__device__ __forceinline__ void warp_write_chan(const Plan& plan, const OutPlan& op, bool active, uint32_t nrows,
-                                                const ChanAcc& A, int c, int64_t base, int lane, uint32_t act,
-                                                const NullSink& sink)
-{
-  const Channel& ch = plan.chan[c];
-  const RegView V{A, nrows};
-  const int64_t g   = base + lane;
-  for (int o = 0; o < op.nout; ++o) {
-    const OutCol& oc = op.out[o];
-    if (oc.chan != c) continue;
-    bool valid = false;
-    uint64_t v = active ? finalize_from(ch, oc, V, valid) : 0;
-    if (active) store_bits(oc.data, g, oc.out_width, v);
-    if (oc.mask != nullptr) {
-      const uint32_t bits = __ballot_sync(kFull, active && valid);
-      if (lane == 0) {
-        or_mask_bits(oc.mask, base, bits);
-        const uint32_t nulls = __popc(act & ~bits);
-        if (nulls) sink.add(kMaxKeyCols + o, nulls);
-      }
-    }
-  }
-}
-
 }  // namespace dev
 }  // namespace gbx
