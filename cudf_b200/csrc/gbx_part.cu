@@ -158,51 +158,49 @@ __device__ __forceinline__ void part_bucket_ranked(const Plan& plan, const PartP
   }
 }
 
-// The value columns of the groups that part_bucket_ranked emitted (output
-// rows [0, *pp.out_counter) when it ran first): one thread per output row
-// folds its group's run of sorted rows into registers (ChanAcc), one channel
-// at a time, and writes that channel's outputs.  Warps own aligned 32-row
-// runs of output rows, so validity words are stored whole.
-__device__ __forceinline__ void fold_group_rows(const Plan& plan, const PartPlan& pp, const PartBufs& sorted,
-                                                const OutPlan& op, int64_t G, uint32_t* cta_nulls)
+// Channel c's outputs for a warp's 32 output rows [base, base + 32): lane i
+// folds its group's run of sorted rows into registers (ChanAcc) and writes
+// the channel's outputs.  Specialised on the channel's physical type PT, so
+// the accumulate and finalise code has no type switches left.  Warps own
+// aligned 32-row runs of output rows, so validity words are stored whole.
+template <int PT>
+__device__ __forceinline__ void fold_channel(const Plan& plan, const OutPlan& op, const PartCol& pc, int c,
+                                             uint2 run, bool active, int64_t base, int lane, uint32_t act,
+                                             uint32_t* cta_nulls)
 {
-  const int lane         = threadIdx.x & 31;
-  const int64_t wstride  = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < G;
-       base += wstride) {
-    const int64_t g     = base + lane;
-    const bool active   = g < G;
-    const uint2 run     = active ? pp.group_run[g] : make_uint2(0u, 0u);
-    const uint32_t act  = __ballot_sync(kFull, active);
-    for (int c = 0; c < plan.nchan; ++c) {
-      const Channel& ch = plan.chan[c];
-      const PartCol& pc = sorted.col[c];
-      ChanAcc A;
-      chan_acc_init(A);
-      for (uint32_t j = 0; j < run.y; ++j) {
-        const int64_t r  = static_cast<int64_t>(run.x) + j;
-        const uint64_t b = load_bits(pc.vals, r, pc.width);
-        if (pc.valid == nullptr || __ldg(pc.valid + r) != 0) chan_acc_add(ch, A, b);
-      }
-      const RegView V{A, run.y};
-      for (int o = 0; o < op.nout; ++o) {
-        const OutCol& oc = op.out[o];
-        if (oc.chan != c) continue;
-        bool valid = false;
-        const uint64_t v = active ? finalize_from(ch, oc, V, valid) : 0;
-        if (active) store_bits(oc.data, g, oc.out_width, v);
-        if (oc.mask != nullptr) {
-          const uint32_t bits = __ballot_sync(kFull, active && valid);
-          if (lane == 0) {
-            oc.mask[base >> 5] = bits;
-            const uint32_t nulls = __popc(act & ~bits);
-            if (nulls != 0) atomicAdd(cta_nulls + kMaxKeyCols + o, nulls);
-          }
-        }
+  using Word        = typename std::conditional<pt_width(PT) == 1, uint8_t,
+                        typename std::conditional<pt_width(PT) == 2, uint16_t,
+                          typename std::conditional<pt_width(PT) == 4, uint32_t,
+                                                    unsigned long long>::type>::type>::type;
+  const Channel& ch     = plan.chan[c];
+  const uint32_t roles  = chan_roles(ch);
+  const Word* vals      = reinterpret_cast<const Word*>(pc.vals);
+  ChanAcc A;
+  chan_acc_init(A);
+  for (uint32_t j = 0; j < run.y; ++j) {
+    const int64_t r = static_cast<int64_t>(run.x) + j;
+    const uint64_t b = __ldg(vals + r);
+    if (pc.valid == nullptr || __ldg(pc.valid + r) != 0) chan_acc_add<PT>(ch, roles, A, b);
+  }
+  const RegView V{A, run.y};
+  const int64_t g = base + lane;
+  for (int o = 0; o < op.nout; ++o) {
+    const OutCol& oc = op.out[o];
+    if (oc.chan != c) continue;
+    bool valid       = false;
+    const uint64_t v = active ? finalize_from<PT>(ch, oc, V, valid) : 0;
+    if (active) store_bits(oc.data, g, oc.out_width, v);
+    if (oc.mask != nullptr) {
+      const uint32_t bits = __ballot_sync(kFull, active && valid);
+      if (lane == 0) {
+        oc.mask[base >> 5] = bits;
+        const uint32_t nulls = __popc(act & ~bits);
+        if (nulls != 0) atomicAdd(cta_nulls + kMaxKeyCols + o, nulls);
       }
     }
   }
 }
+
 }  // namespace
 
 // Rows per bucket (warp-aggregated: one atomic per bucket present in a warp).
@@ -350,17 +348,40 @@ __global__ void __launch_bounds__(256, kRankedCtasPerSm) k_part_ranked(const __g
   cta_nulls_flush(s_nulls, op.null_counts);
 }
 
-// Value outputs of the groups k_part_ranked emitted (fold_group_rows);
-// launched right after it, before any slice adds output rows.
+// Channel c's value outputs of the groups k_part_ranked emitted (output rows
+// [0, *pp.out_counter): it runs right after k_part_ranked, before any slice
+// adds output rows), one thread per group; one launch per channel, each
+// specialised on that channel's physical type PT.
+template <int PT>
 __global__ void __launch_bounds__(256) k_part_fold(const __grid_constant__ Plan plan,
                                                    const __grid_constant__ PartPlan pp,
                                                    const __grid_constant__ PartBufs sorted,
-                                                   const __grid_constant__ OutPlan op)
+                                                   const __grid_constant__ OutPlan op, int c)
 {
   __shared__ uint32_t s_nulls[kNullSlots];
   cta_nulls_zero(s_nulls);
-  fold_group_rows(plan, pp, sorted, op, static_cast<int64_t>(*pp.out_counter), s_nulls);
+  const int64_t G       = static_cast<int64_t>(*pp.out_counter);
+  const int lane        = threadIdx.x & 31;
+  const int64_t wstride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < G;
+       base += wstride) {
+    const bool active  = base + lane < G;
+    const uint2 run    = active ? pp.group_run[base + lane] : make_uint2(0u, 0u);
+    const uint32_t act = __ballot_sync(kFull, active);
+    fold_channel<PT>(plan, op, sorted.col[c], c, run, active, base, lane, act, s_nulls);
+  }
   cta_nulls_flush(s_nulls, op.null_counts);
+}
+
+template <int PT>
+cudaError_t launch_fold(const Plan& p, const PartPlan& pp, const PartBufs& sorted, const OutPlan& op, int c,
+                        int num_sms, cudaStream_t st)
+{
+  int per_sm    = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_fold<PT>, 256, 0);
+  if (e != cudaSuccess) return e;
+  k_part_fold<PT><<<num_sms * std::max(per_sm, 1), 256, 0, st>>>(p, pp, sorted, op, c);
+  return cudaGetLastError();
 }
 
 // Slices of the buckets larger than slice_rows (see the file comment):
@@ -617,9 +638,23 @@ cudaError_t launch_part_ranked_nw(const Plan& p, const PartPlan& pp, const PartB
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   k_part_ranked<NW><<<num_sms * per_sm, block, smem, st>>>(p, pp, in, sorted, sl, rl, op);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_fold, block, 0)) != cudaSuccess) return e;
-  k_part_fold<<<num_sms * std::max(per_sm, 1), block, 0, st>>>(p, pp, sorted, op);
-  return cudaGetLastError();
+  for (int c = 0; c < p.nchan; ++c) {
+    switch (p.chan[c].ptype) {
+      case P_I8: e = launch_fold<P_I8>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_I16: e = launch_fold<P_I16>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_I32: e = launch_fold<P_I32>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_I64: e = launch_fold<P_I64>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_U8: e = launch_fold<P_U8>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_U16: e = launch_fold<P_U16>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_U32: e = launch_fold<P_U32>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_U64: e = launch_fold<P_U64>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_F32: e = launch_fold<P_F32>(p, pp, sorted, op, c, num_sms, st); break;
+      case P_F64: e = launch_fold<P_F64>(p, pp, sorted, op, c, num_sms, st); break;
+      default: e = launch_fold<P_BOOL>(p, pp, sorted, op, c, num_sms, st); break;
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 }  // namespace
 

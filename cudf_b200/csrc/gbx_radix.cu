@@ -113,9 +113,8 @@ __global__ void __launch_bounds__(kRadixBlock) k_radix_hist(const __grid_constan
     for (int u = 0; u < kLoadGroup; ++u) {
       const uint64_t h   = act[u] ? hash_key<NW>(k[u]) : 0;
       const uint32_t bkt = dg.bits == 0 ? 0u : static_cast<uint32_t>(h >> (64 - dg.bits));
-      const uint32_t d   = act[u] ? ((bkt >> dg.shift) & ((1u << dg.width) - 1u)) : 0xffffffffu;
-      const uint32_t pe  = __match_any_sync(kFull, d);
-      if (act[u] && lane == __ffs(pe) - 1) atomicAdd(&hist[d], static_cast<uint32_t>(__popc(pe)));
+      const uint32_t d   = (bkt >> dg.shift) & ((1u << dg.width) - 1u);
+      if (act[u]) atomicAdd(&hist[d], 1u);  // shared 32-bit atomics: cheaper than grouping the warp first
       if (bucket_counts != nullptr) {
         const uint32_t pb = __match_any_sync(kFull, act[u] ? bkt : 0xffffffffu);
         if (act[u] && lane == __ffs(pb) - 1) atomicAdd(bucket_counts + bkt, static_cast<uint32_t>(__popc(pb)));
@@ -312,6 +311,321 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
   }
 }
 
+// ------------------------------------------------------------- bulk passes
+//
+// Passes after the first read the previous pass's copies, where each column
+// of a tile is one contiguous run of bytes.  k_radix_scatter_bulk moves such
+// a column into shared memory with one cp.async.bulk (the copy engine, not
+// the threads, performs the loads; completion is counted on an mbarrier),
+// two columns in flight at a time: while a column is written out the next
+// but one is already arriving.  The digits come from the key words in shared
+// memory, every local position's output row is computed once, and each
+// column's write-out is then a shared-memory gather by local position and a
+// store to consecutive rows of a digit's run.  A tile that is not full, or a
+// column that is not 16-byte aligned, is copied by the threads instead.
+
+struct BulkSmem {
+  unsigned long long raw[2][kTileRows];  // two column buffers, in tile-row order
+  uint32_t gp[kTileRows];                // output row of local position i
+  uint16_t src[kTileRows];               // tile row at local position i
+  uint8_t dig[kTileRows];                // digit of tile row r
+  uint32_t cnt[kRadixWarps][kMaxRadix];  // per warp: rows of each digit, then its first local position
+  uint32_t tstart[kMaxRadix];            // first local position of each digit in the tile
+  uint32_t goff[kMaxRadix];              // first output row of the tile's rows of each digit
+  unsigned long long bar[2];             // completion of each buffer's copy
+};
+constexpr size_t kBulkSmem = sizeof(BulkSmem);
+
+// ~1 s at the B200's clocks: a wait for a copy this long means the copy is
+// not coming; the kernel then reports S_SPIN_LIMIT instead of hanging.
+constexpr long long kCopyWaitCycles = 2000000000LL;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+    "{\n\t.reg .pred p;\n\t"
+    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+    "selp.u32 %0, 1, 0, p;\n\t}"
+    : "=r"(ok)
+    : "r"(bar), "r"(parity)
+    : "memory");
+  return ok != 0;
+}
+// Waits for phase `parity` of a barrier to complete, for at most
+// kCopyWaitCycles; false if it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
+{
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kCopyWaitCycles) return false;
+  return true;
+}
+
+// dst[at[k]] = column[from[k]] for this thread's local positions (elements
+// of type T; from[k] == all-ones: none), all gathers issued before the stores.
+template <class T, int KPER>
+__device__ __forceinline__ void gather_column(const unsigned long long* column, const uint32_t (&from)[KPER],
+                                              const uint32_t (&at)[KPER], unsigned char* dst)
+{
+  const T* s = reinterpret_cast<const T*>(column);
+  T* d       = reinterpret_cast<T*>(dst);
+  T v[KPER];
+#pragma unroll
+  for (int k = 0; k < KPER; ++k) v[k] = from[k] != 0xffffffffu ? s[from[k]] : T(0);
+#pragma unroll
+  for (int k = 0; k < KPER; ++k)
+    if (from[k] != 0xffffffffu) d[at[k]] = v[k];
+}
+
+// Column j of a pass: key words first, then each channel's values followed
+// by its validity bytes when it has them.
+struct PassCol {
+  const unsigned char* src;
+  unsigned char* dst;
+  int width;
+};
+template <int NW>
+__device__ __forceinline__ PassCol pass_col(const Plan& plan, const PartBufs& in, const PartBufs& out, int j)
+{
+  if (j < NW)
+    return PassCol{reinterpret_cast<const unsigned char*>(in.keys[j]),
+                   const_cast<unsigned char*>(reinterpret_cast<const unsigned char*>(out.keys[j])), 8};
+  j -= NW;
+  for (int c = 0; c < plan.nchan; ++c) {
+    const PartCol& a = in.col[c];
+    const PartCol& b = out.col[c];
+    if (j == 0)
+      return PassCol{static_cast<const unsigned char*>(a.vals),
+                     static_cast<unsigned char*>(const_cast<void*>(b.vals)), a.width};
+    --j;
+    if (a.valid != nullptr) {
+      if (j == 0) return PassCol{a.valid, const_cast<uint8_t*>(b.valid), 1};
+      --j;
+    }
+  }
+  return PassCol{nullptr, nullptr, 0};
+}
+
+template <int NW>
+__global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __grid_constant__ Plan plan,
+                                                                    const __grid_constant__ PartBufs in,
+                                                                    const uint32_t* n_active, const Digit dg,
+                                                                    const uint32_t* __restrict__ offsets,
+                                                                    int ntiles,
+                                                                    const __grid_constant__ PartBufs out,
+                                                                    int32_t* status)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BulkSmem& sm        = *reinterpret_cast<BulkSmem*>(smem_raw);
+  const int64_t rows  = static_cast<int64_t>(*n_active);
+  const int64_t start = static_cast<int64_t>(blockIdx.x) * kTileRows;
+  if (start >= rows) return;  // an empty tile: nothing to move
+  const int nrows = static_cast<int>(rows - start < kTileRows ? rows - start : kTileRows);
+  const int radix = 1 << dg.width;
+  const int lane  = threadIdx.x & 31;
+  const int warp  = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t bar[2] = {smem_addr(&sm.bar[0]), smem_addr(&sm.bar[1])};
+
+  int ncol  = NW;
+  bool bulk = nrows == kTileRows;
+  for (int c = 0; c < plan.nchan; ++c) ncol += in.col[c].valid != nullptr ? 2 : 1;
+  for (int j = 0; j < ncol; ++j)
+    bulk = bulk && (reinterpret_cast<uintptr_t>(pass_col<NW>(plan, in, out, j).src) & 15u) == 0;
+
+  if (threadIdx.x == 0 && bulk) {
+    mbar_init(bar[0]);
+    mbar_init(bar[1]);
+    mbar_fence_init();
+  }
+  for (int i = threadIdx.x; i < kRadixWarps * kMaxRadix; i += kRadixBlock) (&sm.cnt[0][0])[i] = 0;
+  // the tile's first output row of each digit, loaded now so that the load
+  // overlaps the copies and the ranking (one digit per thread)
+  static_assert(kRadixBlock >= kMaxRadix, "one digit per thread");
+  const uint32_t my_goff =
+    threadIdx.x < radix ? __ldg(offsets + static_cast<size_t>(threadIdx.x) * ntiles + blockIdx.x) : 0u;
+  __syncthreads();
+
+  uint32_t parity  = 0;  // bit b: phase of buffer b's next completion
+  uint32_t pending = 0;  // bit b: a bulk copy into buffer b not yet waited for
+  // column j into buffer b (all threads call it right after a barrier that
+  // freed the buffer)
+  auto issue = [&](int j, int b) {
+    const PassCol pc = pass_col<NW>(plan, in, out, j);
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        const uint32_t bytes = static_cast<uint32_t>(kTileRows) * pc.width;
+        fence_proxy_async();  // the threads' reads of the buffer come first
+        mbar_expect_tx(bar[b], bytes);
+        bulk_copy_g2s(smem_addr(sm.raw[b]), pc.src + start * pc.width, bytes, bar[b]);
+      }
+      pending |= 1u << b;
+    } else {
+      unsigned char* d = reinterpret_cast<unsigned char*>(sm.raw[b]);
+      for (int i = threadIdx.x; i < nrows; i += kRadixBlock) {
+        const int64_t r = start + i;
+        switch (pc.width) {
+          case 1: d[i] = __ldg(pc.src + r); break;
+          case 2: reinterpret_cast<uint16_t*>(d)[i] = __ldg(reinterpret_cast<const uint16_t*>(pc.src) + r); break;
+          case 4: reinterpret_cast<uint32_t*>(d)[i] = __ldg(reinterpret_cast<const uint32_t*>(pc.src) + r); break;
+          default:
+            reinterpret_cast<unsigned long long*>(d)[i] =
+              __ldg(reinterpret_cast<const unsigned long long*>(pc.src) + r);
+            break;
+        }
+      }
+    }
+  };
+  // buffer b's column is in shared memory (uniform result: false when a copy
+  // did not arrive in time)
+  auto wait = [&](int b) -> bool {
+    bool got = true;
+    if (bulk) {
+      got = mbar_wait_bounded(bar[b], (parity >> b) & 1u);
+      parity ^= 1u << b;
+      if (got) pending &= ~(1u << b);
+    }
+    return __syncthreads_and(got) != 0;
+  };
+  auto give_up = [&]() {
+    if (threadIdx.x == 0) atomicOr(status, S_SPIN_LIMIT);
+    for (int b = 0; b < 2; ++b)
+      if (pending & (1u << b)) (void)mbar_wait_bounded(bar[b], (parity >> b) & 1u);
+  };
+
+  issue(0, 0);
+  if (ncol > 1) issue(1, 1);
+  bool ok = wait(0);
+  if (ok && NW == 2) ok = wait(1);
+  if (!ok) {
+    give_up();
+    return;
+  }
+
+  // per warp: rows of each digit; each row's digit kept
+  for (int j0 = 0; j0 < kRowsPerWarp / 32; ++j0) {
+    const int r    = warp * kRowsPerWarp + j0 * 32 + lane;
+    const bool act = r < nrows;
+    uint64_t k[NW];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) k[w] = act ? sm.raw[w][r] : 0;
+    const uint32_t d  = act ? digit_of<NW>(k, dg) : 0xffffffffu;
+    const uint32_t pe = __match_any_sync(kFull, d);
+    if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
+    if (act) sm.dig[r] = static_cast<uint8_t>(d);
+    __syncwarp();
+  }
+  __syncthreads();
+  // digit totals -> first local position of each digit (warp 0, 8 digits a lane)
+  if (warp == 0) {
+    uint32_t tot[kMaxRadix / 32];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int q = 0; q < kMaxRadix / 32; ++q) {
+      const int d = lane * (kMaxRadix / 32) + q;
+      uint32_t c  = 0;
+      if (d < radix)
+        for (int w = 0; w < kRadixWarps; ++w) c += sm.cnt[w][d];
+      tot[q] = c;
+      sum += c;
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, incl, off);
+      if (lane >= off) incl += v;
+    }
+    uint32_t run = incl - sum;
+#pragma unroll
+    for (int q = 0; q < kMaxRadix / 32; ++q) {
+      const int d = lane * (kMaxRadix / 32) + q;
+      if (d < radix) sm.tstart[d] = run;
+      run += tot[q];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < radix) {
+    const int d  = threadIdx.x;
+    sm.goff[d]   = my_goff;
+    uint32_t run = sm.tstart[d];
+    for (int w = 0; w < kRadixWarps; ++w) {
+      const uint32_t c = sm.cnt[w][d];
+      sm.cnt[w][d]     = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  // local position of every row (stable: warp, batch, lane order), with the
+  // tile row and the output row stored at it
+  for (int j0 = 0; j0 < kRowsPerWarp / 32; ++j0) {
+    const int r       = warp * kRowsPerWarp + j0 * 32 + lane;
+    const bool act    = r < nrows;
+    const uint32_t d  = act ? sm.dig[r] : 0xffffffffu;
+    const uint32_t pe = __match_any_sync(kFull, d);
+    const uint32_t lp = act ? sm.cnt[warp][d] + static_cast<uint32_t>(__popc(pe & lt)) : 0u;
+    __syncwarp();
+    if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
+    if (act) {
+      sm.src[lp] = static_cast<uint16_t>(r);
+      sm.gp[lp]  = sm.goff[d] + (lp - sm.tstart[d]);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // this thread's local positions i = threadIdx.x + k * kRadixBlock: tile row
+  // and output row, kept in registers for every column (kNoRow: past the tile)
+  constexpr int kPer = kTileRows / kRadixBlock;
+  constexpr uint32_t kNoRow = 0xffffffffu;
+  uint32_t from[kPer], at[kPer];
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int i = threadIdx.x + k * kRadixBlock;
+    from[k]     = i < nrows ? sm.src[i] : kNoRow;
+    at[k]       = i < nrows ? sm.gp[i] : 0u;
+  }
+
+  for (int j = 0; j < ncol; ++j) {
+    const int b = j & 1;
+    if (j >= NW) {  // the key words were waited for before the ranking
+      if (!wait(b)) {
+        give_up();
+        return;
+      }
+    }
+    const PassCol pc = pass_col<NW>(plan, in, out, j);
+    switch (pc.width) {
+      case 1: gather_column<uint8_t, kPer>(sm.raw[b], from, at, pc.dst); break;
+      case 2: gather_column<uint16_t, kPer>(sm.raw[b], from, at, pc.dst); break;
+      case 4: gather_column<uint32_t, kPer>(sm.raw[b], from, at, pc.dst); break;
+      default: gather_column<unsigned long long, kPer>(sm.raw[b], from, at, pc.dst); break;
+    }
+    __syncthreads();  // buffer b is free again
+    if (j + 2 < ncol) issue(j + 2, b);
+  }
+}
+
 }  // namespace
 
 size_t part_radix_count_bytes(int64_t n)
@@ -356,6 +670,12 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint3
   const int items = ntiles << dg.width;
   e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offsets, items, st);
   if (e != cudaSuccess) return e;
+  if constexpr (!FROM_COLUMNS) {
+    e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter_bulk<NW>), kBulkSmem);
+    if (e != cudaSuccess) return e;
+    k_radix_scatter_bulk<NW><<<ntiles, kRadixBlock, kBulkSmem, st>>>(p, in, n_active, dg, offsets, ntiles, out, status);
+    return cudaGetLastError();
+  }
   e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter<NW, FROM_COLUMNS>), kScatterSmem);
   if (e != cudaSuccess) return e;
   k_radix_scatter<NW, FROM_COLUMNS>

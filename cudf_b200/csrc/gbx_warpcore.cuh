@@ -385,30 +385,61 @@ __device__ __forceinline__ void chan_acc_init(ChanAcc& a)
   a.s2   = 0.0;
 }
 
+// The accumulator roles a channel uses, as bits (read once per channel
+// instead of once per row).
+enum ChanRole : uint32_t { R_MIN = 1, R_MAX = 2, R_SUM = 4, R_SQ = 8, R_PROD = 16, R_VAR = 32 };
+__device__ __forceinline__ uint32_t chan_roles(const Channel& ch)
+{
+  return (ch.a_min >= 0 ? R_MIN : 0u) | (ch.a_max >= 0 ? R_MAX : 0u) | (ch.a_sum >= 0 ? R_SUM : 0u) |
+         (ch.a_sq >= 0 ? R_SQ : 0u) | (ch.a_prod >= 0 ? R_PROD : 0u) | (ch.a_k >= 0 ? R_VAR : 0u);
+}
+
+// Physical type of a channel: the compile-time PT when it is >= 0 (a
+// specialised fold), else the channel's runtime ptype.
+template <int PT>
+__device__ __forceinline__ int chan_ptype(const Channel& ch)
+{
+  return PT >= 0 ? PT : ch.ptype;
+}
+template <int PT>
+__device__ __forceinline__ bool chan_is_float(const Channel& ch)
+{
+  return PT >= 0 ? (PT == P_F32 || PT == P_F64) : ch.is_float != 0;
+}
+constexpr int pt_width(int pt)
+{
+  return (pt == P_I8 || pt == P_U8 || pt == P_BOOL) ? 1 : (pt == P_I16 || pt == P_U16) ? 2
+         : (pt == P_I32 || pt == P_U32 || pt == P_F32)                                 ? 4
+                                                                                        : 8;
+}
+
 // Folds one valid value (raw bits) into a channel's registers, with the
 // arithmetic of apply_row (integers wrap, floats in double, the shift K is
 // the first non-NaN value).  Products start from 1 on the first value.
-__device__ __forceinline__ void chan_acc_add(const Channel& ch, ChanAcc& a, uint64_t b)
+// `roles` is chan_roles(ch).
+template <int PT = -1>
+__device__ __forceinline__ void chan_acc_add(const Channel& ch, uint32_t roles, ChanAcc& a, uint64_t b)
 {
+  const int pt     = chan_ptype<PT>(ch);
   const bool first = a.cnt == 0;
   a.cnt += 1;
-  if (ch.a_min >= 0) a.mn = min(a.mn, enc_minmax(b, ch.ptype, true));
-  if (ch.a_max >= 0) a.mx = max(a.mx, enc_minmax(b, ch.ptype, false));
+  if (roles & R_MIN) a.mn = min(a.mn, enc_minmax(b, pt, true));
+  if (roles & R_MAX) a.mx = max(a.mx, enc_minmax(b, pt, false));
   double xf;
-  if (ch.is_float) {
-    xf = as_f64(b, ch.ptype);
-    if (ch.a_sum >= 0) a.sum = static_cast<uint64_t>(__double_as_longlong(__longlong_as_double(static_cast<long long>(a.sum)) + xf));
-    if (ch.a_sq >= 0) a.sq = static_cast<uint64_t>(__double_as_longlong(__longlong_as_double(static_cast<long long>(a.sq)) + xf * xf));
-    if (ch.a_prod >= 0)
+  if (chan_is_float<PT>(ch)) {
+    xf = as_f64(b, pt);
+    if (roles & R_SUM) a.sum = static_cast<uint64_t>(__double_as_longlong(__longlong_as_double(static_cast<long long>(a.sum)) + xf));
+    if (roles & R_SQ) a.sq = static_cast<uint64_t>(__double_as_longlong(__longlong_as_double(static_cast<long long>(a.sq)) + xf * xf));
+    if (roles & R_PROD)
       a.prod = static_cast<uint64_t>(__double_as_longlong(first ? xf : __longlong_as_double(static_cast<long long>(a.prod)) * xf));
   } else {
-    const int64_t x = as_i64(b, ch.ptype);
-    if (ch.a_sum >= 0) a.sum += static_cast<uint64_t>(x);
-    if (ch.a_sq >= 0) a.sq += static_cast<uint64_t>(x) * static_cast<uint64_t>(x);
-    if (ch.a_prod >= 0) a.prod = first ? static_cast<uint64_t>(x) : a.prod * static_cast<uint64_t>(x);
-    xf = (ch.ptype == P_U64) ? static_cast<double>(static_cast<uint64_t>(x)) : static_cast<double>(x);
+    const int64_t x = as_i64(b, pt);
+    if (roles & R_SUM) a.sum += static_cast<uint64_t>(x);
+    if (roles & R_SQ) a.sq += static_cast<uint64_t>(x) * static_cast<uint64_t>(x);
+    if (roles & R_PROD) a.prod = first ? static_cast<uint64_t>(x) : a.prod * static_cast<uint64_t>(x);
+    xf = (pt == P_U64) ? static_cast<double>(static_cast<uint64_t>(x)) : static_cast<double>(x);
   }
-  if (ch.a_k >= 0) {
+  if (roles & R_VAR) {
     if (a.k == kShiftUnset && !(xf != xf)) a.k = static_cast<uint64_t>(__double_as_longlong(xf));
     const double d = xf - __longlong_as_double(static_cast<long long>(a.k));
     a.s2 += d * d;
@@ -417,10 +448,12 @@ __device__ __forceinline__ void chan_acc_add(const Channel& ch, ChanAcc& a, uint
 
 // Final value and validity of output column `oc` of one group from its
 // channel's accumulators (hash_compound_agg_finalizer,
-// hash/groupby.cu:183-349).
-template <class View>
+// hash/groupby.cu:183-349); PT as for chan_acc_add.
+template <int PT = -1, class View>
 __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCol& oc, const View& V, bool& valid)
 {
+  const int pt        = chan_ptype<PT>(ch);
+  const bool is_float = chan_is_float<PT>(ch);
   const uint32_t rows = V.rows();
   const uint32_t cnt  = V.cnt();
   valid               = cnt > 0;
@@ -432,7 +465,7 @@ __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCo
     case GBX_AGG_SUM_OF_SQUARES:
     case GBX_AGG_PRODUCT: {
       uint64_t raw = (oc.kind == GBX_AGG_SUM) ? V.sum() : (oc.kind == GBX_AGG_PRODUCT ? V.prod() : V.sq());
-      if (ch.is_float) {
+      if (is_float) {
         double x = __longlong_as_double(static_cast<long long>(raw));
         vbits    = (oc.out_ptype == P_F32) ? __float_as_uint(static_cast<float>(x))
                                            : static_cast<uint64_t>(__double_as_longlong(x));
@@ -444,7 +477,7 @@ __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCo
     case GBX_AGG_MIN:
     case GBX_AGG_MAX: {
       bool mn = oc.kind == GBX_AGG_MIN;
-      vbits   = dec_minmax(V.minmax(mn), ch.ptype, mn);
+      vbits   = dec_minmax(V.minmax(mn), pt, mn);
       break;
     }
     case GBX_AGG_MEAN: {
@@ -453,8 +486,8 @@ __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCo
       if (oc.out_ptype == P_F64) {
         // integer SUMs are INT64 (target_type): the mean divides the signed sum,
         // as binary_operation(DIV) does on it (hash/groupby.cu:298-304)
-        double sum = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
-                                 : static_cast<double>(static_cast<int64_t>(raw));
+        double sum = is_float ? __longlong_as_double(static_cast<long long>(raw))
+                              : static_cast<double>(static_cast<int64_t>(raw));
         vbits = static_cast<uint64_t>(__double_as_longlong(sum / static_cast<double>(cnt)));
       } else {
         // duration / decimal MEAN: the SUM wraps to the source width, then
@@ -480,9 +513,9 @@ __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCo
       } else {
         double K     = __longlong_as_double(static_cast<long long>(kb));
         uint64_t raw = V.sum();
-        double sum   = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
-                                   : (ch.ptype == P_U64 ? static_cast<double>(raw)
-                                                        : static_cast<double>(static_cast<int64_t>(raw)));
+        double sum   = is_float ? __longlong_as_double(static_cast<long long>(raw))
+                                : (pt == P_U64 ? static_cast<double>(raw)
+                                               : static_cast<double>(static_cast<int64_t>(raw)));
         double S1 = sum - static_cast<double>(nn) * K;
         double M2 = s2 - S1 * S1 / static_cast<double>(nn);
         if (M2 < 0.0) M2 = 0.0;
