@@ -133,19 +133,20 @@ struct ScatterSmem {
   uint32_t tstart[kMaxRadix];             // first local position of each digit in the tile
   uint32_t goff[kMaxRadix];               // first global position of the tile's rows of each digit
   uint16_t lpos[kTileRows];               // local position of tile row (warp, batch, lane); 0xffff: dropped
-  uint8_t dig[kTileRows];                 // digit of each local position
+  uint32_t gp[kTileRows];                 // output row of each local position
   uint8_t vstage[kTileRows];              // validity of the staged values
   uint32_t active;                        // rows of the tile kept
 };
 constexpr size_t kScatterSmem = sizeof(ScatterSmem);
 
-// Moves the rows of tile blockIdx.x to offsets[d * ntiles + t] + their rank
-// among the tile's rows of digit d (tile order: warp, then batch, then lane).
-// Rows are first ranked in digit order inside the tile (local positions);
-// each column is then staged in shared memory at those positions and written
-// out by consecutive threads, so a digit's run of rows is stored by
-// consecutive lanes into consecutive addresses.
-template <int NW, bool FROM_COLUMNS>
+// The first pass: moves the rows of tile blockIdx.x of the caller's columns
+// to offsets[d * ntiles + t] + their rank among the tile's rows of digit d
+// (tile order: warp, then batch, then lane).  Rows are first ranked in digit
+// order inside the tile (local positions); each column is then staged in
+// shared memory at those positions and written out by consecutive threads,
+// so a digit's run of rows is stored by consecutive lanes into consecutive
+// addresses.
+template <int NW, bool FROM_COLUMNS = true>
 __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_constant__ Plan plan,
                                                                const __grid_constant__ PartBufs in, int64_t n,
                                                                const uint32_t* n_active, const Digit dg, int ntiles,
@@ -156,6 +157,11 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
   ScatterSmem& sm = *reinterpret_cast<ScatterSmem*>(smem_raw);
   const int radix = 1 << dg.width;
   for (int i = threadIdx.x; i < kRadixWarps * kMaxRadix; i += kRadixBlock) (&sm.cnt[0][0])[i] = 0;
+  // the tile's first output row of each digit, loaded now so that the load
+  // overlaps the ranking (one digit per thread)
+  static_assert(kRadixBlock >= kMaxRadix, "one digit per thread");
+  const uint32_t my_goff =
+    threadIdx.x < radix ? __ldg(offsets + static_cast<size_t>(threadIdx.x) * ntiles + blockIdx.x) : 0u;
   __syncthreads();
   const PassSource<NW, FROM_COLUMNS> src{&plan, &in};
   const int64_t rows = source_rows(n, n_active, FROM_COLUMNS);
@@ -214,8 +220,9 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
     if (lane == 31) sm.active = incl;
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < radix; d += kRadixBlock) {
-    sm.goff[d]   = offsets[static_cast<size_t>(d) * ntiles + blockIdx.x];
+  if (threadIdx.x < radix) {
+    const int d  = threadIdx.x;
+    sm.goff[d]   = my_goff;
     uint32_t run = sm.tstart[d];
     for (int w = 0; w < kRadixWarps; ++w) {
       const uint32_t c = sm.cnt[w][d];
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
   }
   __syncthreads();
   // local positions (the digits come back from lpos, which then takes the
-  // position); key word 0 staged on the way
+  // position) and the output row of each; key word 0 staged on the way
   for (int j0 = 0; j0 < kRowsPerWarp / 32; j0 += kLoadGroup) {
     uint64_t k0[kLoadGroup];
     uint32_t dd[kLoadGroup];
@@ -250,7 +257,7 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
       if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
       sm.lpos[warp * kRowsPerWarp + (j0 + u) * 32 + lane] = static_cast<uint16_t>(lp);
       if (act) {
-        sm.dig[lp]   = static_cast<uint8_t>(d);
+        sm.gp[lp]    = sm.goff[d] + (lp - sm.tstart[d]);
         sm.stage[lp] = k0[u];
       }
       __syncwarp();
@@ -258,10 +265,7 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
   }
   __syncthreads();
   const uint32_t active = sm.active;
-  auto global_pos = [&](uint32_t i) -> uint32_t {
-    const uint32_t d = sm.dig[i];
-    return sm.goff[d] + (i - sm.tstart[d]);
-  };
+  auto global_pos = [&](uint32_t i) -> uint32_t { return sm.gp[i]; };
   for (uint32_t i = threadIdx.x; i < active; i += kRadixBlock)
     const_cast<uint64_t*>(out.keys[0])[global_pos(i)] = sm.stage[i];
   __syncthreads();
@@ -674,12 +678,11 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint3
     e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter_bulk<NW>), kBulkSmem);
     if (e != cudaSuccess) return e;
     k_radix_scatter_bulk<NW><<<ntiles, kRadixBlock, kBulkSmem, st>>>(p, in, n_active, dg, offsets, ntiles, out, status);
-    return cudaGetLastError();
+  } else {
+    e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter<NW>), kScatterSmem);
+    if (e != cudaSuccess) return e;
+    k_radix_scatter<NW><<<ntiles, kRadixBlock, kScatterSmem, st>>>(p, in, n, n_active, dg, ntiles, offsets, out, status);
   }
-  e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter<NW, FROM_COLUMNS>), kScatterSmem);
-  if (e != cudaSuccess) return e;
-  k_radix_scatter<NW, FROM_COLUMNS>
-    <<<ntiles, kRadixBlock, kScatterSmem, st>>>(p, in, n, n_active, dg, ntiles, offsets, out, status);
   return cudaGetLastError();
 }
 
