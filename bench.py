@@ -69,8 +69,14 @@ def parse_args(argv=None):
     p.add_argument("--batch-tune-save", type=str, default=None,
                    help="write the tuning table the batch used (and extended) to this path")
     p.add_argument("--served-requests", type=int, default=200)
-    p.add_argument("--served-workers", type=int, default=8)
-    p.add_argument("--served-batch-rows", type=int, default=1_000_000)
+    # 4 workers and merging only requests of at most 32K rows: measured on B200
+    # against 8/16 workers and 128K/1M-row merge limits on this request mix
+    # (a merged launch's planning costs more than it saves above ~32K rows)
+    p.add_argument("--served-workers", type=int, default=4)
+    p.add_argument("--served-batch-rows", type=int, default=32_768)
+    p.add_argument("--served-large-rows", type=int, default=0,
+                   help="served: requests of at least this many rows run one at a time (0: library default, "
+                        "-1: none)")
     return p.parse_args(argv)
 
 
@@ -741,7 +747,8 @@ def run_served(args, rank, device, stream):
 
     def server(workers, batch_rows):
         opts = _abi.gbx_server_options(workers=workers, null_policy=0, hbm_budget_bytes=150 << 30,
-                                       batch_max_rows=batch_rows, batch_max_requests=64)
+                                       batch_max_rows=batch_rows, batch_max_requests=64,
+                                       large_rows=args.served_large_rows if workers > 1 else -1)
         h = C.c_void_p()
         _lib.check(lib.gbx_server_create(C.byref(opts), C.byref(h)))
         return h

@@ -285,7 +285,8 @@ class gbx_server_options(C.Structure):
         ("hbm_budget_bytes", C.c_int64),
         ("batch_max_rows", C.c_int64),
         ("batch_max_requests", C.c_int32),
-        ("reserved", C.c_int32),
+        ("large_in_flight", C.c_int32),
+        ("large_rows", C.c_int64),
     ]
 
 

@@ -54,6 +54,7 @@ struct Job {
   int worker         = -1;
   bool finished      = false;
   bool mergeable     = true;  // dictionary keys never share a batched launch
+  bool large         = false;  // at least opt.large_rows rows
 };
 
 // Device bytes a request may hold at once on the plain path, bounded from
@@ -109,6 +110,7 @@ struct gbx_server {
   uint64_t next_ticket = 1;
   int64_t reserved     = 0;
   int in_flight        = 0;
+  int large_in_flight  = 0;
   bool stopping        = false;
   double busy_since    = 0;
   gbx_server_stats st{};
@@ -121,14 +123,18 @@ namespace gbx {
 namespace {
 
 // Picks the next launch under the lock: the first waiting request whose
-// charge fits; small ones take the waiting small requests of their schema
-// along.  Empty when nothing fits.
+// charge fits and, when it is large, while fewer than opt.large_in_flight
+// large requests run (a large request fills the GPU by itself: two of them
+// only interleave their kernels and evict each other's L2-resident tables);
+// small ones take the waiting small requests of their schema along.  Empty
+// when nothing fits.
 std::vector<std::shared_ptr<Job>> pick(gbx_server& s)
 {
   std::vector<std::shared_ptr<Job>> out;
   const int64_t budget = s.opt.hbm_budget_bytes;
   for (auto it = s.waiting.begin(); it != s.waiting.end(); ++it) {
     const auto j = *it;
+    if (j->large && s.large_in_flight >= s.opt.large_in_flight) continue;
     const bool alone_ok = s.in_flight == 0 && s.reserved == 0;  // larger than the budget: runs alone
     if (s.reserved + j->charge > budget && !(j->charge > budget && alone_ok)) continue;
     out.push_back(j);
@@ -282,8 +288,14 @@ void run_merged(gbx_server& s, std::vector<std::shared_ptr<Job>>& js, cudaStream
 void worker_main(gbx_server* s, int w)
 {
   cudaSetDevice(s->device);
-  cudaStream_t st = nullptr;
-  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  // small requests on a high-priority stream, large ones on a low-priority
+  // one: blocks of a small request's kernels are scheduled ahead of a large
+  // request's waiting blocks
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  cudaStream_t st = nullptr, st_large = nullptr;
+  cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi);
+  cudaStreamCreateWithPriority(&st_large, cudaStreamNonBlocking, prio_lo);
   int num_sms = 148;
   cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, s->device);
   std::unique_lock<std::mutex> lk(s->mu);
@@ -304,16 +316,19 @@ void worker_main(gbx_server* s, int w)
     }
     s->reserved += charge;
     if (s->in_flight++ == 0) s->busy_since = t;
+    const bool large = js.size() == 1 && js[0]->large;
+    if (large) s->large_in_flight += 1;
     s->st.max_in_flight       = std::max(s->st.max_in_flight, s->in_flight);
     s->st.peak_reserved_bytes = std::max(s->st.peak_reserved_bytes, s->reserved);
     lk.unlock();
 
-    if (js.size() == 1) run_single(*s, *js[0], st);
+    if (js.size() == 1) run_single(*s, *js[0], large ? st_large : st);
     else run_merged(*s, js, st, num_sms);
 
     lk.lock();
     const double d = s->now();
     s->reserved -= charge;
+    if (large) s->large_in_flight -= 1;
     if (--s->in_flight == 0) s->st.busy_s += d - s->busy_since;
     if (js.size() > 1) {
       s->st.batches += 1;
@@ -334,7 +349,9 @@ void worker_main(gbx_server* s, int w)
   }
   lk.unlock();
   cudaStreamSynchronize(st);
+  cudaStreamSynchronize(st_large);
   cudaStreamDestroy(st);
+  cudaStreamDestroy(st_large);
 }
 
 }  // namespace
@@ -350,10 +367,13 @@ int gbx_server_create(const gbx_server_options* options, gbx_server** out)
     *out = nullptr;
     gbx_server_options o{};
     if (options) o = *options;
-    if (o.workers == 0) o.workers = 8;
+    if (o.workers == 0) o.workers = 4;
     if (o.hbm_budget_bytes == 0) o.hbm_budget_bytes = int64_t(150) << 30;
     if (o.batch_max_requests == 0) o.batch_max_requests = 64;
+    if (o.large_in_flight == 0) o.large_in_flight = 1;
+    if (o.large_rows == 0) o.large_rows = int64_t(1) << 22;
     GBX_EXPECTS(o.workers >= 1 && o.workers <= 256, "workers must be in [1, 256]");
+    GBX_EXPECTS(o.large_in_flight >= 1, "large_in_flight must be >= 1");
     GBX_EXPECTS(o.null_policy == GBX_NULL_EXCLUDE || o.null_policy == GBX_NULL_INCLUDE, "invalid null_policy");
     GBX_EXPECTS(o.hbm_budget_bytes > 0 && o.batch_max_rows >= 0 && o.batch_max_requests >= 1,
                 "invalid budget or batching limits");
@@ -409,6 +429,7 @@ int gbx_server_submit(gbx_server* s, const gbx_table_view* keys, const gbx_reque
     }
     j->charge = memory_charge(*j);
     j->schema = schema_of(*j);
+    j->large  = s->opt.large_rows > 0 && j->rows >= s->opt.large_rows;
     std::lock_guard<std::mutex> lk(s->mu);
     GBX_EXPECTS(!s->stopping, "the server is shutting down");
     j->ticket          = s->next_ticket++;

@@ -74,13 +74,15 @@ def request_array(requests: Sequence[GroupByRequest]):
 class Server:
     """A groupby server on the current CUDA device (gbx_server)."""
 
-    def __init__(self, workers: int = 8, null_handling: _abi.NullPolicy = _abi.NullPolicy.EXCLUDE,
-                 hbm_budget_bytes: int = 0, batch_max_rows: int = 0, batch_max_requests: int = 0):
+    def __init__(self, workers: int = 4, null_handling: _abi.NullPolicy = _abi.NullPolicy.EXCLUDE,
+                 hbm_budget_bytes: int = 0, batch_max_rows: int = 0, batch_max_requests: int = 0,
+                 large_rows: int = 0, large_in_flight: int = 0):
         self._h = None
         self._held: Dict[int, tuple] = {}
         opts = _abi.gbx_server_options(workers=int(workers), null_policy=int(null_handling),
                                        hbm_budget_bytes=int(hbm_budget_bytes), batch_max_rows=int(batch_max_rows),
-                                       batch_max_requests=int(batch_max_requests))
+                                       batch_max_requests=int(batch_max_requests),
+                                       large_in_flight=int(large_in_flight), large_rows=int(large_rows))
         h = C.c_void_p()
         _lib.check(_lib.lib().gbx_server_create(C.byref(opts), C.byref(h)))
         self._h = h

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define GBX_ABI_VERSION 1
+#define GBX_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define GBX_API __attribute__((visibility("default")))
@@ -459,12 +459,15 @@ GBX_API void gbx_batch_destroy(gbx_batch* batch);
 typedef struct gbx_server gbx_server;
 
 typedef struct gbx_server_options {
-  int32_t workers;              /* requests on the GPU at once (streams); 0: 8 */
+  int32_t workers;              /* requests on the GPU at once (streams); 0: 4 */
   int32_t null_policy;          /* GBX_NULL_EXCLUDE / INCLUDE for every request */
   int64_t hbm_budget_bytes;     /* device memory admitted requests may hold; 0: 150 GB */
   int64_t batch_max_rows;       /* requests of at most this many rows may be merged (0: never) */
   int32_t batch_max_requests;   /* at most this many requests per merged launch; 0: 64 */
-  int32_t reserved;
+  int32_t large_in_flight;      /* large requests on the GPU at once; 0: 1 */
+  int64_t large_rows;           /* a request of at least this many rows is large (it fills the GPU
+                                   by itself and runs on a low-priority stream; smaller requests
+                                   may pass a waiting large one); 0: 4M rows, < 0: none is large */
 } gbx_server_options;
 
 typedef struct gbx_server_timing {

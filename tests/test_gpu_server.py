@@ -109,6 +109,33 @@ def test_small_requests_merge_behind_a_large_one():
     srv.close()
 
 
+def test_large_requests_run_one_at_a_time():
+    """Requests of at least large_rows rows never overlap on the GPU (at most
+    large_in_flight = 1 of them at once) while small ones still run beside
+    them; every result matches the oracle."""
+    from cudf_b200 import Server
+
+    rng = np.random.default_rng(10)
+    reqs = []
+    for i in range(15):
+        n = 300_000 if i % 3 == 0 else int(rng.integers(1000, 20_000))
+        reqs.append(served_request(rng, n, int(rng.integers(10, 50_000))))
+    srv = Server(workers=4, large_rows=200_000, large_in_flight=1)
+    dev = [to_device(k, r) for k, r in reqs]
+    ts = [srv.submit(kt, rq) for kt, rq in dev]
+    spans = []
+    for (k, r), t in zip(reqs, ts):
+        kt, res, timing = srv.wait(t)
+        if len(k[0].values) >= 200_000:
+            spans.append((timing["admitted_s"], timing["done_s"]))
+        assert_parity(k, r, NullPolicy.EXCLUDE, gpu=host_result(kt, res))
+    srv.close()
+    spans.sort()
+    assert len(spans) == 5
+    for (a0, d0), (a1, _) in zip(spans, spans[1:]):
+        assert a1 >= d0, "two large requests were on the GPU at once"
+
+
 def test_nullable_requests_merge_and_match():
     from cudf_b200 import Server
 
