@@ -12,8 +12,10 @@ per groupby) are larger than L2 (126 MB), so no L2 flush is needed.
             public API (cudf_b200.GroupBy.aggregate), CUDA events on the stream
   e2e    -- same metric with host (pinned) inputs: every step copies inputs
             host->device and reads all results back device->host
-  roofline -- the aggregation kernel: algorithmic input bytes / its
-            CUDA-event duration, against the measured HBM copy bandwidth
+  roofline -- the partitioned path's aggregation phase (k_part_ranked and one
+            k_part_fold per value channel): its algorithmic bytes (rows read,
+            groups written) / its CUDA-event duration, against the measured
+            HBM copy bandwidth
 
 `--impl reference` times the reference's CPU algorithm (the oracle
 restatement, all host threads) on a bounded sample of the same workload.
@@ -43,9 +45,11 @@ BYTES_PER_ROW_IN = 8 + 8 + 4 + 1.0 / 8  # key + a + b + b's validity bit
 BYTES_PER_GROUP_OUT = 8 + (8 + 4 + 8 + 8 + 8 + 8) + (4 + 4 + 4 + 4 + 8 + 8) + 6.0 / 8
 METRIC = "groupby rows/s (plain hash groupby, 100M rows, int64 key, cardinality 1e2/1e4/1e6/1e8)"
 PARTITIONED = 3  # gbx_strategy of the radix-partitioned path
-# DRAM bytes per row of one k_part_agg launch measured by ncu (20M rows,
-# cardinality 2e7: 0.436 GB read + 1.017 GB written)
-K_PART_AGG_DRAM_BYTES_PER_ROW = (0.435927e9 + 1.016502e9) / 20_000_000
+# DRAM bytes per row of the aggregation phase measured by ncu (20M rows,
+# cardinality 2e7): k_part_ranked 0.429 GB read + 0.423 GB written,
+# k_part_fold (int64 channel) 0.262 + 0.504, k_part_fold (float32 channel)
+# 0.204 + 0.360
+AGG_PHASE_DRAM_BYTES_PER_ROW = (0.428523e9 + 0.423397e9 + 0.261882e9 + 0.503935e9 + 0.204437e9 + 0.360262e9) / 20_000_000
 
 
 def parse_args(argv=None):
@@ -272,9 +276,10 @@ def run_ours(args, rank, world, local):
 
     peaks = _load_peaks()
     per = {}
-    # the dominant kernel is k_part_agg (the partitioned strategy's aggregation
-    # pass, which also writes the outputs): its algorithmic bytes per launch
-    # are the rows read and the groups written
+    # the roofline follows the partitioned strategy's aggregation phase
+    # (k_part_ranked + the k_part_fold launches, which also write the
+    # outputs): its algorithmic bytes per call are the rows read and the
+    # groups written
     agg_ms_total = 0.0
     agg_bytes_total = 0.0
     agg_launches = 0
@@ -307,17 +312,17 @@ def run_ours(args, rank, world, local):
         }
     achieved = (agg_bytes_total / (agg_ms_total / 1e3)) / 1e9 if agg_ms_total > 0 else None
     roofline = {
-        "bound": "hbm", "kernel": "k_part_agg (cardinality 1e4 / 1e6 / 1e8 launches)",
+        "bound": "hbm", "kernel": "k_part_ranked + k_part_fold (cardinality 1e6 / 1e8 calls)",
         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
         "peak_source": peaks["source"],
         "algorithmic_bytes_per_launch": agg_bytes_total / agg_launches if agg_launches else None,
         "launches_per_step": agg_launches // max(1, args.steps),
-        # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_part_agg
-        # launch on 20M rows of cardinality 2e7 (1.452 GB), scaled by rows to
-        # the 100M-row cardinality-1e8 launch; that launch's algorithmic bytes
-        # are 100M x 20.125 + 63.2M x 85 = 7.39 GB
-        "traffic": K_PART_AGG_DRAM_BYTES_PER_ROW * n,
+        # ncu dram__bytes_read.sum + dram__bytes_write.sum of the aggregation
+        # phase on 20M rows of cardinality 2e7 (2.18 GB), scaled by rows to the
+        # 100M-row cardinality-1e8 call; that call's algorithmic bytes are
+        # 100M x 20.125 + 63.2M x 85 = 7.39 GB
+        "traffic": AGG_PHASE_DRAM_BYTES_PER_ROW * n,
         "traffic_launch": "cardinality 1e8",
     }
 

@@ -1024,7 +1024,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         pp.group_run = group_runs;
         timer.mark(2);
         GBX_CUDA(launch_part_ranked(plan, pp, pbufs, tbufs, S, pop, call.dev.num_sms, s));
-        launches += 2;
+        launches += 1 + plan.nchan;  // grouping, one fold per value channel
         if (h_items > 0) {
           GBX_CUDA(launch_part_agg(plan, pp, pbufs, t2, sl, call.dev.num_sms, s));
           timer.mark(3);
