@@ -1093,7 +1093,12 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         int grid        = call.dev.num_sms * std::max<int>(1, std::min<int>(4, static_cast<int>((200 * 1024) / (sl.total + 1024))));
         int64_t max_grid = (call.n + block * 4 - 1) / (block * 4);
         grid             = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(grid, max_grid)));
-        GBX_CUDA(launch_agg_privatized(plan, t, sl, call.n, block, grid, std::min<uint32_t>(S, 32), max_probes, s));
+        if (tiled_fits(sl, plan.nchan)) {
+          // few groups: tiles grouped in shared memory before the table is touched
+          GBX_CUDA(launch_agg_tiled(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 32), max_probes, s));
+        } else {
+          GBX_CUDA(launch_agg_privatized(plan, t, sl, call.n, block, grid, std::min<uint32_t>(S, 32), max_probes, s));
+        }
       } else {
         GBX_CUDA(launch_agg_global(plan, t, call.n, max_probes, call.dev.num_sms, s));
       }

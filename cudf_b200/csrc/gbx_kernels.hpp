@@ -47,6 +47,12 @@ cudaError_t launch_agg_global(const Plan& p, const TableRef& t, int64_t n, uint3
                               cudaStream_t st);
 cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int block,
                                   int grid, uint32_t smem_probes, uint32_t max_probes, cudaStream_t st);
+// Per-CTA tables fed by tile-local grouping (gbx_tiled.cu), for tables where
+// tiled_fits() (at most 1,024 slots, table and a tile's staged values within
+// half an SM's shared memory).
+bool tiled_fits(const SmemLayout& sl, int nchan);
+cudaError_t launch_agg_tiled(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int num_sms,
+                             uint32_t smem_probes, uint32_t max_probes, cudaStream_t st);
 // ---- radix-partitioned path
 // Row-partitioned copies of the inputs: packed key words (SoA), each
 // channel's resolved value bits, and a validity byte per row for channels
