@@ -408,33 +408,43 @@ struct PassCol {
   const unsigned char* src;
   unsigned char* dst;
   int width;
+  int chan;       // channel of a value or validity column, else -1
+  bool validity;  // the channel's validity bytes
 };
+// The columns follow `out`: a channel has a validity column when its copies
+// keep validity bytes.
 template <int NW>
 __device__ __forceinline__ PassCol pass_col(const Plan& plan, const PartBufs& in, const PartBufs& out, int j)
 {
   if (j < NW)
     return PassCol{reinterpret_cast<const unsigned char*>(in.keys[j]),
-                   const_cast<unsigned char*>(reinterpret_cast<const unsigned char*>(out.keys[j])), 8};
+                   const_cast<unsigned char*>(reinterpret_cast<const unsigned char*>(out.keys[j])), 8, -1, false};
   j -= NW;
   for (int c = 0; c < plan.nchan; ++c) {
     const PartCol& a = in.col[c];
     const PartCol& b = out.col[c];
     if (j == 0)
       return PassCol{static_cast<const unsigned char*>(a.vals),
-                     static_cast<unsigned char*>(const_cast<void*>(b.vals)), a.width};
+                     static_cast<unsigned char*>(const_cast<void*>(b.vals)), b.width, c, false};
     --j;
-    if (a.valid != nullptr) {
-      if (j == 0) return PassCol{a.valid, const_cast<uint8_t*>(b.valid), 1};
+    if (b.valid != nullptr) {
+      if (j == 0) return PassCol{a.valid, const_cast<uint8_t*>(b.valid), 1, c, true};
       --j;
     }
   }
-  return PassCol{nullptr, nullptr, 0};
+  return PassCol{nullptr, nullptr, 0, -1, false};
 }
 
+// `first_pass`: `in` points at the caller's columns themselves (a plain
+// 8-byte key column without nulls, value columns without dictionaries, each
+// pointer already advanced by its column's offset), all n rows are kept and
+// the validity bytes come from the channels' bitmasks; otherwise `in` holds
+// the previous pass's copies and *n_active rows.
 template <int NW>
 __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __grid_constant__ Plan plan,
                                                                     const __grid_constant__ PartBufs in,
-                                                                    const uint32_t* n_active, const Digit dg,
+                                                                    const uint32_t* n_active, int64_t n,
+                                                                    bool first_pass, const Digit dg,
                                                                     const uint32_t* __restrict__ offsets,
                                                                     int ntiles,
                                                                     const __grid_constant__ PartBufs out,
@@ -442,7 +452,7 @@ __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __g
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BulkSmem& sm        = *reinterpret_cast<BulkSmem*>(smem_raw);
-  const int64_t rows  = static_cast<int64_t>(*n_active);
+  const int64_t rows  = first_pass ? n : static_cast<int64_t>(*n_active);
   const int64_t start = static_cast<int64_t>(blockIdx.x) * kTileRows;
   if (start >= rows) return;  // an empty tile: nothing to move
   const int nrows = static_cast<int>(rows - start < kTileRows ? rows - start : kTileRows);
@@ -454,9 +464,12 @@ __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __g
 
   int ncol  = NW;
   bool bulk = nrows == kTileRows;
-  for (int c = 0; c < plan.nchan; ++c) ncol += in.col[c].valid != nullptr ? 2 : 1;
-  for (int j = 0; j < ncol; ++j)
-    bulk = bulk && (reinterpret_cast<uintptr_t>(pass_col<NW>(plan, in, out, j).src) & 15u) == 0;
+  for (int c = 0; c < plan.nchan; ++c) ncol += out.col[c].valid != nullptr ? 2 : 1;
+  for (int j = 0; j < ncol; ++j) {
+    const PassCol pc = pass_col<NW>(plan, in, out, j);
+    if (first_pass && pc.validity) continue;  // filled from the bitmask
+    bulk = bulk && (reinterpret_cast<uintptr_t>(pc.src) & 15u) == 0;
+  }
 
   if (threadIdx.x == 0 && bulk) {
     mbar_init(bar[0]);
@@ -477,7 +490,12 @@ __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __g
   // freed the buffer)
   auto issue = [&](int j, int b) {
     const PassCol pc = pass_col<NW>(plan, in, out, j);
-    if (bulk) {
+    if (first_pass && pc.validity) {
+      // validity bytes of the caller's column from its bitmask
+      const Channel& ch = plan.chan[pc.chan];
+      unsigned char* d  = reinterpret_cast<unsigned char*>(sm.raw[b]);
+      for (int i = threadIdx.x; i < nrows; i += kRadixBlock) d[i] = bit_valid(ch.mask, start + i + ch.offset) ? 1 : 0;
+    } else if (bulk) {
       if (threadIdx.x == 0) {
         const uint32_t bytes = static_cast<uint32_t>(kTileRows) * pc.width;
         fence_proxy_async();  // the threads' reads of the buffer come first
@@ -505,10 +523,12 @@ __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __g
   // did not arrive in time)
   auto wait = [&](int b) -> bool {
     bool got = true;
-    if (bulk) {
+    if (pending & (1u << b)) {  // a bulk copy (thread-filled buffers only need the barrier)
       got = mbar_wait_bounded(bar[b], (parity >> b) & 1u);
-      parity ^= 1u << b;
-      if (got) pending &= ~(1u << b);
+      if (got) {
+        parity ^= 1u << b;
+        pending &= ~(1u << b);
+      }
     }
     return __syncthreads_and(got) != 0;
   };
@@ -661,6 +681,27 @@ Digit pass_digit(int bits, int i)
 
 int tiles_of(int64_t n) { return static_cast<int>(std::max<int64_t>((n + kTileRows - 1) / kTileRows, 1)); }
 
+// Whether the first pass can read the caller's columns as raw runs of bytes
+// (a single plain 8-byte key column without nulls -- its bits are the packed
+// key -- and value columns without dictionaries); `src` then points at them,
+// each pointer advanced by its column's offset.
+bool first_pass_columns(const Plan& p, const PartBufs& out, PartBufs& src)
+{
+  const KeyCol& kc = p.key.cols[0];
+  if (p.key.nwords != 1 || p.key.ncols != 1 || kc.width != 8 || kc.is_float || kc.is_bool || kc.null_bit ||
+      kc.mask != nullptr || kc.shift != 0)
+    return false;
+  src         = PartBufs{};
+  src.keys[0] = reinterpret_cast<const uint64_t*>(static_cast<const unsigned char*>(kc.data) + kc.offset * 8);
+  for (int c = 0; c < p.nchan; ++c) {
+    const Channel& ch = p.chan[c];
+    if (ch.dict_data != nullptr) return false;
+    src.col[c].width = out.col[c].width;
+    src.col[c].vals  = static_cast<const unsigned char*>(ch.data) + ch.offset * out.col[c].width;
+  }
+  return true;
+}
+
 template <int NW, bool FROM_COLUMNS>
 cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint32_t* n_active, const Digit& dg,
                        int ntiles, uint32_t* counts, uint32_t* offsets, void* temp, size_t temp_bytes,
@@ -674,10 +715,13 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint3
   const int items = ntiles << dg.width;
   e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offsets, items, st);
   if (e != cudaSuccess) return e;
-  if constexpr (!FROM_COLUMNS) {
+  PartBufs user{};
+  const bool bulk_first = FROM_COLUMNS && first_pass_columns(p, out, user);
+  if (!FROM_COLUMNS || bulk_first) {
     e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter_bulk<NW>), kBulkSmem);
     if (e != cudaSuccess) return e;
-    k_radix_scatter_bulk<NW><<<ntiles, kRadixBlock, kBulkSmem, st>>>(p, in, n_active, dg, offsets, ntiles, out, status);
+    k_radix_scatter_bulk<NW><<<ntiles, kRadixBlock, kBulkSmem, st>>>(p, bulk_first ? user : in, n_active, n,
+                                                                     bulk_first, dg, offsets, ntiles, out, status);
   } else {
     e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter<NW>), kScatterSmem);
     if (e != cudaSuccess) return e;
