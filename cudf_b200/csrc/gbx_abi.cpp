@@ -933,6 +933,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       uint32_t* roffsets = nullptr;
       void* rtemp        = nullptr;
       size_t rtemp_bytes = 0;
+      uint32_t* n_kept   = nullptr;  // rows the radix passes keep (device)
       uint2* group_runs  = nullptr;  // (first sorted row, rows) per output row
       // outputs sized for the upper bound (every row its own group): the group
       // count is only known once the buckets have been written out
@@ -968,24 +969,33 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         // many buckets: coalesced radix passes (gbx_radix.cu), whose first
         // histogram also counts the rows per bucket
         const bool use_radix = pp.shard_bits == 0 && bits >= 9;
+        size_t temp_bytes    = 0;
+        GBX_CUDA(launch_part_layout(pp, nullptr, &temp_bytes, call.dev.num_sms, s));
+        void* temp = scratch.get(temp_bytes);
         if (use_radix) {
+          // the rows go to bucket order first; the bucket offsets are then
+          // read off the partitioned keys (no per-row counter atomics)
           if (rcounts == nullptr) {
             tbufs    = part_bufs();
             rcounts  = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
             roffsets = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
             GBX_CUDA(part_radix_temp_bytes(call.n, &rtemp_bytes));
-            rtemp = scratch.get(rtemp_bytes);
+            rtemp  = scratch.get(rtemp_bytes);
+            n_kept = static_cast<uint32_t*>(scratch.get(sizeof(uint32_t)));
           }
-          GBX_CUDA(cudaMemsetAsync(pp.counts, 0, nctr * sizeof(uint32_t), s));
-          GBX_CUDA(launch_part_radix_hist0(plan, call.n, bits, rcounts, pp.counts, s));
+          GBX_CUDA(launch_part_radix_hist0(plan, call.n, bits, rcounts, nullptr, s));
+          GBX_CUDA(launch_part_radix(plan, call.n, bits, n_kept, pbufs, tbufs, rcounts, roffsets, rtemp, rtemp_bytes,
+                                     d_status, /*hist0_done=*/true, s));
+          GBX_CUDA(launch_part_bounds(plan.key.nwords, pbufs.keys, n_kept, bits, pp.offsets, call.dev.num_sms, s));
+          GBX_CUDA(launch_part_layout(pp, temp, &temp_bytes, call.dev.num_sms, s, /*offsets_ready=*/true));
+          // first histogram, 3 launches per pass (the first: scan, kept rows,
+          // scatter), bounds, slices + 2 scans
+          launches += 1 + 3 * ((bits + 7) / 8) + 1 + 3;
         } else {
           GBX_CUDA(launch_part_hist(plan.key, call.n, pp, call.dev.num_sms, s));
+          GBX_CUDA(launch_part_layout(pp, temp, &temp_bytes, call.dev.num_sms, s));
+          launches += 5;  // histogram, scan, slices, 2 scans
         }
-        size_t temp_bytes = 0;
-        GBX_CUDA(launch_part_layout(pp, nullptr, &temp_bytes, call.dev.num_sms, s));
-        void* temp = scratch.get(temp_bytes);
-        GBX_CUDA(launch_part_layout(pp, temp, &temp_bytes, call.dev.num_sms, s));
-        launches += 5;  // histogram, scan, slices, 2 scans
         uint32_t h_counts[2] = {0, 0};  // regions, work items
         GBX_CUDA(cudaMemcpyAsync(&h_counts[0], pp.region + P, 4, cudaMemcpyDeviceToHost, s));
         GBX_CUDA(cudaMemcpyAsync(&h_counts[1], pp.item_start + P, 4, cudaMemcpyDeviceToHost, s));
@@ -1006,11 +1016,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
           GBX_CUDA(launch_init_table(t2, plan.acc, plan.key.nwords, call.dev.num_sms, s));
           launches += 2;
         }
-        if (use_radix) {
-          GBX_CUDA(launch_part_radix(plan, call.n, bits, pp.offsets + P, pbufs, tbufs, rcounts, roffsets, rtemp,
-                                     rtemp_bytes, d_status, /*hist0_done=*/true, s));
-          launches += 3 * ((bits + 7) / 8) - 2;
-        } else {
+        if (!use_radix) {
           GBX_CUDA(launch_part_scatter(plan, call.n, pp, pbufs, call.dev.num_sms, s));
           launches += 1;
           if (tbufs.keys[0] == nullptr) tbufs = part_bufs();

@@ -95,8 +95,15 @@ struct PartPlan {
 };
 
 cudaError_t launch_part_hist(const KeyPlan& kp, int64_t n, const PartPlan& pp, int num_sms, cudaStream_t st);
-// counts -> offsets, nslices, item_start, multi, region (device scans)
-cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_bytes, int num_sms, cudaStream_t st);
+// counts -> offsets (unless offsets_ready), nslices, item_start, multi,
+// region (device scans)
+cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_bytes, int num_sms, cudaStream_t st,
+                               bool offsets_ready = false);
+// offsets[b] = first row of bucket b (b <= P) of *n_rows rows already in
+// bucket order (one word per key word in `keys`): the bucket offsets read off
+// the partitioned copies, for unsharded counters.
+cudaError_t launch_part_bounds(int nwords, const uint64_t* const* keys, const uint32_t* n_rows, int bits,
+                               uint32_t* offsets, int num_sms, cudaStream_t st);
 // item_bucket[item_start[b] + j] = b for every slice j of every bucket b
 cudaError_t launch_part_items(const PartPlan& pp, int64_t n, int num_sms, cudaStream_t st);
 cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, const PartBufs& out, int num_sms,
@@ -104,18 +111,18 @@ cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, co
 // Radix partitioning into bucket order (gbx_radix.cu): the same result as
 // launch_part_scatter for 2^bits buckets with unsharded counters, in
 // ceil(bits / 8) coalesced passes that alternate between `dst` and `tmp`
-// (same layout) and end in `dst`.  *n_active (device) is the number of rows
-// kept (the bucket histogram's total); `counts` and `offsets` hold
-// part_radix_count_bytes(n) bytes each, `temp` part_radix_temp_bytes(n).
-// launch_part_radix_hist0 runs the first pass's tile histogram early and
-// adds every kept row to bucket_counts[its bucket] (zeroed by the caller),
-// which then stands in for launch_part_hist; launch_part_radix is told so
-// with hist0_done.
+// (same layout) and end in `dst`.  The rows kept (a null key under EXCLUDE
+// drops a row) are written to *n_kept (device) after the first pass;
+// `counts` and `offsets` hold part_radix_count_bytes(n) bytes each, `temp`
+// part_radix_temp_bytes(n).  launch_part_radix_hist0 runs the first pass's
+// tile histogram early (and adds every kept row to bucket_counts[its bucket]
+// when that is set, zeroed by the caller); launch_part_radix is told so with
+// hist0_done.
 size_t part_radix_count_bytes(int64_t n);
 cudaError_t part_radix_temp_bytes(int64_t n, size_t* temp_bytes);
 cudaError_t launch_part_radix_hist0(const Plan& p, int64_t n, int bits, uint32_t* counts, uint32_t* bucket_counts,
                                     cudaStream_t st);
-cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
+cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, uint32_t* n_kept, const PartBufs& dst,
                               const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
                               size_t temp_bytes, int32_t* status, bool hist0_done, cudaStream_t st);
 // Aggregates every bucket of at most slice_rows rows (S-slot warp tables)

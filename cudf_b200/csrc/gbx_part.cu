@@ -541,22 +541,61 @@ cudaError_t launch_part_hist(const KeyPlan& kp, int64_t n, const PartPlan& pp, i
   return cudaGetLastError();
 }
 
-cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_bytes, int num_sms, cudaStream_t st)
+cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_bytes, int num_sms, cudaStream_t st,
+                               bool offsets_ready)
 {
   const int items    = (1 << pp.bits) + 1;
   const int counters = (1 << (pp.bits + pp.shard_bits)) + 1;
-  if (temp == nullptr) {
+  if (temp == nullptr) {  // sized for the largest scan (counters >= items)
     return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, pp.counts, pp.offsets, counters, st);
   }
-  cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.counts, pp.offsets, counters, st);
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  if (!offsets_ready) {
+    e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.counts, pp.offsets, counters, st);
+    if (e != cudaSuccess) return e;
+  }
   k_part_slices<<<grid_rows(items, 256, num_sms * 4), 256, 0, st>>>(pp);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.nslices, pp.item_start, items, st)) != cudaSuccess)
     return e;
   if ((e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.multi, pp.region, items, st)) != cudaSuccess)
     return e;
+  if (offsets_ready) return cudaSuccess;  // cursors are only used by the one-pass scatter
   return cudaMemcpyAsync(pp.cursor, pp.offsets, (counters - 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+}
+
+namespace {
+// offsets[b] = i for the buckets b in (bucket of row i - 1, bucket of row i]
+// (row -1 in bucket -1, row *n_rows in bucket P): every bucket's first row,
+// each entry written once.
+template <int NW>
+__global__ void k_part_bounds(const uint64_t* k0, const uint64_t* k1, const uint32_t* n_rows, int bits,
+                              uint32_t* offsets)
+{
+  const int64_t n      = static_cast<int64_t>(*n_rows);
+  const int64_t P      = int64_t(1) << bits;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  auto bucket = [&](int64_t r) -> int64_t {
+    uint64_t k[NW];
+    k[0] = __ldg(k0 + r);
+    if constexpr (NW == 2) k[1] = __ldg(k1 + r);
+    return static_cast<int64_t>(bucket_of(hash_key<NW>(k), bits));
+  };
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= n; i += stride) {
+    const int64_t prev = i > 0 ? bucket(i - 1) : -1;
+    const int64_t cur  = i < n ? bucket(i) : P;
+    for (int64_t b = prev + 1; b <= cur; ++b) offsets[b] = static_cast<uint32_t>(i);
+  }
+}
+}  // namespace
+
+cudaError_t launch_part_bounds(int nwords, const uint64_t* const* keys, const uint32_t* n_rows, int bits,
+                               uint32_t* offsets, int num_sms, cudaStream_t st)
+{
+  const int grid = num_sms * 8;
+  if (nwords == 1) k_part_bounds<1><<<grid, 256, 0, st>>>(keys[0], nullptr, n_rows, bits, offsets);
+  else k_part_bounds<2><<<grid, 256, 0, st>>>(keys[0], keys[1], n_rows, bits, offsets);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_part_items(const PartPlan& pp, int64_t n, int num_sms, cudaStream_t st)

@@ -681,6 +681,12 @@ Digit pass_digit(int bits, int i)
 
 int tiles_of(int64_t n) { return static_cast<int>(std::max<int64_t>((n + kTileRows - 1) / kTileRows, 1)); }
 
+// *total = offsets[items - 1] + counts[items - 1]: the rows of an exclusive scan.
+__global__ void k_radix_total(const uint32_t* counts, const uint32_t* offsets, int items, uint32_t* total)
+{
+  *total = offsets[items - 1] + counts[items - 1];
+}
+
 // Whether the first pass can read the caller's columns as raw runs of bytes
 // (a single plain 8-byte key column without nulls -- its bits are the packed
 // key -- and value columns without dictionaries); `src` then points at them,
@@ -702,8 +708,10 @@ bool first_pass_columns(const Plan& p, const PartBufs& out, PartBufs& src)
   return true;
 }
 
+// One pass; the first (FROM_COLUMNS) writes the rows it keeps to *n_active,
+// which the later passes read.
 template <int NW, bool FROM_COLUMNS>
-cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint32_t* n_active, const Digit& dg,
+cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, uint32_t* n_active, const Digit& dg,
                        int ntiles, uint32_t* counts, uint32_t* offsets, void* temp, size_t temp_bytes,
                        const PartBufs& out, int32_t* status, bool hist_done, cudaStream_t st)
 {
@@ -715,6 +723,11 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint3
   const int items = ntiles << dg.width;
   e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offsets, items, st);
   if (e != cudaSuccess) return e;
+  if constexpr (FROM_COLUMNS) {
+    // rows kept by the first pass: the later passes' row count
+    k_radix_total<<<1, 1, 0, st>>>(counts, offsets, items, n_active);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   PartBufs user{};
   const bool bulk_first = FROM_COLUMNS && first_pass_columns(p, out, user);
   if (!FROM_COLUMNS || bulk_first) {
@@ -731,7 +744,7 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, const uint3
 }
 
 template <int NW>
-cudaError_t radix_all(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
+cudaError_t radix_all(const Plan& p, int64_t n, int bits, uint32_t* n_active, const PartBufs& dst,
                       const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp, size_t temp_bytes,
                       int32_t* status, bool hist0_done, cudaStream_t st)
 {
@@ -770,14 +783,14 @@ cudaError_t launch_part_radix_hist0(const Plan& p, int64_t n, int bits, uint32_t
   return cudaGetLastError();
 }
 
-cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, const uint32_t* n_active, const PartBufs& dst,
+cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, uint32_t* n_kept, const PartBufs& dst,
                               const PartBufs& tmp, uint32_t* counts, uint32_t* offsets, void* temp,
                               size_t temp_bytes, int32_t* status, bool hist0_done, cudaStream_t st)
 {
-  if (n <= 0) return cudaSuccess;
+  if (n <= 0) return cudaMemsetAsync(n_kept, 0, sizeof(uint32_t), st);
   return p.key.nwords == 1
-           ? radix_all<1>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, hist0_done, st)
-           : radix_all<2>(p, n, bits, n_active, dst, tmp, counts, offsets, temp, temp_bytes, status, hist0_done, st);
+           ? radix_all<1>(p, n, bits, n_kept, dst, tmp, counts, offsets, temp, temp_bytes, status, hist0_done, st)
+           : radix_all<2>(p, n, bits, n_kept, dst, tmp, counts, offsets, temp, temp_bytes, status, hist0_done, st);
 }
 
 }  // namespace gbx
