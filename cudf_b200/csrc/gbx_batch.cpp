@@ -109,8 +109,14 @@ void append_tune_file(const char* path, const std::vector<std::pair<TuneKey, Cho
       << ' ' << r.second.smul << ' ' << r.second.tile_log2 << ' ' << static_cast<long long>(r.second.rate) << '\n';
 }
 
+// Remembered per device: cudaGetDeviceProperties costs milliseconds.
 std::string device_tag(int device)
 {
+  static std::mutex mu;
+  static std::map<int, std::string> known;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = known.find(device);
+  if (it != known.end()) return it->second;
   cudaDeviceProp p{};
   if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return "unknown";
   std::string s = p.name;
@@ -118,7 +124,7 @@ std::string device_tag(int device)
     if (ch == ' ' || ch == '\t') ch = '_';
   char buf[64];
   snprintf(buf, sizeof(buf), "_sm%d%d_%d", p.major, p.minor, p.multiProcessorCount);
-  return s + buf;
+  return known[device] = s + buf;
 }
 
 // What the kernels' cost depends on: key words and accumulators per channel.
@@ -197,10 +203,14 @@ struct gbx_batch {
   cudaEvent_t ev[2]    = {nullptr, nullptr};                    // around the launch
   cudaEvent_t phase[4] = {nullptr, nullptr, nullptr, nullptr};  // recorded by the execution itself
 
-  // pinned host copies written by each execution
+  // host copies written by each execution: pinned for a captured graph,
+  // pageable for a one-shot batch (pinned allocation and release synchronise
+  // with the whole device, which would stall every other stream's work)
   int64_t* h_offsets          = nullptr;
   int32_t* h_status           = nullptr;
   unsigned long long* h_nulls = nullptr;
+  bool pinned_host            = true;
+  bool owns_stream            = true;  // a one-shot batch runs on the caller's stream
 
   gbx_batch_output output{};
   gbx_batch_stats stats{};
@@ -230,14 +240,20 @@ struct gbx_batch {
   ~gbx_batch()
   {
     release_device();
-    if (h_offsets) cudaFreeHost(h_offsets);
-    if (h_status) cudaFreeHost(h_status);
-    if (h_nulls) cudaFreeHost(h_nulls);
+    if (pinned_host) {
+      if (h_offsets) cudaFreeHost(h_offsets);
+      if (h_status) cudaFreeHost(h_status);
+      if (h_nulls) cudaFreeHost(h_nulls);
+    } else {
+      delete[] h_offsets;
+      delete[] h_status;
+      delete[] h_nulls;
+    }
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (auto& e : phase)
       if (e) cudaEventDestroy(e);
-    if (cs) cudaStreamDestroy(cs);
+    if (cs && owns_stream) cudaStreamDestroy(cs);
   }
 };
 
@@ -664,7 +680,7 @@ void plan_batch(gbx_batch& b, const gbx_batch_options& o)
     class_rows[b.inst[i].cls] += b.inst[i].n;
   }
   b.stats.classes          = static_cast<int32_t>(classes.size());
-  const std::string device = device_tag(b.dev.device);
+  const std::string device = o.tune != GBX_TUNE_OFF ? device_tag(b.dev.device) : std::string();
   const std::string sig    = schema_signature(b.schema);
   std::map<TuneKey, Choice> table;
   if (o.tune != GBX_TUNE_OFF) {
@@ -801,17 +817,28 @@ int gbx_batch_create(const gbx_batch_instance* instances, int32_t num_instances,
     }
     build_schema(*b, instances, num_instances);  // host-only checks first
     b->dev = current_device();
-    GBX_CUDA(cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking));
-    // the caller's stream may still be producing the inputs
-    cudaEvent_t ready;
-    GBX_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-    GBX_CUDA(cudaEventRecord(ready, static_cast<cudaStream_t>(stream)));
-    GBX_CUDA(cudaStreamWaitEvent(b->cs, ready, 0));
-    cudaEventDestroy(ready);
+    if (b->one_shot) {
+      // no graph to capture: the caller's stream orders everything, and the
+      // host copies need not be pinned
+      b->cs          = static_cast<cudaStream_t>(stream);
+      b->owns_stream = false;
+      b->pinned_host = false;
+      b->h_offsets   = new int64_t[static_cast<size_t>(num_instances) + 1];
+      b->h_status    = new int32_t[static_cast<size_t>(num_instances)];
+      b->h_nulls     = new unsigned long long[kMaxKeyCols + kMaxOut];
+    } else {
+      GBX_CUDA(cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking));
+      // the caller's stream may still be producing the inputs
+      cudaEvent_t ready;
+      GBX_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+      GBX_CUDA(cudaEventRecord(ready, static_cast<cudaStream_t>(stream)));
+      GBX_CUDA(cudaStreamWaitEvent(b->cs, ready, 0));
+      cudaEventDestroy(ready);
+      GBX_CUDA(cudaMallocHost(&b->h_offsets, (static_cast<size_t>(num_instances) + 1) * 8));
+      GBX_CUDA(cudaMallocHost(&b->h_status, static_cast<size_t>(num_instances) * 4));
+      GBX_CUDA(cudaMallocHost(&b->h_nulls, (kMaxKeyCols + kMaxOut) * 8));
+    }
     b->alloc.st = b->cs;
-    GBX_CUDA(cudaMallocHost(&b->h_offsets, (static_cast<size_t>(num_instances) + 1) * 8));
-    GBX_CUDA(cudaMallocHost(&b->h_status, static_cast<size_t>(num_instances) * 4));
-    GBX_CUDA(cudaMallocHost(&b->h_nulls, (kMaxKeyCols + kMaxOut) * 8));
     for (auto& e : b->ev) GBX_CUDA(cudaEventCreate(&e));
     for (auto& e : b->phase) GBX_CUDA(cudaEventCreate(&e));
 
