@@ -204,6 +204,8 @@ class gbx_stats(C.Structure):
         ("compact_ms", C.c_float),
         ("finalize_ms", C.c_float),
         ("total_ms", C.c_float),
+        ("partition_bits", C.c_int32),
+        ("bucket_slots", C.c_int32),
     ]
 
 

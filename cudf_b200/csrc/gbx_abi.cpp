@@ -508,24 +508,38 @@ void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_c
 
 // Invert the expected distinct count of a uniform draw, d = C (1 - exp(-m / C)),
 // then G = C (1 - exp(-N / C)).
+namespace {
+// Distinct keys expected among `rows` rows drawn uniformly from a population
+// of C keys, where C is solved from `distinct` keys seen in `sampled` rows
+// (D(m) = C (1 - e^{-m/C})).
+double project_distinct(double sampled, double distinct, double rows)
+{
+  if (distinct >= sampled) return rows;
+  double lo = distinct, hi = 1e12;
+  for (int it = 0; it < 200; ++it) {
+    double mid = 0.5 * (lo + hi);
+    double d   = mid * (1.0 - std::exp(-sampled / mid));
+    if (d < distinct) lo = mid;
+    else hi = mid;
+  }
+  const double C = 0.5 * (lo + hi);
+  return C * (1.0 - std::exp(-rows / C));
+}
+}  // namespace
+
 double estimate_groups(double sampled, double distinct, int64_t n, int64_t nsample)
 {
-  double est;
-  if (nsample >= n) {
-    est = distinct;
-  } else if (distinct >= sampled) {
-    est = static_cast<double>(n);
-  } else {
-    double lo = distinct, hi = 1e12;
-    for (int it = 0; it < 200; ++it) {
-      double mid = 0.5 * (lo + hi);
-      double d   = mid * (1.0 - std::exp(-sampled / mid));
-      if (d < distinct) lo = mid;
-      else hi = mid;
-    }
-    double C = 0.5 * (lo + hi);
-    est      = C * (1.0 - std::exp(-static_cast<double>(n) / C));
-  }
+  const double est = nsample >= n ? distinct : project_distinct(sampled, distinct, static_cast<double>(n));
+  return std::max(1.0, std::min(est, static_cast<double>(n)));
+}
+
+double estimate_groups(double sampled, double distinct, double heavy, double heavy_rows, int64_t n, int64_t nsample)
+{
+  if (nsample >= n) return estimate_groups(sampled, distinct, n, nsample);
+  const double light_sampled = sampled - heavy_rows, light_distinct = distinct - heavy;
+  double est = heavy;
+  if (light_sampled > 0 && light_distinct > 0)
+    est += project_distinct(light_sampled, light_distinct, static_cast<double>(n) * (light_sampled / sampled));
   return std::max(1.0, std::min(est, static_cast<double>(n)));
 }
 
@@ -756,8 +770,10 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     PhaseTimer timer(gb, s, call.dev.device);
     int launches = 0;
     timer.mark(0);
-    // control block: [0..1] sample counters, [2..25] valid counts, [26] status, [27] num_selected
-    constexpr int kCtlWords = 32;
+    // control block: [0..1] sample counters, [2..25] valid counts, [26] status,
+    // [27] num_selected, [28..31] partitioned-path counters, [32..33] heavy keys
+    // of the sample and their rows
+    constexpr int kCtlWords = 34;
     auto* ctl = static_cast<unsigned long long*>(scratch.get(kCtlWords * 8));
     GBX_CUDA(cudaMemsetAsync(ctl, 0, kCtlWords * 8, s));
     int32_t* d_status        = reinterpret_cast<int32_t*>(ctl + 26);
@@ -774,9 +790,10 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     // ---- sampled distinct count
     const int64_t nsample = std::min<int64_t>(call.n, 1 << 16);
     const uint64_t set_cap = 1 << 18;
-    auto* set = static_cast<uint64_t*>(scratch.get(set_cap * 8));
-    GBX_CUDA(launch_sample(kp_sample, call.n, nsample, set, set_cap, ctl, call.dev.num_sms, s));
-    launches += 2;
+    auto* set      = static_cast<uint64_t*>(scratch.get(set_cap * 8));
+    auto* set_rows = static_cast<uint32_t*>(scratch.get(set_cap * 4));
+    GBX_CUDA(launch_sample(kp_sample, call.n, nsample, set, set_rows, set_cap, ctl, ctl + 32, call.dev.num_sms, s));
+    launches += 3;
     timer.mark(1);
 
     unsigned long long h_ctl[kCtlWords];
@@ -787,7 +804,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       if (span_owner[i].first == 0) key_nulls[span_owner[i].second] = nulls;
       else chan_nulls[span_owner[i].second] = nulls;
     }
-    double est = estimate_groups(static_cast<double>(h_ctl[0]), static_cast<double>(h_ctl[1]), call.n, nsample);
+    double est = estimate_groups(static_cast<double>(h_ctl[0]), static_cast<double>(h_ctl[1]),
+                                 static_cast<double>(h_ctl[32]), static_cast<double>(h_ctl[33]), call.n, nsample);
     gb->stats.estimated_groups = static_cast<int64_t>(est);
 
     // ---- plan
@@ -907,6 +925,22 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       const double gpb  = S * 0.5;
       int bits          = 0;
       while (static_cast<double>(1ull << bits) * gpb < est && bits < 22) ++bits;
+      // one table per CTA (up to 4,096 slots, ~2,048 groups per bucket) where
+      // that needs fewer 8-bit radix passes than warp tables do; the bucket
+      // count is then rounded up to whole passes (smaller buckets, same
+      // passes) and the table sized for twice a bucket's mean groups
+      const int warp_bits = bits;
+      int cta_bits        = 0;
+      while (static_cast<double>(1ull << cta_bits) * 2048.0 < est && cta_bits < 22) ++cta_bits;
+      bool cta_rank  = false;
+      uint32_t S_cta = 0;
+      if (cta_bits >= 9 && (cta_bits + 7) / 8 < (warp_bits + 7) / 8) {
+        cta_rank = true;
+        bits     = 8 * ((cta_bits + 7) / 8);
+        S_cta    = static_cast<uint32_t>(
+          std::min<uint64_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * est / static_cast<double>(1ull << bits), 256.0))),
+                             4096));
+      }
       // bucket-ordered copies of the rows: packed key words, resolved value
       // bits, a validity byte per row of a nullable channel
       auto part_bufs = [&]() {
@@ -946,7 +980,9 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         PartPlan pp{};
         pp.bits         = bits;
         pp.shard_bits   = std::max(0, std::min(5, 12 - bits));
-        pp.slice_rows   = 16384;  // < 65536: ranks and counts of a whole bucket fit 16 bits
+        // whole buckets up to the rows whose ranks fit a record: 16 bits beside
+        // a warp table's slot, 19 beside a CTA table's
+        pp.slice_rows = cta_rank ? (1u << 19) : 16384;
         pp.region_slots = S;
         pp.status       = d_status;
         auto arr        = [&]() { return static_cast<uint32_t*>(scratch.get((static_cast<size_t>(P) + 1) * 4)); };
@@ -1029,7 +1065,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         if (group_runs == nullptr) group_runs = static_cast<uint2*>(scratch.get(static_cast<size_t>(call.n) * 8));
         pp.group_run = group_runs;
         timer.mark(2);
-        GBX_CUDA(launch_part_ranked(plan, pp, pbufs, tbufs, S, pop, call.dev.num_sms, s));
+        if (cta_rank) GBX_CUDA(launch_part_ranked_cta(plan, pp, pbufs, tbufs, S_cta, pop, call.dev.num_sms, s));
+        else GBX_CUDA(launch_part_ranked(plan, pp, pbufs, tbufs, S, pop, call.dev.num_sms, s));
         launches += 1 + plan.nchan;  // grouping, one fold per value channel
         if (h_items > 0) {
           GBX_CUDA(launch_part_agg(plan, pp, pbufs, t2, sl, call.dev.num_sms, s));
@@ -1048,13 +1085,21 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         if (status & S_SPIN_LIMIT) fail(GBX_ERR_DEVICE, "a bounded device loop gave up (status 0x%x)", status);
         if (status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
         if ((status & S_TABLE_FULL) == 0) {
-          gb->stats.table_capacity = static_cast<int64_t>(P) * S;
+          gb->stats.table_capacity = static_cast<int64_t>(P) * (cta_rank ? S_cta : S);
+          gb->stats.partition_bits = bits;
+          gb->stats.bucket_slots   = static_cast<int32_t>(cta_rank ? S_cta : S);
           break;
         }
-        // a bucket held more groups than its table: split into 4x the buckets
+        // a bucket held more groups than its table: warp tables at their own
+        // bucket count, else 4x the buckets
         if (attempt >= 3 || bits >= 24) fail(GBX_ERR_DEVICE, "partitioned aggregation overflow at %u buckets", P);
         gb->stats.retries++;
-        bits += 2;
+        if (cta_rank) {
+          cta_rank = false;
+          bits     = warp_bits;
+        } else {
+          bits += 2;
+        }
       }
       timer.mark(5);
       std::vector<unsigned long long> h_nulls(kMaxKeyCols + kMaxOut, 0);

@@ -178,6 +178,10 @@ void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_c
 // Group count of `n` rows from a sample of `sampled` rows with `distinct`
 // distinct keys (uniform-draw inversion, clamped to [1, n]).
 double estimate_groups(double sampled, double distinct, int64_t n, int64_t nsample);
+// The same with the sample's `heavy` frequent keys (and their `heavy_rows`
+// sampled rows) counted exactly and the inversion applied to the remaining
+// rows only, so that a few frequent keys do not hide many rare ones.
+double estimate_groups(double sampled, double distinct, double heavy, double heavy_rows, int64_t n, int64_t nsample);
 
 // Bytes of one table slot: packed key, row count and every accumulator.
 size_t slot_bytes(const Plan& plan);

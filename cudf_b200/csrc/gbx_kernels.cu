@@ -133,12 +133,14 @@ __global__ void __launch_bounds__(512) k_agg_privatized(const __grid_constant__ 
 }
 
 // Sampled distinct count: inserts a strided sample of packed keys (folded to
-// 64 bits) into a small global set and counts first insertions.
+// 64 bits) into a small global set, counts first insertions and, per set
+// slot, the sampled rows of its key.
 template <int NW>
 __global__ void k_sample_distinct(const __grid_constant__ KeyPlan kp,
                                   int64_t n,
                                   int64_t nsample,
                                   uint64_t* set,
+                                  uint32_t* set_rows,
                                   uint64_t set_mask,
                                   unsigned long long* counters)
 {
@@ -154,12 +156,26 @@ __global__ void k_sample_distinct(const __grid_constant__ KeyPlan kp,
     uint64_t s = fmix64(f[0] ^ 0x5bd1e995ULL) & set_mask;
     for (uint64_t p = 0; p <= set_mask; ++p) {
       uint64_t old = atomicCAS(reinterpret_cast<unsigned long long*>(set + s), kEmptyWord, f[0]);
-      if (old == kEmptyWord) {
-        atomicAdd(&counters[1], 1ULL);
+      if (old == kEmptyWord) atomicAdd(&counters[1], 1ULL);
+      if (old == kEmptyWord || old == f[0]) {
+        atomicAdd(set_rows + s, 1u);
         break;
       }
-      if (old == f[0]) break;
       s = (s + 1) & set_mask;
+    }
+  }
+}
+
+// Keys sampled at least kHeavySample times: heavy[0] += their number,
+// heavy[1] += their sampled rows.
+__global__ void k_sample_heavy(const uint32_t* set_rows, uint64_t set_cap, unsigned long long* heavy)
+{
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < set_cap; i += stride) {
+    const uint32_t c = set_rows[i];
+    if (c >= kHeavySample) {
+      atomicAdd(&heavy[0], 1ULL);
+      atomicAdd(&heavy[1], static_cast<unsigned long long>(c));
     }
   }
 }
@@ -352,14 +368,20 @@ cudaError_t launch_init_table(const TableRef& t, const AccLayout& al, int nwords
   return cudaGetLastError();
 }
 
-cudaError_t launch_sample(const KeyPlan& kp, int64_t n, int64_t nsample, uint64_t* set, uint64_t set_cap,
-                          unsigned long long* counters, int num_sms, cudaStream_t st)
+cudaError_t launch_sample(const KeyPlan& kp, int64_t n, int64_t nsample, uint64_t* set, uint32_t* set_rows,
+                          uint64_t set_cap, unsigned long long* counters, unsigned long long* heavy, int num_sms,
+                          cudaStream_t st)
 {
-  k_fill_u64<<<grid_for(static_cast<int64_t>(set_cap), 256, num_sms * 8), 256, 0, st>>>(set, set_cap, kEmptyWord);
-  cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st);
+  const int fill_grid = grid_for(static_cast<int64_t>(set_cap), 256, num_sms * 8);
+  k_fill_u64<<<fill_grid, 256, 0, st>>>(set, set_cap, kEmptyWord);
+  cudaError_t e = cudaMemsetAsync(set_rows, 0, set_cap * sizeof(uint32_t), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(heavy, 0, 2 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
   int grid = grid_for(nsample, 256, num_sms * 8);
-  if (kp.nwords == 1) k_sample_distinct<1><<<grid, 256, 0, st>>>(kp, n, nsample, set, set_cap - 1, counters);
-  else k_sample_distinct<2><<<grid, 256, 0, st>>>(kp, n, nsample, set, set_cap - 1, counters);
+  if (kp.nwords == 1) k_sample_distinct<1><<<grid, 256, 0, st>>>(kp, n, nsample, set, set_rows, set_cap - 1, counters);
+  else k_sample_distinct<2><<<grid, 256, 0, st>>>(kp, n, nsample, set, set_rows, set_cap - 1, counters);
+  k_sample_heavy<<<fill_grid, 256, 0, st>>>(set_rows, set_cap, heavy);
   return cudaGetLastError();
 }
 

@@ -41,8 +41,14 @@ struct OutPlan {
 };
 
 cudaError_t launch_init_table(const TableRef& t, const AccLayout& al, int nwords, int num_sms, cudaStream_t st);
-cudaError_t launch_sample(const KeyPlan& kp, int64_t n, int64_t nsample, uint64_t* set, uint64_t set_cap,
-                          unsigned long long* counters, int num_sms, cudaStream_t st);
+// Sampled distinct count of nsample strided rows: counters[0] = sampled rows,
+// counters[1] = their distinct keys; heavy[0] = keys sampled at least
+// kHeavySample times, heavy[1] = their sampled rows.  `set` holds set_cap
+// words and `set_rows` set_cap counts (set_cap a power of two).
+constexpr uint32_t kHeavySample = 4;
+cudaError_t launch_sample(const KeyPlan& kp, int64_t n, int64_t nsample, uint64_t* set, uint32_t* set_rows,
+                          uint64_t set_cap, unsigned long long* counters, unsigned long long* heavy, int num_sms,
+                          cudaStream_t st);
 cudaError_t launch_agg_global(const Plan& p, const TableRef& t, int64_t n, uint32_t max_probes, int num_sms,
                               cudaStream_t st);
 cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int block,
@@ -85,9 +91,9 @@ struct PartPlan {
   unsigned long long* out_counter;   // output rows written so far
   uint32_t region_slots;     // slots per region table (= the warp table size)
   int32_t* status;           // device status word
-  // [n], indexed by partitioned row: a bucket handled by one warp whose rows
-  // do not fit the warp's shared memory ranks them here (slot << 16 | rank
-  // within the slot; slice_rows < 65536)
+  // [n], indexed by partitioned row: a whole bucket whose rows do not fit
+  // its warp's or CTA's shared memory ranks them here (slot above the rank
+  // within the slot: 16 rank bits for warp tables, 19 for CTA tables)
   uint32_t* rank_rec;
   // [n], indexed by output row: (first row, row count) of a whole bucket's
   // group in the group-ordered copies
@@ -132,6 +138,11 @@ cudaError_t launch_part_radix(const Plan& p, int64_t n, int bits, uint32_t* n_ke
 // grouping, then one thread per group).
 cudaError_t launch_part_ranked(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
                                uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st);
+// The same with one bucket per CTA at a time over one S-slot shared table
+// (S a power of two in [256, 4096]; pp.slice_rows <= 2^19), for buckets of
+// up to a few thousand groups.
+cudaError_t launch_part_ranked_cta(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
+                                   uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st);
 // Aggregates the slices of the larger buckets (item_start[P] of them, > 0)
 // into region tables of `t` (t.cap = regions * region_slots) that
 // launch_part_region_finalize then writes out.

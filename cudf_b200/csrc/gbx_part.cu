@@ -348,6 +348,192 @@ __global__ void __launch_bounds__(256, kRankedCtasPerSm) k_part_ranked(const __g
   cta_nulls_flush(s_nulls, op.null_counts);
 }
 
+// Shared memory of k_part_ranked_cta: a keys table of slots + 1 entries
+// (slot `slots` is the reserved all-ones key), slots + 2 counters (rows of
+// each slot, then each slot's first position, then the total), the occupied
+// slots in slot order and rec_rows rank records.
+struct CtaRankLayout {
+  uint32_t slots;  // power of two, a multiple of the block size
+  uint32_t cnt_off;
+  uint32_t list_off;
+  uint32_t rec_off;
+  uint32_t rec_rows;
+  uint32_t total;
+};
+
+constexpr int kCtaRankThreads = 256;
+// Rank records of k_part_ranked_cta: slot (up to 4,096, 13 bits) above a
+// 19-bit rank, so that one CTA takes buckets of up to 2^19 rows.
+constexpr int kCtaRankBits          = 19;
+constexpr uint32_t kCtaRankMask     = (1u << kCtaRankBits) - 1u;
+constexpr uint32_t kCtaMaxSliceRows = 1u << kCtaRankBits;
+
+// Exclusive scan of one 64-bit value per thread over the block; *total gets
+// the block's sum.  `part` holds one entry per warp.  Ends with the block
+// synchronised.
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* part, uint64_t* total)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint64_t incl  = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint64_t y = __shfl_up_sync(kFull, incl, d);
+    if (lane >= d) incl += y;
+  }
+  if (lane == 31) part[warp] = incl;
+  __syncthreads();
+  uint64_t before = 0, all = 0;
+  for (int w = 0; w < nwarps; ++w) {
+    const uint64_t p = part[w];
+    before += w < warp ? p : 0;
+    all += p;
+  }
+  *total = all;
+  __syncthreads();  // `part` may be reused after the return
+  return before + incl - v;
+}
+
+// Whole buckets, one per CTA at a time: the same four steps as
+// part_bucket_ranked with the bucket's rows spread over the block and one
+// table of cl.slots slots for the whole CTA, so that a bucket may hold a few
+// thousand groups (2^8 times fewer buckets than the warp form needs for the
+// same groups: one radix pass less).  Each row's rank within its slot comes
+// from a 32-bit shared atomic, so a group's rows are contiguous in `sorted`
+// but not in partitioned order (floating-point sums may round differently
+// from run to run; every other result is order-independent).
+template <int NW>
+__global__ void __launch_bounds__(kCtaRankThreads, 4) k_part_ranked_cta(const __grid_constant__ Plan plan,
+                                                                      const __grid_constant__ PartPlan pp,
+                                                                      const __grid_constant__ PartBufs in,
+                                                                      const __grid_constant__ PartBufs sorted,
+                                                                      const __grid_constant__ CtaRankLayout cl,
+                                                                      const __grid_constant__ OutPlan op)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t s_nulls[kNullSlots];
+  __shared__ uint64_t s_part[kCtaRankThreads / 32];
+  __shared__ unsigned long long s_claim, s_out;
+  const uint32_t S       = cl.slots;
+  uint64_t* keys         = reinterpret_cast<uint64_t*>(smem);
+  const uint32_t keys_sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  uint32_t* cnt          = reinterpret_cast<uint32_t*>(smem + cl.cnt_off);
+  uint32_t* list         = reinterpret_cast<uint32_t*>(smem + cl.list_off);
+  uint32_t* rec_smem     = reinterpret_cast<uint32_t*>(smem + cl.rec_off);
+  const PartSource src{&in};
+  const uint32_t P   = 1u << pp.bits;
+  const int lane     = threadIdx.x & 31;
+  const uint32_t tid = threadIdx.x;
+  const NullSink sink{op.null_counts, s_nulls};
+  cta_nulls_zero(s_nulls);
+
+  for (;;) {
+    if (tid == 0) s_claim = atomicAdd(pp.bucket_counter, 1ull);
+    __syncthreads();
+    const unsigned long long b = s_claim;
+    __syncthreads();  // every thread has read s_claim before thread 0 claims again
+    if (b >= P) break;
+    if (pp.multi[b] != 0) continue;  // sliced: k_part_agg
+    const int64_t r0 = pp.offsets[b << pp.shard_bits];
+    const int64_t r1 = pp.offsets[(b + 1) << pp.shard_bits];
+    if (r1 == r0) continue;
+    const uint32_t len = static_cast<uint32_t>(r1 - r0);
+    uint32_t* rec      = len <= cl.rec_rows ? rec_smem : pp.rank_rec + r0;
+
+    for (uint32_t s = tid; s <= S + 1; s += blockDim.x) {
+      if (s <= S) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) keys[s * NW + w] = kEmptyWord;
+      }
+      cnt[s] = 0;
+    }
+    __syncthreads();
+
+    // 1. rank
+    for (uint32_t i = tid; i < len; i += blockDim.x) {
+      uint64_t k[NW];
+      uint32_t v = kNoRank;
+      if (src.key<NW>(r0 + i, k)) {
+        int64_t slot = S;
+        if (!key_is_empty<NW>(k)) {
+          slot = find_or_insert<Shared, NW>(keys_sa, S - 1, k, hash_key<NW>(k), S);
+          if (slot < 0) atomicOr(pp.status, S_TABLE_FULL);  // more groups than the table: host retries
+        }
+        if (slot >= 0) {
+          const uint32_t rank = atomicAdd(cnt + slot, 1u);
+          v                   = (static_cast<uint32_t>(slot) << kCtaRankBits) | rank;
+        }
+      }
+      rec[i] = v;
+    }
+    __syncthreads();
+
+    // 2. scan: first position of every slot (in place), occupied slots listed
+    // in slot order; each thread scans S / blockDim.x consecutive slots
+    const uint32_t per = S / blockDim.x;
+    const uint32_t sb  = tid * per;
+    uint32_t csum = 0, occ = 0;
+    for (uint32_t j = 0; j < per; ++j) {
+      const uint32_t c = cnt[sb + j];
+      csum += c;
+      occ += c != 0;
+    }
+    uint64_t total;
+    const uint64_t ex = block_exclusive_scan((static_cast<uint64_t>(occ) << 32) | csum, s_part, &total);
+    uint32_t pos = static_cast<uint32_t>(ex), gi = static_cast<uint32_t>(ex >> 32);
+    for (uint32_t j = 0; j < per; ++j) {
+      const uint32_t c = cnt[sb + j];
+      cnt[sb + j]      = pos;
+      pos += c;
+      if (c != 0) list[gi++] = sb + j;
+    }
+    const uint32_t tot_rows = static_cast<uint32_t>(total), tot_groups = static_cast<uint32_t>(total >> 32);
+    const uint32_t cs       = cnt[S];  // the reserved slot's rows (read by all before thread 0 rewrites it)
+    const uint32_t ngroups  = tot_groups + (cs != 0);
+    __syncthreads();
+    if (tid == 0) {
+      cnt[S]     = tot_rows;
+      cnt[S + 1] = tot_rows + cs;
+      if (cs != 0) list[tot_groups] = S;
+      s_out = atomicAdd(pp.out_counter, static_cast<unsigned long long>(ngroups));
+    }
+    __syncthreads();
+
+    // 3. permute
+    for (uint32_t i = tid; i < len; i += blockDim.x) {
+      const uint32_t v = rec[i];
+      if (v == kNoRank) continue;
+      const int64_t from = r0 + i;
+      const int64_t to   = r0 + cnt[v >> kCtaRankBits] + (v & kCtaRankMask);
+      for (int c = 0; c < plan.nchan; ++c) {
+        const PartCol& a = in.col[c];
+        const PartCol& d = sorted.col[c];
+        store_bits(const_cast<void*>(d.vals), to, a.width, load_bits(a.vals, from, a.width));
+        if (a.valid != nullptr) const_cast<uint8_t*>(d.valid)[to] = __ldg(a.valid + from);
+      }
+    }
+
+    // 4. emit: the bucket's groups at output rows s_out + [0, ngroups), each
+    // with its key columns and (first sorted row, row count)
+    const unsigned long long ob = s_out;
+    for (uint32_t g0 = tid & ~31u; g0 < ngroups; g0 += blockDim.x) {
+      const bool active = g0 + lane < ngroups;
+      const uint32_t ss = active ? list[g0 + lane] : 0u;
+      const uint32_t act = __ballot_sync(kFull, active);
+      uint64_t k2[2]     = {0, 0};
+      const int64_t base = static_cast<int64_t>(ob + g0);
+      if (active) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) k2[w] = keys[ss * NW + w];
+        if (ss == S) k2[0] = k2[1] = kEmptyWord;
+        pp.group_run[base + lane] = make_uint2(static_cast<uint32_t>(r0) + cnt[ss], cnt[ss + 1] - cnt[ss]);
+      }
+      warp_write_keys(plan, op, active, k2, base, lane, act, sink);
+    }
+    __syncthreads();  // the table is reset for the next bucket
+  }
+  cta_nulls_flush(s_nulls, op.null_counts);
+}
+
 // Channel c's value outputs of the groups k_part_ranked emitted (output rows
 // [0, *pp.out_counter): it runs right after k_part_ranked, before any slice
 // adds output rows), one thread per group; one launch per channel, each
@@ -615,6 +801,9 @@ cudaError_t launch_part_scatter(const Plan& p, int64_t n, const PartPlan& pp, co
 }
 
 namespace {
+cudaError_t launch_folds(const Plan& p, const PartPlan& pp, const PartBufs& sorted, const OutPlan& op, int num_sms,
+                         cudaStream_t st);
+
 template <int NW, int NCH>
 cudaError_t launch_part_agg_impl(const Plan& p, const PartPlan& pp, const PartBufs& in, const TableRef& t,
                                  const SmemLayout& sl, int num_sms, cudaStream_t st)
@@ -677,6 +866,59 @@ cudaError_t launch_part_ranked_nw(const Plan& p, const PartPlan& pp, const PartB
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   k_part_ranked<NW><<<num_sms * per_sm, block, smem, st>>>(p, pp, in, sorted, sl, rl, op);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return launch_folds(p, pp, sorted, op, num_sms, st);
+}
+
+// Shared memory of k_part_ranked_cta: the table, counters and list, and as
+// many rank records as leave room for up to four CTAs per SM (at least 2,048
+// records each); buckets with more rows keep their records in global memory.
+template <int NW>
+cudaError_t launch_part_ranked_cta_nw(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
+                                      uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st)
+{
+  if (S < static_cast<uint32_t>(kCtaRankThreads) || S > 4096 || (S & (S - 1)) != 0 || pp.slice_rows > kCtaMaxSliceRows)
+    return cudaErrorInvalidValue;
+  int dev = 0, per_sm_bytes = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&per_sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+    return e;
+  CtaRankLayout cl{};
+  cl.slots    = S;
+  cl.cnt_off  = ((S + 1) * NW * 8 + 15) & ~15u;
+  cl.list_off = (cl.cnt_off + (S + 2) * 4 + 15) & ~15u;
+  cl.rec_off  = (cl.list_off + (S + 1) * 4 + 15) & ~15u;
+  int ctas    = 4;
+  while (ctas > 1 && static_cast<int64_t>(per_sm_bytes) / ctas - 2048 < cl.rec_off + 2048 * 4) --ctas;
+  const int64_t rec_bytes = static_cast<int64_t>(per_sm_bytes) / ctas - 2048 - cl.rec_off;
+  cl.rec_rows = rec_bytes > 0 ? static_cast<uint32_t>(std::min<int64_t>(rec_bytes / 4, pp.slice_rows)) & ~31u : 0u;
+  cl.total    = (cl.rec_off + cl.rec_rows * 4 + 15) & ~15u;
+  if ((e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_part_ranked_cta<NW>), cl.total)) != cudaSuccess)
+    return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_part_ranked_cta<NW>, kCtaRankThreads,
+                                                         cl.total)) != cudaSuccess)
+    return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  k_part_ranked_cta<NW><<<num_sms * per_sm, kCtaRankThreads, cl.total, st>>>(p, pp, in, sorted, cl, op);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return launch_folds(p, pp, sorted, op, num_sms, st);
+}
+}  // namespace
+
+cudaError_t launch_part_ranked_cta(const Plan& p, const PartPlan& pp, const PartBufs& in, const PartBufs& sorted,
+                                   uint32_t S, const OutPlan& op, int num_sms, cudaStream_t st)
+{
+  return p.key.nwords == 1 ? launch_part_ranked_cta_nw<1>(p, pp, in, sorted, S, op, num_sms, st)
+                           : launch_part_ranked_cta_nw<2>(p, pp, in, sorted, S, op, num_sms, st);
+}
+
+namespace {
+// One k_part_fold launch per value channel, each on its physical type.
+cudaError_t launch_folds(const Plan& p, const PartPlan& pp, const PartBufs& sorted, const OutPlan& op, int num_sms,
+                         cudaStream_t st)
+{
+  cudaError_t e = cudaSuccess;
   for (int c = 0; c < p.nchan; ++c) {
     switch (p.chan[c].ptype) {
       case P_I8: e = launch_fold<P_I8>(p, pp, sorted, op, c, num_sms, st); break;

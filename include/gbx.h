@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define GBX_ABI_VERSION 2
+#define GBX_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define GBX_API __attribute__((visibility("default")))
@@ -269,6 +269,11 @@ typedef struct gbx_stats {
   float compact_ms;      /* occupied-slot compaction */
   float finalize_ms;     /* output keys/results + null counts */
   float total_ms;        /* first to last event of the call */
+  /* partitioned strategy: log2 of the bucket count and the slots of each
+   * bucket's grouping table (a warp's, or, with buckets of a few thousand
+   * groups, a CTA's); 0 for the other strategies */
+  int32_t partition_bits;
+  int32_t bucket_slots;
 } gbx_stats;
 
 GBX_API int gbx_groupby_last_stats(const gbx_groupby* gb, gbx_stats* out);

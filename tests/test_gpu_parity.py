@@ -307,6 +307,27 @@ def test_partitioned_every_kind_and_type(card):
     assert got["stats"]["strategy"] == Strategy.PARTITIONED
 
 
+@pytest.mark.parametrize("two_words", [False, True], ids=["one_word", "two_words"])
+def test_partitioned_cta_tables(two_words):
+    """~7.8M groups of ~1 row: one grouping table per CTA over 2^16 buckets
+    (two radix passes, where warp tables would need 2^17 buckets and three),
+    with the all-ones key, null keys kept (INCLUDE) and null values."""
+    rng = np.random.default_rng(31 + two_words)
+    n = 8_000_000
+    a = rng.integers(0, 1 << 40, size=n).astype(np.int64)
+    a[::89] = -1
+    keys = [hc(a, rng.random(n) > 0.01)]
+    if two_words:
+        keys.append(hc(rng.integers(0, 3, size=n).astype(np.int32)))
+    x = rng.integers(-1000, 1000, size=n).astype(np.int32)
+    y = rng.standard_normal(n)
+    reqs = [(hc(x), ALL6), (hc(y, rng.random(n) > 0.2), ALL6)]
+    got, _ = T.assert_parity(keys, reqs, NullPolicy.INCLUDE, Strategy.PARTITIONED)
+    st = got["stats"]
+    assert (st["partition_bits"], st["retries"]) == (16, 0)
+    assert st["bucket_slots"] >= 256
+
+
 def test_partitioned_skewed_keys():
     """Zipf-skewed composite keys: one bucket holds a large share of the rows."""
     d = W.plain_200m(n=1_500_000, ranks=50_000)
