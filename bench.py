@@ -61,7 +61,7 @@ def parse_args(argv=None):
     p.add_argument("--rows", type=int, default=ROWS)
     p.add_argument("--cards", type=str, default=",".join(str(c) for c in CARDS))
     p.add_argument("--cpu-sample-rows", type=int, default=2_000_000)
-    p.add_argument("--strategy", choices=["auto", "warp", "privatized", "global", "partitioned"], default="auto",
+    p.add_argument("--strategy", choices=["auto", "warp", "privatized", "global", "partitioned", "bucketed"], default="auto",
                    help="force one aggregation strategy (default: chosen per call)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")

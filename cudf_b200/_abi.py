@@ -96,6 +96,7 @@ class Strategy(enum.IntEnum):
     GLOBAL = 2
     PARTITIONED = 3
     WARP = 4
+    BUCKETED = 5
 
 
 # element width in bytes of each fixed-width type (0: not fixed width)

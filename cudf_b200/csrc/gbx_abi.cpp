@@ -621,7 +621,7 @@ int gbx_groupby_set_strategy(gbx_groupby* gb, int32_t strategy)
     GBX_EXPECTS(gb != nullptr, "null groupby");
     GBX_EXPECTS(strategy == GBX_STRATEGY_AUTO || strategy == GBX_STRATEGY_PRIVATIZED ||
                   strategy == GBX_STRATEGY_GLOBAL || strategy == GBX_STRATEGY_WARP ||
-                  strategy == GBX_STRATEGY_PARTITIONED,
+                  strategy == GBX_STRATEGY_PARTITIONED || strategy == GBX_STRATEGY_BUCKETED,
                 "strategy %d not available", strategy);
     gb->strategy = strategy;
   });
@@ -831,7 +831,34 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     // partitioned path's 19.5 ms
     const bool global_in_l2 =
       static_cast<double>(cap + 1) * static_cast<double>(slot_bytes) <= static_cast<double>(call.dev.l2_bytes);
+    // BUCKETED: one radix pass into 2^8 buckets (two passes, 2^16, when a
+    // bucket holds too many groups), then the tiled kernel over contiguous
+    // runs of the bucket-ordered rows, one run per CTA (two CTAs per SM): a run
+    // meets about est / runs groups plus those of the bucket or two it cuts,
+    // which must fit a tiled table at load <= 1/2
+    // (below kBucketedMinRows rows the partitioning costs more than the global
+    // table's atomics it saves)
+    constexpr int64_t kBucketedMinRows = int64_t(1) << 22;
+    int bucket_bits       = 0;
+    uint32_t bucket_slots = 0;
+    for (int bb : {8, 16}) {
+      const double groups = est / (2.0 * call.dev.num_sms) + est / static_cast<double>(1u << bb);
+      const auto Sb = static_cast<uint32_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * groups, 64.0))));
+      if (Sb <= 1024 && tiled_fits(make_smem_layout(plan, Sb), plan.nchan)) {
+        bucket_bits  = bb;
+        bucket_slots = Sb;
+        break;
+      }
+    }
     int strategy = gb->strategy;
+    if (strategy == GBX_STRATEGY_BUCKETED && bucket_bits == 0) {
+      // forced with more groups than a tiled table holds: the largest table
+      // that fits (rows of groups beyond it go to the global table directly)
+      bucket_bits = 16;
+      for (uint32_t Sb = 1024; Sb >= 64 && bucket_slots == 0; Sb >>= 1)
+        if (tiled_fits(make_smem_layout(plan, Sb), plan.nchan)) bucket_slots = Sb;
+      if (bucket_slots == 0) strategy = GBX_STRATEGY_GLOBAL;
+    }
     if (strategy == GBX_STRATEGY_AUTO) {
       // measured on B200 (100M rows, 12 accumulators): at 100 groups the shared
       // table with 32/64-bit shared atomics 4.0 ms, warp-private tables 7.2 ms;
@@ -839,7 +866,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       // path 21.4 ms; at 1e6 groups (table beyond L2) 32.6 ms against 17.2 ms
       if (est * 2.0 <= static_cast<double>(s_max)) strategy = GBX_STRATEGY_PRIVATIZED;
       else if (warp_fits) strategy = GBX_STRATEGY_WARP;
-      else if (global_in_l2) strategy = GBX_STRATEGY_GLOBAL;
+      else if (global_in_l2)
+        strategy = bucket_bits > 0 && call.n >= kBucketedMinRows ? GBX_STRATEGY_BUCKETED : GBX_STRATEGY_GLOBAL;
       else strategy = GBX_STRATEGY_PARTITIONED;
     }
     if (strategy == GBX_STRATEGY_WARP && !warp_fits) strategy = GBX_STRATEGY_PRIVATIZED;
@@ -907,6 +935,22 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         for (int k = 0; k < requests[q].num_aggregations; ++k, ++o) fn(res->requests[q].results[k], kMaxKeyCols + o);
     };
 
+    // bucket-ordered copies of the rows (radix partitioning): packed key
+    // words, resolved value bits, a validity byte per row of a nullable channel
+    auto part_bufs = [&]() {
+      PartBufs pb{};
+      for (int w = 0; w < plan.key.nwords; ++w)
+        pb.keys[w] = static_cast<const uint64_t*>(scratch.get(static_cast<size_t>(call.n) * 8));
+      for (int c = 0; c < plan.nchan; ++c) {
+        const int width = pt_width(plan.chan[c].ptype);
+        pb.col[c].width = width;
+        pb.col[c].vals  = scratch.get(static_cast<size_t>(call.n) * width);
+        pb.col[c].valid =
+          plan.chan[c].a_cnt >= 0 ? static_cast<const uint8_t*>(scratch.get(static_cast<size_t>(call.n))) : nullptr;
+      }
+      return pb;
+    };
+
     if (strategy == GBX_STRATEGY_PARTITIONED) {
       // ---- radix-partitioned path (gbx_part.cu)
       // warp table slots (two CTAs per SM), halved until eight warps' tables
@@ -941,25 +985,6 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
           std::min<uint64_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * est / static_cast<double>(1ull << bits), 256.0))),
                              4096));
       }
-      // bucket-ordered copies of the rows: packed key words, resolved value
-      // bits, a validity byte per row of a nullable channel
-      auto part_bufs = [&]() {
-        PartBufs pb{};
-        for (int w = 0; w < plan.key.nwords; ++w)
-          pb.keys[w] = static_cast<const uint64_t*>(scratch.get(static_cast<size_t>(call.n) * 8));
-        for (int c = 0; c < plan.nchan; ++c) {
-          const int8_t pt = plan.chan[c].ptype;
-          const int width = (pt == P_I8 || pt == P_U8 || pt == P_BOOL) ? 1
-                            : (pt == P_I16 || pt == P_U16)             ? 2
-                            : (pt == P_I32 || pt == P_U32 || pt == P_F32) ? 4
-                                                                          : 8;
-          pb.col[c].width = width;
-          pb.col[c].vals  = scratch.get(static_cast<size_t>(call.n) * width);
-          pb.col[c].valid =
-            plan.chan[c].a_cnt >= 0 ? static_cast<const uint8_t*>(scratch.get(static_cast<size_t>(call.n))) : nullptr;
-        }
-        return pb;
-      };
       PartBufs pbufs = part_bufs();
       // the radix passes' second set of copies and their counters
       PartBufs tbufs{};
@@ -1150,6 +1175,23 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         } else {
           GBX_CUDA(launch_agg_privatized(plan, t, sl, call.n, block, grid, std::min<uint32_t>(S, 32), max_probes, s));
         }
+      } else if (strategy == GBX_STRATEGY_BUCKETED) {
+        // radix passes into bucket order, then tiles of the bucket-ordered
+        // rows grouped in shared memory (gbx_tiled.cu)
+        const PartBufs pb  = part_bufs();
+        const PartBufs tmp = bucket_bits > 8 ? part_bufs() : pb;  // one pass writes `pb` only
+        auto* rcounts      = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
+        auto* roffsets     = static_cast<uint32_t*>(scratch.get(part_radix_count_bytes(call.n)));
+        size_t rtemp_bytes = 0;
+        GBX_CUDA(part_radix_temp_bytes(call.n, &rtemp_bytes));
+        void* rtemp  = scratch.get(rtemp_bytes);
+        auto* n_kept = static_cast<uint32_t*>(scratch.get(sizeof(uint32_t)));
+        GBX_CUDA(launch_part_radix_hist0(plan, call.n, bucket_bits, rcounts, nullptr, s));
+        GBX_CUDA(launch_part_radix(plan, call.n, bucket_bits, n_kept, pb, tmp, rcounts, roffsets, rtemp, rtemp_bytes,
+                                   d_status, /*hist0_done=*/true, s));
+        GBX_CUDA(launch_agg_tiled_part(plan, t, make_smem_layout(plan, bucket_slots), pb, n_kept, call.n,
+                                       call.dev.num_sms, std::min<uint32_t>(bucket_slots, 32), max_probes, s));
+        launches += 1 + 3 * ((bucket_bits + 7) / 8);  // first histogram, 3 per pass
       } else {
         GBX_CUDA(launch_agg_global(plan, t, call.n, max_probes, call.dev.num_sms, s));
       }
@@ -1182,11 +1224,16 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       // the groups present can number at most the rows: size for that bound
       cap = std::min<uint64_t>(std::max<uint64_t>(cap * 4, next_pow2(2 * static_cast<uint64_t>(call.n) + 2)),
                                1ULL << 31);
-      if (strategy == GBX_STRATEGY_PRIVATIZED || strategy == GBX_STRATEGY_WARP) strategy = GBX_STRATEGY_GLOBAL;
+      if (strategy == GBX_STRATEGY_PRIVATIZED || strategy == GBX_STRATEGY_WARP || strategy == GBX_STRATEGY_BUCKETED)
+        strategy = GBX_STRATEGY_GLOBAL;
       est = static_cast<double>(call.n);
     }
     gb->stats.strategy        = strategy;
     gb->stats.table_capacity  = static_cast<int64_t>(cap);
+    if (strategy == GBX_STRATEGY_BUCKETED) {
+      gb->stats.partition_bits = bucket_bits;
+      gb->stats.bucket_slots   = static_cast<int32_t>(bucket_slots);
+    }
     gb->stats.num_groups      = G;
     gb->stats.scratch_bytes   = static_cast<int64_t>(scratch.total());
     gb->stats.kernel_launches = launches + (G > 0 ? 1 : 0);  // + finalize

@@ -100,6 +100,13 @@ struct PartPlan {
   uint2* group_run;
 };
 
+// launch_agg_tiled over the bucket-ordered copies `in` of a radix
+// partitioning (*n_rows rows, at most n): each CTA takes one contiguous run of
+// tiles, so its table holds the groups of the few buckets that run covers.
+cudaError_t launch_agg_tiled_part(const Plan& p, const TableRef& t, const SmemLayout& sl, const PartBufs& in,
+                                  const uint32_t* n_rows, int64_t n, int num_sms, uint32_t smem_probes,
+                                  uint32_t max_probes, cudaStream_t st);
+
 cudaError_t launch_part_hist(const KeyPlan& kp, int64_t n, const PartPlan& pp, int num_sms, cudaStream_t st);
 // counts -> offsets (unless offsets_ready), nslices, item_start, multi,
 // region (device scans)

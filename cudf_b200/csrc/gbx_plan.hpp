@@ -40,6 +40,14 @@ enum PhysType : int8_t {
   P_NONE
 };
 
+// Bytes of one element of a physical type.
+constexpr int pt_width(int pt)
+{
+  return (pt == P_I8 || pt == P_U8 || pt == P_BOOL) ? 1 : (pt == P_I16 || pt == P_U16) ? 2
+         : (pt == P_I32 || pt == P_U32 || pt == P_F32)                                 ? 4
+                                                                                        : 8;
+}
+
 // Accumulator element kinds: decide identity, merge op and width.
 enum AccKind : int8_t {
   A_U32_ADD = 0,  // counts

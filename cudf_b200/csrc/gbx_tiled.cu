@@ -134,12 +134,18 @@ TiledLayout pick_tiled_layout(const SmemLayout& sl, int nchan)
   return none;
 }
 
-template <int NW>
+// PART: the rows are the bucket-ordered copies `pb` of the radix
+// partitioning (*n_part of them) and each CTA takes one contiguous run of
+// tiles, so that its table only sees the groups of the few buckets the run
+// covers; otherwise the caller's n rows, tiles dealt round-robin.
+template <int NW, bool PART>
 __global__ void __launch_bounds__(kTiledBlock, 2) k_agg_tiled(const __grid_constant__ Plan plan,
                                                            const __grid_constant__ TableRef t,
                                                            const __grid_constant__ SmemLayout sl,
                                                            const __grid_constant__ TiledLayout tl, int64_t n,
-                                                           uint32_t smem_probes, uint32_t max_probes)
+                                                           const __grid_constant__ PartBufs pb,
+                                                           const uint32_t* n_part, uint32_t smem_probes,
+                                                           uint32_t max_probes)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   using BlockScan = cub::BlockScan<uint32_t, kTiledBlock>;
@@ -177,8 +183,13 @@ __global__ void __launch_bounds__(kTiledBlock, 2) k_agg_tiled(const __grid_const
 
   const Level<Global> G = global_level(t);
   const RowSource src{&plan};
-  const int64_t ntiles = (n + tile_rows - 1) / tile_rows;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  const PartSource psrc{&pb};
+  if constexpr (PART) n = *n_part;
+  const int64_t ntiles     = (n + tile_rows - 1) / tile_rows;
+  const int64_t tile_begin = PART ? ntiles * blockIdx.x / gridDim.x : blockIdx.x;
+  const int64_t tile_end   = PART ? ntiles * (blockIdx.x + 1) / gridDim.x : ntiles;
+  const int64_t tile_step  = PART ? 1 : gridDim.x;
+  for (int64_t tile = tile_begin; tile < tile_end; tile += tile_step) {
     const int64_t t0 = tile * tile_rows;
     // 1a. keys (this thread's rows threadIdx.x + q * kTiledBlock)
     uint64_t k[kTiledPer][NW];
@@ -186,14 +197,32 @@ __global__ void __launch_bounds__(kTiledBlock, 2) k_agg_tiled(const __grid_const
 #pragma unroll
     for (int q = 0; q < kTiledPer; ++q) {
       const int64_t r = t0 + threadIdx.x + q * kTiledBlock;
-      kept[q]         = q < per && r < n && pack_key<NW>(plan.key, r, k[q]);
+      if constexpr (PART) kept[q] = q < per && r < n && psrc.key<NW>(r, k[q]);
+      else kept[q] = q < per && r < n && pack_key<NW>(plan.key, r, k[q]);
     }
     // 1b. values and validity of the kept rows, staged channel by channel
     for (int c = 0; c < plan.nchan; ++c) {
       const Channel& ch = plan.chan[c];
       uint64_t* cv      = vals + static_cast<size_t>(c) * tile_rows;
       uint8_t* cvv      = valid + static_cast<size_t>(c) * tile_rows;
-      if (ch.dict_data == nullptr) {
+      if constexpr (PART) {
+        const PartCol& pc = pb.col[c];
+        uint64_t b[kTiledPer];
+        bool v[kTiledPer];
+#pragma unroll
+        for (int q = 0; q < kTiledPer; ++q) {
+          const int64_t i = t0 + threadIdx.x + q * kTiledBlock;
+          b[q]            = kept[q] ? load_bits(pc.vals, i, pc.width) : 0;
+          v[q]            = kept[q] && (pc.valid == nullptr || __ldg(pc.valid + i) != 0);
+        }
+#pragma unroll
+        for (int q = 0; q < kTiledPer; ++q) {
+          if (!kept[q]) continue;
+          const int li = threadIdx.x + q * kTiledBlock;
+          cv[li]       = v[q] ? b[q] : 0;
+          cvv[li]      = v[q] ? 1 : 0;
+        }
+      } else if (ch.dict_data == nullptr) {
         const int w = pt_width(ch.ptype);
         uint64_t b[kTiledPer];
         bool v[kTiledPer];
@@ -240,7 +269,11 @@ __global__ void __launch_bounds__(kTiledBlock, 2) k_agg_tiled(const __grid_const
         rec[q]              = (static_cast<uint32_t>(s) << 16) | rank;
       } else {
         const int64_t g = global_slot<NW>(t, k[q], max_probes);
-        if (g >= 0) accumulate_row<Global>(plan, G, g, t0 + threadIdx.x + q * kTiledBlock, t.status);
+        const int64_t r = t0 + threadIdx.x + q * kTiledBlock;
+        if (g >= 0) {
+          if constexpr (PART) accumulate_row_from<Global>(plan, psrc, G, g, r, t.status);
+          else accumulate_row<Global>(plan, G, g, r, t.status);
+        }
       }
     }
     __syncthreads();
@@ -356,20 +389,22 @@ __global__ void __launch_bounds__(kTiledBlock, 2) k_agg_tiled(const __grid_const
   }
 }
 
-template <int NW>
+template <int NW, bool PART>
 cudaError_t launch_tiled_nw(const Plan& p, const TableRef& t, const SmemLayout& sl, const TiledLayout& tl,
-                            int64_t n, int num_sms, uint32_t smem_probes, uint32_t max_probes, cudaStream_t st)
+                            int64_t n, const PartBufs& pb, const uint32_t* n_part, int num_sms,
+                            uint32_t smem_probes, uint32_t max_probes, cudaStream_t st)
 {
-  cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_agg_tiled<NW>), tl.total);
+  const void* fn = reinterpret_cast<const void*>(k_agg_tiled<NW, PART>);
+  cudaError_t e  = ensure_dynamic_smem(fn, tl.total);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_agg_tiled<NW>, kTiledBlock, tl.total)) !=
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_agg_tiled<NW, PART>, kTiledBlock, tl.total)) !=
       cudaSuccess)
     return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   const int64_t ntiles = (n + tl.tile_rows - 1) / tl.tile_rows;
   const int grid       = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(num_sms) * per_sm)));
-  k_agg_tiled<NW><<<grid, kTiledBlock, tl.total, st>>>(p, t, sl, tl, n, smem_probes, max_probes);
+  k_agg_tiled<NW, PART><<<grid, kTiledBlock, tl.total, st>>>(p, t, sl, tl, n, pb, n_part, smem_probes, max_probes);
   return cudaGetLastError();
 }
 
@@ -386,8 +421,20 @@ cudaError_t launch_agg_tiled(const Plan& p, const TableRef& t, const SmemLayout&
   if (!tiled_fits(sl, p.nchan)) return cudaErrorInvalidValue;
   if (n <= 0) return cudaSuccess;
   const TiledLayout tl = pick_tiled_layout(sl, p.nchan);
-  return p.key.nwords == 1 ? launch_tiled_nw<1>(p, t, sl, tl, n, num_sms, smem_probes, max_probes, st)
-                           : launch_tiled_nw<2>(p, t, sl, tl, n, num_sms, smem_probes, max_probes, st);
+  const PartBufs none{};
+  return p.key.nwords == 1 ? launch_tiled_nw<1, false>(p, t, sl, tl, n, none, nullptr, num_sms, smem_probes, max_probes, st)
+                           : launch_tiled_nw<2, false>(p, t, sl, tl, n, none, nullptr, num_sms, smem_probes, max_probes, st);
+}
+
+cudaError_t launch_agg_tiled_part(const Plan& p, const TableRef& t, const SmemLayout& sl, const PartBufs& in,
+                                  const uint32_t* n_rows, int64_t n, int num_sms, uint32_t smem_probes,
+                                  uint32_t max_probes, cudaStream_t st)
+{
+  if (!tiled_fits(sl, p.nchan)) return cudaErrorInvalidValue;
+  if (n <= 0) return cudaSuccess;
+  const TiledLayout tl = pick_tiled_layout(sl, p.nchan);
+  return p.key.nwords == 1 ? launch_tiled_nw<1, true>(p, t, sl, tl, n, in, n_rows, num_sms, smem_probes, max_probes, st)
+                           : launch_tiled_nw<2, true>(p, t, sl, tl, n, in, n_rows, num_sms, smem_probes, max_probes, st);
 }
 
 }  // namespace gbx

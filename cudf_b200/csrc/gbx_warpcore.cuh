@@ -406,12 +406,6 @@ __device__ __forceinline__ bool chan_is_float(const Channel& ch)
 {
   return PT >= 0 ? (PT == P_F32 || PT == P_F64) : ch.is_float != 0;
 }
-constexpr int pt_width(int pt)
-{
-  return (pt == P_I8 || pt == P_U8 || pt == P_BOOL) ? 1 : (pt == P_I16 || pt == P_U16) ? 2
-         : (pt == P_I32 || pt == P_U32 || pt == P_F32)                                 ? 4
-                                                                                        : 8;
-}
 
 // Folds one valid value (raw bits) into a channel's registers, with the
 // arithmetic of apply_row (integers wrap, floats in double, the shift K is

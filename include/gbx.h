@@ -245,7 +245,9 @@ typedef enum gbx_strategy {
   GBX_STRATEGY_PRIVATIZED = 1, /* per-CTA shared-memory tables, flushed to a global table */
   GBX_STRATEGY_GLOBAL     = 2, /* every row updates the global open-addressing table */
   GBX_STRATEGY_PARTITIONED = 3, /* radix-partition rows by key hash, then per-partition smem tables */
-  GBX_STRATEGY_WARP       = 4  /* per-warp private shared-memory tables, no atomics on the hot path */
+  GBX_STRATEGY_WARP       = 4, /* per-warp private shared-memory tables, no atomics on the hot path */
+  GBX_STRATEGY_BUCKETED   = 5  /* radix-partition rows into 2^8 or 2^16 buckets, then group tiles of the
+                                  bucket-ordered rows in per-CTA shared-memory tables, flushed to a global table */
 } gbx_strategy;
 
 /* Force a strategy for subsequent calls on this gb object (AUTO restores). */

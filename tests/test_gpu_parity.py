@@ -17,7 +17,8 @@ from tests import gbx_testing as T
 pytestmark = pytest.mark.gpu
 
 ALL6 = [(Kind.SUM, 0), (Kind.COUNT_VALID, 0), (Kind.MIN, 0), (Kind.MAX, 0), (Kind.MEAN, 0), (Kind.VARIANCE, 1)]
-STRATS = [Strategy.AUTO, Strategy.PRIVATIZED, Strategy.GLOBAL, Strategy.WARP, Strategy.PARTITIONED]
+STRATS = [Strategy.AUTO, Strategy.PRIVATIZED, Strategy.GLOBAL, Strategy.WARP, Strategy.PARTITIONED,
+          Strategy.BUCKETED]
 
 
 def hc(a, v=None, **kw):
@@ -326,6 +327,23 @@ def test_partitioned_cta_tables(two_words):
     st = got["stats"]
     assert (st["partition_bits"], st["retries"]) == (16, 0)
     assert st["bucket_slots"] >= 256
+
+
+@pytest.mark.parametrize("card,bits", [(10_000, 8), (40_000, 16)])
+def test_bucketed_chosen_for_mid_cardinality(card, bits):
+    """5M rows over 1e4 / 4e4 groups: AUTO partitions the rows into buckets
+    and groups tiles of the bucket-ordered rows in shared memory -- one radix
+    pass (2^8 buckets) at 1e4; at 4e4 a CTA's run would meet ~290 groups, more
+    than a 512-slot table holds at half load, so two passes (2^16)."""
+    rng = np.random.default_rng(40 + card)
+    n = 5_000_000
+    k = rng.integers(0, card, size=n).astype(np.int64) * 7919 - 3
+    a = rng.integers(-10**6, 10**6, size=n).astype(np.int64)
+    b = rng.standard_normal(n).astype(np.float32)
+    bv = rng.random(n) > 0.1
+    got, _ = T.assert_parity([hc(k)], [(hc(a), ALL6), (hc(b, bv), ALL6)])
+    st = got["stats"]
+    assert (st["strategy"], st["partition_bits"], st["retries"]) == (Strategy.BUCKETED, bits, 0)
 
 
 def test_partitioned_skewed_keys():
