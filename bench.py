@@ -11,7 +11,9 @@ per groupby) are larger than L2 (126 MB), so no L2 flush is needed.
   value  -- rows/s over the whole job with inputs resident in HBM, through the
             public API (cudf_b200.GroupBy.aggregate), CUDA events on the stream
   e2e    -- same metric with host (pinned) inputs: every step copies inputs
-            host->device and reads all results back device->host
+            host->device and reads all results back device->host, the four
+            calls pipelined over PCIe (uploads on one copy stream, read-backs
+            on another, overlapping the other calls' transfers and compute)
   roofline -- the partitioned path's aggregation phase (k_part_ranked and one
             k_part_fold per value channel): its algorithmic bytes (rows read,
             groups written) / its CUDA-event duration, against the measured
@@ -399,9 +401,9 @@ def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
     out_host = torch.empty(int(max_groups * BYTES_PER_GROUP_OUT * 1.1) + (1 << 20), dtype=torch.uint8,
                            pin_memory=True)
 
-    def read_back(outs):
-        """D2H of each column's rows (data and mask) into the pinned buffer."""
-        off = 0
+    def read_back(outs, off):
+        """D2H of each column's rows (data and mask) into the pinned buffer from
+        byte `off` on; returns the offset after them."""
         for col in outs:
             if col.size == 0:
                 continue
@@ -415,12 +417,30 @@ def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
                 off += nb
         return off
 
+    # The step's four groupbys are pipelined over PCIe, which carries both
+    # directions at once: every upload is queued on one copy stream, each
+    # call starts when its own inputs have landed, and its results are read
+    # back on a second copy stream while the later calls upload and compute.
+    # The call with the most output goes first, so that its read-back
+    # overlaps the other uploads.
+    order = sorted(cards, key=lambda c: -c)
+    up = torch.cuda.Stream(device)
+    down = torch.cuda.Stream(device)
+
     def step():
-        for c in cards:
-            hk, ha, hb, hm = host[c]
+        up.wait_stream(stream)
+        landed = {}
+        with torch.cuda.stream(up):
+            for c in order:
+                for s_, d_ in zip(host[c], dev[c]):
+                    d_.copy_(s_, non_blocking=True)
+                landed[c] = torch.cuda.Event()
+                landed[c].record(up)
+        off = 0
+        keep = []
+        for c in order:
             dk, da, db, dm = dev[c]
-            for s_, d_ in zip(host[c], dev[c]):
-                d_.copy_(s_, non_blocking=True)
+            stream.wait_event(landed[c])
             n = dk.numel()
             kc = Column(data[c][0].type_id, n, dk)
             ac = Column(data[c][1].type_id, n, da)
@@ -429,9 +449,12 @@ def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
             kt, res = gb.aggregate([GroupByRequest(ac, aggs()), GroupByRequest(bc, aggs())], stream=stream,
                                    allocator=alloc)
             outs = [col for col in kt.columns()] + [col for t in res for col in t.columns()]
-            got = read_back(outs)
-            stream.synchronize()
-            d2h_bytes[0] = got if c == cards[0] else d2h_bytes[0] + got
+            down.wait_stream(stream)
+            with torch.cuda.stream(down):
+                off = read_back(outs, off)
+            keep.append(outs)  # alive until the read-back is ordered before reuse
+        stream.wait_stream(down)
+        d2h_bytes[0] = off
 
     step()
     torch.cuda.synchronize()
