@@ -969,18 +969,22 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       const double gpb  = S * 0.5;
       int bits          = 0;
       while (static_cast<double>(1ull << bits) * gpb < est && bits < 22) ++bits;
-      // one table per CTA (up to 4,096 slots, ~2,048 groups per bucket) where
-      // that needs fewer 8-bit radix passes than warp tables do; the bucket
-      // count is then rounded up to whole passes (smaller buckets, same
-      // passes) and the table sized for twice a bucket's mean groups
+      // one table per CTA instead (up to 4,096 slots, ~2,048 groups per
+      // bucket) from 2^9 such buckets on: where that needs fewer 8-bit radix
+      // passes than warp tables do, the bucket count is rounded up to whole
+      // passes (smaller buckets, same passes), else it stays the warp tables'
+      // (measured at 1e6 groups in 100M rows, 2^14 buckets: grouping and folds
+      // 3.4 ms with CTA tables against 5.6 ms with warp tables; at 1e8, 2^16
+      // buckets of 256-2,048 slots ran 9.2 ms against 10.5 ms for 2^15 of
+      // 4,096); the table is sized for twice a bucket's mean groups
       const int warp_bits = bits;
       int cta_bits        = 0;
       while (static_cast<double>(1ull << cta_bits) * 2048.0 < est && cta_bits < 22) ++cta_bits;
       bool cta_rank  = false;
       uint32_t S_cta = 0;
-      if (cta_bits >= 9 && (cta_bits + 7) / 8 < (warp_bits + 7) / 8) {
+      if (cta_bits >= 9 && (cta_bits + 7) / 8 <= (warp_bits + 7) / 8) {
         cta_rank = true;
-        bits     = 8 * ((cta_bits + 7) / 8);
+        bits     = (cta_bits + 7) / 8 < (warp_bits + 7) / 8 ? 8 * ((cta_bits + 7) / 8) : warp_bits;
         S_cta    = static_cast<uint32_t>(
           std::min<uint64_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * est / static_cast<double>(1ull << bits), 256.0))),
                              4096));
@@ -1115,13 +1119,14 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
           gb->stats.bucket_slots   = static_cast<int32_t>(cta_rank ? S_cta : S);
           break;
         }
-        // a bucket held more groups than its table: warp tables at their own
-        // bucket count, else 4x the buckets
+        // a bucket held more groups than its table: warp tables (whose slices
+        // of very large buckets merge through their own region tables) at
+        // their own bucket count or 4x the failed one, else 4x the buckets
         if (attempt >= 3 || bits >= 24) fail(GBX_ERR_DEVICE, "partitioned aggregation overflow at %u buckets", P);
         gb->stats.retries++;
         if (cta_rank) {
           cta_rank = false;
-          bits     = warp_bits;
+          bits     = std::max(warp_bits, bits + 2);
         } else {
           bits += 2;
         }
