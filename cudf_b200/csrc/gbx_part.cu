@@ -362,6 +362,7 @@ struct CtaRankLayout {
 };
 
 constexpr int kCtaRankThreads = 256;
+constexpr int kCtaBatch       = 4;  // rows a thread loads together in k_part_ranked_cta's row loops
 // Rank records of k_part_ranked_cta: slot (up to 4,096, 13 bits) above a
 // 19-bit rank, so that one CTA takes buckets of up to 2^19 rows.
 constexpr int kCtaRankBits          = 19;
@@ -448,22 +449,33 @@ __global__ void __launch_bounds__(kCtaRankThreads, 4) k_part_ranked_cta(const __
     }
     __syncthreads();
 
-    // 1. rank
-    for (uint32_t i = tid; i < len; i += blockDim.x) {
-      uint64_t k[NW];
-      uint32_t v = kNoRank;
-      if (src.key<NW>(r0 + i, k)) {
-        int64_t slot = S;
-        if (!key_is_empty<NW>(k)) {
-          slot = find_or_insert<Shared, NW>(keys_sa, S - 1, k, hash_key<NW>(k), S);
-          if (slot < 0) atomicOr(pp.status, S_TABLE_FULL);  // more groups than the table: host retries
-        }
-        if (slot >= 0) {
-          const uint32_t rank = atomicAdd(cnt + slot, 1u);
-          v                   = (static_cast<uint32_t>(slot) << kCtaRankBits) | rank;
-        }
+    // 1. rank (kCtaBatch rows a thread: their key loads in flight together)
+    for (uint32_t i0 = tid; i0 < len; i0 += kCtaBatch * blockDim.x) {
+      uint64_t k[kCtaBatch][NW];
+      bool act[kCtaBatch];
+#pragma unroll
+      for (int q = 0; q < kCtaBatch; ++q) {
+        const uint32_t i = i0 + q * blockDim.x;
+        act[q]           = i < len && src.key<NW>(r0 + i, k[q]);
       }
-      rec[i] = v;
+#pragma unroll
+      for (int q = 0; q < kCtaBatch; ++q) {
+        const uint32_t i = i0 + q * blockDim.x;
+        if (i >= len) break;
+        uint32_t v = kNoRank;
+        if (act[q]) {
+          int64_t slot = S;
+          if (!key_is_empty<NW>(k[q])) {
+            slot = find_or_insert<Shared, NW>(keys_sa, S - 1, k[q], hash_key<NW>(k[q]), S);
+            if (slot < 0) atomicOr(pp.status, S_TABLE_FULL);  // more groups than the table: host retries
+          }
+          if (slot >= 0) {
+            const uint32_t rank = atomicAdd(cnt + slot, 1u);
+            v                   = (static_cast<uint32_t>(slot) << kCtaRankBits) | rank;
+          }
+        }
+        rec[i] = v;
+      }
     }
     __syncthreads();
 
@@ -498,17 +510,33 @@ __global__ void __launch_bounds__(kCtaRankThreads, 4) k_part_ranked_cta(const __
     }
     __syncthreads();
 
-    // 3. permute
-    for (uint32_t i = tid; i < len; i += blockDim.x) {
-      const uint32_t v = rec[i];
-      if (v == kNoRank) continue;
-      const int64_t from = r0 + i;
-      const int64_t to   = r0 + cnt[v >> kCtaRankBits] + (v & kCtaRankMask);
+    // 3. permute (kCtaBatch rows a thread, each channel's loads in flight
+    // together before its stores)
+    for (uint32_t i0 = tid; i0 < len; i0 += kCtaBatch * blockDim.x) {
+      int64_t to[kCtaBatch];
+#pragma unroll
+      for (int q = 0; q < kCtaBatch; ++q) {
+        const uint32_t i = i0 + q * blockDim.x;
+        const uint32_t v = i < len ? rec[i] : kNoRank;
+        to[q]            = v == kNoRank ? -1 : r0 + cnt[v >> kCtaRankBits] + (v & kCtaRankMask);
+      }
       for (int c = 0; c < plan.nchan; ++c) {
         const PartCol& a = in.col[c];
         const PartCol& d = sorted.col[c];
-        store_bits(const_cast<void*>(d.vals), to, a.width, load_bits(a.vals, from, a.width));
-        if (a.valid != nullptr) const_cast<uint8_t*>(d.valid)[to] = __ldg(a.valid + from);
+        uint64_t x[kCtaBatch];
+        uint8_t ok[kCtaBatch];
+#pragma unroll
+        for (int q = 0; q < kCtaBatch; ++q) {
+          const int64_t from = r0 + i0 + q * blockDim.x;
+          x[q]               = to[q] >= 0 ? load_bits(a.vals, from, a.width) : 0;
+          ok[q]              = to[q] >= 0 && a.valid != nullptr ? __ldg(a.valid + from) : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < kCtaBatch; ++q) {
+          if (to[q] < 0) continue;
+          store_bits(const_cast<void*>(d.vals), to[q], a.width, x[q]);
+          if (a.valid != nullptr) const_cast<uint8_t*>(d.valid)[to[q]] = ok[q];
+        }
       }
     }
 
