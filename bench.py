@@ -14,7 +14,7 @@ per groupby) are larger than L2 (126 MB), so no L2 flush is needed.
             host->device and reads all results back device->host, the four
             calls pipelined over PCIe (uploads on one copy stream, read-backs
             on another, overlapping the other calls' transfers and compute)
-  roofline -- the partitioned path's aggregation phase (k_part_ranked and one
+  roofline -- the partitioned path's aggregation phase (k_part_ranked_cta and one
             k_part_fold per value channel): its algorithmic bytes (rows read,
             groups written) / its CUDA-event duration, against the measured
             HBM copy bandwidth
@@ -48,10 +48,10 @@ BYTES_PER_GROUP_OUT = 8 + (8 + 4 + 8 + 8 + 8 + 8) + (4 + 4 + 4 + 4 + 8 + 8) + 6.
 METRIC = "groupby rows/s (plain hash groupby, 100M rows, int64 key, cardinality 1e2/1e4/1e6/1e8)"
 PARTITIONED = 3  # gbx_strategy of the radix-partitioned path
 # DRAM bytes per row of the aggregation phase measured by ncu (20M rows,
-# cardinality 2e7): k_part_ranked 0.429 GB read + 0.423 GB written,
-# k_part_fold (int64 channel) 0.262 + 0.504, k_part_fold (float32 channel)
-# 0.204 + 0.360
-AGG_PHASE_DRAM_BYTES_PER_ROW = (0.428523e9 + 0.423397e9 + 0.261882e9 + 0.503935e9 + 0.204437e9 + 0.360262e9) / 20_000_000
+# cardinality 2e7): k_part_ranked_cta 0.421 GB read + 0.418 GB written,
+# k_part_fold (int64 channel) 0.261 + 0.503, k_part_fold (float32 channel)
+# 0.201 + 0.361
+AGG_PHASE_DRAM_BYTES_PER_ROW = (0.421107e9 + 0.417534e9 + 0.261240e9 + 0.503070e9 + 0.201434e9 + 0.360507e9) / 20_000_000
 
 
 def parse_args(argv=None):
@@ -75,9 +75,10 @@ def parse_args(argv=None):
     p.add_argument("--batch-tune-save", type=str, default=None,
                    help="write the tuning table the batch used (and extended) to this path")
     p.add_argument("--served-requests", type=int, default=200)
-    # 4 workers and merging only requests of at most 32K rows: measured on B200
-    # against 8/16 workers and 128K/1M-row merge limits on this request mix
-    # (a merged launch's planning costs more than it saves above ~32K rows)
+    # 4 workers (measured on B200 against 8 and 16 on this request mix) and
+    # requests of at most 32K rows merged (no merging, 32K and 128K all kept
+    # p99 below the per-request loop's at the three rates; few requests of
+    # this mix are small enough to merge)
     p.add_argument("--served-workers", type=int, default=4)
     p.add_argument("--served-batch-rows", type=int, default=32_768)
     p.add_argument("--served-large-rows", type=int, default=0,
@@ -279,7 +280,7 @@ def run_ours(args, rank, world, local):
     peaks = _load_peaks()
     per = {}
     # the roofline follows the partitioned strategy's aggregation phase
-    # (k_part_ranked + the k_part_fold launches, which also write the
+    # (k_part_ranked_cta + the k_part_fold launches, which also write the
     # outputs): its algorithmic bytes per call are the rows read and the
     # groups written
     agg_ms_total = 0.0
@@ -314,7 +315,7 @@ def run_ours(args, rank, world, local):
         }
     achieved = (agg_bytes_total / (agg_ms_total / 1e3)) / 1e9 if agg_ms_total > 0 else None
     roofline = {
-        "bound": "hbm", "kernel": "k_part_ranked + k_part_fold (cardinality 1e6 / 1e8 calls)",
+        "bound": "hbm", "kernel": "k_part_ranked_cta + k_part_fold (cardinality 1e6 / 1e8 calls)",
         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
         "peak_source": peaks["source"],
