@@ -101,6 +101,8 @@ int32_t target_type(int32_t t, int32_t kind)
       return GBX_TYPE_EMPTY;
     case GBX_AGG_MIN:
     case GBX_AGG_MAX: return t;
+    case GBX_AGG_ARGMIN:
+    case GBX_AGG_ARGMAX: return GBX_TYPE_INT32;  // size_type row index
     case GBX_AGG_COUNT_VALID:
     case GBX_AGG_COUNT_ALL: return GBX_TYPE_INT32;
     case GBX_AGG_MEAN:
@@ -115,8 +117,7 @@ int32_t target_type(int32_t t, int32_t kind)
   }
 }
 
-// Kinds libcudf accepts on its hash path (hash/groupby.cu:73-84).  ARGMIN /
-// ARGMAX are hash kinds there too but are not provided by this library.
+// Kinds libcudf accepts on its hash path (hash/groupby.cu:73-84).
 bool is_hash_kind(int32_t k)
 {
   switch (k) {
@@ -124,6 +125,8 @@ bool is_hash_kind(int32_t k)
     case GBX_AGG_PRODUCT:
     case GBX_AGG_MIN:
     case GBX_AGG_MAX:
+    case GBX_AGG_ARGMIN:
+    case GBX_AGG_ARGMAX:
     case GBX_AGG_COUNT_VALID:
     case GBX_AGG_COUNT_ALL:
     case GBX_AGG_SUM_OF_SQUARES:
@@ -300,7 +303,7 @@ void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n)
       int32_t kind = r.aggregations[k].kind;
       // verify_valid_requests (groupby.cu:176-192)
       if (!is_hash_kind(kind)) {
-        if (kind == GBX_AGG_ARGMIN || kind == GBX_AGG_ARGMAX || kind == GBX_AGG_NTH_ELEMENT ||
+        if (kind == GBX_AGG_NTH_ELEMENT ||
             kind == GBX_AGG_MEDIAN || kind == GBX_AGG_QUANTILE || kind == GBX_AGG_NUNIQUE ||
             kind == GBX_AGG_M2 || kind == GBX_AGG_ANY || kind == GBX_AGG_ALL || kind > GBX_AGG_NTH_ELEMENT)
           fail(GBX_ERR_UNSUPPORTED,
@@ -479,6 +482,8 @@ void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_c
           case GBX_AGG_PRODUCT: need |= N_PROD; break;
           case GBX_AGG_MIN: need |= N_MIN; break;
           case GBX_AGG_MAX: need |= N_MAX; break;
+          case GBX_AGG_ARGMIN: need |= N_AMIN; break;
+          case GBX_AGG_ARGMAX: need |= N_AMAX; break;
           case GBX_AGG_COUNT_VALID: need |= N_CNT; break;
           case GBX_AGG_SUM_OF_SQUARES: need |= N_SQ; break;
           case GBX_AGG_MEAN: need |= N_SUM | N_CNT; break;
@@ -498,6 +503,10 @@ void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_c
     if (need & N_MAX) ch.a_max = add_acc(m64 ? A_U64_MAX : A_U32_MAX);
     if (need & N_SQ) ch.a_sq = add_acc(ch.is_float ? A_F64_ADD : A_I64_ADD);
     if (need & N_PROD) ch.a_prod = add_acc(ch.is_float ? A_F64_MUL : A_I64_MUL);
+    // ARGMIN / ARGMAX: a packed (value, row) word for values of up to 32
+    // bits, a row index updated by compare-and-swap for 64-bit values
+    if (need & N_AMIN) ch.a_amin = add_acc(m64 ? A_I32_ARGMIN_CAS : A_U64_ARGMIN);
+    if (need & N_AMAX) ch.a_amax = add_acc(m64 ? A_I32_ARGMAX_CAS : A_U64_ARGMAX);
     if (need & N_VAR) {
       ch.a_k  = add_acc(A_F64_SHIFT);
       ch.a_s2 = add_acc(A_F64_ADD);
@@ -871,6 +880,12 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       else strategy = GBX_STRATEGY_PARTITIONED;
     }
     if (strategy == GBX_STRATEGY_WARP && !warp_fits) strategy = GBX_STRATEGY_PRIVATIZED;
+    // ARGMIN / ARGMAX record each row's own index where it is accumulated:
+    // only the kernels that read the caller's rows in place (the privatised
+    // shared table, untiled, and the global table) do
+    const bool arg_kinds = plan_has_arg(plan);
+    if (arg_kinds && strategy != GBX_STRATEGY_PRIVATIZED && strategy != GBX_STRATEGY_GLOBAL)
+      strategy = est * 2.0 <= static_cast<double>(s_max) ? GBX_STRATEGY_PRIVATIZED : GBX_STRATEGY_GLOBAL;
 
     gb->stats.strategy = strategy;
 
@@ -1174,7 +1189,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         int grid        = call.dev.num_sms * std::max<int>(1, std::min<int>(4, static_cast<int>((200 * 1024) / (sl.total + 1024))));
         int64_t max_grid = (call.n + block * 4 - 1) / (block * 4);
         grid             = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(grid, max_grid)));
-        if (tiled_fits(sl, plan.nchan)) {
+        if (tiled_fits(sl, plan.nchan) && !arg_kinds) {
           // few groups: tiles grouped in shared memory before the table is touched
           GBX_CUDA(launch_agg_tiled(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 32), max_probes, s));
         } else {

@@ -287,6 +287,12 @@ struct Shared {
     asm volatile("atom.shared.cas.b64 %0, [%1], %2, %3;" : "=l"(o) : "r"(a), "l"(c), "l"(v) : "memory");
     return o;
   }
+  static __device__ __forceinline__ uint32_t cas_u32(addr_t a, uint32_t c, uint32_t v)
+  {
+    uint32_t o;
+    asm volatile("atom.shared.cas.b32 %0, [%1], %2, %3;" : "=r"(o) : "r"(a), "r"(c), "r"(v) : "memory");
+    return o;
+  }
   static __device__ __forceinline__ uint64_t ld_u64(addr_t a)
   {
     uint64_t v;
@@ -348,6 +354,12 @@ struct Global {
   {
     uint64_t o;
     asm volatile("atom.global.cas.b64 %0, [%1], %2, %3;" : "=l"(o) : "l"(a), "l"(c), "l"(v) : "memory");
+    return o;
+  }
+  static __device__ __forceinline__ uint32_t cas_u32(addr_t a, uint32_t c, uint32_t v)
+  {
+    uint32_t o;
+    asm volatile("atom.global.cas.b32 %0, [%1], %2, %3;" : "=r"(o) : "l"(a), "r"(c), "r"(v) : "memory");
     return o;
   }
   static __device__ __forceinline__ uint64_t ld_u64(addr_t a)

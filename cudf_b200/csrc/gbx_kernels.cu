@@ -52,7 +52,8 @@ __global__ void k_init_table(const __grid_constant__ TableRef t, const __grid_co
   if (blockIdx.x == 0 && threadIdx.x == 0) *t.special_used = 0;
 }
 
-template <int NW>
+// ARG: the plan carries ARGMIN / ARGMAX accumulators.
+template <int NW, bool ARG>
 __global__ void k_agg_global(const __grid_constant__ Plan plan, const __grid_constant__ TableRef t, int64_t n, uint32_t max_probes)
 {
   const Level<Global> G = global_level(t);
@@ -62,13 +63,13 @@ __global__ void k_agg_global(const __grid_constant__ Plan plan, const __grid_con
     if (!pack_key<NW>(plan.key, r, k)) continue;
     int64_t g = global_slot<NW>(t, k, max_probes);
     if (g < 0) continue;
-    accumulate_row<Global>(plan, G, g, r, t.status);
+    accumulate_row<Global, ARG>(plan, G, g, r, t.status);
   }
 }
 
 // Per-CTA privatised aggregation.  Shared memory holds S+1 slots (slot S is
 // the reserved all-ones key): keys, row counts and every accumulator array.
-template <int NW>
+template <int NW, bool ARG>
 __global__ void __launch_bounds__(512) k_agg_privatized(const __grid_constant__ Plan plan,
                                                         const __grid_constant__ TableRef t,
                                                         const __grid_constant__ SmemLayout sl,
@@ -113,10 +114,10 @@ __global__ void __launch_bounds__(512) k_agg_privatized(const __grid_constant__ 
       s = find_or_insert<Shared, NW>(keys, S - 1, k, hash_key<NW>(k), smem_probes);
     }
     if (s >= 0) {
-      accumulate_row<Shared>(plan, L, s, r, t.status);
+      accumulate_row<Shared, ARG>(plan, L, s, r, t.status);
     } else {
       int64_t g = global_slot<NW>(t, k, max_probes);
-      if (g >= 0) accumulate_row<Global>(plan, G, g, r, t.status);
+      if (g >= 0) accumulate_row<Global, ARG>(plan, G, g, r, t.status);
     }
   }
   __syncthreads();
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(512) k_agg_privatized(const __grid_constant__ 
     bool occupied = (s < S) ? !key_is_empty<NW>(k) : (s_special != 0);
     if (!occupied) continue;
     int64_t g = global_slot<NW>(t, k, max_probes);
-    if (g >= 0) merge_slot<Shared>(plan, L, s, G, g, t.status);
+    if (g >= 0) merge_slot<Shared, ARG>(plan, L, s, G, g, t.status);
   }
 }
 
@@ -287,6 +288,25 @@ __global__ void k_finalize(const __grid_constant__ Plan plan, const __grid_const
             vbits        = dec_minmax(raw, ch.ptype, mn);
             break;
           }
+          case GBX_AGG_ARGMIN:
+          case GBX_AGG_ARGMAX: {
+            // the row of the group's extreme value; null (data -1, the
+            // reference's ARGMIN/ARGMAX_SENTINEL) when no value was valid
+            bool mn = oc.kind == GBX_AGG_ARGMIN;
+            int a   = mn ? ch.a_amin : ch.a_amax;
+            uint32_t row;
+            if (minmax_is64(ch.ptype)) {
+              row = static_cast<uint32_t>(ld_acc(t, a, s, 4));
+            } else {
+              uint64_t w = ld_acc(t, a, s, 8);
+              row        = (w == identity_bits(plan.acc.kind[a])) ? 0xffffffffu
+                           : mn                                   ? static_cast<uint32_t>(w)
+                                                                  : ~static_cast<uint32_t>(w);
+            }
+            valid = row != 0xffffffffu;
+            vbits = row;
+            break;
+          }
           case GBX_AGG_MEAN: {
             if (!valid) break;
             uint64_t raw = ld_acc(t, ch.a_sum, s, 8);
@@ -335,7 +355,8 @@ __global__ void k_finalize(const __grid_constant__ Plan plan, const __grid_const
           }
           default: break;
         }
-        store_bits(oc.data, g, oc.out_width, valid ? vbits : 0);
+        const bool arg = oc.kind == GBX_AGG_ARGMIN || oc.kind == GBX_AGG_ARGMAX;
+        store_bits(oc.data, g, oc.out_width, valid ? vbits : (arg ? 0xffffffffULL : 0));
       }
       if (oc.mask != nullptr) {
         uint32_t bal = __ballot_sync(0xffffffffu, active && valid);
@@ -388,9 +409,15 @@ cudaError_t launch_sample(const KeyPlan& kp, int64_t n, int64_t nsample, uint64_
 cudaError_t launch_agg_global(const Plan& p, const TableRef& t, int64_t n, uint32_t max_probes, int num_sms,
                               cudaStream_t st)
 {
-  int grid = grid_for(n, 256, num_sms * 8);
-  if (p.key.nwords == 1) k_agg_global<1><<<grid, 256, 0, st>>>(p, t, n, max_probes);
-  else k_agg_global<2><<<grid, 256, 0, st>>>(p, t, n, max_probes);
+  int grid       = grid_for(n, 256, num_sms * 8);
+  const bool arg = plan_has_arg(p);
+  if (p.key.nwords == 1) {
+    if (arg) k_agg_global<1, true><<<grid, 256, 0, st>>>(p, t, n, max_probes);
+    else k_agg_global<1, false><<<grid, 256, 0, st>>>(p, t, n, max_probes);
+  } else {
+    if (arg) k_agg_global<2, true><<<grid, 256, 0, st>>>(p, t, n, max_probes);
+    else k_agg_global<2, false><<<grid, 256, 0, st>>>(p, t, n, max_probes);
+  }
   return cudaGetLastError();
 }
 
@@ -398,17 +425,15 @@ cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLa
                                   int grid, uint32_t smem_probes, uint32_t max_probes, cudaStream_t st)
 {
   int64_t rpb = (n + grid - 1) / grid;
-  cudaError_t e;
-  if (p.key.nwords == 1) {
-    e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_agg_privatized<1>), sl.total);
+  auto run    = [&](auto kernel) -> cudaError_t {
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(kernel), sl.total);
     if (e != cudaSuccess) return e;
-    k_agg_privatized<1><<<grid, block, sl.total, st>>>(p, t, sl, n, rpb, smem_probes, max_probes);
-  } else {
-    e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_agg_privatized<2>), sl.total);
-    if (e != cudaSuccess) return e;
-    k_agg_privatized<2><<<grid, block, sl.total, st>>>(p, t, sl, n, rpb, smem_probes, max_probes);
-  }
-  return cudaGetLastError();
+    kernel<<<grid, block, sl.total, st>>>(p, t, sl, n, rpb, smem_probes, max_probes);
+    return cudaGetLastError();
+  };
+  const bool arg = plan_has_arg(p);
+  if (p.key.nwords == 1) return arg ? run(k_agg_privatized<1, true>) : run(k_agg_privatized<1, false>);
+  return arg ? run(k_agg_privatized<2, true>) : run(k_agg_privatized<2, false>);
 }
 
 cudaError_t compact_occupied(const TableRef& t, int nwords, uint32_t* map, int64_t* num_selected, void* temp,

@@ -154,6 +154,14 @@ struct Plan {
   AccLayout acc;
 };
 
+// True when some channel of the plan carries an ARGMIN or ARGMAX accumulator.
+inline bool plan_has_arg(const Plan& plan)
+{
+  for (int c = 0; c < plan.nchan; ++c)
+    if (plan.chan[c].a_amin >= 0 || plan.chan[c].a_amax >= 0) return true;
+  return false;
+}
+
 // Device status bits.
 enum StatusBits : int32_t {
   S_TABLE_FULL   = 1,  // a global probe sequence hit its limit: retry with a larger table

@@ -420,6 +420,10 @@ int gbx_server_submit(gbx_server* s, const gbx_table_view* keys, const gbx_reque
     j->aggs.resize(num_requests);
     j->val_dicts.resize(num_requests);
     for (int q = 0; q < num_requests; ++q) {
+      // ARGMIN / ARGMAX run on the plain path only (the batched form lacks them)
+      for (int k = 0; k < requests[q].num_aggregations; ++k)
+        if (requests[q].aggregations[k].kind == GBX_AGG_ARGMIN || requests[q].aggregations[k].kind == GBX_AGG_ARGMAX)
+          j->mergeable = false;
       j->aggs[q].assign(requests[q].aggregations, requests[q].aggregations + requests[q].num_aggregations);
       j->reqs[q].aggregations = j->aggs[q].data();
       if (j->reqs[q].values.dict_keys) {

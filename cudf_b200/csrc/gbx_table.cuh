@@ -91,6 +91,89 @@ __device__ __forceinline__ double get_shift(typename Space::addr_t a, double x)
   return __longlong_as_double(static_cast<long long>(kb));
 }
 
+// ------------------------------------------------------------ ARGMIN / ARGMAX
+
+// Order key of a value for ARGMIN (`for_min`) or ARGMAX: the MIN/MAX encoding
+// (NaN loses to every number) with -0.0 folded into +0.0, so that the two
+// zeros tie as they do under the reference's `<` / `>` comparisons
+// (detail/aggregation/aggregation.cuh:436-491).  Ties go to the lowest row.
+__device__ __forceinline__ uint64_t arg_order(uint64_t b, int ptype, bool for_min)
+{
+  if (ptype == P_F32 && (static_cast<uint32_t>(b) << 1) == 0) b = 0;
+  if (ptype == P_F64 && (b << 1) == 0) b = 0;
+  return enc_minmax(b, ptype, for_min);
+}
+
+// Values of at most 32 bits: one 64-bit word per group, the order key in the
+// high half and the row (ARGMIN) or its complement (ARGMAX) in the low half,
+// so that a single 64-bit min / max keeps the extreme value and, among equal
+// values, the lowest row.  Rows are below 2^31, so neither identity (all
+// ones for ARGMIN, zero for ARGMAX) is a packed row.
+__device__ __forceinline__ uint64_t arg_pack(uint64_t order, bool for_min, uint32_t row)
+{
+  return (order << 32) | (for_min ? row : ~row);
+}
+
+// 64-bit values: the group's row index, replaced by compare-and-swap while
+// the new row's value beats the value re-read at the stored row (the
+// reference's loop, aggregation.cuh:449-458, with the lowest-row tie rule).
+// Values never change during a call, so the loop ends with the best row.
+template <class Space>
+__device__ __forceinline__ void arg_cas(typename Space::addr_t a, const Channel& ch, uint64_t order, uint32_t row,
+                                     bool for_min, int32_t* status)
+{
+  uint32_t cur = Space::ld_u32(a);
+  for (int it = 0; it < (1 << 20); ++it) {
+    if (cur != 0xffffffffu) {
+      bool ok;
+      const uint64_t held = arg_order(value_bits(ch, cur, ok), ch.ptype, for_min);
+      const bool wins     = for_min ? order < held : order > held;
+      if (!wins && !(order == held && row < cur)) return;
+    }
+    const uint32_t old = Space::cas_u32(a, cur, row);
+    if (old == cur) return;
+    cur = old;
+  }
+  atomicOr(status, S_SPIN_LIMIT);
+}
+
+// Folds (value bits `b`, row) into a channel's ARGMIN / ARGMAX accumulator at
+// `acc` (the array base) for slot `slot`.
+template <class Space>
+__device__ __forceinline__ void arg_update(typename Space::addr_t acc, int64_t slot, const Channel& ch, uint64_t b,
+                                        uint32_t row, bool for_min, int32_t* status)
+{
+  using A              = typename Space::addr_t;
+  const uint64_t order = arg_order(b, ch.ptype, for_min);
+  if (minmax_is64(ch.ptype)) {
+    arg_cas<Space>(acc + static_cast<A>(slot * 4), ch, order, row, for_min, status);
+  } else if (for_min) {
+    Space::min_u64(acc + static_cast<A>(slot * 8), arg_pack(order, true, row));
+  } else {
+    Space::max_u64(acc + static_cast<A>(slot * 8), arg_pack(order, false, row));
+  }
+}
+
+// Merges a partial table's ARGMIN / ARGMAX accumulator (slot `s` at `src`)
+// into the global one (slot `g` at `dst`).
+template <class Src>
+__device__ __forceinline__ void arg_merge(typename Src::addr_t src, int64_t s, uint64_t dst, int64_t g,
+                                       const Channel& ch, bool for_min, int32_t* status)
+{
+  using SA = typename Src::addr_t;
+  if (minmax_is64(ch.ptype)) {
+    const uint32_t row = Src::ld_u32(src + static_cast<SA>(s * 4));
+    if (row == 0xffffffffu) return;
+    bool ok;
+    const uint64_t order = arg_order(value_bits(ch, row, ok), ch.ptype, for_min);
+    arg_cas<Global>(dst + static_cast<uint64_t>(g * 4), ch, order, row, for_min, status);
+  } else {
+    const uint64_t w = Src::ld_u64(src + static_cast<SA>(s * 8));
+    if (for_min) Global::min_u64(dst + static_cast<uint64_t>(g * 8), w);
+    else Global::max_u64(dst + static_cast<uint64_t>(g * 8), w);
+  }
+}
+
 // ------------------------------------------------------------- row sources
 
 // Rows of the caller's columns as the plan names them.
@@ -119,8 +202,10 @@ struct RowSource {
 
 // Folds row `row` of `src` into slot `slot` of a table level (aggregate_row,
 // detail/aggregation/aggregation.cuh:558-573, with update_target_element's
-// null skipping, :116-491).
-template <class Space, class Src>
+// null skipping, :116-491).  ARGMIN / ARGMAX accumulators are updated only in
+// the `kArg` instantiations (kernels launched for plans that carry them), so
+// the other kernels keep their registers.
+template <class Space, class Src, bool kArg = false>
 __device__ __forceinline__ void accumulate_row_from(const Plan& plan,
                                                     const Src& src,
                                                     const Level<Space>& L,
@@ -145,6 +230,10 @@ __device__ __forceinline__ void accumulate_row_from(const Plan& plan,
       uint64_t e = enc_minmax(b, ch.ptype, false);
       if (is64) Space::max_u64(L.acc(ch.a_max) + static_cast<A>(slot * 8), e);
       else Space::max_u32(L.acc(ch.a_max) + static_cast<A>(slot * 4), static_cast<uint32_t>(e));
+    }
+    if constexpr (kArg) {
+      if (ch.a_amin >= 0) arg_update<Space>(L.acc(ch.a_amin), slot, ch, b, static_cast<uint32_t>(row), true, status);
+      if (ch.a_amax >= 0) arg_update<Space>(L.acc(ch.a_amax), slot, ch, b, static_cast<uint32_t>(row), false, status);
     }
     if (ch.is_float) {
       double x = as_f64(b, ch.ptype);
@@ -174,19 +263,19 @@ __device__ __forceinline__ void accumulate_row_from(const Plan& plan,
   }
 }
 
-template <class Space>
+template <class Space, bool kArg = false>
 __device__ __forceinline__ void accumulate_row(const Plan& plan,
                                                const Level<Space>& L,
                                                int64_t slot,
                                                int64_t row,
                                                int32_t* status)
 {
-  accumulate_row_from<Space>(plan, RowSource{&plan}, L, slot, row, status);
+  accumulate_row_from<Space, RowSource, kArg>(plan, RowSource{&plan}, L, slot, row, status);
 }
 
 // Merges slot `s` of a (shared-memory) partial level into slot `g` of the
-// global level.
-template <class Src>
+// global level (ARGMIN / ARGMAX in the `kArg` instantiations only).
+template <class Src, bool kArg = false>
 __device__ __forceinline__ void merge_slot(const Plan& plan,
                                            const Level<Src>& S,
                                            int64_t s,
@@ -213,6 +302,10 @@ __device__ __forceinline__ void merge_slot(const Plan& plan,
     if (ch.a_max >= 0) {
       if (is64) Global::max_u64(G.acc(ch.a_max) + static_cast<uint64_t>(g * 8), Src::ld_u64(S.acc(ch.a_max) + static_cast<SA>(s * 8)));
       else Global::max_u32(G.acc(ch.a_max) + static_cast<uint64_t>(g * 4), Src::ld_u32(S.acc(ch.a_max) + static_cast<SA>(s * 4)));
+    }
+    if constexpr (kArg) {
+      if (ch.a_amin >= 0) arg_merge<Src>(S.acc(ch.a_amin), s, G.acc(ch.a_amin), g, ch, true, status);
+      if (ch.a_amax >= 0) arg_merge<Src>(S.acc(ch.a_amax), s, G.acc(ch.a_amax), g, ch, false, status);
     }
     if (ch.is_float) {
       if (ch.a_sum >= 0)

@@ -116,6 +116,31 @@ def cases():
             _case(f"max_tests.cpp:109-130 null_keys_and_values[{v.name}]", K, K11, v, V11, Kind.MAX, [1, 2, 3, 4],
                   [3, 5, 8, 0], kvalid=K11_VALID, vvalid=V11_VALID_MAX, evalid=[1, 1, 1, 0], rtype=v),
         ]
+    # ---- argmin_tests.cpp / argmax_tests.cpp (FixedWidthTypes; the gtests skip
+    # bool, and fixed-point needs a scale the wrapper here does not carry)
+    vdesc = [9, 8, 7, 6, 5, 4, 3, 2, 1, 0]
+    vdesc11 = vdesc + [4]
+    for v in INTS + UINTS + FLOATS + TIMESTAMPS + DURATIONS:
+        out += [
+            _case(f"argmin_tests.cpp:34-52 basic[{v.name}]", K, K10, v, vdesc, Kind.ARGMIN, [1, 2, 3], [6, 9, 8],
+                  rtype=T.INT32),
+            _case(f"argmin_tests.cpp:54-72 zero_valid_keys[{v.name}]", K, [1, 2, 3], v, [3, 4, 5], Kind.ARGMIN, [], [],
+                  kvalid=[0, 0, 0], rtype=T.INT32),
+            _case(f"argmin_tests.cpp:74-92 zero_valid_values[{v.name}]", K, [1, 1, 1], v, [3, 4, 5], Kind.ARGMIN, [1],
+                  [0], vvalid=[0, 0, 0], evalid=[0], rtype=T.INT32),
+            _case(f"argmin_tests.cpp:94-118 null_keys_and_values[{v.name}]", K, K11, v, vdesc11, Kind.ARGMIN,
+                  [1, 2, 3, 4], [3, 9, 8, 0], kvalid=K11_VALID, vvalid=[1, 1, 1, 1, 1, 0, 0, 1, 1, 1, 0],
+                  evalid=[1, 1, 1, 0], rtype=T.INT32),
+            _case(f"argmax_tests.cpp:33-51 basic[{v.name}]", K, K10, v, vdesc, Kind.ARGMAX, [1, 2, 3], [0, 1, 2],
+                  rtype=T.INT32),
+            _case(f"argmax_tests.cpp:53-71 zero_valid_keys[{v.name}]", K, [1, 2, 3], v, [3, 4, 5], Kind.ARGMAX, [], [],
+                  kvalid=[0, 0, 0], rtype=T.INT32),
+            _case(f"argmax_tests.cpp:73-91 zero_valid_values[{v.name}]", K, [1, 1, 1], v, [3, 4, 5], Kind.ARGMAX, [1],
+                  [0], vvalid=[0, 0, 0], evalid=[0], rtype=T.INT32),
+            _case(f"argmax_tests.cpp:93-117 null_keys_and_values[{v.name}]", K, K11, v, vdesc11, Kind.ARGMAX,
+                  [1, 2, 3, 4], [3, 4, 7, 0], kvalid=[1, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1],
+                  vvalid=[0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 0], evalid=[1, 1, 1, 0], rtype=T.INT32),
+        ]
     dvals = [0xABC, 0xBBB, 0xF1, 0xAAA, 0xFFF, 0xBAA, 0xAAA, 0x01, 0xF1, 0xEEE]
     out += [
         _case("min_tests.cpp:232-255 dictionary fixed_width", K, K10, T.INT64, dvals, Kind.MIN, [1, 2, 3],

@@ -66,7 +66,7 @@ def test_ctypes_layout_matches_c_header(tmp_path):
 def test_target_types_match_oracle():
     lib = _lib.lib()
     hash_kinds = {Kind.SUM, Kind.PRODUCT, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.COUNT_ALL,
-                  Kind.SUM_OF_SQUARES, Kind.MEAN, Kind.VARIANCE, Kind.STD}
+                  Kind.SUM_OF_SQUARES, Kind.MEAN, Kind.VARIANCE, Kind.STD, Kind.ARGMIN, Kind.ARGMAX}
     for t in TypeId:
         for k in Kind:
             want = orc.target_type(t, k) if k in hash_kinds else 0
@@ -113,7 +113,7 @@ def test_size_mismatch_is_logic_error():
 
 @pytest.mark.parametrize("kind,status", [(Kind.NTH_ELEMENT, _abi.Status.ERR_UNSUPPORTED),
                                          (Kind.MEDIAN, _abi.Status.ERR_UNSUPPORTED),
-                                         (Kind.ARGMAX, _abi.Status.ERR_UNSUPPORTED)])
+                                         (Kind.QUANTILE, _abi.Status.ERR_UNSUPPORTED)])
 def test_sort_only_kinds_are_reported(kind, status):
     lib = _lib.lib()
     tv, keep = _keys_view(3)
@@ -151,7 +151,8 @@ def test_create_rejects_string_keys_and_bad_policy():
 
 def test_can_use_hash_groupby_for_hash_kinds():
     lib = _lib.lib()
-    for k in (Kind.SUM, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.MEAN, Kind.VARIANCE, Kind.STD):
+    for k in (Kind.SUM, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.MEAN, Kind.VARIANCE, Kind.STD, Kind.ARGMIN,
+              Kind.ARGMAX):
         r, keep = _request(3, k)
         assert lib.gbx_can_use_hash_groupby(C.byref(r), 1) == 1
 
@@ -213,3 +214,12 @@ def test_batch_rejects_dictionary_keys_and_sort_kinds():
     b, kb = _batch_instance(4, kind=Kind.MEDIAN)
     st, _ = _create_batch([b])
     assert st == _abi.Status.ERR_UNSUPPORTED
+
+
+def test_batch_rejects_argmin_argmax():
+    """The batched kernels address rows within their instance, so the row
+    indices ARGMIN/ARGMAX return are left to the plain form."""
+    for kind in (Kind.ARGMIN, Kind.ARGMAX):
+        a, ka = _batch_instance(4, kind=kind)
+        st, msg = _create_batch([a])
+        assert st == _abi.Status.ERR_UNSUPPORTED and b"ARGMIN/ARGMAX" in msg
