@@ -184,11 +184,50 @@ __device__ __forceinline__ void fold_channel(const Plan& plan, const OutPlan& op
   }
   const RegView V{A, run.y};
   const int64_t g = base + lane;
+  // Shared by the channel's outputs, once per group: the mean (one FP64
+  // division) and, with VAR/STD, the centred sum of squares
+  // M2 = sum (x-K)^2 - S1 (S1 / n), S1 = sum - n K, with S1 / n taken as
+  // mean - K instead of a second division (its extra rounding is of order
+  // 1e-16 (var + mean^2)).  MEAN divides the signed INT64 SUM of an integer
+  // column; VAR reads a UINT64 sum unsigned, as finalize_from does.
+  const bool is_float = PT == P_F32 || PT == P_F64;
+  const double n      = static_cast<double>(A.cnt);
+  const double sum_m  = is_float ? __longlong_as_double(static_cast<long long>(A.sum))
+                                 : static_cast<double>(static_cast<int64_t>(A.sum));
+  const double mean   = (roles & R_SUM) && A.cnt > 0 ? sum_m / n : 0.0;
+  double m2           = 0.0;
+  if ((roles & R_VAR) && A.cnt > 0) {
+    if (A.k == kShiftUnset) {
+      m2 = A.s2;  // NaN inputs only
+    } else {
+      const double K      = __longlong_as_double(static_cast<long long>(A.k));
+      const double mean_v = PT == P_U64 ? static_cast<double>(A.sum) / n : mean;
+      const double sum_v  = PT == P_U64 ? static_cast<double>(A.sum) : sum_m;
+      m2                  = A.s2 - (sum_v - n * K) * (mean_v - K);
+      if (m2 < 0.0) m2 = 0.0;
+    }
+  }
   for (int o = 0; o < op.nout; ++o) {
     const OutCol& oc = op.out[o];
     if (oc.chan != c) continue;
-    bool valid       = false;
-    const uint64_t v = active ? finalize_from<PT>(ch, oc, V, valid) : 0;
+    bool valid = false;
+    uint64_t v = 0;
+    if (active) {
+      if (oc.kind == GBX_AGG_MEAN && oc.out_ptype == P_F64) {
+        valid = A.cnt > 0;
+        v     = valid ? static_cast<uint64_t>(__double_as_longlong(mean)) : 0;
+      } else if (oc.kind == GBX_AGG_VARIANCE || oc.kind == GBX_AGG_STD) {
+        const int64_t nn = A.cnt;
+        valid            = nn > 0 && nn - oc.ddof > 0;
+        if (valid) {
+          double var = A.k == kShiftUnset ? m2 : m2 / static_cast<double>(nn - oc.ddof);
+          if (oc.kind == GBX_AGG_STD) var = sqrt(var);
+          v = static_cast<uint64_t>(__double_as_longlong(var));
+        }
+      } else {
+        v = finalize_from<PT>(ch, oc, V, valid);
+      }
+    }
     if (active) store_bits(oc.data, g, oc.out_width, v);
     if (oc.mask != nullptr) {
       const uint32_t bits = __ballot_sync(kFull, active && valid);
