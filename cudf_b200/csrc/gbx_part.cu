@@ -177,7 +177,22 @@ __device__ __forceinline__ void fold_channel(const Plan& plan, const OutPlan& op
   const Word* vals      = reinterpret_cast<const Word*>(pc.vals);
   ChanAcc A;
   chan_acc_init(A);
-  for (uint32_t j = 0; j < run.y; ++j) {
+  // the run's first kFoldBatch rows are loaded together (one round trip for
+  // almost every group at high cardinality), then folded in row order
+  constexpr uint32_t kFoldBatch = 4;
+  uint64_t pre[kFoldBatch];
+  bool pok[kFoldBatch];
+#pragma unroll
+  for (uint32_t j = 0; j < kFoldBatch; ++j) {
+    const int64_t r = static_cast<int64_t>(run.x) + j;
+    const bool in   = j < run.y;
+    pre[j]          = in ? static_cast<uint64_t>(__ldg(vals + r)) : 0;
+    pok[j]          = in && (pc.valid == nullptr || __ldg(pc.valid + r) != 0);
+  }
+#pragma unroll
+  for (uint32_t j = 0; j < kFoldBatch; ++j)
+    if (pok[j]) chan_acc_add<PT>(ch, roles, A, pre[j]);
+  for (uint32_t j = kFoldBatch; j < run.y; ++j) {
     const int64_t r = static_cast<int64_t>(run.x) + j;
     const uint64_t b = __ldg(vals + r);
     if (pc.valid == nullptr || __ldg(pc.valid + r) != 0) chan_acc_add<PT>(ch, roles, A, b);
@@ -616,10 +631,14 @@ __global__ void __launch_bounds__(256) k_part_fold(const __grid_constant__ Plan 
   const int64_t G       = static_cast<int64_t>(*pp.out_counter);
   const int lane        = threadIdx.x & 31;
   const int64_t wstride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < G;
-       base += wstride) {
+  int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31);
+  // each group's (first row, rows) is loaded one iteration ahead
+  uint2 next = base + lane < G ? pp.group_run[base + lane] : make_uint2(0u, 0u);
+  for (; base < G; base += wstride) {
     const bool active  = base + lane < G;
-    const uint2 run    = active ? pp.group_run[base + lane] : make_uint2(0u, 0u);
+    const uint2 run    = next;
+    const int64_t nb   = base + wstride + lane;
+    next               = nb < G ? pp.group_run[nb] : make_uint2(0u, 0u);
     const uint32_t act = __ballot_sync(kFull, active);
     fold_channel<PT>(plan, op, sorted.col[c], c, run, active, base, lane, act, s_nulls);
   }
