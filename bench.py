@@ -49,9 +49,9 @@ METRIC = "groupby rows/s (plain hash groupby, 100M rows, int64 key, cardinality 
 PARTITIONED = 3  # gbx_strategy of the radix-partitioned path
 # DRAM bytes per row of the aggregation phase measured by ncu (20M rows,
 # cardinality 2e7): k_part_ranked_cta 0.421 GB read + 0.418 GB written,
-# k_part_fold (int64 channel) 0.261 + 0.503, k_part_fold (float32 channel)
-# 0.201 + 0.361
-AGG_PHASE_DRAM_BYTES_PER_ROW = (0.421107e9 + 0.417534e9 + 0.261240e9 + 0.503070e9 + 0.201434e9 + 0.360507e9) / 20_000_000
+# k_part_fold (int64 channel) 0.262 + 0.503, k_part_fold (float32 channel)
+# 0.202 + 0.358
+AGG_PHASE_DRAM_BYTES_PER_ROW = (0.421107e9 + 0.417534e9 + 0.261609e9 + 0.502701e9 + 0.201567e9 + 0.358031e9) / 20_000_000
 
 
 def parse_args(argv=None):
