@@ -84,8 +84,10 @@ __device__ __forceinline__ int64_t source_rows(int64_t n, const uint32_t* n_acti
 
 // counts[d * ntiles + t] = rows of tile t whose digit is d; when
 // bucket_counts is set, also adds every row to its bucket's count there
-// (the bucket histogram of the partitioned path, warp-aggregated).
-template <int NW, bool FROM_COLUMNS>
+// (the bucket histogram of the partitioned path, warp-aggregated).  PLAIN (a
+// first pass over a single plain 8-byte key column without nulls): the key
+// words are read straight from in.keys[0], the caller's column, n rows.
+template <int NW, bool FROM_COLUMNS, bool PLAIN = false>
 __global__ void __launch_bounds__(kRadixBlock) k_radix_hist(const __grid_constant__ Plan plan,
                                                             const __grid_constant__ PartBufs in, int64_t n,
                                                             const uint32_t* n_active, const Digit dg, int ntiles,
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(kRadixBlock) k_radix_hist(const __grid_constan
   const int radix = 1 << dg.width;
   for (int i = threadIdx.x; i < radix; i += kRadixBlock) hist[i] = 0;
   __syncthreads();
-  const PassSource<NW, FROM_COLUMNS> src{&plan, &in};
+  const PassSource<NW, FROM_COLUMNS && !PLAIN> src{&plan, &in};
   const int64_t rows = source_rows(n, n_active, FROM_COLUMNS);
   const int lane     = threadIdx.x & 31;
   const int warp     = threadIdx.x >> 5;
@@ -691,14 +693,23 @@ __global__ void k_radix_total(const uint32_t* counts, const uint32_t* offsets, i
 // (a single plain 8-byte key column without nulls -- its bits are the packed
 // key -- and value columns without dictionaries); `src` then points at them,
 // each pointer advanced by its column's offset.
-bool first_pass_columns(const Plan& p, const PartBufs& out, PartBufs& src)
+// The caller's key column when it is a single plain 8-byte column without
+// nulls (its bits are the packed key), advanced by its offset; else nullptr.
+const uint64_t* plain_key_column(const Plan& p)
 {
   const KeyCol& kc = p.key.cols[0];
   if (p.key.nwords != 1 || p.key.ncols != 1 || kc.width != 8 || kc.is_float || kc.is_bool || kc.null_bit ||
       kc.mask != nullptr || kc.shift != 0)
-    return false;
+    return nullptr;
+  return reinterpret_cast<const uint64_t*>(static_cast<const unsigned char*>(kc.data) + kc.offset * 8);
+}
+
+bool first_pass_columns(const Plan& p, const PartBufs& out, PartBufs& src)
+{
+  const uint64_t* key = plain_key_column(p);
+  if (key == nullptr) return false;
   src         = PartBufs{};
-  src.keys[0] = reinterpret_cast<const uint64_t*>(static_cast<const unsigned char*>(kc.data) + kc.offset * 8);
+  src.keys[0] = key;
   for (int c = 0; c < p.nchan; ++c) {
     const Channel& ch = p.chan[c];
     if (ch.dict_data != nullptr) return false;
@@ -776,7 +787,12 @@ cudaError_t launch_part_radix_hist0(const Plan& p, int64_t n, int bits, uint32_t
   const Digit dg   = pass_digit(bits, 0);
   const int ntiles = tiles_of(n);
   const PartBufs none{};
-  if (p.key.nwords == 1)
+  if (const uint64_t* key = plain_key_column(p)) {
+    // the key column read as it lies (no per-row key packing)
+    PartBufs src{};
+    src.keys[0] = key;
+    k_radix_hist<1, true, true><<<ntiles, kRadixBlock, 0, st>>>(p, src, n, nullptr, dg, ntiles, counts, bucket_counts);
+  } else if (p.key.nwords == 1)
     k_radix_hist<1, true><<<ntiles, kRadixBlock, 0, st>>>(p, none, n, nullptr, dg, ntiles, counts, bucket_counts);
   else
     k_radix_hist<2, true><<<ntiles, kRadixBlock, 0, st>>>(p, none, n, nullptr, dg, ntiles, counts, bucket_counts);
