@@ -853,10 +853,17 @@ __global__ void k_part_bounds(const uint64_t* k0, const uint64_t* k1, const uint
     if constexpr (NW == 2) k[1] = __ldg(k1 + r);
     return static_cast<int64_t>(bucket_of(hash_key<NW>(k), bits));
   };
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= n; i += stride) {
-    const int64_t prev = i > 0 ? bucket(i - 1) : -1;
-    const int64_t cur  = i < n ? bucket(i) : P;
-    for (int64_t b = prev + 1; b <= cur; ++b) offsets[b] = static_cast<uint32_t>(i);
+  // offsets[b] = first row whose bucket is >= b (n for b = P): the rows are
+  // in bucket order, so a lower-bound search per bucket (~log2 n probes)
+  // replaces reading every row
+  for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b <= P; b += stride) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const int64_t mid = lo + ((hi - lo) >> 1);
+      if (bucket(mid) < b) lo = mid + 1;
+      else hi = mid;
+    }
+    offsets[b] = static_cast<uint32_t>(lo);
   }
 }
 }  // namespace
@@ -864,7 +871,7 @@ __global__ void k_part_bounds(const uint64_t* k0, const uint64_t* k1, const uint
 cudaError_t launch_part_bounds(int nwords, const uint64_t* const* keys, const uint32_t* n_rows, int bits,
                                uint32_t* offsets, int num_sms, cudaStream_t st)
 {
-  const int grid = num_sms * 8;
+  const int grid = static_cast<int>(std::min<int64_t>(((int64_t(1) << bits) + 256) / 256, int64_t(num_sms) * 8));
   if (nwords == 1) k_part_bounds<1><<<grid, 256, 0, st>>>(keys[0], nullptr, n_rows, bits, offsets);
   else k_part_bounds<2><<<grid, 256, 0, st>>>(keys[0], keys[1], n_rows, bits, offsets);
   return cudaGetLastError();
