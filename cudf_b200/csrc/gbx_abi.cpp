@@ -458,7 +458,7 @@ void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_c
     const gbx_column_view& col = *chan_cols[c];
     Channel& ch                = plan.chan[c];
     std::memset(&ch, 0, sizeof(ch));
-    ch.a_cnt = ch.a_sum = ch.a_min = ch.a_max = ch.a_sq = ch.a_k = ch.a_s2 = ch.a_prod = ch.a_amin = ch.a_amax = -1;
+    ch.a_cnt = ch.a_sum = ch.a_min = ch.a_max = ch.a_sq = ch.a_k = ch.a_s2 = ch.a_prod = ch.a_amin = ch.a_amax = ch.a_s1 = -1;
     int32_t vt = value_type(col);
     ch.data    = col.data;
     ch.mask    = chan_nulls[c] != 0 ? col.null_mask : nullptr;
@@ -510,6 +510,7 @@ void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_c
     if (need & N_VAR) {
       ch.a_k  = add_acc(A_F64_SHIFT);
       ch.a_s2 = add_acc(A_F64_ADD);
+      if (ch.is_float) ch.a_s1 = add_acc(A_F64_ADD);
     }
   }
   plan.acc.nacc = nacc;

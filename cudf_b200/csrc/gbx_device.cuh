@@ -199,6 +199,21 @@ __device__ __forceinline__ double as_f64(uint64_t b, int ptype)
   }
 }
 
+// S1 = sum over a group's valid values of (x - K), K its VAR shift, for the
+// centred square sum M2 = sum (x - K)^2 - S1^2 / n.  A floating channel keeps
+// S1 as its own accumulator (`s1_raw`, double bits): deriving it from the
+// plain sum as sum - n K would cancel and lose every digit of the variance
+// once |mean| >> std.  An integer channel's sum is exact (wrapping int64), so
+// S1 is the exact wrapping difference sum - n K, read as a signed 64-bit
+// value (K is an integer-valued double: the group's first value).
+__device__ __forceinline__ double shifted_sum(bool is_float, int ptype, uint64_t sum_raw, uint64_t s1_raw, int64_t n,
+                                              double K)
+{
+  if (is_float) return __longlong_as_double(static_cast<long long>(s1_raw));
+  const uint64_t k = ptype == P_U64 ? static_cast<uint64_t>(K) : static_cast<uint64_t>(static_cast<int64_t>(K));
+  return static_cast<double>(static_cast<int64_t>(sum_raw - static_cast<uint64_t>(n) * k));
+}
+
 // Order-preserving unsigned encodings for MIN/MAX.  NaN maps next to the
 // identity so that it loses to every other value and survives only when the
 // group's valid values are all NaN (see the oracle's stated NaN order).

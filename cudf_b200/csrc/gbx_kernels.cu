@@ -338,13 +338,10 @@ __global__ void k_finalize(const __grid_constant__ Plan plan, const __grid_const
             if (kb == kShiftUnset) {
               var = s2;  // NaN inputs only
             } else {
-              double K      = __longlong_as_double(static_cast<long long>(kb));
-              uint64_t raw  = ld_acc(t, ch.a_sum, s, 8);
-              double sum    = ch.is_float ? __longlong_as_double(static_cast<long long>(raw))
-                                          : (ch.ptype == P_U64 ? static_cast<double>(raw)
-                                                               : static_cast<double>(static_cast<int64_t>(raw)));
-              double S1 = sum - static_cast<double>(nn) * K;
-              double M2 = s2 - S1 * S1 / static_cast<double>(nn);
+              double K  = __longlong_as_double(static_cast<long long>(kb));
+              double S1 = shifted_sum(ch.is_float, ch.ptype, ld_acc(t, ch.a_sum, s, 8),
+                                      ch.a_s1 >= 0 ? ld_acc(t, ch.a_s1, s, 8) : 0, nn, K);
+              double M2 = s2 - S1 * (S1 / static_cast<double>(nn));
               if (M2 < 0.0) M2 = 0.0;
               var = M2 / static_cast<double>(nn - oc.ddof);
             }

@@ -201,10 +201,9 @@ __device__ __forceinline__ void fold_channel(const Plan& plan, const OutPlan& op
   const int64_t g = base + lane;
   // Shared by the channel's outputs, once per group: the mean (one FP64
   // division) and, with VAR/STD, the centred sum of squares
-  // M2 = sum (x-K)^2 - S1 (S1 / n), S1 = sum - n K, with S1 / n taken as
-  // mean - K instead of a second division (its extra rounding is of order
-  // 1e-16 (var + mean^2)).  MEAN divides the signed INT64 SUM of an integer
-  // column; VAR reads a UINT64 sum unsigned, as finalize_from does.
+  // M2 = sum (x-K)^2 - S1 (S1 / n), S1 = sum (x - K) (shifted_sum: the
+  // folded shifted sum of a floating channel, the exact integer difference
+  // otherwise).  MEAN divides the signed INT64 SUM of an integer column.
   const bool is_float = PT == P_F32 || PT == P_F64;
   const double n      = static_cast<double>(A.cnt);
   const double sum_m  = is_float ? __longlong_as_double(static_cast<long long>(A.sum))
@@ -215,10 +214,9 @@ __device__ __forceinline__ void fold_channel(const Plan& plan, const OutPlan& op
     if (A.k == kShiftUnset) {
       m2 = A.s2;  // NaN inputs only
     } else {
-      const double K      = __longlong_as_double(static_cast<long long>(A.k));
-      const double mean_v = PT == P_U64 ? static_cast<double>(A.sum) / n : mean;
-      const double sum_v  = PT == P_U64 ? static_cast<double>(A.sum) : sum_m;
-      m2                  = A.s2 - (sum_v - n * K) * (mean_v - K);
+      const double K  = __longlong_as_double(static_cast<long long>(A.k));
+      const double S1 = shifted_sum(is_float, PT, A.sum, static_cast<uint64_t>(__double_as_longlong(A.s1)), A.cnt, K);
+      m2              = A.s2 - S1 * (S1 / n);
       if (m2 < 0.0) m2 = 0.0;
     }
   }

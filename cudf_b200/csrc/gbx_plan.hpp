@@ -128,9 +128,10 @@ struct Channel {
   int8_t idx_signed;
   int8_t is_float;          // ptype is F32/F64
   uint32_t need;            // ChanNeed bits
-  // accumulator indices into TableRef::acc (-1: absent)
-  int8_t a_cnt, a_sum, a_min, a_max, a_sq, a_k, a_s2, a_prod, a_amin, a_amax;
-  int8_t pad[2];
+  // accumulator indices into TableRef::acc (-1: absent); a_s1 (floating
+  // channels with VAR/STD only) is the shifted sum sum(x - K)
+  int8_t a_cnt, a_sum, a_min, a_max, a_sq, a_k, a_s2, a_prod, a_amin, a_amax, a_s1;
+  int8_t pad[1];
 };
 
 struct TableRef {

@@ -244,6 +244,7 @@ __device__ __forceinline__ void accumulate_row_from(const Plan& plan,
         double K = get_shift<Space>(L.acc(ch.a_k) + static_cast<A>(slot * 8), x);
         double d = x - K;
         Space::add_f64(L.acc(ch.a_s2) + static_cast<A>(slot * 8), d * d);
+        Space::add_f64(L.acc(ch.a_s1) + static_cast<A>(slot * 8), d);
       }
     } else {
       int64_t x = as_i64(b, ch.ptype);
@@ -330,19 +331,20 @@ __device__ __forceinline__ void merge_slot(const Plan& plan,
     if (ch.a_k >= 0) {
       uint64_t kpb = Src::ld_u64(S.acc(ch.a_k) + static_cast<SA>(s * 8));
       double s2p   = __longlong_as_double(static_cast<long long>(Src::ld_u64(S.acc(ch.a_s2) + static_cast<SA>(s * 8))));
+      const uint64_t s1b = ch.a_s1 >= 0 ? Src::ld_u64(S.acc(ch.a_s1) + static_cast<SA>(s * 8)) : 0;
       if (kpb == kShiftUnset) {
-        // every valid value was NaN: the partial square sum is NaN already
+        // every valid value was NaN: the partial sums are NaN already
         Global::add_f64(G.acc(ch.a_s2) + static_cast<uint64_t>(g * 8), s2p);
+        if (ch.a_s1 >= 0) Global::add_f64(G.acc(ch.a_s1) + static_cast<uint64_t>(g * 8), __longlong_as_double(static_cast<long long>(s1b)));
       } else {
-        double Kp   = __longlong_as_double(static_cast<long long>(kpb));
-        double Kg   = get_shift<Global>(G.acc(ch.a_k) + static_cast<uint64_t>(g * 8), Kp);
-        double sump = ch.is_float
-                        ? __longlong_as_double(static_cast<long long>(Src::ld_u64(S.acc(ch.a_sum) + static_cast<SA>(s * 8))))
-                        : (ch.ptype == P_U64 ? static_cast<double>(Src::ld_u64(S.acc(ch.a_sum) + static_cast<SA>(s * 8)))
-                                             : static_cast<double>(static_cast<int64_t>(Src::ld_u64(S.acc(ch.a_sum) + static_cast<SA>(s * 8)))));
-        double S1 = sump - static_cast<double>(n) * Kp;
+        // re-centre the partial sums on the global shift: with d = Kp - Kg,
+        // sum (x-Kg)^2 = sum (x-Kp)^2 + 2 d S1 + n d^2, sum (x-Kg) = S1 + n d
+        double Kp = __longlong_as_double(static_cast<long long>(kpb));
+        double Kg = get_shift<Global>(G.acc(ch.a_k) + static_cast<uint64_t>(g * 8), Kp);
+        double S1 = shifted_sum(ch.is_float, ch.ptype, Src::ld_u64(S.acc(ch.a_sum) + static_cast<SA>(s * 8)), s1b, n, Kp);
         double d  = Kp - Kg;
         Global::add_f64(G.acc(ch.a_s2) + static_cast<uint64_t>(g * 8), s2p + 2.0 * d * S1 + static_cast<double>(n) * d * d);
+        if (ch.a_s1 >= 0) Global::add_f64(G.acc(ch.a_s1) + static_cast<uint64_t>(g * 8), S1 + static_cast<double>(n) * d);
       }
     }
   }

@@ -61,7 +61,7 @@ __device__ __forceinline__ void fold_chunk(const Channel& ch, const uint64_t* cv
 
 // Merges a chunk's accumulators into slot s of the CTA table with shared
 // atomics (several chunks of a group merge at once).  The slot's shift was
-// fixed before the chunks were folded, so A.s2 is relative to it.
+// fixed before the chunks were folded, so A.s2 and A.s1 are relative to it.
 __device__ __forceinline__ void merge_partial(const Channel& ch, const ChanAcc& A, const Level<Shared>& L, uint32_t s,
                                               int32_t* status)
 {
@@ -87,6 +87,7 @@ __device__ __forceinline__ void merge_partial(const Channel& ch, const ChanAcc& 
     if (ch.a_prod >= 0) mul_cas_i64<Shared>(L.acc(ch.a_prod) + s * 8, static_cast<int64_t>(A.prod), status);
   }
   if (ch.a_k >= 0) Shared::add_f64(L.acc(ch.a_s2) + s * 8, A.s2);
+  if (ch.a_s1 >= 0) Shared::add_f64(L.acc(ch.a_s1) + s * 8, A.s1);
 }
 
 // Byte offsets of the per-tile staging areas in dynamic shared memory, after

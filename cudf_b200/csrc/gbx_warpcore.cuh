@@ -128,6 +128,7 @@ __device__ __forceinline__ void apply_row(const Plan& plan, unsigned char* tb, c
       if (*kp == kShiftUnset && !(xf != xf)) *kp = static_cast<uint64_t>(__double_as_longlong(xf));
       const double d = xf - __longlong_as_double(static_cast<long long>(*kp));
       reinterpret_cast<double*>(tb + sl.acc_off[ch.a_s2])[s] += d * d;
+      if (ch.a_s1 >= 0) reinterpret_cast<double*>(tb + sl.acc_off[ch.a_s1])[s] += d;
     }
   }
 }
@@ -345,6 +346,7 @@ struct SlotView {
   }
   __device__ __forceinline__ uint64_t shift() const { return A.acc(ch.a_k, s, 8); }
   __device__ __forceinline__ uint64_t s2() const { return A.acc(ch.a_s2, s, 8); }
+  __device__ __forceinline__ uint64_t s1() const { return ch.a_s1 >= 0 ? A.acc(ch.a_s1, s, 8) : 0; }
 };
 
 // ... or one thread's registers (a group folded by a single lane).  Every
@@ -358,6 +360,7 @@ struct ChanAcc {
   uint64_t prod;  // product, same encoding as sum
   uint64_t k;     // VAR shift (first non-NaN value) or kShiftUnset
   double s2;      // sum of (x - K)^2
+  double s1;      // sum of (x - K) (read for floating channels)
 };
 
 struct RegView {
@@ -371,6 +374,7 @@ struct RegView {
   __device__ __forceinline__ uint64_t minmax(bool mn) const { return mn ? a.mn : a.mx; }
   __device__ __forceinline__ uint64_t shift() const { return a.k; }
   __device__ __forceinline__ uint64_t s2() const { return static_cast<uint64_t>(__double_as_longlong(a.s2)); }
+  __device__ __forceinline__ uint64_t s1() const { return static_cast<uint64_t>(__double_as_longlong(a.s1)); }
 };
 
 __device__ __forceinline__ void chan_acc_init(ChanAcc& a)
@@ -383,6 +387,7 @@ __device__ __forceinline__ void chan_acc_init(ChanAcc& a)
   a.prod = 0;
   a.k    = kShiftUnset;
   a.s2   = 0.0;
+  a.s1   = 0.0;
 }
 
 // The accumulator roles a channel uses, as bits (read once per channel
@@ -437,6 +442,7 @@ __device__ __forceinline__ void chan_acc_add(const Channel& ch, uint32_t roles, 
     if (a.k == kShiftUnset && !(xf != xf)) a.k = static_cast<uint64_t>(__double_as_longlong(xf));
     const double d = xf - __longlong_as_double(static_cast<long long>(a.k));
     a.s2 += d * d;
+    if (chan_is_float<PT>(ch)) a.s1 += d;
   }
 }
 
@@ -505,13 +511,9 @@ __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCo
       if (kb == kShiftUnset) {
         var = s2;  // NaN inputs only
       } else {
-        double K     = __longlong_as_double(static_cast<long long>(kb));
-        uint64_t raw = V.sum();
-        double sum   = is_float ? __longlong_as_double(static_cast<long long>(raw))
-                                : (pt == P_U64 ? static_cast<double>(raw)
-                                               : static_cast<double>(static_cast<int64_t>(raw)));
-        double S1 = sum - static_cast<double>(nn) * K;
-        double M2 = s2 - S1 * S1 / static_cast<double>(nn);
+        double K  = __longlong_as_double(static_cast<long long>(kb));
+        double S1 = shifted_sum(is_float, pt, V.sum(), V.s1(), nn, K);
+        double M2 = s2 - S1 * (S1 / static_cast<double>(nn));
         if (M2 < 0.0) M2 = 0.0;
         var = M2 / static_cast<double>(nn - oc.ddof);
       }

@@ -128,3 +128,91 @@ def plain_200m(n: int = 200_000_000, seed: int = SEED0 + 3, ranks: int = 100_000
     v2 = rng.random(n) >= 0.02
     v = rng.lognormal(0.0, 1.0, n)
     return PlainInput([c1, c2], [v1, v2], [v], [None], f"plain (int32,int16) Zipf(1.2) key, {n} rows")
+
+
+# ------------------------------------------------------- device-side inputs
+# The benchmark generates its full-size inputs on the device (seconds instead
+# of minutes on the host); the full-size parity tests copy the same columns
+# back to the host for the oracle.
+
+def _bitmask_device(valid):
+    """Bool tensor -> cudf bitmask words (int32, LSB-first) padded to 64 bytes."""
+    import torch
+
+    n = valid.numel()
+    nbits = ((n + 511) // 512) * 512
+    v = torch.zeros(nbits, dtype=torch.int64, device=valid.device)
+    v[:n] = valid.to(torch.int64)
+    w = (v.view(-1, 32) << torch.arange(32, device=valid.device, dtype=torch.int64)).sum(dim=1)
+    return torch.where(w >= (1 << 31), w - (1 << 32), w).to(torch.int32)
+
+
+def plain_100m_device(card: int, n: int, seed: int, device):
+    """The 100M-row workload (int64 key uniform over `card` values, int64 a in
+    [-1e6, 1e6], float32 b ~N(0,1) with 10% nulls) generated on `device`.
+    Returns (key, a, b) Columns."""
+    import torch
+
+    from .column import Column
+    from ._abi import TypeId
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed * 1_000_003 + card)
+    k = torch.randint(0, card, (n,), generator=g, device=device, dtype=torch.int64)
+    a = torch.randint(-1_000_000, 1_000_001, (n,), generator=g, device=device, dtype=torch.int64)
+    b = torch.randn(n, generator=g, device=device, dtype=torch.float32)
+    bvalid = torch.rand(n, generator=g, device=device) >= 0.10
+    words = _bitmask_device(bvalid)
+    nulls = int(n - int(bvalid.sum().item()))
+    return (Column(TypeId.INT64, n, k), Column(TypeId.INT64, n, a),
+            Column(TypeId.FLOAT32, n, b, words, 0, nulls))
+
+
+def plain_200m_device(n: int, seed: int, device, ranks: int = 100_000, s: float = 1.2):
+    """The 200M-row composite-key workload generated on `device`: `ranks`
+    fixed random distinct (int32, int16) pairs (drawn on the host, seeded),
+    the joint key index Zipf(s) by inverse-CDF sampling, 2% nulls per key
+    column (independent Bernoulli), float64 value ~LogNormal(0, 1).
+    Returns (k32, k16, v) Columns."""
+    import torch
+
+    from .column import Column
+    from ._abi import TypeId
+
+    rng = np.random.default_rng(seed)
+    # distinct pairs: draw with replacement, keep first occurrences, top up
+    a = np.empty(0, np.int64)
+    b = np.empty(0, np.int64)
+    while len(a) < ranks:
+        ca = rng.integers(-2**31, 2**31 - 1, size=2 * ranks)
+        cb = rng.integers(-2**15, 2**15 - 1, size=2 * ranks)
+        a = np.concatenate([a, ca])
+        b = np.concatenate([b, cb])
+        joint = (a << 16) ^ (b & 0xffff)
+        _, first = np.unique(joint, return_index=True)
+        first.sort()
+        a, b = a[first], b[first]
+    pa = torch.from_numpy(a[:ranks].astype(np.int32)).to(device)
+    pb = torch.from_numpy(b[:ranks].astype(np.int16)).to(device)
+    w = torch.arange(1, ranks + 1, dtype=torch.float64, device=device) ** (-s)
+    cdf = torch.cumsum(w, 0)
+    cdf /= cdf[-1].clone()
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    j = torch.empty(n, dtype=torch.int64, device=device)
+    chunk = 1 << 26
+    for lo in range(0, n, chunk):
+        hi = min(n, lo + chunk)
+        u = torch.rand(hi - lo, generator=g, device=device, dtype=torch.float64)
+        j[lo:hi] = torch.clamp(torch.searchsorted(cdf, u, right=True), max=ranks - 1)
+    k32 = pa[j]
+    k16 = pb[j]
+    del j
+    v1 = torch.rand(n, generator=g, device=device) >= 0.02
+    v2 = torch.rand(n, generator=g, device=device) >= 0.02
+    v = torch.randn(n, generator=g, device=device, dtype=torch.float64).exp_()
+    m1, m2 = _bitmask_device(v1), _bitmask_device(v2)
+    n1, n2 = int(n - int(v1.sum().item())), int(n - int(v2.sum().item()))
+    del v1, v2
+    return (Column(TypeId.INT32, n, k32, m1, 0, n1), Column(TypeId.INT16, n, k16, m2, 0, n2),
+            Column(TypeId.FLOAT64, n, v))

@@ -7,8 +7,16 @@ Tolerances (stated here, used by every float comparison):
     rounding, where `scale` is sum(|x|) of the group's contributing values
     (the standard summation error bound), FLOAT_RTOL = 1e-12 for float64
     accumulation; float32 outputs add half an ulp of float32;
-  * VAR/STD: |got - want| <= VAR_RTOL * (var + mean^2) (the bound of the
-    shifted one-pass moments against a two-pass FP64 oracle), VAR_RTOL = 1e-9;
+  * VAR/STD: |got - want| <= VAR_EPS * n * (var + range^2), n the group's
+    valid values, var its population variance, range = max - min, VAR_EPS =
+    16 * 2^-52.  This is the rounding bound of the shifted one-pass moments
+    (sum (x-K)^2 and sum (x-K) with K one of the group's values, so
+    (mean - K)^2 <= range^2, each sum accurate to (n-1) 2^-53 of its
+    magnitude) against a two-pass long-double oracle.  It scales with the
+    variance, not with mean^2: sum x^2 - n mean^2 misses it by many orders of
+    magnitude once |mean| >> std.  Integer columns beyond 2^53 add the
+    rounding of their conversion to double, 4 * 2^-52 * max|x| * range.
+    STD's bound is VAR's divided by 2 std (or its square root near 0);
   * MIN/MAX: bit-exact (values are selected, not computed), NaN == NaN.
 """
 from __future__ import annotations
@@ -23,7 +31,7 @@ from oracle.oracle import HostCol
 from oracle import oracle as orc
 
 FLOAT_RTOL = 1e-12
-VAR_RTOL = 1e-9
+VAR_EPS = 16.0 * 2.0 ** -52
 KAT_RTOL = 1e-12  # known answers are exact rationals
 
 
@@ -128,11 +136,11 @@ def compare_values(kind, got, want, go, wo, scale=None, var_scale=None, ctx=""):
         assert np.array_equal(a64[fin], b64[fin]), f"{ctx}: min/max differ"
         return
     if kind in (Kind.VARIANCE, Kind.STD) and var_scale is not None:
-        tol = VAR_RTOL * np.asarray(var_scale)[wo][wmask][fin] + 1e-300
+        vtol = np.asarray(var_scale)[wo][wmask][fin] + 1e-300
+        tol = vtol
         if kind == Kind.STD:
             # d(sqrt v) = dv / (2 sqrt v)
-            tol = tol / np.maximum(2.0 * b64[fin], 1e-300)
-            tol = np.maximum(tol, np.sqrt(VAR_RTOL * np.asarray(var_scale)[wo][wmask][fin]))
+            tol = np.minimum(vtol / np.maximum(2.0 * b64[fin], 1e-300), np.sqrt(vtol))
     elif scale is not None:
         tol = FLOAT_RTOL * np.asarray(scale)[wo][wmask][fin]
     elif kind == Kind.PRODUCT:
@@ -149,24 +157,70 @@ def compare_values(kind, got, want, go, wo, scale=None, var_scale=None, ctx=""):
         f"{float((diff[bad] / np.maximum(np.abs(b64[fin][bad]), 1e-300)).max()):.3e}")
 
 
-def group_scales(keys: Sequence[HostCol], values: HostCol, null_policy) -> dict:
+def var_bound(cnt, var_pop, vmin, vmax, exact_in_f64=True):
+    """Absolute VAR tolerance per group (module doc): VAR_EPS * n * (var +
+    range^2), plus the int-to-double rounding term for integers beyond 2^53."""
+    cnt = np.asarray(cnt, dtype=np.float64)
+    rng = np.asarray(vmax, dtype=np.float64) - np.asarray(vmin, dtype=np.float64)
+    tol = VAR_EPS * np.maximum(cnt, 1.0) * (np.asarray(var_pop, dtype=np.float64) + rng * rng)
+    if not exact_in_f64:
+        big = np.maximum(np.abs(np.asarray(vmin, dtype=np.float64)), np.abs(np.asarray(vmax, dtype=np.float64)))
+        tol = tol + 4.0 * 2.0 ** -52 * big * np.abs(rng)
+    return tol
+
+
+def group_scales(keys: Sequence[HostCol], values: HostCol, null_policy, threads: int = 1) -> dict:
     """Per-group error scales in oracle group order, computed with the oracle
-    itself: sum|x|, sum x^2, count and mean x^2 (= var_pop + mean^2)."""
+    itself: sum|x|, sum x^2, count, and the VAR bound var_bound() of the
+    group's population variance and range."""
     vals = values.values if values.dict_keys is None else values.dict_keys.values[values.values]
     x = vals.astype(np.float64)
     absx = HostCol(np.abs(x), values.valid)
     sq = HostCol(x * x, values.valid)
-    r = orc.groupby(keys, [(absx, [(Kind.SUM, 0), (Kind.COUNT_VALID, 0)]), (sq, [(Kind.SUM, 0), (Kind.MEAN, 0)])],
-                    null_policy)
+    xc = HostCol(x, values.valid)
+    r = orc.groupby(keys, [(absx, [(Kind.SUM, 0), (Kind.COUNT_VALID, 0)]), (sq, [(Kind.SUM, 0)]),
+                           (xc, [(Kind.VARIANCE, 0), (Kind.MIN, 0), (Kind.MAX, 0)])], null_policy, threads)
     # the oracle is deterministic: same first-occurrence group order as the checked call
-    f = lambda a: np.nan_to_num(np.asarray(a, dtype=np.float64), nan=0.0, posinf=0.0)
-    return {"abs": f(r["results"][0][0][1]), "cnt": np.asarray(r["results"][0][1][1], dtype=np.float64),
-            "sq": f(r["results"][1][0][1]), "msq": f(r["results"][1][1][1])}
+    f = lambda a: np.nan_to_num(np.asarray(a, dtype=np.float64), nan=0.0, posinf=0.0, neginf=0.0)
+    cnt = np.asarray(r["results"][0][1][1], dtype=np.float64)
+    exact = vals.dtype.kind == "f" or (len(vals) == 0 or float(np.max(np.abs(x))) <= 2.0 ** 53)
+    vb = var_bound(cnt, f(r["results"][2][0][1]), f(r["results"][2][1][1]), f(r["results"][2][2][1]), exact)
+    return {"abs": f(r["results"][0][0][1]), "cnt": cnt, "sq": f(r["results"][1][0][1]), "var": vb}
 
 
-def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, strategy=None, gpu=None):
+def sorted_group_scales(key: np.ndarray, x: np.ndarray, valid: Optional[np.ndarray]) -> dict:
+    """The tolerance scales of group_scales() computed with numpy for one key
+    column without nulls, for the groups in ascending key order (for inputs
+    too large for the oracle to run a second time): sum|x|, count, and the
+    VAR bound of each group's population variance and range."""
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    xs = x[order].astype(np.float64)
+    vs = np.ones(len(xs), dtype=bool) if valid is None else np.asarray(valid, dtype=bool)[order]
+    del order
+    starts = np.flatnonzero(np.r_[True, ks[1:] != ks[:-1]]) if len(ks) else np.zeros(0, np.int64)
+    del ks
+    lengths = np.diff(np.r_[starts, len(xs)])
+    cnt = np.add.reduceat(vs.astype(np.int64), starts).astype(np.float64)
+    xz = np.where(vs, xs, 0.0)
+    absx = np.add.reduceat(np.abs(xz), starts)
+    mean = np.add.reduceat(xz, starts) / np.maximum(cnt, 1.0)
+    d = np.where(vs, xs - np.repeat(mean, lengths), 0.0)
+    var = np.add.reduceat(d * d, starts) / np.maximum(cnt, 1.0)
+    del d
+    mn = np.minimum.reduceat(np.where(vs, xs, np.inf), starts)
+    mx = np.maximum.reduceat(np.where(vs, xs, -np.inf), starts)
+    empty = cnt == 0
+    mn[empty] = 0.0
+    mx[empty] = 0.0
+    exact = x.dtype.kind == "f" or (len(x) == 0 or float(np.max(np.abs(xs))) <= 2.0 ** 53)
+    return {"abs": absx, "cnt": cnt, "var": var_bound(cnt, var, mn, mx, exact)}
+
+
+def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, strategy=None, gpu=None,
+                  threads: int = 1):
     """Full parity check of libgbx against the oracle on the same inputs."""
-    want = orc.groupby(keys, requests, null_policy)
+    want = orc.groupby(keys, requests, null_policy, threads)
     got = gpu if gpu is not None else run_gpu(keys, requests, null_policy, strategy)
     assert got["num_groups"] == want["num_groups"], f"groups {got['num_groups']} != {want['num_groups']}"
     go = sort_order(got["keys"])
@@ -182,7 +236,7 @@ def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCL
             s = v = None
             if kind in (Kind.VARIANCE, Kind.STD) or (is_float and kind in (Kind.SUM, Kind.MEAN, Kind.SUM_OF_SQUARES)):
                 if sc is None:
-                    sc = group_scales(keys, vals, null_policy)
+                    sc = group_scales(keys, vals, null_policy, threads)
                 if kind == Kind.SUM:
                     s = sc["abs"]
                 elif kind == Kind.MEAN:
@@ -190,6 +244,6 @@ def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCL
                 elif kind == Kind.SUM_OF_SQUARES:
                     s = sc["sq"]
                 else:
-                    v = sc["msq"]
+                    v = sc["var"]
             compare_values(kind, got["results"][q][k], want["results"][q][k], go, wo, s, v, ctx)
     return got, want
