@@ -14,10 +14,19 @@ per groupby) are larger than L2 (126 MB), so no L2 flush is needed.
             host->device and reads all results back device->host, the four
             calls pipelined over PCIe (uploads on one copy stream, read-backs
             on another, overlapping the other calls' transfers and compute)
-  roofline -- the partitioned path's aggregation phase (k_part_ranked_cta and one
-            k_part_fold per value channel): its algorithmic bytes (rows read,
-            groups written) / its CUDA-event duration, against the measured
-            HBM copy bandwidth
+  roofline -- the whole aggregate() call (every kernel of the four calls):
+            algorithmic bytes (20.125 B per row read + 85.75 B per group
+            written) / the step's device time, against the measured HBM
+            copy bandwidth; per-cardinality fractions over each call's own
+            event time; `traffic` = ncu DRAM bytes of all of a call's kernels
+  checks -- size-independent properties of the timed calls' results at full
+            size (group count, COUNT totals, exact int64 SUM total, extremes)
+
+Further sections in the same JSON line: config1 (10M rows, 1e3 groups, with
+the oracle, pandas and pyarrow over the same rows), config3 (200M rows,
+Zipf(1.2) composite key with null keys), batched (4,096 instances in one
+graph launch against a plain loop and an async 4-stream plain loop) and
+served (Poisson arrivals at three rates, plus each form's capacity).
 
 `--impl reference` times the reference's CPU algorithm (the oracle
 restatement, all host threads) on a bounded sample of the same workload.
@@ -47,11 +56,11 @@ BYTES_PER_ROW_IN = 8 + 8 + 4 + 1.0 / 8  # key + a + b + b's validity bit
 BYTES_PER_GROUP_OUT = 8 + (8 + 4 + 8 + 8 + 8 + 8) + (4 + 4 + 4 + 4 + 8 + 8) + 6.0 / 8
 METRIC = "groupby rows/s (plain hash groupby, 100M rows, int64 key, cardinality 1e2/1e4/1e6/1e8)"
 PARTITIONED = 3  # gbx_strategy of the radix-partitioned path
-# DRAM bytes per row of the aggregation phase measured by ncu (20M rows,
-# cardinality 2e7): k_part_ranked_cta 0.421 GB read + 0.418 GB written,
-# k_part_fold (int64 channel) 0.262 + 0.503, k_part_fold (float32 channel)
-# 0.202 + 0.358
-AGG_PHASE_DRAM_BYTES_PER_ROW = (0.421107e9 + 0.417534e9 + 0.261609e9 + 0.502701e9 + 0.201567e9 + 0.358031e9) / 20_000_000
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of every
+# kernel of one 100M-row call, per cardinality: 20M-row captures scaled by
+# rows (None: not captured)
+WHOLE_CALL_DRAM_BYTES = {}
+STRATEGY_NAMES = {1: "privatized", 2: "global", 3: "partitioned", 4: "warp", 5: "bucketed"}
 
 
 def parse_args(argv=None):
@@ -67,9 +76,11 @@ def parse_args(argv=None):
                    help="force one aggregation strategy (default: chosen per call)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--sections", type=str, default="plain,batched,served",
-                   help="comma list of: plain (the headline line), batched (4,096-instance batch), "
-                        "served (Poisson request stream)")
+    p.add_argument("--c3-rows", type=int, default=200_000_000)
+    p.add_argument("--sections", type=str, default="plain,config1,config3,batched,served",
+                   help="comma list of: plain (the headline line), config1 (10M rows, 1e3 groups), config3 "
+                        "(200M rows, Zipf composite key), batched (4,096-instance batch), served (Poisson "
+                        "request stream)")
     p.add_argument("--batch-instances", type=int, default=4096)
     p.add_argument("--batch-tune", choices=["off", "cached", "missing", "all"], default="missing")
     p.add_argument("--batch-tune-save", type=str, default=None,
@@ -178,32 +189,16 @@ class ClockSampler:
 
 def device_inputs(card: int, n: int, seed: int, device):
     """The 100M-row workload's columns generated on the device (seeded)."""
-    import torch
+    from cudf_b200 import workloads as W
 
-    from cudf_b200 import Column, TypeId
-
-    g = torch.Generator(device=device)
-    g.manual_seed(seed * 1_000_003 + card)
-    k = torch.randint(0, card, (n,), generator=g, device=device, dtype=torch.int64)
-    a = torch.randint(-1_000_000, 1_000_001, (n,), generator=g, device=device, dtype=torch.int64)
-    b = torch.randn(n, generator=g, device=device, dtype=torch.float32)
-    bvalid = torch.rand(n, generator=g, device=device) >= 0.10
-    words = pack_mask_torch(bvalid)
-    nulls = int(n - int(bvalid.sum().item()))
-    return (Column(TypeId.INT64, n, k), Column(TypeId.INT64, n, a),
-            Column(TypeId.FLOAT32, n, b, words, 0, nulls))
+    return W.plain_100m_device(card, n, seed, device)
 
 
 def pack_mask_torch(valid):
     """Bool tensor -> cudf bitmask words (int32, LSB-first) padded to 64 bytes."""
-    import torch
+    from cudf_b200 import workloads as W
 
-    n = valid.numel()
-    nbits = ((n + 511) // 512) * 512
-    v = torch.zeros(nbits, dtype=torch.int64, device=valid.device)
-    v[:n] = valid.to(torch.int64)
-    w = (v.view(-1, 32) << torch.arange(32, device=valid.device, dtype=torch.int64)).sum(dim=1)
-    return torch.where(w >= (1 << 31), w - (1 << 32), w).to(torch.int32)
+    return W._bitmask_device(valid)
 
 
 def aggs():
@@ -213,6 +208,43 @@ def aggs():
 
 
 # --------------------------------------------------------------- our arm
+
+def check_plain_results(n, cols, kt, res):
+    """Size-independent properties of one timed call's results, on the
+    device: the group count equals the distinct keys, COUNTs add up to the
+    (valid) rows, the int64 SUMs add up exactly to the column's sum, and the
+    extreme MIN / MAX equal the column's extremes."""
+    import torch
+
+    k, a, b = cols
+    G = kt.num_rows()
+
+    def typed(col, dt):
+        return col.data[: G * torch.empty(0, dtype=dt).element_size()].view(dt)
+
+    def valid_rows(col, size):
+        words = col.mask[: (size + 31) // 32].to(torch.int64) & 0xFFFFFFFF
+        bits = (words.view(-1, 1) >> torch.arange(32, device=words.device)) & 1
+        return bits.view(-1)[:size].bool()
+
+    kd, ad, bd = k.data[:n], a.data[:n], b.data[:n]
+    bvalid = valid_rows(b, n)
+    ra, rb = res[0].columns(), res[1].columns()
+    out = {
+        "groups": G == int(torch.unique(kd).numel()),
+        "count_a": int(typed(ra[1], torch.int32).to(torch.int64).sum()) == n,
+        "count_b": int(typed(rb[1], torch.int32).to(torch.int64).sum()) == int(bvalid.sum()),
+        "sum_a_exact": int(typed(ra[0], torch.int64).sum()) == int(ad.sum()),
+        "min_a": int(typed(ra[2], torch.int64).min()) == int(ad.min()),
+        "max_a": int(typed(ra[3], torch.int64).max()) == int(ad.max()),
+    }
+    gvalid = valid_rows(rb[2], G)
+    bv = bd[bvalid]
+    out["min_b"] = float(typed(rb[2], torch.float32)[gvalid].min()) == float(bv.min())
+    out["max_b"] = float(typed(rb[3], torch.float32)[valid_rows(rb[3], G)].max()) == float(bv.max())
+    out["ok"] = all(out.values())
+    return out
+
 
 def run_ours(args, rank, world, local):
     import torch
@@ -274,59 +306,63 @@ def run_ours(args, rank, world, local):
     rows_per_step = n * len(cards)
     value = world * rows_per_step * args.steps / (ms / 1e3)
 
-    # per-cardinality breakdown and the aggregation kernel's roofline
-    import json as _json
+    # the timed calls' results, checked once more after the timed region
+    checks = {}
+    for c in cards:
+        kt, res = gbs[c].aggregate(reqs[c], stream=stream, allocator=alloc)
+        checks[f"{c:g}"] = check_plain_results(n, data[c], kt, res)
+        del kt, res
 
+    # whole-call roofline: every kernel of every aggregate() call.  Algorithmic
+    # bytes per call = rows read (20.125 B) + groups written (85.75 B), over
+    # the step's device time (ms_per_step, host gaps between calls included);
+    # per cardinality over that call's own first-to-last event time.
     peaks = _load_peaks()
     per = {}
-    # the roofline follows the partitioned strategy's aggregation phase
-    # (k_part_ranked_cta + the k_part_fold launches, which also write the
-    # outputs): its algorithmic bytes per call are the rows read and the
-    # groups written
-    agg_ms_total = 0.0
-    agg_bytes_total = 0.0
-    agg_launches = 0
     launches = 0
     for c, st, g in rec:
-        d = per.setdefault(c, {"calls": 0, "total_ms": 0.0, "aggregate_ms": 0.0, "groups": g,
-                               "strategy": st["strategy"], "phases_ms": {}})
+        d = per.setdefault(c, {"calls": 0, "total_ms": 0.0, "groups": g, "strategy": st["strategy"],
+                               "phases_ms": {}, "partition_bits": st["partition_bits"],
+                               "bucket_slots": st["bucket_slots"]})
         d["calls"] += 1
         d["total_ms"] += st["total_ms"]
-        d["aggregate_ms"] += st["aggregate_ms"]
-        for ph in ("sample_ms", "init_ms", "aggregate_ms", "compact_ms", "finalize_ms"):
+        for ph in ("sample_ms", "init_ms", "partition_ms", "aggregate_ms", "compact_ms", "finalize_ms"):
             d["phases_ms"][ph] = d["phases_ms"].get(ph, 0.0) + st[ph]
-        if st["strategy"] == PARTITIONED:
-            agg_ms_total += st["aggregate_ms"]
-            agg_bytes_total += n * BYTES_PER_ROW_IN + g * BYTES_PER_GROUP_OUT
-            agg_launches += 1
         launches += st["kernel_launches"]
     per_out = {}
+    alg_step = 0.0
     for c, d in per.items():
         calls = d["calls"]
         call_ms = d["total_ms"] / calls
         groups = d["groups"]
         alg = n * BYTES_PER_ROW_IN + groups * BYTES_PER_GROUP_OUT
+        alg_step += alg
         per_out[f"{c:g}"] = {
-            "groups": groups, "strategy": d["strategy"],
+            "groups": groups, "strategy": STRATEGY_NAMES.get(d["strategy"], d["strategy"]),
+            "partition_bits": d["partition_bits"], "bucket_slots": d["bucket_slots"],
             "ms_per_call": round(call_ms, 4),
             "rows_per_s": n / (call_ms / 1e3),
+            "algorithmic_bytes": alg,
             "hbm_frac_whole_call": (alg / (call_ms / 1e3)) / 1e9 / peaks["hbm_gbs"],
+            "dram_traffic_bytes": WHOLE_CALL_DRAM_BYTES.get(c),
             "phases_ms": {k: round(v / calls, 4) for k, v in d["phases_ms"].items()},
         }
-    achieved = (agg_bytes_total / (agg_ms_total / 1e3)) / 1e9 if agg_ms_total > 0 else None
+    step_s = ms / args.steps / 1e3
+    achieved = alg_step / step_s / 1e9
+    traffic = [WHOLE_CALL_DRAM_BYTES.get(c) for c in cards]
     roofline = {
-        "bound": "hbm", "kernel": "k_part_ranked_cta + k_part_fold (cardinality 1e6 / 1e8 calls)",
-        "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-        "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
+        "bound": "hbm",
+        "kernel": "whole aggregate() call: every kernel of the four 100M-row calls (1e2, 1e4, 1e6, 1e8)",
+        "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
         "peak_source": peaks["source"],
-        "algorithmic_bytes_per_launch": agg_bytes_total / agg_launches if agg_launches else None,
-        "launches_per_step": agg_launches // max(1, args.steps),
-        # ncu dram__bytes_read.sum + dram__bytes_write.sum of the aggregation
-        # phase on 20M rows of cardinality 2e7 (2.18 GB), scaled by rows to the
-        # 100M-row cardinality-1e8 call; that call's algorithmic bytes are
-        # 100M x 20.125 + 63.2M x 85 = 7.39 GB
-        "traffic": AGG_PHASE_DRAM_BYTES_PER_ROW * n,
-        "traffic_launch": "cardinality 1e8",
+        "algorithmic_bytes_per_launch": alg_step / len(cards),
+        "algorithmic_bytes_per_step": alg_step,
+        "bytes_per_row_in": BYTES_PER_ROW_IN, "bytes_per_group_out": BYTES_PER_GROUP_OUT,
+        "per_cardinality_frac": {k: v["hbm_frac_whole_call"] for k, v in per_out.items()},
+        # ncu dram__bytes_read.sum + dram__bytes_write.sum summed over every
+        # kernel of one call (20M-row captures scaled by rows to 100M)
+        "traffic": (sum(traffic) / len(traffic)) if all(t is not None for t in traffic) else None,
+        "traffic_per_cardinality": {f"{c:g}": WHOLE_CALL_DRAM_BYTES.get(c) for c in cards},
     }
 
     e2e = None
@@ -337,19 +373,20 @@ def run_ours(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, cards)
 
-    # release the plain workload before the batched and served ones
+    # release the plain workload before the other sections
     del gbs, reqs, data
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     sections = args.sections.split(",")
-    batched = None
-    if "batched" in sections:
-        batched = run_batched(args, rank, world, device, stream, alloc)
-        torch.cuda.synchronize()
-        torch.cuda.empty_cache()
-    served = None
-    if "served" in sections:
-        served = run_served(args, rank, device, stream)
+    extra = {}
+    for name, fn in (("config1", run_config1), ("config3", run_config3), ("batched", run_batched),
+                     ("served", run_served)):
+        if name not in sections:
+            continue
+        if name == "served":
+            extra[name] = fn(args, rank, device, stream)
+        else:
+            extra[name] = fn(args, rank, world, device, stream, alloc)
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
 
@@ -364,14 +401,14 @@ def run_ours(args, rank, world, local):
                    "l2": "inputs (2.01 GB per groupby) larger than L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "per_cardinality": per_out,
+        "checks": checks,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk.summary(),
-        "batched": batched,
-        "served": served,
     }
+    out.update(extra)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -472,6 +509,181 @@ def run_e2e(args, cards, data, gbs, reqs, alloc, stream, world, device):
     rows = args.rows * len(cards) * steps * world
     return {"value": rows / (ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h_bytes[0],
             "steps": steps, "ms_per_step": ms / steps}
+
+
+# ------------------------------------------------- configs 1 and 3 (plain)
+
+C1_ROWS = 10_000_000
+C1_BYTES_PER_ROW = 4 + 8                    # int32 key + float64 value
+C1_BYTES_PER_GROUP = 4 + 8 + 4 + 8 + 8 + 8  # key, SUM, COUNT, MEAN, MIN, MAX
+C3_ROWS = 200_000_000
+C3_BYTES_PER_ROW = 4 + 2 + 0.125 + 0.125 + 8  # int32 + int16 keys, their validity bits, float64 value
+C3_BYTES_PER_GROUP = 4 + 2 + 8 + 8            # keys (EXCLUDE: no null keys out), SUM, MEAN
+
+
+def _time_calls(gb, reqs, stream, alloc, warmup, steps):
+    """CUDA-event time per aggregate() call (ms) and the last call's stats."""
+    import torch
+
+    for _ in range(warmup):
+        kt, res = gb.aggregate(reqs, stream=stream, allocator=alloc)
+        del kt, res
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        kt, res = gb.aggregate(reqs, stream=stream, allocator=alloc)
+        groups = kt.num_rows()
+        del kt, res
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, gb.last_stats(), groups
+
+
+def _host_cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def _cpu_baselines(keys, vals, kinds, rows, pandas_aggs, arrow_aggs, oracle_threads=1):
+    """The oracle (single thread), pandas (single thread by construction) and
+    pyarrow (all host threads) on the same host sample; rows/s each."""
+    import numpy as np
+
+    from oracle import oracle as orc
+
+    t0 = time.perf_counter()
+    orc.groupby(keys, vals, 0, threads=oracle_threads)
+    out = {"value": rows / (time.perf_counter() - t0), "unit": "rows/s", "cores": oracle_threads, "kind": "port"}
+    cols = {}  # pandas: nulls as NaN (what cudf.pandas' CPU fallback holds)
+    masked = []  # pyarrow: nulls as a validity mask
+    for i, k in enumerate(keys):
+        v = k.values.astype(np.float64) if k.valid is not None else k.values
+        cols[f"k{i}"] = np.where(k.valid, v, np.nan) if k.valid is not None else v
+        masked.append((f"k{i}", k.values, k.valid))
+    for j, (hv, _) in enumerate(vals):
+        cols[f"v{j}"] = np.where(hv.valid, hv.values, np.nan) if hv.valid is not None else hv.values
+        masked.append((f"v{j}", hv.values, hv.valid))
+    try:
+        import pandas as pd
+
+        df = pd.DataFrame(cols)
+        t0 = time.perf_counter()
+        df.groupby([f"k{i}" for i in range(len(keys))], sort=False, dropna=True).agg(pandas_aggs)
+        out["pandas_rows_per_s"] = rows / (time.perf_counter() - t0)
+        out["pandas_version"] = pd.__version__
+    except Exception as e:  # pragma: no cover
+        out["pandas_error"] = str(e)
+    try:
+        import pyarrow as pa
+
+        tbl = pa.table({name: pa.array(v, mask=None if m is None else ~m) for name, v, m in masked})
+        t0 = time.perf_counter()
+        tbl.group_by([f"k{i}" for i in range(len(keys))], use_threads=True).aggregate(arrow_aggs)
+        out["pyarrow_rows_per_s"] = rows / (time.perf_counter() - t0)
+        out["pyarrow_threads"] = pa.cpu_count()
+        out["pyarrow_version"] = pa.__version__
+    except Exception as e:  # pragma: no cover
+        out["pyarrow_error"] = str(e)
+    out["host_cpu_count"] = os.cpu_count()
+    out["host_cpu_model"] = _host_cpu_model()
+    return out
+
+
+def run_config1(args, rank, world, device, stream, alloc):
+    """The CPU-runnable config at full size: 10M rows, int32 key uniform over
+    1,000 values, float64 N(0,1), SUM/COUNT/MEAN/MIN/MAX -- on the GPU and,
+    over the same 10M rows, the oracle, pandas and pyarrow."""
+    import torch
+
+    from cudf_b200 import Column, GroupBy, GroupByRequest, Table
+    from cudf_b200 import aggregation as agg
+    from cudf_b200 import workloads as W
+    from cudf_b200._abi import Kind
+    from oracle.oracle import HostCol
+
+    d = W.plain_10m(n=C1_ROWS)
+    k = Column.from_numpy(d.keys[0], device=device)
+    v = Column.from_numpy(d.values[0], device=device)
+    gb = GroupBy(Table([k]))
+    gb.set_timing(True)
+    reqs = [GroupByRequest(v, [agg.sum(), agg.count(), agg.mean(), agg.min(), agg.max()])]
+    ms, st, groups = _time_calls(gb, reqs, stream, alloc, max(args.warmup, 3), max(args.steps, 10))
+    peaks = _load_peaks()
+    alg = C1_ROWS * C1_BYTES_PER_ROW + groups * C1_BYTES_PER_GROUP
+    out = {"metric": "groupby rows/s (10M rows, int32 key, 1e3 groups, float64 value)", "value": C1_ROWS / (ms / 1e3),
+           "unit": "rows/s", "ms_per_call": ms, "groups": groups,
+           "strategy": STRATEGY_NAMES.get(st["strategy"], st["strategy"]),
+           "hbm_frac_whole_call": alg / (ms / 1e3) / 1e9 / peaks["hbm_gbs"],
+           "config": {"rows": C1_ROWS, "key": "int32 U[0, 1000)", "value": "float64 N(0,1)",
+                      "aggregations": ["SUM", "COUNT", "MEAN", "MIN", "MAX"],
+                      "l2": "inputs (120 MB) about the size of L2; no flush (a repeated call re-reads L2-resident rows)"}}
+    del gb, reqs, k, v
+    if rank == 0 and not args.no_cpu:
+        aggs5 = [(Kind.SUM, 0), (Kind.COUNT_VALID, 0), (Kind.MEAN, 0), (Kind.MIN, 0), (Kind.MAX, 0)]
+        cpu = _cpu_baselines([HostCol(d.keys[0])], [(HostCol(d.values[0]), aggs5)], aggs5, C1_ROWS,
+                             {"v0": ["sum", "count", "mean", "min", "max"]},
+                             [("v0", "sum"), ("v0", "count"), ("v0", "mean"), ("v0", "min"), ("v0", "max")])
+        cpu["sample"] = "the whole 10M-row workload"
+        out["cpu_baseline"] = cpu
+        out["speedup_vs_pandas"] = out["value"] / cpu["pandas_rows_per_s"] if "pandas_rows_per_s" in cpu else None
+    return out
+
+
+def run_config3(args, rank, world, device, stream, alloc):
+    """200M rows, (int32, int16) key with 2% nulls per column, Zipf(1.2) over
+    1e5 pairs, float64 LogNormal(0, 1), SUM and MEAN (EXCLUDE)."""
+    import numpy as np
+    import torch
+
+    from cudf_b200 import GroupBy, GroupByRequest, Table
+    from cudf_b200 import aggregation as agg
+    from cudf_b200 import workloads as W
+    from cudf_b200._abi import Kind
+    from oracle.oracle import HostCol
+
+    n = args.c3_rows
+    k1, k2, v = W.plain_200m_device(n, W.SEED0 + 3 + rank, device)
+    gb = GroupBy(Table([k1, k2]))
+    gb.set_timing(True)
+    reqs = [GroupByRequest(v, [agg.sum(), agg.mean()])]
+    with ClockSampler(device.index) as clk:
+        ms, st, groups = _time_calls(gb, reqs, stream, alloc, max(args.warmup, 3), max(args.steps, 5))
+    peaks = _load_peaks()
+    alg = n * C3_BYTES_PER_ROW + groups * C3_BYTES_PER_GROUP
+    out = {"metric": "groupby rows/s (200M rows, (int32, int16) key Zipf(1.2) over 1e5 pairs, 2% null keys)",
+           "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_call": ms, "groups": groups,
+           "strategy": STRATEGY_NAMES.get(st["strategy"], st["strategy"]),
+           "estimated_groups": st["estimated_groups"],
+           "phases_ms": {p: st[p] for p in ("sample_ms", "init_ms", "partition_ms", "aggregate_ms", "compact_ms",
+                                            "finalize_ms")},
+           "roofline": {"bound": "hbm", "kernel": "whole aggregate() call", "achieved": alg / (ms / 1e3) / 1e9,
+                        "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": alg / (ms / 1e3) / 1e9 / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                        "algorithmic_bytes_per_launch": alg, "bytes_per_row_in": C3_BYTES_PER_ROW,
+                        "bytes_per_group_out": C3_BYTES_PER_GROUP},
+           "config": {"rows": n, "key": "(int32, int16), 2% nulls each, Zipf(1.2) over 1e5 distinct pairs",
+                      "value": "float64 LogNormal(0,1)", "aggregations": ["SUM", "MEAN"], "null_policy": "EXCLUDE",
+                      "l2": "inputs (%.2f GB) larger than L2; no flush" % (n * C3_BYTES_PER_ROW / 1e9)},
+           "clocks": clk.summary()}
+    del gb, reqs, k1, k2, v
+    if rank == 0 and not args.no_cpu:
+        rows = min(args.cpu_sample_rows, n)
+        d = W.plain_200m(n=rows)
+        keys = [HostCol(d.keys[0], d.key_valid[0]), HostCol(d.keys[1], d.key_valid[1])]
+        a2 = [(Kind.SUM, 0), (Kind.MEAN, 0)]
+        cpu = _cpu_baselines(keys, [(HostCol(d.values[0]), a2)], a2, rows, {"v0": ["sum", "mean"]},
+                             [("v0", "sum"), ("v0", "mean")])
+        cpu["sample"] = f"{rows} rows of the same distribution (numpy seed)"
+        out["cpu_baseline"] = cpu
+    return out
 
 
 # ------------------------------------------------------------- batched form
@@ -618,6 +830,37 @@ def run_batched(args, rank, world, device, stream, alloc):
     loop_ms = loop_pass(done_ms)
     loop_rows_s = total / (loop_ms / 1e3)
 
+    # the plain form issued asynchronously: 4 host threads, each with its own
+    # stream and allocator, split the instances round-robin (calls overlap on
+    # the GPU while others wait for their group counts)
+    import threading
+
+    from cudf_b200 import TorchAllocator
+
+    workers = 4
+    streams = [torch.cuda.Stream(device) for _ in range(workers)]
+    allocs = [TorchAllocator(device) for _ in range(workers)]
+
+    def async_pass():
+        def work(w):
+            with torch.cuda.stream(streams[w]):
+                for i in range(w, len(insts), workers):
+                    kt, rs = gbs[i].aggregate(insts[i].requests, stream=streams[w], allocator=allocs[w])
+                    del kt, rs
+                streams[w].synchronize()
+
+        t_start = time.perf_counter()
+        ts = [threading.Thread(target=work, args=(w,)) for w in range(workers)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return (time.perf_counter() - t_start) * 1e3
+
+    async_pass()
+    async_ms = async_pass()
+    async_rows_s = total / (async_ms / 1e3)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = _batched_cpu(spec)
@@ -637,6 +880,9 @@ def run_batched(args, rank, world, device, stream, alloc):
                                           note="completion time of instance i when all arrive at once")},
         "plain_loop": {"value": loop_rows_s, "unit": "rows/s", "ms_per_pass": loop_ms, "calls": spec.num_instances},
         "speedup_vs_plain_loop": batch_rows_s / loop_rows_s,
+        "plain_async_loop": {"value": async_rows_s, "unit": "rows/s", "ms_per_pass": async_ms,
+                             "calls": spec.num_instances, "host_threads": workers, "streams": workers},
+        "speedup_vs_plain_async_loop": batch_rows_s / async_rows_s,
         "phases_ms": {"init": stats["init_ms"], "aggregate": agg_avg, "output": stats["output_ms"],
                       "launch": stats["execute_ms"]},
         "roofline": {"bound": "hbm", "kernel": "k_batch_agg", "achieved": achieved, "peak": peaks["hbm_gbs"],
@@ -795,6 +1041,10 @@ def run_served(args, rank, device, stream):
     _, span0, _ = _serve_run(lib, h, prepared, [0.0] * len(prepared))
     lib.gbx_server_destroy(h)
     capacity_rps = len(prepared) / span0
+    # the served configuration's own capacity, every request queued at t = 0
+    h = server(*served_cfg)
+    _, span_served, _ = _serve_run(lib, h, prepared, [0.0] * len(prepared))
+    lib.gbx_server_destroy(h)
     rng = np.random.default_rng(20241003 + 5)
     gaps = rng.exponential(1.0, len(prepared))
     rates = {}
@@ -827,6 +1077,9 @@ def run_served(args, rank, device, stream):
                    "rates": "0.5x, 0.9x, 1.2x of the plain loop's capacity (requests/s with all queued at t=0)"},
         "plain_loop_capacity_requests_per_s": capacity_rps,
         "plain_loop_capacity_rows_per_s": total_rows / span0,
+        "served_capacity_requests_per_s": len(prepared) / span_served,
+        "served_capacity_rows_per_s": total_rows / span_served,
+        "capacity_speedup": span0 / span_served,
         "rates": rates,
         "clocks": clk.summary(),
     }
@@ -849,38 +1102,29 @@ def _oracle_requests(d):
 
 
 def cpu_baseline(args, cards):
-    """The oracle (a C restatement of the reference's hash groupby) on a bounded
-    sample of the workload, single-threaded; pandas on the same sample."""
-    from oracle import oracle as orc
-
+    """The oracle (a C restatement of the reference's hash groupby, single
+    thread), pandas (single thread) and pyarrow (all host threads) on a
+    bounded sample of the workload: `cpu_sample_rows` rows of each
+    cardinality, same distributions."""
     rows = args.cpu_sample_rows
     samples = _sample_inputs(cards, rows)
-    t_total = 0.0
+    names = ["sum", "count", "min", "max", "mean", "var"]
+    pandas_aggs = {"v0": names, "v1": names}
+    arrow_aggs = [(f"v{j}", a if a != "var" else "variance") for j in range(2) for a in names]
+    secs = {"value": 0.0, "pandas_rows_per_s": 0.0, "pyarrow_rows_per_s": 0.0}
+    last = {}
     for c in cards:
         keys, reqs = _oracle_requests(samples[c])
-        t0 = time.perf_counter()
-        orc.groupby(keys, reqs, 0, threads=1)
-        t_total += time.perf_counter() - t0
-    out = {"value": rows * len(cards) / t_total, "unit": "rows/s", "cores": 1, "kind": "port",
-           "sample": f"{rows} rows of each of the {len(cards)} cardinalities (same distributions, numpy seed)"}
-    try:
-        import numpy as np
-        import pandas as pd
-
-        tp = 0.0
-        for c in cards:
-            d = samples[c]
-            df = pd.DataFrame({"k": d.keys[0], "a": d.values[0],
-                               "b": np.where(d.value_valid[1], d.values[1], np.nan).astype(np.float32)})
-            t0 = time.perf_counter()
-            df.groupby("k", sort=False).agg({"a": ["sum", "count", "min", "max", "mean", "var"],
-                                              "b": ["sum", "count", "min", "max", "mean", "var"]})
-            tp += time.perf_counter() - t0
-        out["pandas_rows_per_s"] = rows * len(cards) / tp
-        out["pandas_version"] = pd.__version__
-    except Exception as e:  # pragma: no cover
-        out["pandas_error"] = str(e)
-    out["host_cpu_count"] = os.cpu_count()
+        r = _cpu_baselines(keys, reqs, None, rows, pandas_aggs, arrow_aggs)
+        for k in secs:
+            if k in r:
+                secs[k] += rows / r[k]
+        last = r
+    out = dict(last)
+    for k, t in secs.items():
+        if t > 0:
+            out[k] = rows * len(cards) / t
+    out["sample"] = f"{rows} rows of each of the {len(cards)} cardinalities (same distributions, numpy seed)"
     return out
 
 
@@ -933,12 +1177,36 @@ def _load_peaks():
         return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
 
 
+def replica_command(n: int, argv, port: int):
+    """The torchrun command that runs this benchmark as n replicas (one rank
+    per GPU), as the driver launches it."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+            "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *argv]
+
+
+def _free_port() -> int:
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
 def main(argv=None):
+    argv = list(sys.argv[1:] if argv is None else argv)
     args = parse_args(argv)
     rank, world, local = dist_env()
+    launched = "WORLD_SIZE" in os.environ
+    if launched and world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} does not match WORLD_SIZE={world}", file=sys.stderr)
+        sys.exit(2)
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    if not launched and args.gpus > 1:
+        # N replicas: relaunch under torchrun, one rank per GPU
+        r = subprocess.run(replica_command(args.gpus, argv, _free_port()))
+        sys.exit(r.returncode)
     run_ours(args, rank, world, local)
 
 

@@ -207,6 +207,8 @@ class gbx_stats(C.Structure):
         ("total_ms", C.c_float),
         ("partition_bits", C.c_int32),
         ("bucket_slots", C.c_int32),
+        ("partition_ms", C.c_float),
+        ("reserved1", C.c_int32),
     ]
 
 

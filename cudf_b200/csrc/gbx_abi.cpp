@@ -253,7 +253,11 @@ struct PhaseTimer {
     for (int i = 0; i < 5; ++i) GBX_CUDA(cudaEventElapsedTime(&t[i], gb->events[i], gb->events[i + 1]));
     s.timed        = 1;
     s.sample_ms    = t[0];
-    s.init_ms      = t[1];
+    // phase 1 is the table fill, or the radix partition passes of the
+    // partitioned strategy (which has no table to fill)
+    const bool part = s.strategy == GBX_STRATEGY_PARTITIONED;
+    s.init_ms       = part ? 0.f : t[1];
+    s.partition_ms  = part ? t[1] : 0.f;
     s.aggregate_ms = t[2];
     s.compact_ms   = t[3];
     s.finalize_ms  = t[4];
@@ -1219,12 +1223,9 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       launches += 1;
       timer.mark(3);
       // ---- compaction of occupied slots
-      map               = static_cast<uint32_t*>(scratch.get((cap + 1) * 4));
-      size_t temp_bytes = 0;
-      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, nullptr, &temp_bytes, s));
-      void* temp = scratch.get(temp_bytes);
-      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, temp, &temp_bytes, s));
-      launches += 2;  // cub select: tile-state init + sweep
+      map = static_cast<uint32_t*>(scratch.get((cap + 1) * 4));
+      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, call.dev.num_sms, s));
+      launches += 1;
       timer.mark(4);
       GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
       GBX_CUDA(cudaStreamSynchronize(s));
@@ -1296,7 +1297,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
 // ============================================= groupby without allocation
 
 namespace gbx {
-cudaError_t noalloc_scratch(int device, void** ptr, size_t* bytes);  // gbx_noalloc.cu
+cudaError_t noalloc_scratch(void** ptr, size_t* bytes);  // gbx_noalloc.cu
 }
 
 extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
@@ -1322,10 +1323,11 @@ extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
     DeviceInfo dev  = current_device();
     const int64_t n = gb->keys.empty() ? 0 : gb->keys[0].size;
 
-    // ---- the fixed scratch array of this device (looked up once per device)
+    // ---- the fixed scratch array of this device (and, on the first call in
+    //      this context, the array and the path's kernels loaded there)
     void* base        = nullptr;
     size_t base_bytes = 0;
-    GBX_CUDA(noalloc_scratch(dev.device, &base, &base_bytes));
+    GBX_CUDA(noalloc_scratch(&base, &base_bytes));
     size_t off = 0;
     auto carve = [&](size_t bytes) -> void* {
       off       = (off + 255) & ~size_t(255);
@@ -1401,15 +1403,12 @@ extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
     t.status       = reinterpret_cast<int32_t*>(ctl + 26);
     auto* map      = static_cast<uint32_t*>(carve((cap + 1) * 4));
     auto* d_num_selected = reinterpret_cast<int64_t*>(ctl + 27);
-    size_t temp_bytes    = 0;
-    GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, nullptr, &temp_bytes, s));
-    void* temp = carve(temp_bytes);
 
     int64_t G = 0;
     if (n > 0) {
       GBX_CUDA(launch_init_table(t, plan.acc, plan.key.nwords, dev.num_sms, s));
       GBX_CUDA(launch_agg_global(plan, t, n, static_cast<uint32_t>(std::min<uint64_t>(cap, 1u << 12)), dev.num_sms, s));
-      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, temp, &temp_bytes, s));
+      GBX_CUDA(compact_occupied(t, plan.key.nwords, map, d_num_selected, dev.num_sms, s));
       GBX_CUDA(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, s));
       GBX_CUDA(cudaStreamSynchronize(s));
       int32_t status;

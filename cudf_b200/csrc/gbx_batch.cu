@@ -10,10 +10,10 @@
 // scheme), or direct global updates -- into the instance's own global table.
 // Counting, scanning and writing the groups of all instances then take three
 // more launches, so the whole batch is one CUDA graph.
-#include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
 #include "gbx_batch.hpp"
+#include "gbx_scan.hpp"
 #include "gbx_warpcore.cuh"
 
 namespace gbx {
@@ -476,12 +476,12 @@ cudaError_t batch_agg_max_grid(const Plan& schema, int block, size_t smem, int n
 cudaError_t launch_batch_count(const Plan& schema, const BatchInst* insts, int ninst, int64_t* counts,
                                int64_t* offsets, void* temp, size_t* temp_bytes, cudaStream_t st)
 {
-  if (temp == nullptr) return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, counts, offsets, ninst + 1, st);
+  if (temp == nullptr) return scan_exclusive_i64(nullptr, nullptr, ninst + 1, nullptr, temp_bytes, st);
   if (schema.key.nwords == 1) k_batch_count<1><<<instance_grid(ninst), 256, 0, st>>>(insts, ninst, counts);
   else k_batch_count<2><<<instance_grid(ninst), 256, 0, st>>>(insts, ninst, counts);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, counts, offsets, ninst + 1, st);
+  return scan_exclusive_i64(counts, offsets, ninst + 1, temp, temp_bytes, st);
 }
 
 cudaError_t launch_batch_write(const Plan& schema, const BatchInst* insts, int ninst, const int64_t* offsets,

@@ -19,8 +19,6 @@
 // non-NaN value) and the sum of (x - K)^2; partial tables are merged with the
 // shifted-sums identity sum((x-K2)^2) = sum((x-K1)^2) + 2 d S1 + n d^2,
 // d = K1 - K2, S1 = sum(x) - n K1 (Chan, Golub & LeVeque, 1983).
-#include <cub/device/device_select.cuh>
-#include <thrust/iterator/counting_iterator.h>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -187,18 +185,6 @@ __global__ void k_fill_u64(uint64_t* p, uint64_t n, uint64_t v)
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
 }
 
-struct OccupiedPred {
-  const uint64_t* keys;
-  const uint32_t* special_used;
-  uint64_t cap;
-  int nwords;
-  __device__ __forceinline__ bool operator()(const uint32_t& s) const
-  {
-    if (s == cap) return *special_used != 0;
-    if (nwords == 1) return keys[s] != kEmptyWord;
-    return !(keys[2 * (uint64_t)s] == kEmptyWord && keys[2 * (uint64_t)s + 1] == kEmptyWord);
-  }
-};
 
 // ------------------------------------------------------------- finalize
 
@@ -433,14 +419,6 @@ cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLa
   return arg ? run(k_agg_privatized<2, true>) : run(k_agg_privatized<2, false>);
 }
 
-cudaError_t compact_occupied(const TableRef& t, int nwords, uint32_t* map, int64_t* num_selected, void* temp,
-                             size_t* temp_bytes, cudaStream_t st)
-{
-  OccupiedPred pred{t.keys, t.special_used, t.cap, nwords};
-  thrust::counting_iterator<uint32_t> it(0);
-  return cub::DeviceSelect::If(temp, *temp_bytes, it, map, num_selected, static_cast<int64_t>(t.cap + 1), pred, st);
-}
-
 cudaError_t launch_finalize(const Plan& p, const TableRef& t, const uint32_t* map, int64_t G, const OutPlan& op,
                             int num_sms, cudaStream_t st)
 {
@@ -534,4 +512,31 @@ cudaError_t launch_count_valid(const MaskSpans& ms, unsigned long long* out_vali
   return cudaGetLastError();
 }
 
+}  // namespace gbx
+
+namespace gbx {
+// Loads the code of every kernel gbx_groupby_aggregate_noalloc can launch on
+// the current device (cudaFuncGetAttributes loads a kernel that lazy module
+// loading has not loaded yet), so that the call's first use on a device sets
+// aside all of its device memory before it does any work.
+cudaError_t load_noalloc_kernels()
+{
+  const void* kernels[] = {
+    reinterpret_cast<const void*>(k_count_valid),
+    reinterpret_cast<const void*>(k_init_table),
+    reinterpret_cast<const void*>(k_agg_global<1, false>),
+    reinterpret_cast<const void*>(k_agg_global<1, true>),
+    reinterpret_cast<const void*>(k_agg_global<2, false>),
+    reinterpret_cast<const void*>(k_agg_global<2, true>),
+    compact_kernel(1),
+    compact_kernel(2),
+    reinterpret_cast<const void*>(k_finalize),
+  };
+  for (const void* k : kernels) {
+    cudaFuncAttributes attr;
+    const cudaError_t e = cudaFuncGetAttributes(&attr, k);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
 }  // namespace gbx

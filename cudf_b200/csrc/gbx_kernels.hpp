@@ -161,9 +161,12 @@ cudaError_t launch_part_region_finalize(const Plan& p, const PartPlan& pp, const
 // Warp-private shared-memory tables (sl describes one warp's table).
 cudaError_t launch_agg_warp(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int num_sms,
                             uint32_t max_probes, cudaStream_t st);
-// cub select of occupied slot ids; call once with temp == nullptr to size `temp_bytes`.
-cudaError_t compact_occupied(const TableRef& t, int nwords, uint32_t* map, int64_t* num_selected, void* temp,
-                             size_t* temp_bytes, cudaStream_t st);
+// Occupied slot ids of `t` into map[0, *num_selected) in unspecified order
+// (gbx_scan.cu; *num_selected is zeroed first, on the stream).
+cudaError_t compact_occupied(const TableRef& t, int nwords, uint32_t* map, int64_t* num_selected, int num_sms,
+                             cudaStream_t st);
+// The compaction kernel for `nwords` key words (to load it ahead of use).
+const void* compact_kernel(int nwords);
 cudaError_t launch_finalize(const Plan& p, const TableRef& t, const uint32_t* map, int64_t G, const OutPlan& op,
                             int num_sms, cudaStream_t st);
 

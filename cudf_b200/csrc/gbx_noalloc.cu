@@ -11,11 +11,21 @@
 // In host code `g_noalloc_scratch` only names a host-side stand-in for the
 // symbol, never a device address: passing it to a kernel would fault, or,
 // where the GPU can reach host memory, silently use the wrong memory.  The
-// device address is obtained per device with cudaGetSymbolAddress, with that
-// device current, and handed to the kernels as an ordinary pointer.
+// device address is looked up with cudaGetSymbolAddress on every call, with
+// the call's device current, and handed to the kernels as an ordinary
+// pointer.  Looking it up per call (a few microseconds once the module is
+// loaded) keeps it right after a device reset or a context re-created on the
+// device, which unloads the module and would leave a cached address dangling.
+//
+// Under CUDA's lazy module loading (the default) neither this array nor the
+// code of the kernels the call launches is on the device until first used.
+// The set-up below therefore also loads every kernel the no-allocation path
+// can launch, before the call does any work, so that all of the call's
+// device memory is set aside at once -- by its first call on a device, which
+// an empty input (zero rows) turns into a pure set-up call.  A caller that
+// gives the GPU's memory to its own pool afterwards makes that first call
+// beforehand, or runs with CUDA_MODULE_LOADING=EAGER.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/gbx.h"
 
@@ -23,25 +33,17 @@ namespace gbx {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[GBX_NOALLOC_SCRATCH_BYTES];
 
-namespace {
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
-}  // namespace
+cudaError_t load_noalloc_kernels();  // gbx_kernels.cu
 
-// Device address of the scratch array on `device`, which must be the current
-// device.  The lookup runs once per device (the first no-alloc call on it).
-cudaError_t noalloc_scratch(int device, void** ptr, size_t* bytes)
+// Device address of the scratch array on the current device, after loading
+// the array and the kernels of the no-allocation path there.
+cudaError_t noalloc_scratch(void** ptr, size_t* bytes)
 {
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (g_addr[device] == nullptr) {
-    void* p       = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_addr[device] = p;
-  }
-  *ptr   = g_addr[device];
+  void* p       = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  if ((e = load_noalloc_kernels()) != cudaSuccess) return e;
+  *ptr   = p;
   *bytes = sizeof(g_noalloc_scratch);
   return cudaSuccess;
 }

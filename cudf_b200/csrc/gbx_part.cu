@@ -12,10 +12,10 @@
 // one global set of row indices sized by rows and updates N-row sparse columns
 // with per-row atomics (hash/groupby.cu:424-504, 571-580); here every group's
 // state lives in shared memory until it is final.
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 
+#include "gbx_scan.hpp"
 #include "gbx_warpcore.cuh"
 
 namespace gbx {
@@ -817,19 +817,17 @@ cudaError_t launch_part_layout(const PartPlan& pp, void* temp, size_t* temp_byte
   const int items    = (1 << pp.bits) + 1;
   const int counters = (1 << (pp.bits + pp.shard_bits)) + 1;
   if (temp == nullptr) {  // sized for the largest scan (counters >= items)
-    return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, pp.counts, pp.offsets, counters, st);
+    return scan_exclusive_u32(nullptr, nullptr, counters, nullptr, temp_bytes, st);
   }
   cudaError_t e;
   if (!offsets_ready) {
-    e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.counts, pp.offsets, counters, st);
+    e = scan_exclusive_u32(pp.counts, pp.offsets, counters, temp, temp_bytes, st);
     if (e != cudaSuccess) return e;
   }
   k_part_slices<<<grid_rows(items, 256, num_sms * 4), 256, 0, st>>>(pp);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if ((e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.nslices, pp.item_start, items, st)) != cudaSuccess)
-    return e;
-  if ((e = cub::DeviceScan::ExclusiveSum(temp, *temp_bytes, pp.multi, pp.region, items, st)) != cudaSuccess)
-    return e;
+  if ((e = scan_exclusive_u32(pp.nslices, pp.item_start, items, temp, temp_bytes, st)) != cudaSuccess) return e;
+  if ((e = scan_exclusive_u32(pp.multi, pp.region, items, temp, temp_bytes, st)) != cudaSuccess) return e;
   if (offsets_ready) return cudaSuccess;  // cursors are only used by the one-pass scatter
   return cudaMemcpyAsync(pp.cursor, pp.offsets, (counters - 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
 }

@@ -15,10 +15,10 @@
 // in L2, and no global atomics are used.  After the last pass the rows are in
 // bucket order, stable within a bucket, exactly where the bucket offsets of
 // the histogram (k_part_hist) place them.
-#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 
+#include "gbx_scan.hpp"
 #include "gbx_warpcore.cuh"
 
 namespace gbx {
@@ -664,8 +664,7 @@ cudaError_t part_radix_temp_bytes(int64_t n, size_t* temp_bytes)
 {
   const int64_t ntiles = (n + kTileRows - 1) / kTileRows;
   const int items      = static_cast<int>(std::max<int64_t>(ntiles, 1) * kMaxRadix);
-  return cub::DeviceScan::ExclusiveSum(nullptr, *temp_bytes, static_cast<uint32_t*>(nullptr),
-                                       static_cast<uint32_t*>(nullptr), items, cudaStream_t(nullptr));
+  return scan_exclusive_u32(nullptr, nullptr, items, nullptr, temp_bytes, cudaStream_t(nullptr));
 }
 
 namespace {
@@ -732,7 +731,7 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, uint32_t* n
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   const int items = ntiles << dg.width;
-  e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, counts, offsets, items, st);
+  e = scan_exclusive_u32(counts, offsets, items, temp, &temp_bytes, st);
   if (e != cudaSuccess) return e;
   if constexpr (FROM_COLUMNS) {
     // rows kept by the first pass: the later passes' row count

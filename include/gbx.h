@@ -266,7 +266,7 @@ typedef struct gbx_stats {
   int32_t timed;         /* 1 when the phase times below were recorded */
   /* CUDA-event times on the call's stream (gbx_groupby_set_timing) in ms */
   float sample_ms;       /* null counts + sampled distinct count */
-  float init_ms;         /* table identity fill */
+  float init_ms;         /* table identity fill (0 for the partitioned strategy) */
   float aggregate_ms;    /* the aggregation pass over the rows */
   float compact_ms;      /* occupied-slot compaction */
   float finalize_ms;     /* output keys/results + null counts */
@@ -276,6 +276,8 @@ typedef struct gbx_stats {
    * groups, a CTA's); 0 for the other strategies */
   int32_t partition_bits;
   int32_t bucket_slots;
+  float partition_ms;    /* partitioned strategy: the radix partition passes (else 0) */
+  int32_t reserved1;
 } gbx_stats;
 
 GBX_API int gbx_groupby_last_stats(const gbx_groupby* gb, gbx_stats* out);
@@ -294,9 +296,17 @@ GBX_API int gbx_groupby_set_timing(gbx_groupby* gb, int32_t enable);
  * would block or synchronise the device.  This call computes the same result
  * as gbx_groupby_aggregate but allocates nothing: the hash table, compaction
  * map and control words live in a fixed device array of
- * GBX_NOALLOC_SCRATCH_BYTES inside libgbx (every GPU that loads the library
- * holds it until the process exits), and the caller passes every output
+ * GBX_NOALLOC_SCRATCH_BYTES inside libgbx, and the caller passes every output
  * buffer.
+ *
+ * Set-up: each call looks up the array's device address on the current
+ * device.  Under CUDA's lazy module loading (the default) the array and the
+ * code of the kernels this call launches reach the device only when first
+ * used; the first call on a device (in a CUDA context) loads all of them
+ * before it does any work, and the array then stays on that device until the
+ * process exits or the device is reset.  A caller that hands the GPU's memory
+ * to its own pool makes that first call beforehand -- an input of zero rows
+ * does the set-up and nothing else -- or runs with CUDA_MODULE_LOADING=EAGER.
  *
  * Limits: at most GBX_NOALLOC_MAX_GROUPS groups (more is rejected with
  * GBX_ERR_LOGIC after the aggregation pass, outputs untouched), and the
@@ -304,17 +314,21 @@ GBX_API int gbx_groupby_set_timing(gbx_groupby* gb, int32_t enable);
  *
  * Outputs: `out_keys` has one gbx_column per key column and `out_results` one
  * per aggregation of every request, in request order.  The caller sets each
- * column's `data` (room for `capacity` rows of the output type, see
- * gbx_target_type) and `null_mask` (room for `capacity` bits in 32-bit words;
+ * column's `data` and `null_mask` (room for `capacity` bits in 32-bit words;
  * required where the output can hold nulls, ignored otherwise); the call
- * fills each `view` and `*num_groups`.
+ * fills each `view` and `*num_groups`.  A result column's `data` holds
+ * `capacity` rows of gbx_target_type(value type, kind); a key column's holds
+ * `capacity` rows of the key column's own type -- for a DICTIONARY32 key,
+ * rows of its index type (index_type_id, up to 8 bytes), as the output key
+ * is a dictionary column over the input's keys.
  *
  * Every call shares the one array: calls whose work overlaps on the GPU (on
  * different streams or threads) race and corrupt each other's results, so
  * serialise them.  The array keeps the last call's contents; each call clears
- * what must start at zero itself.  The first call on a device looks up the
- * array's device address (once per device); it synchronises `stream` twice,
- * as gbx_groupby_aggregate does. */
+ * what must start at zero itself.  The call synchronises `stream` up to three
+ * times: after counting nulls (only when some column's null_count is -1),
+ * after the aggregation pass (to learn the group count) and after writing
+ * the outputs (to report their null counts). */
 #define GBX_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define GBX_NOALLOC_MAX_GROUPS 32768
 GBX_API int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
