@@ -1077,7 +1077,7 @@ def run_served(args, rank, device, stream):
                    "rates": "0.5x, 0.9x, 1.2x of the plain loop's capacity (requests/s with all queued at t=0)"},
         "plain_loop_capacity_requests_per_s": capacity_rps,
         "plain_loop_capacity_rows_per_s": total_rows / span0,
-        "served_capacity_requests_per_s": len(prepared) / span_served,
+        "served_capacity_requests_per_s": spec.num_instances / span_served,
         "served_capacity_rows_per_s": total_rows / span_served,
         "capacity_speedup": span0 / span_served,
         "rates": rates,

@@ -1194,7 +1194,10 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         int grid        = call.dev.num_sms * std::max<int>(1, std::min<int>(4, static_cast<int>((200 * 1024) / (sl.total + 1024))));
         int64_t max_grid = (call.n + block * 4 - 1) / (block * 4);
         grid             = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(grid, max_grid)));
-        if (tiled_fits(sl, plan.nchan) && !arg_kinds) {
+        if (stream_fits(plan, sl) && !arg_kinds) {
+          // few groups, one key word: streamed tiles grouped in shared memory
+          GBX_CUDA(launch_agg_stream(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 32), max_probes, s));
+        } else if (tiled_fits(sl, plan.nchan) && !arg_kinds) {
           // few groups: tiles grouped in shared memory before the table is touched
           GBX_CUDA(launch_agg_tiled(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 32), max_probes, s));
         } else {

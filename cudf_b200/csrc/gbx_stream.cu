@@ -1,0 +1,418 @@
+// gbx_stream.cu -- the low-cardinality plain path: each CTA streams tiles of
+// the caller's rows through shared memory and groups every tile before it
+// touches its table.
+//
+// Per tile of kSTile rows (kSPer rows a thread, strided so that every load
+// instruction of a warp is one contiguous run):
+//   1. each row's packed key finds (or takes) its slot in the CTA's table
+//      (open addressing in shared memory) and its rank among the tile's rows
+//      of that slot (one 32-bit shared atomic);
+//   2. one block scan turns the slots' row counts into the first position of
+//      each slot's run;
+//   3. each channel's values are loaded and stored at their row's position,
+//      so the tile's values lie in shared memory group by group;
+//   4. every thread folds kSPer consecutive positions in registers (the
+//      fold of chan_acc_add, specialised on the channel's physical type) and
+//      merges each group's partial into its slot with shared reductions --
+//      about one merge per thread and tile at a few hundred groups.  A
+//      partial's VAR sums are relative to its own shift (its first value);
+//      the merge re-centres them on the slot's shift.
+// After its last tile the CTA merges its table into the global one.
+//
+// This replaces the reference's per-row find-or-insert into a cuco set plus
+// per-row atomics on sparse result columns (cpp/src/groupby/hash/groupby.cu:
+// 548-622, groupby_kernels.cuh:98-105, aggregation.cuh:558-573) for inputs
+// whose groups fit a CTA table.  Every loop is bounded: probes by
+// `smem_probes` (then the row goes to the global table directly), CAS loops
+// by their spin limit.
+#include <algorithm>
+
+#include "gbx_kernels.hpp"
+#include "gbx_warpcore.cuh"
+
+namespace gbx {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kSBlock          = 512;
+constexpr int kSPer            = 8;
+constexpr int kSTile           = kSBlock * kSPer;
+constexpr uint32_t kSNoRec     = 0xffffffffu;
+constexpr int kSMaxSlots       = 2048;
+constexpr size_t kSSmemBudget1 = 220 * 1024;  // one CTA an SM
+
+// Dynamic shared memory after the table (SmemLayout at offset 0): slot
+// offsets (S + 2 words), then per channel kSTile value words and kSTile
+// validity bytes.
+struct StreamLayout {
+  uint32_t off_off;
+  uint32_t vals_off;
+  uint32_t valid_off;
+  uint32_t total;
+};
+
+StreamLayout stream_layout(const SmemLayout& sl, int nchan)
+{
+  StreamLayout ly{};
+  uint32_t o  = sl.total;
+  ly.off_off  = o;
+  o += (sl.slots + 2) * 4;
+  o           = (o + 15) & ~15u;
+  ly.vals_off = o;
+  o += static_cast<uint32_t>(nchan) * kSTile * 8;
+  ly.valid_off = o;
+  o += static_cast<uint32_t>(nchan) * kSTile;
+  ly.total = (o + 15) & ~15u;
+  return ly;
+}
+
+// Key of row r.  KM 0: the plan's packing (any key columns that fit one
+// word); 1 / 2: one plain 8- / 4-byte integer key column without a mask,
+// whose packed key is the column's bits.
+template <int KM>
+__device__ __forceinline__ bool stream_key(const KeyPlan& kp, int64_t r, uint64_t& k)
+{
+  if constexpr (KM == 1) {
+    k = __ldg(reinterpret_cast<const unsigned long long*>(kp.cols[0].data) + kp.cols[0].offset + r);
+    return true;
+  } else if constexpr (KM == 2) {
+    k = __ldg(reinterpret_cast<const uint32_t*>(kp.cols[0].data) + kp.cols[0].offset + r);
+    return true;
+  } else {
+    uint64_t kk[1];
+    const bool kept = pack_key<1>(kp, r, kk);
+    k               = kk[0];
+    return kept;
+  }
+}
+
+// Value bits of channel c at row r (false: null, or a dictionary index out
+// of range, which also sets S_BAD_INDEX).
+__device__ __forceinline__ bool stream_value(const Channel& ch, int64_t r, uint64_t& b, int32_t* status)
+{
+  const int64_t i = r + ch.offset;
+  if (!bit_valid(ch.mask, i)) return false;
+  if (ch.dict_data == nullptr) {
+    b = load_bits(ch.data, i, pt_width(ch.ptype));
+    return true;
+  }
+  bool ok;
+  b = value_bits(ch, r, ok);
+  if (!ok) atomicOr(status, S_BAD_INDEX);
+  return ok;
+}
+
+// Merges a thread's partial accumulators A of one group into slot s of the
+// CTA table.  The partial's VAR sums are relative to its own shift A.k; they
+// are re-centred on the slot's shift Ks (recorded by the first merge):
+// with d = A.k - Ks, sum (x-Ks)^2 = s2 + 2 d S1 + n d^2 and sum (x-Ks) = S1 + n d.
+template <int PT>
+__device__ __forceinline__ void merge_stream_partial(const Channel& ch, const ChanAcc& A, const Level<Shared>& L,
+                                                     uint32_t s, int32_t* status)
+{
+  if (A.cnt == 0) return;
+  constexpr bool kFloat = PT == P_F32 || PT == P_F64;
+  constexpr bool kM64   = PT == P_I64 || PT == P_U64 || PT == P_F64;
+  if (ch.a_cnt >= 0) Shared::add_u32(L.acc(ch.a_cnt) + s * 4, A.cnt);
+  if (ch.a_min >= 0) {
+    if (kM64) Shared::min_u64(L.acc(ch.a_min) + s * 8, A.mn);
+    else Shared::min_u32(L.acc(ch.a_min) + s * 4, static_cast<uint32_t>(A.mn));
+  }
+  if (ch.a_max >= 0) {
+    if (kM64) Shared::max_u64(L.acc(ch.a_max) + s * 8, A.mx);
+    else Shared::max_u32(L.acc(ch.a_max) + s * 4, static_cast<uint32_t>(A.mx));
+  }
+  if (kFloat) {
+    if (ch.a_sum >= 0) Shared::add_f64(L.acc(ch.a_sum) + s * 8, __longlong_as_double(static_cast<long long>(A.sum)));
+    if (ch.a_sq >= 0) Shared::add_f64(L.acc(ch.a_sq) + s * 8, __longlong_as_double(static_cast<long long>(A.sq)));
+    if (ch.a_prod >= 0)
+      mul_cas_f64<Shared>(L.acc(ch.a_prod) + s * 8, __longlong_as_double(static_cast<long long>(A.prod)), status);
+  } else {
+    if (ch.a_sum >= 0) Shared::add_u64(L.acc(ch.a_sum) + s * 8, A.sum);
+    if (ch.a_sq >= 0) Shared::add_u64(L.acc(ch.a_sq) + s * 8, A.sq);
+    if (ch.a_prod >= 0) mul_cas_i64<Shared>(L.acc(ch.a_prod) + s * 8, static_cast<int64_t>(A.prod), status);
+  }
+  if (ch.a_k >= 0) {
+    if (A.k == kShiftUnset) {
+      // every valid value was NaN: the partial sums are NaN already
+      Shared::add_f64(L.acc(ch.a_s2) + s * 8, A.s2);
+      if (ch.a_s1 >= 0) Shared::add_f64(L.acc(ch.a_s1) + s * 8, A.s1);
+    } else {
+      const double Kp = __longlong_as_double(static_cast<long long>(A.k));
+      const double Ks = get_shift<Shared>(L.acc(ch.a_k) + s * 8, Kp);
+      const double S1 = shifted_sum(kFloat, PT, A.sum, static_cast<uint64_t>(__double_as_longlong(A.s1)), A.cnt, Kp);
+      const double d  = Kp - Ks;
+      const double n  = static_cast<double>(A.cnt);
+      Shared::add_f64(L.acc(ch.a_s2) + s * 8, A.s2 + 2.0 * d * S1 + n * d * d);
+      if (ch.a_s1 >= 0) Shared::add_f64(L.acc(ch.a_s1) + s * 8, S1 + n * d);
+    }
+  }
+}
+
+// Folds positions [p0, p1) of one channel's staged values (group order)
+// starting in slot s, merging at every group boundary.
+template <int PT>
+__device__ __forceinline__ void fold_positions(const Channel& ch, const uint64_t* vals, const uint8_t* valid,
+                                               const uint32_t* off, uint32_t p0, uint32_t p1, uint32_t s,
+                                               const Level<Shared>& L, int32_t* status)
+{
+  const uint32_t roles = chan_roles(ch);
+  ChanAcc A;
+  chan_acc_init(A);
+  uint32_t end = off[s + 1];
+  for (uint32_t p = p0; p < p1; ++p) {
+    while (p >= end) {  // group boundary (slots without rows in this tile are skipped)
+      merge_stream_partial<PT>(ch, A, L, s, status);
+      chan_acc_init(A);
+      ++s;
+      end = off[s + 1];
+    }
+    if (valid[p]) chan_acc_add<PT>(ch, roles, A, vals[p]);
+  }
+  merge_stream_partial<PT>(ch, A, L, s, status);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant__ Plan plan,
+                                                        const __grid_constant__ TableRef t,
+                                                        const __grid_constant__ SmemLayout sl,
+                                                        const __grid_constant__ StreamLayout ly, int64_t n,
+                                                        uint32_t smem_probes, uint32_t max_probes)
+{
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t warp_sums[kSBlock / 32];
+  __shared__ uint32_t s_special;
+  const uint32_t S    = sl.slots;
+  uint64_t* skeys     = reinterpret_cast<uint64_t*>(smem + sl.keys_off);
+  uint32_t* srows     = reinterpret_cast<uint32_t*>(smem + sl.rows_off);
+  uint32_t* off       = reinterpret_cast<uint32_t*>(smem + ly.off_off);
+  uint64_t* vals      = reinterpret_cast<uint64_t*>(smem + ly.vals_off);
+  uint8_t* valid      = smem + ly.valid_off;
+  const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const uint32_t keys = base + sl.keys_off;
+  const int lane      = threadIdx.x & 31;
+  const int warp      = threadIdx.x >> 5;
+
+  // identity fill; per-slot counts zeroed
+  for (uint32_t s = threadIdx.x; s <= S; s += kSBlock) {
+    skeys[s] = kEmptyWord;
+    srows[s] = 0;
+    off[s]   = 0;
+    for (int a = 0; a < plan.acc.nacc; ++a) {
+      const uint64_t id = identity_bits(plan.acc.kind[a]);
+      if (acc_bytes(plan.acc.kind[a]) == 4) reinterpret_cast<uint32_t*>(smem + sl.acc_off[a])[s] = static_cast<uint32_t>(id);
+      else reinterpret_cast<uint64_t*>(smem + sl.acc_off[a])[s] = id;
+    }
+  }
+  if (threadIdx.x == 0) {
+    s_special  = 0;
+    off[S + 1] = 0;
+  }
+  __syncthreads();
+
+  const Level<Shared> L{base, &sl};
+  const Level<Global> G = global_level(t);
+  const int64_t ntiles  = (n + kSTile - 1) / kSTile;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t t0 = tile * kSTile;
+    // 1. slot and rank of each of this thread's rows (off[] counts the rows)
+    uint64_t k[kSPer];
+    bool kept[kSPer];
+#pragma unroll
+    for (int q = 0; q < kSPer; ++q) {
+      const int64_t r = t0 + threadIdx.x + q * kSBlock;
+      kept[q]         = r < n && stream_key<KM>(plan.key, r, k[q]);
+    }
+    uint32_t rec[kSPer];
+#pragma unroll
+    for (int q = 0; q < kSPer; ++q) {
+      rec[q] = kSNoRec;
+      if (!kept[q]) continue;
+      int64_t s;
+      if (k[q] == kEmptyWord) {
+        s = S;
+        if (s_special == 0) s_special = 1;
+      } else {
+        const uint64_t kk[1] = {k[q]};
+        s = find_or_insert<Shared, 1>(keys, S - 1, kk, fmix64(k[q]), smem_probes);
+      }
+      if (s >= 0) {
+        const uint32_t rank = atomicAdd(off + s, 1u);
+        rec[q]              = (static_cast<uint32_t>(s) << 16) | rank;
+      } else {
+        // the CTA table is full: this row goes to the global table itself
+        const uint64_t kk[1] = {k[q]};
+        const int64_t g      = global_slot<1>(t, kk, max_probes);
+        if (g >= 0) accumulate_row<Global>(plan, G, g, t0 + threadIdx.x + q * kSBlock, t.status);
+      }
+    }
+    __syncthreads();
+    // 2. row counts -> first position of each slot's run (exclusive scan over
+    //    S + 1 slots, kScanPer per thread); COUNT_ALL rows added per slot
+    {
+      constexpr int kPerMax = (kSMaxSlots + 1 + kSBlock - 1) / kSBlock;
+      const int per         = static_cast<int>((S + 1 + kSBlock - 1) / kSBlock);
+      uint32_t c[kPerMax];
+      uint32_t sum = 0;
+#pragma unroll
+      for (int q = 0; q < kPerMax; ++q) {
+        const uint32_t s = threadIdx.x * per + q;
+        c[q]             = (q < per && s <= S) ? off[s] : 0u;
+        sum += c[q];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += o;
+      }
+      if (lane == 31) warp_sums[warp] = incl;
+      __syncthreads();
+      if (warp == 0) {
+        const uint32_t w = lane < kSBlock / 32 ? warp_sums[lane] : 0u;
+        uint32_t wi      = w;
+#pragma unroll
+        for (int d = 1; d < kSBlock / 32; d <<= 1) {
+          const uint32_t o = __shfl_up_sync(0xffffffffu, wi, d);
+          if (lane >= d) wi += o;
+        }
+        if (lane < kSBlock / 32) warp_sums[lane] = wi - w;
+        if (lane == kSBlock / 32 - 1) off[S + 1] = wi;
+      }
+      __syncthreads();
+      uint32_t run = warp_sums[warp] + incl - sum;
+#pragma unroll
+      for (int q = 0; q < kPerMax; ++q) {
+        const uint32_t s = threadIdx.x * per + q;
+        if (q < per && s <= S) {
+          off[s] = run;
+          srows[s] += c[q];
+          run += c[q];
+        }
+      }
+    }
+    __syncthreads();
+    // 3. each channel's values at their row's position
+    for (int ch = 0; ch < plan.nchan; ++ch) {
+      const Channel& chan = plan.chan[ch];
+      uint64_t b[kSPer];
+      bool v[kSPer];
+#pragma unroll
+      for (int q = 0; q < kSPer; ++q) {
+        b[q] = 0;
+        v[q] = rec[q] != kSNoRec && stream_value(chan, t0 + threadIdx.x + q * kSBlock, b[q], t.status);
+      }
+      uint64_t* cv = vals + static_cast<size_t>(ch) * kSTile;
+      uint8_t* cvv = valid + static_cast<size_t>(ch) * kSTile;
+#pragma unroll
+      for (int q = 0; q < kSPer; ++q) {
+        if (rec[q] == kSNoRec) continue;
+        const uint32_t p = off[rec[q] >> 16] + (rec[q] & 0xffffu);
+        cv[p]            = b[q];
+        cvv[p]           = v[q] ? 1 : 0;
+      }
+    }
+    __syncthreads();
+    // 4. fold kSPer consecutive positions per thread, merging per group
+    const uint32_t total = off[S + 1];
+    const uint32_t p0    = threadIdx.x * kSPer;
+    if (p0 < total) {
+      const uint32_t p1 = min(p0 + kSPer, total);
+      // slot of position p0: the last slot whose run starts at or before it
+      uint32_t lo = 0, hi = S;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= p0) lo = mid;
+        else hi = mid - 1;
+      }
+      for (int ch = 0; ch < plan.nchan; ++ch) {
+        const Channel& chan = plan.chan[ch];
+        const uint64_t* cv  = vals + static_cast<size_t>(ch) * kSTile;
+        const uint8_t* cvv  = valid + static_cast<size_t>(ch) * kSTile;
+#define GBX_FOLD_POS(P) fold_positions<P>(chan, cv, cvv, off, p0, p1, lo, L, t.status)
+        switch (chan.ptype) {
+          case P_I8: GBX_FOLD_POS(P_I8); break;
+          case P_I16: GBX_FOLD_POS(P_I16); break;
+          case P_I32: GBX_FOLD_POS(P_I32); break;
+          case P_I64: GBX_FOLD_POS(P_I64); break;
+          case P_U8: GBX_FOLD_POS(P_U8); break;
+          case P_U16: GBX_FOLD_POS(P_U16); break;
+          case P_U32: GBX_FOLD_POS(P_U32); break;
+          case P_U64: GBX_FOLD_POS(P_U64); break;
+          case P_F32: GBX_FOLD_POS(P_F32); break;
+          case P_F64: GBX_FOLD_POS(P_F64); break;
+          default: GBX_FOLD_POS(P_BOOL); break;
+        }
+#undef GBX_FOLD_POS
+      }
+    }
+    __syncthreads();
+    for (uint32_t s = threadIdx.x; s <= S; s += kSBlock) off[s] = 0;
+    __syncthreads();
+  }
+
+  // merge the CTA's table into the global one
+  for (uint32_t s = threadIdx.x; s <= S; s += kSBlock) {
+    const uint64_t k1[1] = {skeys[s]};
+    const bool occupied  = (s < S) ? k1[0] != kEmptyWord : (s_special != 0);
+    if (!occupied || srows[s] == 0) continue;
+    const int64_t g = global_slot<1>(t, k1, max_probes);
+    if (g >= 0) merge_slot<Shared>(plan, L, s, G, g, t.status);
+  }
+}
+
+template <int KM>
+cudaError_t launch_stream_km(const Plan& p, const TableRef& t, const SmemLayout& sl, const StreamLayout& ly,
+                             int64_t n, int num_sms, uint32_t smem_probes, uint32_t max_probes, cudaStream_t st)
+{
+  const void* fn = reinterpret_cast<const void*>(k_agg_stream<KM>);
+  cudaError_t e  = ensure_dynamic_smem(fn, ly.total);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_agg_stream<KM>, kSBlock, ly.total)) !=
+      cudaSuccess)
+    return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int64_t ntiles = (n + kSTile - 1) / kSTile;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(num_sms) * per_sm)));
+  k_agg_stream<KM><<<grid, kSBlock, ly.total, st>>>(p, t, sl, ly, n, smem_probes, max_probes);
+  return cudaGetLastError();
+}
+
+// Key mode of a plan (see stream_key).
+int stream_key_mode(const KeyPlan& kp)
+{
+  if (kp.ncols == 1) {
+    const KeyCol& kc = kp.cols[0];
+    if (kc.mask == nullptr && !kc.is_float && !kc.is_bool && !kc.null_bit && kc.shift == 0 && kc.word == 0) {
+      if (kc.width == 8) return 1;
+      if (kc.width == 4) return 2;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+bool stream_fits(const Plan& p, const SmemLayout& sl)
+{
+  if (p.key.nwords != 1 || plan_has_arg(p) || sl.slots > static_cast<uint32_t>(kSMaxSlots)) return false;
+  return stream_layout(sl, p.nchan).total <= kSSmemBudget1;
+}
+
+cudaError_t launch_agg_stream(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int num_sms,
+                              uint32_t smem_probes, uint32_t max_probes, cudaStream_t st)
+{
+  if (!stream_fits(p, sl)) return cudaErrorInvalidValue;
+  if (n <= 0) return cudaSuccess;
+  const StreamLayout ly = stream_layout(sl, p.nchan);
+  switch (stream_key_mode(p.key)) {
+    case 1: return launch_stream_km<1>(p, t, sl, ly, n, num_sms, smem_probes, max_probes, st);
+    case 2: return launch_stream_km<2>(p, t, sl, ly, n, num_sms, smem_probes, max_probes, st);
+    default: return launch_stream_km<0>(p, t, sl, ly, n, num_sms, smem_probes, max_probes, st);
+  }
+}
+
+}  // namespace gbx
