@@ -11,12 +11,14 @@
 //      each slot's run;
 //   3. each channel's values are loaded and stored at their row's position,
 //      so the tile's values lie in shared memory group by group;
-//   4. every thread folds kSPer consecutive positions in registers (the
-//      fold of chan_acc_add, specialised on the channel's physical type) and
-//      merges each group's partial into its slot with shared reductions --
-//      about one merge per thread and tile at a few hundred groups.  A
-//      partial's VAR sums are relative to its own shift (its first value);
-//      the merge re-centres them on the slot's shift.
+//   4. the runs are cut into chunks of at most kSChunk rows; each thread
+//      folds one chunk in registers (the fold of chan_acc_add, specialised
+//      on the channel's physical type) and merges it into its slot with
+//      shared reductions.  A warp whose 32 chunks all belong to one group
+//      (a group of thousands of rows in the tile) first combines them with
+//      shuffles and merges once: 64-bit shared reductions that many lanes
+//      aim at one address at once serialise.  A chunk's VAR sums are
+//      relative to its own shift (its first value); merges re-centre them.
 // After its last tile the CTA merges its table into the global one.
 //
 // This replaces the reference's per-row find-or-insert into a cuco set plus
@@ -41,13 +43,15 @@ constexpr int kSPer            = 8;
 constexpr int kSTile           = kSBlock * kSPer;
 constexpr uint32_t kSNoRec     = 0xffffffffu;
 constexpr int kSMaxSlots       = 2048;
+constexpr int kSChunk          = 32;  // rows of one group folded by one thread
 constexpr size_t kSSmemBudget1 = 220 * 1024;  // one CTA an SM
 
-// Dynamic shared memory after the table (SmemLayout at offset 0): slot
-// offsets (S + 2 words), then per channel kSTile value words and kSTile
-// validity bytes.
+// Dynamic shared memory after the table (SmemLayout at offset 0): each
+// slot's first position and first chunk (S + 2 words each), then per
+// channel kSTile value words and kSTile validity bytes.
 struct StreamLayout {
   uint32_t off_off;
+  uint32_t coff_off;
   uint32_t vals_off;
   uint32_t valid_off;
   uint32_t total;
@@ -58,6 +62,8 @@ StreamLayout stream_layout(const SmemLayout& sl, int nchan)
   StreamLayout ly{};
   uint32_t o  = sl.total;
   ly.off_off  = o;
+  o += (sl.slots + 2) * 4;
+  ly.coff_off = o;
   o += (sl.slots + 2) * 4;
   o           = (o + 15) & ~15u;
   ly.vals_off = o;
@@ -151,27 +157,91 @@ __device__ __forceinline__ void merge_stream_partial(const Channel& ch, const Ch
   }
 }
 
-// Folds positions [p0, p1) of one channel's staged values (group order)
-// starting in slot s, merging at every group boundary.
+__device__ __forceinline__ uint64_t shfl_down_u64(uint64_t v, int o)
+{
+  return static_cast<uint64_t>(__shfl_down_sync(0xffffffffu, static_cast<unsigned long long>(v), o));
+}
+
+// The sum of every lane's partial in lane 0 (all 32 lanes call it), field
+// by field so that few registers are live: the identities of chan_acc_init
+// leave MIN/MAX/SUM unchanged by an empty partial; PRODUCT and the VAR sums
+// look at the counts.
 template <int PT>
-__device__ __forceinline__ void fold_positions(const Channel& ch, const uint64_t* vals, const uint8_t* valid,
-                                               const uint32_t* off, uint32_t p0, uint32_t p1, uint32_t s,
-                                               const Level<Shared>& L, int32_t* status)
+__device__ __forceinline__ void warp_combine(uint32_t roles, ChanAcc& A)
+{
+  constexpr bool kFloat = PT == P_F32 || PT == P_F64;
+  auto fadd = [](uint64_t a, uint64_t b) {
+    return static_cast<uint64_t>(__double_as_longlong(__longlong_as_double(static_cast<long long>(a)) +
+                                                      __longlong_as_double(static_cast<long long>(b))));
+  };
+#pragma unroll 1
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint32_t nb = __shfl_down_sync(0xffffffffu, A.cnt, o);
+    if (roles & R_MIN) A.mn = min(A.mn, shfl_down_u64(A.mn, o));
+    if (roles & R_MAX) A.mx = max(A.mx, shfl_down_u64(A.mx, o));
+    uint64_t sumb = 0;
+    if (roles & (R_SUM | R_VAR)) sumb = shfl_down_u64(A.sum, o);
+    if (roles & R_SQ) {
+      const uint64_t v = shfl_down_u64(A.sq, o);
+      A.sq             = kFloat ? fadd(A.sq, v) : A.sq + v;
+    }
+    if (roles & R_PROD) {
+      const uint64_t v = shfl_down_u64(A.prod, o);
+      if (nb != 0)
+        A.prod = A.cnt == 0 ? v
+                 : kFloat   ? static_cast<uint64_t>(__double_as_longlong(
+                              __longlong_as_double(static_cast<long long>(A.prod)) *
+                              __longlong_as_double(static_cast<long long>(v))))
+                            : A.prod * v;
+    }
+    if (roles & R_VAR) {
+      const uint64_t kb = shfl_down_u64(A.k, o);
+      const double s2b  = __shfl_down_sync(0xffffffffu, A.s2, o);
+      const double s1b  = __shfl_down_sync(0xffffffffu, A.s1, o);
+      if (nb != 0) {
+        if (A.cnt == 0) {
+          A.k  = kb;
+          A.s2 = s2b;
+          A.s1 = s1b;
+        } else if (A.k == kShiftUnset || kb == kShiftUnset) {
+          if (A.k == kShiftUnset) A.k = kb;
+          A.s2 += s2b;
+          A.s1 += s1b;
+        } else {
+          const double Ka = __longlong_as_double(static_cast<long long>(A.k));
+          const double Kb = __longlong_as_double(static_cast<long long>(kb));
+          const double S1 = shifted_sum(kFloat, PT, sumb, static_cast<uint64_t>(__double_as_longlong(s1b)), nb, Kb);
+          const double d  = Kb - Ka;
+          const double n  = static_cast<double>(nb);
+          A.s2 += s2b + 2.0 * d * S1 + n * d * d;
+          if (kFloat) A.s1 += S1 + n * d;
+        }
+      }
+    }
+    if (roles & (R_SUM | R_VAR)) A.sum = kFloat ? fadd(A.sum, sumb) : A.sum + sumb;
+    A.cnt += nb;
+  }
+}
+
+// Folds staged positions [p0, p1) (one chunk of one group) of a channel and
+// merges the result into slot s; `uniform`: the warp's 32 chunks are all of
+// slot s, so they are combined with shuffles and lane 0 merges once.
+template <int PT>
+__device__ __forceinline__ void fold_chunk_merge(const Channel& ch, const uint64_t* vals, const uint8_t* valid,
+                                                 uint32_t p0, uint32_t p1, uint32_t s, bool uniform,
+                                                 const Level<Shared>& L, int32_t* status)
 {
   const uint32_t roles = chan_roles(ch);
   ChanAcc A;
   chan_acc_init(A);
-  uint32_t end = off[s + 1];
-  for (uint32_t p = p0; p < p1; ++p) {
-    while (p >= end) {  // group boundary (slots without rows in this tile are skipped)
-      merge_stream_partial<PT>(ch, A, L, s, status);
-      chan_acc_init(A);
-      ++s;
-      end = off[s + 1];
-    }
+  for (uint32_t p = p0; p < p1; ++p)
     if (valid[p]) chan_acc_add<PT>(ch, roles, A, vals[p]);
+  if (uniform) {
+    warp_combine<PT>(roles, A);
+    if ((threadIdx.x & 31) == 0) merge_stream_partial<PT>(ch, A, L, s, status);
+  } else {
+    merge_stream_partial<PT>(ch, A, L, s, status);
   }
-  merge_stream_partial<PT>(ch, A, L, s, status);
 }
 
 template <int KM>
@@ -188,6 +258,7 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
   uint64_t* skeys     = reinterpret_cast<uint64_t*>(smem + sl.keys_off);
   uint32_t* srows     = reinterpret_cast<uint32_t*>(smem + sl.rows_off);
   uint32_t* off       = reinterpret_cast<uint32_t*>(smem + ly.off_off);
+  uint32_t* coff      = reinterpret_cast<uint32_t*>(smem + ly.coff_off);
   uint64_t* vals      = reinterpret_cast<uint64_t*>(smem + ly.vals_off);
   uint8_t* valid      = smem + ly.valid_off;
   const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
@@ -207,8 +278,9 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
     }
   }
   if (threadIdx.x == 0) {
-    s_special  = 0;
-    off[S + 1] = 0;
+    s_special   = 0;
+    off[S + 1]  = 0;
+    coff[S + 1] = 0;
   }
   __syncthreads();
 
@@ -239,14 +311,26 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
         s = find_or_insert<Shared, 1>(keys, S - 1, kk, fmix64(k[q]), smem_probes);
       }
       if (s >= 0) {
-        const uint32_t rank = atomicAdd(off + s, 1u);
-        rec[q]              = (static_cast<uint32_t>(s) << 16) | rank;
+        rec[q] = static_cast<uint32_t>(s) << 16;
       } else {
         // the CTA table is full: this row goes to the global table itself
         const uint64_t kk[1] = {k[q]};
         const int64_t g      = global_slot<1>(t, kk, max_probes);
         if (g >= 0) accumulate_row<Global>(plan, G, g, t0 + threadIdx.x + q * kSBlock, t.status);
       }
+    }
+    // ranks: the lanes of a warp that share a slot take consecutive ranks
+    // from one shared atomic (a few hot groups would otherwise serialise)
+#pragma unroll
+    for (int q = 0; q < kSPer; ++q) {
+      const bool has    = rec[q] != kSNoRec;
+      const uint32_t sk = has ? (rec[q] >> 16) : 0xffffffffu;
+      const uint32_t pe = __match_any_sync(0xffffffffu, sk);
+      const int leader  = __ffs(pe) - 1;
+      uint32_t b        = 0;
+      if (has && lane == leader) b = atomicAdd(off + sk, static_cast<uint32_t>(__popc(pe)));
+      b = __shfl_sync(0xffffffffu, b, leader);
+      if (has) rec[q] |= b + static_cast<uint32_t>(__popc(pe & ((1u << lane) - 1u)));
     }
     __syncthreads();
     // 2. row counts -> first position of each slot's run (exclusive scan over
@@ -258,8 +342,10 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
       uint32_t sum = 0;
 #pragma unroll
       for (int q = 0; q < kPerMax; ++q) {
-        const uint32_t s = threadIdx.x * per + q;
-        c[q]             = (q < per && s <= S) ? off[s] : 0u;
+        // rows in the low half, chunks of at most kSChunk rows in the high half
+        const uint32_t s  = threadIdx.x * per + q;
+        const uint32_t rw = (q < per && s <= S) ? off[s] : 0u;
+        c[q]              = rw | (((rw + kSChunk - 1) / kSChunk) << 16);
         sum += c[q];
       }
       uint32_t incl = sum;
@@ -279,7 +365,10 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
           if (lane >= d) wi += o;
         }
         if (lane < kSBlock / 32) warp_sums[lane] = wi - w;
-        if (lane == kSBlock / 32 - 1) off[S + 1] = wi;
+        if (lane == kSBlock / 32 - 1) {
+          off[S + 1]  = wi & 0xffffu;
+          coff[S + 1] = wi >> 16;
+        }
       }
       __syncthreads();
       uint32_t run = warp_sums[warp] + incl - sum;
@@ -287,8 +376,9 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
       for (int q = 0; q < kPerMax; ++q) {
         const uint32_t s = threadIdx.x * per + q;
         if (q < per && s <= S) {
-          off[s] = run;
-          srows[s] += c[q];
+          off[s]  = run & 0xffffu;
+          coff[s] = run >> 16;
+          srows[s] += c[q] & 0xffffu;
           run += c[q];
         }
       }
@@ -315,37 +405,46 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
       }
     }
     __syncthreads();
-    // 4. fold kSPer consecutive positions per thread, merging per group
-    const uint32_t total = off[S + 1];
-    const uint32_t p0    = threadIdx.x * kSPer;
-    if (p0 < total) {
-      const uint32_t p1 = min(p0 + kSPer, total);
-      // slot of position p0: the last slot whose run starts at or before it
-      uint32_t lo = 0, hi = S;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        if (off[mid] <= p0) lo = mid;
-        else hi = mid - 1;
+    // 4. one chunk (<= kSChunk rows of one group) per thread; warps whose
+    //    chunks are all of one group combine them before merging
+    const uint32_t nchunks = coff[S + 1];
+    for (uint32_t c0 = static_cast<uint32_t>(warp) * 32; c0 < nchunks; c0 += kSBlock) {
+      const uint32_t ci  = c0 + lane;
+      const bool active  = ci < nchunks;
+      uint32_t s = 0, p0 = 0, p1 = 0;
+      if (active) {
+        // the chunk's slot: the last slot whose chunks start at or before it
+        uint32_t lo = 0, hi = S;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi + 1) >> 1;
+          if (coff[mid] <= ci) lo = mid;
+          else hi = mid - 1;
+        }
+        s  = lo;
+        p0 = off[s] + (ci - coff[s]) * kSChunk;
+        p1 = min(p0 + kSChunk, off[s + 1]);
       }
+      const bool uniform = __all_sync(0xffffffffu, active && s == __shfl_sync(0xffffffffu, s, 0));
+      if (!active) continue;
       for (int ch = 0; ch < plan.nchan; ++ch) {
         const Channel& chan = plan.chan[ch];
         const uint64_t* cv  = vals + static_cast<size_t>(ch) * kSTile;
         const uint8_t* cvv  = valid + static_cast<size_t>(ch) * kSTile;
-#define GBX_FOLD_POS(P) fold_positions<P>(chan, cv, cvv, off, p0, p1, lo, L, t.status)
+#define GBX_FOLD_CHUNK(P) fold_chunk_merge<P>(chan, cv, cvv, p0, p1, s, uniform, L, t.status)
         switch (chan.ptype) {
-          case P_I8: GBX_FOLD_POS(P_I8); break;
-          case P_I16: GBX_FOLD_POS(P_I16); break;
-          case P_I32: GBX_FOLD_POS(P_I32); break;
-          case P_I64: GBX_FOLD_POS(P_I64); break;
-          case P_U8: GBX_FOLD_POS(P_U8); break;
-          case P_U16: GBX_FOLD_POS(P_U16); break;
-          case P_U32: GBX_FOLD_POS(P_U32); break;
-          case P_U64: GBX_FOLD_POS(P_U64); break;
-          case P_F32: GBX_FOLD_POS(P_F32); break;
-          case P_F64: GBX_FOLD_POS(P_F64); break;
-          default: GBX_FOLD_POS(P_BOOL); break;
+          case P_I8: GBX_FOLD_CHUNK(P_I8); break;
+          case P_I16: GBX_FOLD_CHUNK(P_I16); break;
+          case P_I32: GBX_FOLD_CHUNK(P_I32); break;
+          case P_I64: GBX_FOLD_CHUNK(P_I64); break;
+          case P_U8: GBX_FOLD_CHUNK(P_U8); break;
+          case P_U16: GBX_FOLD_CHUNK(P_U16); break;
+          case P_U32: GBX_FOLD_CHUNK(P_U32); break;
+          case P_U64: GBX_FOLD_CHUNK(P_U64); break;
+          case P_F32: GBX_FOLD_CHUNK(P_F32); break;
+          case P_F64: GBX_FOLD_CHUNK(P_F64); break;
+          default: GBX_FOLD_CHUNK(P_BOOL); break;
         }
-#undef GBX_FOLD_POS
+#undef GBX_FOLD_CHUNK
       }
     }
     __syncthreads();
