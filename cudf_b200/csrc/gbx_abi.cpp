@@ -873,13 +873,33 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         if (tiled_fits(make_smem_layout(plan, Sb), plan.nchan)) bucket_slots = Sb;
       if (bucket_slots == 0) strategy = GBX_STRATEGY_GLOBAL;
     }
+    // Skewed keys: when the keys sampled 4 or more times hold most sampled
+    // rows and fit a CTA table of the streamed-tile kernel, that kernel keeps
+    // them in shared memory and sends the rare keys' rows to the global table
+    // (a Zipf key whose hottest group holds a fifth of the rows would
+    // otherwise serialise the global table's atomics on one slot).
+    const double s_heavy = static_cast<double>(h_ctl[32]), s_heavy_rows = static_cast<double>(h_ctl[33]);
+    const bool skewed    = h_ctl[0] > 0 && s_heavy_rows >= 0.75 * static_cast<double>(h_ctl[0]);
+    uint32_t stream_slots = 0;
+    if (plan.key.nwords == 1 && !plan_has_arg(plan))
+      for (uint32_t Ss = 2048; Ss >= 64 && stream_slots == 0; Ss >>= 1)
+        if (stream_fits(plan, make_smem_layout(plan, Ss)) &&
+            stream_smem_bytes(plan, make_smem_layout(plan, Ss)) <= 110 * 1024)
+          stream_slots = Ss;
+    bool skew_stream = false;
     if (strategy == GBX_STRATEGY_AUTO) {
       // measured on B200 (100M rows, 12 accumulators): at 100 groups the shared
       // table with 32/64-bit shared atomics 4.0 ms, warp-private tables 7.2 ms;
       // at 1e4 groups the L2-resident global table 9.4 ms, the partitioned
       // path 21.4 ms; at 1e6 groups (table beyond L2) 32.6 ms against 17.2 ms
       if (est * 2.0 <= static_cast<double>(s_max)) strategy = GBX_STRATEGY_PRIVATIZED;
-      else if (warp_fits) strategy = GBX_STRATEGY_WARP;
+      else if (skewed && stream_slots > 0 && 2.0 * s_heavy <= static_cast<double>(stream_slots)) {
+        strategy    = GBX_STRATEGY_PRIVATIZED;
+        skew_stream = true;
+        // the rare keys land in the global table: room for more of them than
+        // the sample saw
+        cap = std::min<uint64_t>(cap * 4, 1ULL << 31);
+      } else if (warp_fits) strategy = GBX_STRATEGY_WARP;
       else if (global_in_l2)
         strategy = bucket_bits > 0 && call.n >= kBucketedMinRows ? GBX_STRATEGY_BUCKETED : GBX_STRATEGY_GLOBAL;
       else strategy = GBX_STRATEGY_PARTITIONED;
@@ -1189,6 +1209,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         GBX_CUDA(launch_agg_warp(plan, t, make_smem_layout(plan, s_warp), call.n, call.dev.num_sms, max_probes, s));
       } else if (strategy == GBX_STRATEGY_PRIVATIZED) {
         uint32_t S = static_cast<uint32_t>(std::min<uint64_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * est, 64.0))), s_max));
+        if (skew_stream) S = stream_slots;
         const SmemLayout sl = make_smem_layout(plan, S);
         const int block = 512;
         int grid        = call.dev.num_sms * std::max<int>(1, std::min<int>(4, static_cast<int>((200 * 1024) / (sl.total + 1024))));
@@ -1239,19 +1260,22 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       if (status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
       if ((status & S_TABLE_FULL) == 0) break;
       // table too small for the groups present: grow and redo
-      if (cap >= (1ULL << 31) || attempt >= 2) fail(GBX_ERR_DEVICE, "hash table overflow at capacity %llu", (unsigned long long)cap);
+      if (cap >= (1ULL << 31) || attempt >= 3) fail(GBX_ERR_DEVICE, "hash table overflow at capacity %llu", (unsigned long long)cap);
       gb->stats.retries++;
       scratch.release_all();
       ctl = static_cast<unsigned long long*>(scratch.get(kCtlWords * 8));
       GBX_CUDA(cudaMemsetAsync(ctl, 0, kCtlWords * 8, s));
       d_status       = reinterpret_cast<int32_t*>(ctl + 26);
       d_num_selected = reinterpret_cast<int64_t*>(ctl + 27);
-      // the groups present can number at most the rows: size for that bound
-      cap = std::min<uint64_t>(std::max<uint64_t>(cap * 4, next_pow2(2 * static_cast<uint64_t>(call.n) + 2)),
+      // grow 16x (an underestimate of a skewed key's tail is usually within
+      // that), then to the bound of every row being a group
+      const uint64_t bound = next_pow2(2 * static_cast<uint64_t>(call.n) + 2);
+      cap = std::min<uint64_t>(attempt == 0 ? std::min<uint64_t>(cap * 16, bound) : std::max<uint64_t>(cap * 4, bound),
                                1ULL << 31);
-      if (strategy == GBX_STRATEGY_PRIVATIZED || strategy == GBX_STRATEGY_WARP || strategy == GBX_STRATEGY_BUCKETED)
+      if (strategy == GBX_STRATEGY_WARP || strategy == GBX_STRATEGY_BUCKETED ||
+          (strategy == GBX_STRATEGY_PRIVATIZED && !skew_stream))
         strategy = GBX_STRATEGY_GLOBAL;
-      est = static_cast<double>(call.n);
+      est = static_cast<double>(cap / 2);
     }
     gb->stats.strategy        = strategy;
     gb->stats.table_capacity  = static_cast<int64_t>(cap);

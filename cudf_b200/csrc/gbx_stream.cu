@@ -501,6 +501,8 @@ bool stream_fits(const Plan& p, const SmemLayout& sl)
   return stream_layout(sl, p.nchan).total <= kSSmemBudget1;
 }
 
+size_t stream_smem_bytes(const Plan& p, const SmemLayout& sl) { return stream_layout(sl, p.nchan).total; }
+
 cudaError_t launch_agg_stream(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int num_sms,
                               uint32_t smem_probes, uint32_t max_probes, cudaStream_t st)
 {
