@@ -1153,6 +1153,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         Gp = static_cast<int64_t>(h_ctl[30]);
         if (status & S_SPIN_LIMIT) fail(GBX_ERR_DEVICE, "a bounded device loop gave up (status 0x%x)", status);
         if (status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
+        if (status & S_CHECK_FAILED) fail(GBX_ERR_DEVICE, "partitioned path: rows out of bucket order (status 0x%x)", status);
         if ((status & S_TABLE_FULL) == 0) {
           gb->stats.table_capacity = static_cast<int64_t>(P) * (cta_rank ? S_cta : S);
           gb->stats.partition_bits = bits;
@@ -1258,6 +1259,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       std::memcpy(&G, reinterpret_cast<char*>(h_ctl) + 27 * 8, 8);
       if (status & S_SPIN_LIMIT) fail(GBX_ERR_DEVICE, "a bounded device loop gave up (status 0x%x)", status);
       if (status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
+      if (status & S_CHECK_FAILED) fail(GBX_ERR_DEVICE, "bucketed path: rows out of bucket order (status 0x%x)", status);
       if ((status & S_TABLE_FULL) == 0) break;
       // table too small for the groups present: grow and redo
       if (cap >= (1ULL << 31) || attempt >= 3) fail(GBX_ERR_DEVICE, "hash table overflow at capacity %llu", (unsigned long long)cap);

@@ -282,7 +282,10 @@ __global__ void k_part_slices(const __grid_constant__ PartPlan pp)
     } else {
       // a bucket of at most slice_rows rows is a whole-bucket item of
       // k_part_ranked, not a slice
-      const uint32_t c  = pp.offsets[(b + 1) << pp.shard_bits] - pp.offsets[b << pp.shard_bits];
+      const uint32_t o0 = pp.offsets[b << pp.shard_bits];
+      const uint32_t o1 = pp.offsets[(b + 1) << pp.shard_bits];
+      if (o1 < o0) atomicOr(pp.status, S_CHECK_FAILED);  // rows not in bucket order
+      const uint32_t c  = o1 >= o0 ? o1 - o0 : 0u;
       const uint32_t ns = (c + pp.slice_rows - 1) / pp.slice_rows;
       pp.nslices[b]     = ns > 1 ? ns : 0u;
       pp.multi[b]       = ns > 1 ? 1u : 0u;
@@ -685,7 +688,8 @@ __global__ void __launch_bounds__(256, 2) k_part_agg(const __grid_constant__ Pla
     const uint32_t ns  = pp.nslices[b];
     const uint64_t j   = item - pp.item_start[b];
     const uint64_t b0  = pp.offsets[b << pp.shard_bits];
-    const uint64_t len = pp.offsets[(b + 1) << pp.shard_bits] - b0;
+    const uint64_t b1  = pp.offsets[(b + 1) << pp.shard_bits];
+    const uint64_t len = b1 >= b0 ? b1 - b0 : 0;
     const int64_t r0   = static_cast<int64_t>(b0 + len * j / ns);
     const int64_t r1   = static_cast<int64_t>(b0 + len * (j + 1) / ns);
 

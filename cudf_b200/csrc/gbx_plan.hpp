@@ -167,7 +167,8 @@ inline bool plan_has_arg(const Plan& plan)
 enum StatusBits : int32_t {
   S_TABLE_FULL   = 1,  // a global probe sequence hit its limit: retry with a larger table
   S_SPIN_LIMIT   = 2,  // a bounded CAS / publication loop gave up
-  S_BAD_INDEX    = 4   // a dictionary index was out of range
+  S_BAD_INDEX    = 4,  // a dictionary index was out of range
+  S_CHECK_FAILED = 8   // a consistency check of the partitioned path failed (rows out of bucket order)
 };
 
 }  // namespace gbx

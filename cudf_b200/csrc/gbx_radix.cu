@@ -899,6 +899,12 @@ __global__ void __launch_bounds__(kRadixBlock) k_radix_scatter_persist(const __g
       const int li = threadIdx.x + q * kRadixBlock;
       from[q]      = li < nrows ? sm.src[li] : kNoRow;
       at[q]        = li < nrows ? sm.gp[li] : 0u;
+      // an output row past the pass's rows means inconsistent offsets: the
+      // row is not moved and the call fails
+      if (from[q] != kNoRow && at[q] >= rows) {
+        atomicOr(status, S_CHECK_FAILED);
+        from[q] = kNoRow;
+      }
     }
     for (int j = 0; j < pc.ncol; ++j) {
       const PersistCol& c = pc.c[j];

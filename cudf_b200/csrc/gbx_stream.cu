@@ -424,7 +424,10 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
         p0 = off[s] + (ci - coff[s]) * kSChunk;
         p1 = min(p0 + kSChunk, off[s + 1]);
       }
-      const bool uniform = __all_sync(0xffffffffu, active && s == __shfl_sync(0xffffffffu, s, 0));
+      // every lane takes part in both warp operations (an inactive lane
+      // must not skip the shuffle, or the warp waits for it forever)
+      const uint32_t s_lane0 = __shfl_sync(0xffffffffu, s, 0);
+      const bool uniform     = __all_sync(0xffffffffu, active && s == s_lane0);
       if (!active) continue;
       for (int ch = 0; ch < plan.nchan; ++ch) {
         const Channel& chan = plan.chan[ch];
