@@ -1216,8 +1216,9 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         int grid        = call.dev.num_sms * std::max<int>(1, std::min<int>(4, static_cast<int>((200 * 1024) / (sl.total + 1024))));
         int64_t max_grid = (call.n + block * 4 - 1) / (block * 4);
         grid             = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(grid, max_grid)));
-        if (stream_fits(plan, sl) && !arg_kinds) {
-          // few groups, one key word: streamed tiles grouped in shared memory
+        if (skew_stream) {
+          // skewed keys: the streamed-tile kernel keeps the hot keys in shared
+          // memory and sends the rare keys' rows to the global table
           GBX_CUDA(launch_agg_stream(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 32), max_probes, s));
         } else if (tiled_fits(sl, plan.nchan) && !arg_kinds) {
           // few groups: tiles grouped in shared memory before the table is touched

@@ -652,287 +652,6 @@ __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __g
   }
 }
 
-// --------------------------------------------------- persistent bulk passes
-//
-// k_radix_scatter_persist moves the same rows as k_radix_scatter_bulk with
-// the loads of the next half tile always in flight: each CTA owns count
-// tiles blockIdx.x, blockIdx.x + gridDim.x, ... and walks their halves of
-// kHalfRows rows; when it starts a half it issues the cp.async.bulk copies
-// of every column of the next one into its other buffer, so that the copy
-// engine streams while the threads rank and gather.  Rows keep the count
-// tile's order: a half's rows of digit d follow the earlier half's (base).
-// Used when every column of the pass is 16-byte aligned and both buffers
-// fit in shared memory.
-
-constexpr int kHalfRows  = kTileRows / 2;
-constexpr int kHalfPer   = kHalfRows / kRadixBlock;        // positions per thread
-constexpr int kHalfBatch = kHalfRows / kRadixWarps / 32;   // 32-row batches per warp
-constexpr int kPersistMaxCols = 2 + 2 * kMaxChannels;
-
-// One column of a persistent pass: source and destination of its elements
-// (`width` bytes each; width 0: validity bits of the caller's bitmask, read
-// as words from `src` at bit `bit_offset + row`, written as bytes), and its
-// region in a half-tile buffer.
-struct PersistCol {
-  const unsigned char* src;
-  unsigned char* dst;
-  int32_t width;
-  uint32_t region;
-  int64_t bit_offset;
-};
-struct PersistCols {
-  int32_t ncol;
-  uint32_t buf_bytes;  // one half tile, every region
-  uint32_t tx_bytes;   // bytes the copies of a full half tile deliver
-  uint32_t pad;
-  PersistCol c[kPersistMaxCols];
-};
-
-struct PersistMeta {
-  uint32_t gp[kHalfRows];                // output row of local position i
-  uint16_t src[kHalfRows];               // half-tile row at local position i
-  uint8_t dig[kHalfRows];                // digit of half-tile row r
-  uint32_t cnt[kRadixWarps][kMaxRadix];  // per warp: rows of each digit, then its first local position
-  uint32_t tstart[kMaxRadix];            // first local position of each digit in the half
-  uint32_t goff[kMaxRadix];              // first output row of the count tile's rows of each digit
-  uint32_t base[kMaxRadix];              // rows of each digit in the count tile's earlier half
-  unsigned long long bar[2];             // completion of each buffer's copies
-};
-constexpr size_t kPersistMetaBytes = (sizeof(PersistMeta) + 127) & ~size_t(127);
-
-size_t persist_smem_bytes(const PersistCols& pc) { return kPersistMetaBytes + 2 * size_t(pc.buf_bytes); }
-
-template <int NW>
-__global__ void __launch_bounds__(kRadixBlock) k_radix_scatter_persist(const __grid_constant__ PersistCols pc,
-                                                                      const uint32_t* n_active, int64_t n,
-                                                                      bool first_pass, const Digit dg,
-                                                                      const uint32_t* __restrict__ offsets,
-                                                                      int ntiles, int32_t* status)
-{
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  PersistMeta& sm          = *reinterpret_cast<PersistMeta*>(smem_raw);
-  unsigned char* bufs[2]   = {smem_raw + kPersistMetaBytes, smem_raw + kPersistMetaBytes + pc.buf_bytes};
-  const int64_t rows       = first_pass ? n : static_cast<int64_t>(*n_active);
-  const int64_t halves     = (rows + kHalfRows - 1) / kHalfRows;
-  const int radix          = 1 << dg.width;
-  const int lane           = threadIdx.x & 31;
-  const int warp           = threadIdx.x >> 5;
-  const uint32_t lt        = (1u << lane) - 1u;
-  const uint32_t bar[2]    = {smem_addr(&sm.bar[0]), smem_addr(&sm.bar[1])};
-  if (static_cast<int64_t>(blockIdx.x) * 2 >= halves) return;
-
-  if (threadIdx.x == 0) {
-    mbar_init(bar[0]);
-    mbar_init(bar[1]);
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  // the CTA's halves in order: count tile T = blockIdx.x + k * gridDim.x, half h
-  auto half_of = [&](int64_t i, int64_t& T, int& h) -> bool {
-    T = static_cast<int64_t>(blockIdx.x) + (i >> 1) * gridDim.x;
-    h = static_cast<int>(i & 1);
-    return T * 2 + h < halves;
-  };
-  uint32_t parity  = 0;  // bit b: phase of buffer b's next completion
-  uint32_t pending = 0;  // bit b: bulk copies into buffer b not yet waited for
-  // every column of half (T, h) into buffer b (called by all threads)
-  auto issue = [&](int64_t T, int h, int b) {
-    const int64_t start = T * kTileRows + h * kHalfRows;
-    const int nr        = static_cast<int>(rows - start < kHalfRows ? rows - start : kHalfRows);
-    if (nr == kHalfRows) {
-      if (threadIdx.x == 0) {
-        fence_proxy_async();  // the threads' reads of the buffer come first
-        mbar_expect_tx(bar[b], pc.tx_bytes);
-        for (int j = 0; j < pc.ncol; ++j) {
-          const PersistCol& c = pc.c[j];
-          if (c.width == 0)
-            bulk_copy_g2s(smem_addr(bufs[b] + c.region), c.src + (c.bit_offset + start) / 8, kHalfRows / 8, bar[b]);
-          else
-            bulk_copy_g2s(smem_addr(bufs[b] + c.region), c.src + start * c.width,
-                          static_cast<uint32_t>(kHalfRows) * c.width, bar[b]);
-        }
-      }
-      pending |= 1u << b;
-    } else {
-      // a partial half (the last): loaded by the threads
-      for (int j = 0; j < pc.ncol; ++j) {
-        const PersistCol& c = pc.c[j];
-        unsigned char* d    = bufs[b] + c.region;
-        if (c.width == 0) {
-          // bit_offset + start is a multiple of 128 (a condition of this kernel)
-          const uint32_t* words = reinterpret_cast<const uint32_t*>(c.src) + (c.bit_offset + start) / 32;
-          for (int w = threadIdx.x; w * 32 < nr; w += kRadixBlock) reinterpret_cast<uint32_t*>(d)[w] = __ldg(words + w);
-        } else {
-          for (int i = threadIdx.x; i < nr; i += kRadixBlock) {
-            const int64_t r = start + i;
-            switch (c.width) {
-              case 1: d[i] = __ldg(c.src + r); break;
-              case 2: reinterpret_cast<uint16_t*>(d)[i] = __ldg(reinterpret_cast<const uint16_t*>(c.src) + r); break;
-              case 4: reinterpret_cast<uint32_t*>(d)[i] = __ldg(reinterpret_cast<const uint32_t*>(c.src) + r); break;
-              default:
-                reinterpret_cast<unsigned long long*>(d)[i] = __ldg(reinterpret_cast<const unsigned long long*>(c.src) + r);
-                break;
-            }
-          }
-        }
-      }
-    }
-  };
-
-  int64_t T0;
-  int h0;
-  half_of(0, T0, h0);
-  issue(T0, h0, 0);
-  uint32_t my_goff = threadIdx.x < radix ? __ldg(offsets + static_cast<size_t>(threadIdx.x) * ntiles + T0) : 0u;
-  for (int64_t i = 0;; ++i) {
-    int64_t T;
-    int h;
-    if (!half_of(i, T, h)) break;
-    const int b = static_cast<int>(i & 1);
-    int64_t Tn;
-    int hn;
-    const bool has_next = half_of(i + 1, Tn, hn);
-    if (has_next) issue(Tn, hn, b ^ 1);
-    const int64_t start = T * kTileRows + h * kHalfRows;
-    const int nrows     = static_cast<int>(rows - start < kHalfRows ? rows - start : kHalfRows);
-    for (int q = threadIdx.x; q < kRadixWarps * kMaxRadix; q += kRadixBlock) (&sm.cnt[0][0])[q] = 0;
-    if (h == 0 && threadIdx.x < radix) {
-      // this count tile's offsets into shared memory; the CTA's next count
-      // tile's offsets are loaded now, while this one is ranked and moved
-      sm.goff[threadIdx.x] = my_goff;
-      sm.base[threadIdx.x] = 0;
-      const int64_t Tnext  = T + gridDim.x;
-      if (Tnext < ntiles && Tnext * 2 < halves)
-        my_goff = __ldg(offsets + static_cast<size_t>(threadIdx.x) * ntiles + Tnext);
-    }
-    // wait for this half's copies (bounded; all threads learn the outcome)
-    bool got = true;
-    if (pending & (1u << b)) {
-      got = mbar_wait_bounded(bar[b], (parity >> b) & 1u);
-      if (got) {
-        parity ^= 1u << b;
-        pending &= ~(1u << b);
-      }
-    }
-    if (__syncthreads_and(got) == 0) {
-      if (threadIdx.x == 0) atomicOr(status, S_SPIN_LIMIT);
-      for (int q = 0; q < 2; ++q)
-        if (pending & (1u << q)) (void)mbar_wait_bounded(bar[q], (parity >> q) & 1u);
-      return;
-    }
-    const unsigned char* buf = bufs[b];
-    // per warp: rows of each digit; each row's digit kept
-    for (int j0 = 0; j0 < kHalfBatch; ++j0) {
-      const int r    = warp * (kHalfRows / kRadixWarps) + j0 * 32 + lane;
-      const bool act = r < nrows;
-      uint64_t k[NW];
-#pragma unroll
-      for (int w = 0; w < NW; ++w) k[w] = act ? reinterpret_cast<const unsigned long long*>(buf + pc.c[w].region)[r] : 0;
-      const uint32_t d  = act ? digit_of<NW>(k, dg) : 0xffffffffu;
-      const uint32_t pe = __match_any_sync(kFull, d);
-      if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
-      if (act) sm.dig[r] = static_cast<uint8_t>(d);
-      __syncwarp();
-    }
-    __syncthreads();
-    // digit totals of the half -> first local position of each digit
-    if (warp == 0) {
-      uint32_t tot[kMaxRadix / 32];
-      uint32_t sum = 0;
-#pragma unroll
-      for (int q = 0; q < kMaxRadix / 32; ++q) {
-        const int d = lane * (kMaxRadix / 32) + q;
-        uint32_t c  = 0;
-        if (d < radix)
-          for (int w = 0; w < kRadixWarps; ++w) c += sm.cnt[w][d];
-        tot[q] = c;
-        sum += c;
-      }
-      uint32_t incl = sum;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += v;
-      }
-      uint32_t run = incl - sum;
-#pragma unroll
-      for (int q = 0; q < kMaxRadix / 32; ++q) {
-        const int d = lane * (kMaxRadix / 32) + q;
-        if (d < radix) sm.tstart[d] = run;
-        run += tot[q];
-      }
-    }
-    __syncthreads();
-    uint32_t half_total = 0;  // rows of digit threadIdx.x in this half
-    if (threadIdx.x < radix) {
-      const int d  = threadIdx.x;
-      uint32_t run = sm.tstart[d];
-      for (int w = 0; w < kRadixWarps; ++w) {
-        const uint32_t c = sm.cnt[w][d];
-        sm.cnt[w][d]     = run;
-        run += c;
-      }
-      half_total = run - sm.tstart[d];
-    }
-    __syncthreads();
-    // local position of every row, with its half-tile row and output row
-    for (int j0 = 0; j0 < kHalfBatch; ++j0) {
-      const int r       = warp * (kHalfRows / kRadixWarps) + j0 * 32 + lane;
-      const bool act    = r < nrows;
-      const uint32_t d  = act ? sm.dig[r] : 0xffffffffu;
-      const uint32_t pe = __match_any_sync(kFull, d);
-      const uint32_t lp = act ? sm.cnt[warp][d] + static_cast<uint32_t>(__popc(pe & lt)) : 0u;
-      __syncwarp();
-      if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
-      if (act) {
-        sm.src[lp] = static_cast<uint16_t>(r);
-        sm.gp[lp]  = sm.goff[d] + sm.base[d] + (lp - sm.tstart[d]);
-      }
-      __syncwarp();
-    }
-    __syncthreads();
-    constexpr uint32_t kNoRow = 0xffffffffu;
-    uint32_t from[kHalfPer], at[kHalfPer];
-#pragma unroll
-    for (int q = 0; q < kHalfPer; ++q) {
-      const int li = threadIdx.x + q * kRadixBlock;
-      from[q]      = li < nrows ? sm.src[li] : kNoRow;
-      at[q]        = li < nrows ? sm.gp[li] : 0u;
-      // an output row past the pass's rows means inconsistent offsets: the
-      // row is not moved and the call fails
-      if (from[q] != kNoRow && at[q] >= rows) {
-        atomicOr(status, S_CHECK_FAILED);
-        from[q] = kNoRow;
-      }
-    }
-    for (int j = 0; j < pc.ncol; ++j) {
-      const PersistCol& c = pc.c[j];
-      const unsigned long long* column = reinterpret_cast<const unsigned long long*>(buf + c.region);
-      switch (c.width) {
-        case 0: {
-          const uint32_t* words = reinterpret_cast<const uint32_t*>(column);
-          uint8_t v[kHalfPer];
-#pragma unroll
-          for (int q = 0; q < kHalfPer; ++q)
-            v[q] = from[q] != kNoRow ? static_cast<uint8_t>((words[from[q] >> 5] >> (from[q] & 31)) & 1u) : 0;
-#pragma unroll
-          for (int q = 0; q < kHalfPer; ++q)
-            if (from[q] != kNoRow) c.dst[at[q]] = v[q];
-          break;
-        }
-        case 1: gather_column<uint8_t, kHalfPer>(column, from, at, c.dst); break;
-        case 2: gather_column<uint16_t, kHalfPer>(column, from, at, c.dst); break;
-        case 4: gather_column<uint32_t, kHalfPer>(column, from, at, c.dst); break;
-        default: gather_column<unsigned long long, kHalfPer>(column, from, at, c.dst); break;
-      }
-    }
-    // the second half of this count tile places its rows after this half's
-    if (h == 0 && threadIdx.x < radix) sm.base[threadIdx.x] = half_total;
-    __syncthreads();  // buffer b, the digits and positions are free again
-  }
-}
-
 }  // namespace
 
 size_t part_radix_count_bytes(int64_t n)
@@ -999,72 +718,6 @@ bool first_pass_columns(const Plan& p, const PartBufs& out, PartBufs& src)
   return true;
 }
 
-// The columns of a pass for k_radix_scatter_persist, or false when that
-// kernel cannot run it (a column not 16-byte aligned, a first-pass validity
-// mask that does not start on a 128-bit boundary, too many bytes a row for
-// two half-tile buffers).  `first`: `in` holds the caller's columns (see
-// first_pass_columns); validity then comes from the channels' bitmasks.
-template <int NW>
-bool persist_cols(const Plan& p, const PartBufs& in, const PartBufs& out, bool first, PersistCols& pc)
-{
-  pc           = PersistCols{};
-  uint32_t off = 0;
-  auto add = [&](const void* src, void* dst, int width, int64_t bit_offset) -> bool {
-    if (pc.ncol >= kPersistMaxCols) return false;
-    if ((reinterpret_cast<uintptr_t>(src) & 15u) != 0) return false;
-    PersistCol& c = pc.c[pc.ncol++];
-    c.src         = static_cast<const unsigned char*>(src);
-    c.dst         = static_cast<unsigned char*>(dst);
-    c.width       = width;
-    c.region      = off;
-    c.bit_offset  = bit_offset;
-    off += width == 0 ? kHalfRows / 8 : static_cast<uint32_t>(kHalfRows) * width;
-    return true;
-  };
-  for (int w = 0; w < NW; ++w)
-    if (!add(in.keys[w], const_cast<uint64_t*>(out.keys[w]), 8, 0)) return false;
-  for (int c = 0; c < p.nchan; ++c) {
-    if (!add(in.col[c].vals, const_cast<void*>(out.col[c].vals), out.col[c].width, 0)) return false;
-    if (out.col[c].valid == nullptr) continue;
-    if (first) {
-      const Channel& ch = p.chan[c];
-      if (ch.mask == nullptr || ch.offset % 128 != 0) return false;
-      if (!add(ch.mask, const_cast<uint8_t*>(out.col[c].valid), 0, ch.offset)) return false;
-    } else if (!add(in.col[c].valid, const_cast<uint8_t*>(out.col[c].valid), 1, 0)) {
-      return false;
-    }
-  }
-  pc.buf_bytes = off;
-  pc.tx_bytes  = off;
-  return persist_smem_bytes(pc) <= 227 * 1024;
-}
-
-int device_sm_count()
-{
-  int dev = 0, sms = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 148;
-  return sms;
-}
-
-template <int NW>
-cudaError_t launch_persist(const PersistCols& pc, const uint32_t* n_active, int64_t n, bool first, const Digit& dg,
-                           const uint32_t* offsets, int ntiles, int32_t* status, cudaStream_t st)
-{
-  const size_t smem = persist_smem_bytes(pc);
-  const void* fn    = reinterpret_cast<const void*>(k_radix_scatter_persist<NW>);
-  cudaError_t e     = ensure_dynamic_smem(fn, smem);
-  if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radix_scatter_persist<NW>, kRadixBlock, smem)) !=
-      cudaSuccess)
-    return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  const int grid = std::max(1, std::min(ntiles, device_sm_count() * per_sm));
-  k_radix_scatter_persist<NW><<<grid, kRadixBlock, smem, st>>>(pc, n_active, n, first, dg, offsets, ntiles, status);
-  return cudaGetLastError();
-}
-
 // One pass; the first (FROM_COLUMNS) writes the rows it keeps to *n_active,
 // which the later passes read.
 template <int NW, bool FROM_COLUMNS>
@@ -1087,10 +740,7 @@ cudaError_t radix_pass(const Plan& p, const PartBufs& in, int64_t n, uint32_t* n
   }
   PartBufs user{};
   const bool bulk_first = FROM_COLUMNS && first_pass_columns(p, out, user);
-  PersistCols pc;
-  if ((!FROM_COLUMNS || bulk_first) && persist_cols<NW>(p, bulk_first ? user : in, out, bulk_first, pc)) {
-    e = launch_persist<NW>(pc, n_active, n, bulk_first, dg, offsets, ntiles, status, st);
-  } else if (!FROM_COLUMNS || bulk_first) {
+  if (!FROM_COLUMNS || bulk_first) {
     e = ensure_dynamic_smem(reinterpret_cast<const void*>(k_radix_scatter_bulk<NW>), kBulkSmem);
     if (e != cudaSuccess) return e;
     k_radix_scatter_bulk<NW><<<ntiles, kRadixBlock, kBulkSmem, st>>>(p, bulk_first ? user : in, n_active, n,

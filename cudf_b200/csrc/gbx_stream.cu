@@ -110,6 +110,29 @@ __device__ __forceinline__ bool stream_value(const Channel& ch, int64_t r, uint6
   return ok;
 }
 
+// Slot of key k in the CTA table (inserting it into an empty slot), or -1
+// after `max_probes` slots.  Plain loads and atomicCAS (no volatile asm): the
+// compiler may then keep a thread's row loads in flight across its probes.
+// A stale read of an empty slot is harmless: the CAS then reports the key
+// that won the slot.
+__device__ __forceinline__ int64_t smem_find_or_insert(uint64_t* skeys, uint32_t mask, uint64_t k,
+                                                       uint32_t max_probes)
+{
+  uint32_t s = static_cast<uint32_t>(fmix64(k)) & mask;
+  for (uint32_t p = 0; p < max_probes; ++p) {
+    const uint64_t cur = skeys[s];
+    if (cur == k) return s;
+    if (cur == kEmptyWord) {
+      const unsigned long long old =
+        atomicCAS(reinterpret_cast<unsigned long long*>(skeys + s), static_cast<unsigned long long>(kEmptyWord),
+                  static_cast<unsigned long long>(k));
+      if (old == kEmptyWord || old == k) return s;
+    }
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
+
 // Merges a thread's partial accumulators A of one group into slot s of the
 // CTA table.  The partial's VAR sums are relative to its own shift A.k; they
 // are re-centred on the slot's shift Ks (recorded by the first merge):
@@ -262,7 +285,6 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
   uint64_t* vals      = reinterpret_cast<uint64_t*>(smem + ly.vals_off);
   uint8_t* valid      = smem + ly.valid_off;
   const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-  const uint32_t keys = base + sl.keys_off;
   const int lane      = threadIdx.x & 31;
   const int warp      = threadIdx.x >> 5;
 
@@ -307,8 +329,7 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
         s = S;
         if (s_special == 0) s_special = 1;
       } else {
-        const uint64_t kk[1] = {k[q]};
-        s = find_or_insert<Shared, 1>(keys, S - 1, kk, fmix64(k[q]), smem_probes);
+        s = smem_find_or_insert(skeys, S - 1, k[q], smem_probes);
       }
       if (s >= 0) {
         rec[q] = static_cast<uint32_t>(s) << 16;
