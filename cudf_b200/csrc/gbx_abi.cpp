@@ -880,12 +880,13 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     // otherwise serialise the global table's atomics on one slot).
     const double s_heavy = static_cast<double>(h_ctl[32]), s_heavy_rows = static_cast<double>(h_ctl[33]);
     const bool skewed    = h_ctl[0] > 0 && s_heavy_rows >= 0.75 * static_cast<double>(h_ctl[0]);
+    // table of the streamed-tile kernel: twice the heavy keys (one CTA an SM
+    // when it does not fit two)
     uint32_t stream_slots = 0;
-    if (plan.key.nwords == 1 && !plan_has_arg(plan))
-      for (uint32_t Ss = 2048; Ss >= 64 && stream_slots == 0; Ss >>= 1)
-        if (stream_fits(plan, make_smem_layout(plan, Ss)) &&
-            stream_smem_bytes(plan, make_smem_layout(plan, Ss)) <= 110 * 1024)
-          stream_slots = Ss;
+    if (skewed && plan.key.nwords == 1 && !plan_has_arg(plan)) {
+      const auto need = static_cast<uint32_t>(next_pow2(static_cast<uint64_t>(std::max(2.0 * s_heavy, 64.0))));
+      if (need <= 4096 && stream_fits(plan, make_smem_layout(plan, need))) stream_slots = need;
+    }
     bool skew_stream = false;
     if (strategy == GBX_STRATEGY_AUTO) {
       // measured on B200 (100M rows, 12 accumulators): at 100 groups the shared
@@ -893,7 +894,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       // at 1e4 groups the L2-resident global table 9.4 ms, the partitioned
       // path 21.4 ms; at 1e6 groups (table beyond L2) 32.6 ms against 17.2 ms
       if (est * 2.0 <= static_cast<double>(s_max)) strategy = GBX_STRATEGY_PRIVATIZED;
-      else if (skewed && stream_slots > 0 && 2.0 * s_heavy <= static_cast<double>(stream_slots)) {
+      else if (stream_slots > 0) {
         strategy    = GBX_STRATEGY_PRIVATIZED;
         skew_stream = true;
         // the rare keys land in the global table: room for more of them than

@@ -58,7 +58,7 @@ cudaError_t launch_agg_privatized(const Plan& p, const TableRef& t, const SmemLa
 // half an SM's shared memory).
 bool tiled_fits(const SmemLayout& sl, int nchan);
 // Streamed tiles grouped in shared memory (gbx_stream.cu): one packed key
-// word, no ARGMIN/ARGMAX, a table of at most 2,048 slots.
+// word, no ARGMIN/ARGMAX, a table of at most 4,096 slots.
 bool stream_fits(const Plan& p, const SmemLayout& sl);
 size_t stream_smem_bytes(const Plan& p, const SmemLayout& sl);
 cudaError_t launch_agg_stream(const Plan& p, const TableRef& t, const SmemLayout& sl, int64_t n, int num_sms,

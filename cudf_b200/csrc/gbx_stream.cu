@@ -42,7 +42,7 @@ constexpr int kSBlock          = 512;
 constexpr int kSPer            = 8;
 constexpr int kSTile           = kSBlock * kSPer;
 constexpr uint32_t kSNoRec     = 0xffffffffu;
-constexpr int kSMaxSlots       = 2048;
+constexpr int kSMaxSlots       = 4096;
 constexpr int kSChunk          = 32;  // rows of one group folded by one thread
 constexpr size_t kSSmemBudget1 = 220 * 1024;  // one CTA an SM
 

@@ -357,14 +357,14 @@ def test_partitioned_skewed_keys():
 
 @pytest.mark.parametrize("policy", [NullPolicy.EXCLUDE, NullPolicy.INCLUDE], ids=lambda p: p.name)
 def test_skewed_keys_stream_kernel(policy):
-    """Zipf(1.3) keys over 50,000 ranks: AUTO keeps the hot keys in the
+    """Zipf(1.5) keys over 50,000 ranks: AUTO keeps the hot keys in the
     streamed-tile kernel's shared tables and sends the rare keys' rows to the
     global table, so one group's partials arrive both ways (VAR shifts merged
     across them)."""
     rng = np.random.default_rng(31)
     n = 1_500_000
     ranks = 50_000
-    w = np.arange(1, ranks + 1, dtype=np.float64) ** -1.3
+    w = np.arange(1, ranks + 1, dtype=np.float64) ** -1.5
     cdf = np.cumsum(w) / w.sum()
     j = np.minimum(np.searchsorted(cdf, rng.random(n), side="right"), ranks - 1)
     key_of_rank = rng.permutation(ranks).astype(np.int64) * 7 - 3
@@ -373,7 +373,7 @@ def test_skewed_keys_stream_kernel(policy):
     a = rng.integers(-1_000_000, 1_000_000, size=n).astype(np.int64)
     b = (1e6 + rng.standard_normal(n)).astype(np.float64)
     bvalid = rng.random(n) >= 0.2
-    c = rng.integers(-100, 100, size=n).astype(np.int32)
-    aggs = ALL6 + [(Kind.COUNT_ALL, 0), (Kind.SUM_OF_SQUARES, 0), (Kind.STD, 0)]
-    got, _ = T.assert_parity([hc(k, kvalid)], [(hc(a), aggs), (hc(b, bvalid), aggs), (hc(c), ALL6)], policy)
+    reqs = [(hc(a), [(Kind.SUM, 0), (Kind.MIN, 0), (Kind.MAX, 0), (Kind.COUNT_ALL, 0)]),
+            (hc(b, bvalid), [(Kind.MEAN, 0), (Kind.VARIANCE, 1), (Kind.STD, 0), (Kind.COUNT_VALID, 0)])]
+    got, _ = T.assert_parity([hc(k, kvalid)], reqs, policy)
     assert got["stats"]["strategy"] == Strategy.PRIVATIZED
