@@ -367,7 +367,7 @@ def test_skewed_keys_stream_kernel(policy):
     w = np.arange(1, ranks + 1, dtype=np.float64) ** -1.5
     cdf = np.cumsum(w) / w.sum()
     j = np.minimum(np.searchsorted(cdf, rng.random(n), side="right"), ranks - 1)
-    key_of_rank = rng.permutation(ranks).astype(np.int64) * 7 - 3
+    key_of_rank = (rng.permutation(ranks) * 7 - 3).astype(np.int32)  # 33 packed bits with a null bit: one word
     k = key_of_rank[j]
     kvalid = rng.random(n) >= 0.01
     a = rng.integers(-1_000_000, 1_000_000, size=n).astype(np.int64)
