@@ -1220,7 +1220,9 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         if (skew_stream) {
           // skewed keys: the streamed-tile kernel keeps the hot keys in shared
           // memory and sends the rare keys' rows to the global table
-          GBX_CUDA(launch_agg_stream(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 32), max_probes, s));
+          // a short probe: a hot key was inserted early and sits near its home
+          // slot; a rare key that misses goes to the global table
+          GBX_CUDA(launch_agg_stream(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 8), max_probes, s));
         } else if (tiled_fits(sl, plan.nchan) && !arg_kinds) {
           // few groups: tiles grouped in shared memory before the table is touched
           GBX_CUDA(launch_agg_tiled(plan, t, sl, call.n, call.dev.num_sms, std::min<uint32_t>(S, 32), max_probes, s));

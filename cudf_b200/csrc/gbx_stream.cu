@@ -52,6 +52,7 @@ constexpr size_t kSSmemBudget1 = 220 * 1024;  // one CTA an SM
 struct StreamLayout {
   uint32_t off_off;
   uint32_t coff_off;
+  uint32_t spill_off;  // kSTile u16: tile rows whose key found no slot
   uint32_t vals_off;
   uint32_t valid_off;
   uint32_t total;
@@ -65,6 +66,8 @@ StreamLayout stream_layout(const SmemLayout& sl, int nchan)
   o += (sl.slots + 2) * 4;
   ly.coff_off = o;
   o += (sl.slots + 2) * 4;
+  ly.spill_off = o;
+  o += kSTile * 2;
   o           = (o + 15) & ~15u;
   ly.vals_off = o;
   o += static_cast<uint32_t>(nchan) * kSTile * 8;
@@ -277,11 +280,13 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t warp_sums[kSBlock / 32];
   __shared__ uint32_t s_special;
+  __shared__ uint32_t s_nspill;
   const uint32_t S    = sl.slots;
   uint64_t* skeys     = reinterpret_cast<uint64_t*>(smem + sl.keys_off);
   uint32_t* srows     = reinterpret_cast<uint32_t*>(smem + sl.rows_off);
   uint32_t* off       = reinterpret_cast<uint32_t*>(smem + ly.off_off);
   uint32_t* coff      = reinterpret_cast<uint32_t*>(smem + ly.coff_off);
+  uint16_t* spill     = reinterpret_cast<uint16_t*>(smem + ly.spill_off);
   uint64_t* vals      = reinterpret_cast<uint64_t*>(smem + ly.vals_off);
   uint8_t* valid      = smem + ly.valid_off;
   const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
@@ -301,6 +306,7 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
   }
   if (threadIdx.x == 0) {
     s_special   = 0;
+    s_nspill    = 0;
     off[S + 1]  = 0;
     coff[S + 1] = 0;
   }
@@ -322,22 +328,29 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
     uint32_t rec[kSPer];
 #pragma unroll
     for (int q = 0; q < kSPer; ++q) {
-      rec[q] = kSNoRec;
-      if (!kept[q]) continue;
-      int64_t s;
-      if (k[q] == kEmptyWord) {
-        s = S;
-        if (s_special == 0) s_special = 1;
-      } else {
-        s = smem_find_or_insert(skeys, S - 1, k[q], smem_probes);
+      rec[q]        = kSNoRec;
+      bool to_spill = false;
+      if (kept[q]) {
+        int64_t s;
+        if (k[q] == kEmptyWord) {
+          s = S;
+          if (s_special == 0) s_special = 1;
+        } else {
+          s = smem_find_or_insert(skeys, S - 1, k[q], smem_probes);
+        }
+        if (s >= 0) rec[q] = static_cast<uint32_t>(s) << 16;
+        else to_spill = true;
       }
-      if (s >= 0) {
-        rec[q] = static_cast<uint32_t>(s) << 16;
-      } else {
-        // the CTA table is full: this row goes to the global table itself
-        const uint64_t kk[1] = {k[q]};
-        const int64_t g      = global_slot<1>(t, kk, max_probes);
-        if (g >= 0) accumulate_row<Global>(plan, G, g, t0 + threadIdx.x + q * kSBlock, t.status);
+      // rows whose key found no slot in the CTA table are listed and sent to
+      // the global table below by all threads together (one lane per row
+      // would run the global path with most of the warp idle)
+      const uint32_t bal = __ballot_sync(0xffffffffu, to_spill);
+      if (bal != 0) {
+        uint32_t sb = 0;
+        if (lane == 0) sb = atomicAdd(&s_nspill, static_cast<uint32_t>(__popc(bal)));
+        sb = __shfl_sync(0xffffffffu, sb, 0);
+        if (to_spill)
+          spill[sb + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint16_t>(threadIdx.x + q * kSBlock);
       }
     }
     // ranks: the lanes of a warp that share a slot take consecutive ranks
@@ -354,6 +367,17 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
       if (has) rec[q] |= b + static_cast<uint32_t>(__popc(pe & ((1u << lane) - 1u)));
     }
     __syncthreads();
+    // 1b. the listed rows update the global table directly
+    {
+      const uint32_t nsp = s_nspill;
+      for (uint32_t i = threadIdx.x; i < nsp; i += kSBlock) {
+        const int64_t r = t0 + spill[i];
+        uint64_t kk[1];
+        stream_key<KM>(plan.key, r, kk[0]);
+        const int64_t g = global_slot<1>(t, kk, max_probes);
+        if (g >= 0) accumulate_row<Global>(plan, G, g, r, t.status);
+      }
+    }
     // 2. row counts -> first position of each slot's run (exclusive scan over
     //    S + 1 slots, kScanPer per thread); COUNT_ALL rows added per slot
     {
@@ -473,6 +497,7 @@ __global__ void __launch_bounds__(kSBlock, 2) k_agg_stream(const __grid_constant
     }
     __syncthreads();
     for (uint32_t s = threadIdx.x; s <= S; s += kSBlock) off[s] = 0;
+    if (threadIdx.x == 0) s_nspill = 0;
     __syncthreads();
   }
 
