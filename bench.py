@@ -59,8 +59,10 @@ PARTITIONED = 3  # gbx_strategy of the radix-partitioned path
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of every
 # kernel of one 100M-row call, per cardinality: 20M-row captures scaled by
 # rows (None: not captured)
-WHOLE_CALL_DRAM_BYTES = {}
+WHOLE_CALL_DRAM_BYTES = {100: 2.07e9, 10_000: 6.95e9, 1_000_000: 14.48e9, 100_000_000: 20.63e9}
 STRATEGY_NAMES = {1: "privatized", 2: "global", 3: "partitioned", 4: "warp", 5: "bucketed"}
+# bytes of one row's copies in a radix pass: packed key 8 + a 8 + b 4 + b's validity byte 1
+PART_BYTES_PER_ROW = 21
 
 
 def parse_args(argv=None):
@@ -364,6 +366,21 @@ def run_ours(args, rank, world, local):
         "traffic": (sum(traffic) / len(traffic)) if all(t is not None for t in traffic) else None,
         "traffic_per_cardinality": {f"{c:g}": WHOLE_CALL_DRAM_BYTES.get(c) for c in cards},
     }
+    # the dominant kernel (k_radix_scatter_bulk, a third of the sweep's GPU
+    # time): the partition phase of the partitioned calls, its bytes the
+    # copies each radix pass must move (21 B a row read + 21 B written)
+    pbytes = pms = 0.0
+    for c, st, g in rec:
+        if st["strategy"] == PARTITIONED and st["partition_ms"] > 0:
+            passes = (st["partition_bits"] + 7) // 8
+            pbytes += passes * n * 2 * PART_BYTES_PER_ROW
+            pms += st["partition_ms"]
+    if pms > 0:
+        pa = pbytes / (pms / 1e3) / 1e9
+        roofline["dominant_kernel"] = {
+            "kernel": "k_radix_scatter_bulk (the partition phase of the 1e6 / 1e8 calls: histograms, scans, passes)",
+            "achieved": pa, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": pa / peaks["hbm_gbs"],
+            "bytes_per_row_per_pass": 2 * PART_BYTES_PER_ROW}
 
     e2e = None
     if not args.no_e2e:
