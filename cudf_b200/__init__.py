@@ -5,7 +5,7 @@ include/gbx.h); this package is the Python host-side mirror of pylibcudf's
 groupby interface.  There is no CPU fallback: if libgbx.so is missing the
 first use raises ImportError.
 """
-from ._abi import BatchMode, Kind, NullPolicy, Sorted, Status, Strategy, Tune, TypeId  # noqa: F401
+from ._abi import BatchMode, Interpolation, Kind, NullPolicy, Sorted, Status, Strategy, Tune, TypeId  # noqa: F401
 from ._lib import GbxError, LogicError, UnsupportedError  # noqa: F401
 from . import aggregation  # noqa: F401
 from .column import Column, Table  # noqa: F401
@@ -16,6 +16,6 @@ from .server import Server  # noqa: F401
 __all__ = [
     "Column", "Table", "GroupBy", "GroupByRequest", "TorchAllocator", "aggregation",
     "BatchGroupBy", "BatchInstance", "BatchResult", "BatchMode", "Tune", "Server",
-    "Kind", "NullPolicy", "Sorted", "Status", "Strategy", "TypeId",
+    "Interpolation", "Kind", "NullPolicy", "Sorted", "Status", "Strategy", "TypeId",
     "GbxError", "LogicError", "UnsupportedError",
 ]

@@ -138,8 +138,65 @@ class gbx_table_view(C.Structure):
     ]
 
 
+class Interpolation(enum.IntEnum):
+    """cudf::interpolation (types.hpp:192-198), for QUANTILE."""
+
+    LINEAR = 0
+    LOWER = 1
+    HIGHER = 2
+    MIDPOINT = 3
+    NEAREST = 4
+
+
 class gbx_aggregation(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("ddof", C.c_int32)]
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("ddof", C.c_int32),
+        ("null_policy", C.c_int32),
+        ("interpolation", C.c_int32),
+        ("num_quantiles", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("quantiles", C.POINTER(C.c_double)),
+    ]
+
+
+def fill_aggregation(dst: "gbx_aggregation", agg, keep: list) -> None:
+    """Writes one aggregation -- an object with .kind/.ddof (and optionally
+    .null_policy, .interpolation, .quantiles) or a (kind, ddof[, extra]) tuple,
+    extra a dict of those fields -- into a gbx_aggregation; arrays it
+    allocates are appended to `keep`."""
+    if isinstance(agg, tuple):
+        kind, ddof = agg[0], agg[1]
+        extra = agg[2] if len(agg) > 2 else {}
+        null_policy = extra.get("null_policy", 0)
+        interp = extra.get("interpolation", 0)
+        quantiles = tuple(extra.get("quantiles", ()))
+    else:
+        kind, ddof = agg.kind, agg.ddof
+        null_policy = getattr(agg, "null_policy", 0)
+        interp = getattr(agg, "interpolation", 0)
+        quantiles = tuple(getattr(agg, "quantiles", ()))
+    dst.kind = int(kind)
+    dst.ddof = int(ddof)
+    dst.null_policy = int(null_policy)
+    dst.interpolation = int(interp)
+    dst.num_quantiles = len(quantiles)
+    if quantiles:
+        arr = (C.c_double * len(quantiles))(*[float(q) for q in quantiles])
+        keep.append(arr)
+        dst.quantiles = C.cast(arr, C.POINTER(C.c_double))
+    else:
+        dst.quantiles = None
+
+
+def aggregation_array(aggs):
+    """A gbx_aggregation array for `aggs` and the objects it borrows."""
+    keep = []
+    arr = (gbx_aggregation * max(1, len(aggs)))()
+    for j, a in enumerate(aggs):
+        fill_aggregation(arr[j], a, keep)
+    keep.append(arr)
+    return arr, keep
 
 
 class gbx_request(C.Structure):

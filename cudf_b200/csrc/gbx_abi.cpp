@@ -18,6 +18,7 @@
 #include "../../include/gbx.h"
 #include "gbx_host.hpp"
 #include "gbx_kernels.hpp"
+#include "gbx_sort.hpp"
 
 namespace gbx {
 
@@ -113,9 +114,31 @@ int32_t target_type(int32_t t, int32_t kind)
     case GBX_AGG_STD:
       if (is_integral(t) || is_floating(t)) return GBX_TYPE_FLOAT64;
       return GBX_TYPE_EMPTY;
+    // the sort-path kinds (detail/aggregation/aggregation.hpp:1318-1367):
+    // M2 / MEDIAN / QUANTILE are double over arithmetic values (group_m2.cu
+    // and group_quantiles.cu accept those only), NUNIQUE a size_type count,
+    // NTH_ELEMENT the value's own type
+    case GBX_AGG_M2:
+    case GBX_AGG_MEDIAN:
+    case GBX_AGG_QUANTILE:
+      if (is_integral(t) || is_floating(t)) return GBX_TYPE_FLOAT64;
+      return GBX_TYPE_EMPTY;
+    case GBX_AGG_NUNIQUE: return GBX_TYPE_INT32;
+    case GBX_AGG_NTH_ELEMENT: return t;
     default: return GBX_TYPE_EMPTY;
   }
 }
+
+// Kinds libcudf computes on its sort path (groupby/sort/aggregate.cpp) that
+// are computed here by ordering each group's values (gbx_sort.cu); M2, also
+// a sort-path kind there, comes from the hash table's shifted moments.
+bool is_sort_kind(int32_t k)
+{
+  return k == GBX_AGG_MEDIAN || k == GBX_AGG_QUANTILE || k == GBX_AGG_NUNIQUE || k == GBX_AGG_NTH_ELEMENT;
+}
+
+// Kinds the batched form computes: the hash kinds but ARGMIN / ARGMAX.
+bool is_batch_kind(int32_t k) { return is_hash_kind(k) && k != GBX_AGG_ARGMIN && k != GBX_AGG_ARGMAX; }
 
 // Kinds libcudf accepts on its hash path (hash/groupby.cu:73-84).
 bool is_hash_kind(int32_t k)
@@ -306,16 +329,24 @@ void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n)
     for (int32_t k = 0; k < r.num_aggregations; ++k) {
       int32_t kind = r.aggregations[k].kind;
       // verify_valid_requests (groupby.cu:176-192)
-      if (!is_hash_kind(kind)) {
-        if (kind == GBX_AGG_NTH_ELEMENT ||
-            kind == GBX_AGG_MEDIAN || kind == GBX_AGG_QUANTILE || kind == GBX_AGG_NUNIQUE ||
-            kind == GBX_AGG_M2 || kind == GBX_AGG_ANY || kind == GBX_AGG_ALL || kind > GBX_AGG_NTH_ELEMENT)
+      if (!is_hash_kind(kind) && !is_sort_kind(kind) && kind != GBX_AGG_M2) {
+        if (kind == GBX_AGG_ANY || kind == GBX_AGG_ALL || kind > GBX_AGG_NTH_ELEMENT)
           fail(GBX_ERR_UNSUPPORTED,
-               "aggregation kind %d is computed by libcudf's sort-based groupby, which this library does not "
-               "provide",
+               "aggregation kind %d is computed by libcudf's sort-based groupby only, and not by this library",
                kind);
         fail(GBX_ERR_LOGIC, "Invalid type/aggregation combination.");
       }
+      const gbx_aggregation& ag = r.aggregations[k];
+      if (kind == GBX_AGG_QUANTILE) {
+        GBX_EXPECTS(ag.num_quantiles >= 0 && (ag.num_quantiles == 0 || ag.quantiles != nullptr),
+                    "invalid quantile array");
+        // select_quantile_data (quantiles_util.hpp:171-190) fails on others
+        GBX_EXPECTS(ag.interpolation >= GBX_INTERP_LINEAR && ag.interpolation <= GBX_INTERP_NEAREST,
+                    "Invalid interpolation operation for quantiles.");
+      }
+      if (kind == GBX_AGG_NUNIQUE || kind == GBX_AGG_NTH_ELEMENT)
+        GBX_EXPECTS(ag.null_policy == GBX_NULL_EXCLUDE || ag.null_policy == GBX_NULL_INCLUDE,
+                    "invalid null_policy %d", ag.null_policy);
       if (vt == GBX_TYPE_STRING || vt == GBX_TYPE_LIST || vt == GBX_TYPE_STRUCT || vt == GBX_TYPE_DECIMAL128)
         fail(GBX_ERR_UNSUPPORTED,
              "value type %d is aggregated by libcudf's sort-based groupby, which this library does not provide", vt);
@@ -492,7 +523,8 @@ void fill_channels(Plan& plan, const std::vector<const gbx_column_view*>& chan_c
           case GBX_AGG_SUM_OF_SQUARES: need |= N_SQ; break;
           case GBX_AGG_MEAN: need |= N_SUM | N_CNT; break;
           case GBX_AGG_VARIANCE:
-          case GBX_AGG_STD: need |= N_SUM | N_CNT | N_VAR; break;
+          case GBX_AGG_STD:
+          case GBX_AGG_M2: need |= N_SUM | N_CNT | N_VAR; break;
           default: break;  // COUNT_ALL uses the row count
         }
       }
@@ -585,7 +617,7 @@ const char* gbx_last_error(void) { return g_last_error.c_str(); }
 int32_t gbx_abi_version(void) { return GBX_ABI_VERSION; }
 int32_t gbx_target_type(int32_t type_id, int32_t kind)
 {
-  if (!is_hash_kind(kind)) return GBX_TYPE_EMPTY;
+  if (!is_hash_kind(kind) && !is_sort_kind(kind) && kind != GBX_AGG_M2) return GBX_TYPE_EMPTY;
   return target_type(type_id, kind);
 }
 
@@ -912,13 +944,28 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     const bool arg_kinds = plan_has_arg(plan);
     if (arg_kinds && strategy != GBX_STRATEGY_PRIVATIZED && strategy != GBX_STRATEGY_GLOBAL)
       strategy = est * 2.0 <= static_cast<double>(s_max) ? GBX_STRATEGY_PRIVATIZED : GBX_STRATEGY_GLOBAL;
+    // MEDIAN / QUANTILE / NUNIQUE / NTH_ELEMENT label each row by a probe of
+    // the finished global table, which the partitioned path does not build
+    bool has_sorted = false;
+    for (int q = 0; q < num_requests; ++q)
+      for (int k = 0; k < requests[q].num_aggregations; ++k)
+        has_sorted = has_sorted || is_sort_kind(requests[q].aggregations[k].kind);
+    if (has_sorted && strategy == GBX_STRATEGY_PARTITIONED) strategy = GBX_STRATEGY_GLOBAL;
 
     gb->stats.strategy = strategy;
 
     // Allocates the key and result columns with room for `rows` groups and
     // describes them for the kernels.
+    // (the sorted kinds' columns are listed in `sorted_outs`, with the index
+    // of their null counter, and written after the finalize kernel)
+    std::vector<SortedOut> sorted_outs;
+    std::vector<int> sorted_out_index;
+    std::vector<double> h_quantiles;
     auto build_outputs = [&](int64_t rows) -> OutPlan {
       OutPlan op{};
+      sorted_outs.clear();
+      sorted_out_index.clear();
+      h_quantiles.clear();
       for (int c = 0; c < nkeys; ++c) {
         const gbx_column_view& kcv = gb->keys[c];
         bool with_mask             = plan.key.cols[c].null_bit != 0;
@@ -943,21 +990,47 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         const gbx_request& r = requests[q];
         int32_t vt           = value_type(r.values);
         for (int k = 0; k < r.num_aggregations; ++k) {
-          int32_t kind   = r.aggregations[k].kind;
+          const gbx_aggregation& ag = r.aggregations[k];
+          int32_t kind   = ag.kind;
           int32_t tt     = target_type(vt, kind);
           bool has_nulls = chan_nulls[req_chan[q]] != 0;
-          // nullable iff the values have nulls; COUNT never; VAR/STD always (hash/groupby.cu:424-454)
-          bool with_mask = (kind == GBX_AGG_COUNT_VALID || kind == GBX_AGG_COUNT_ALL)
+          // nullable iff the values have nulls; COUNT never; VAR/STD always
+          // (hash/groupby.cu:424-454); QUANTILE / MEDIAN always
+          // (group_quantiles.cu); NTH_ELEMENT while some output is null (the
+          // mask is dropped below when none is, as group_nth_element.cu
+          // does); NUNIQUE never (group_nunique.cu)
+          bool with_mask = (kind == GBX_AGG_COUNT_VALID || kind == GBX_AGG_COUNT_ALL || kind == GBX_AGG_NUNIQUE)
                              ? false
-                             : (has_nulls || kind == GBX_AGG_VARIANCE || kind == GBX_AGG_STD);
+                             : (has_nulls || kind == GBX_AGG_VARIANCE || kind == GBX_AGG_STD ||
+                                kind == GBX_AGG_QUANTILE || kind == GBX_AGG_MEDIAN || kind == GBX_AGG_NTH_ELEMENT);
           int32_t scale  = is_decimal(tt) ? (r.values.type_id == GBX_TYPE_DICTIONARY32 ? r.values.dict_keys->scale
                                                                                        : r.values.scale)
                                           : 0;
-          gbx_column& oc = res->requests[q].results[k];
-          alloc_column(call.alloc, oc, tt, scale, rows, with_mask);
+          // QUANTILE: num_quantiles rows per group
+          const int64_t nq = kind == GBX_AGG_QUANTILE ? ag.num_quantiles : 1;
+          gbx_column& oc   = res->requests[q].results[k];
+          alloc_column(call.alloc, oc, tt, scale, rows * nq, with_mask);
           if (op.nout >= kMaxOut) fail(GBX_ERR_UNSUPPORTED, "more than %d results in one call", kMaxOut);
+          if (is_sort_kind(kind)) {
+            SortedOut so{};
+            so.kind          = kind;
+            so.chan          = req_chan[q];
+            so.null_policy   = ag.null_policy;
+            so.interpolation = kind == GBX_AGG_MEDIAN ? GBX_INTERP_LINEAR : ag.interpolation;
+            so.num_quantiles = static_cast<int32_t>(nq);
+            so.out_width     = type_width(tt);
+            so.nth           = ag.ddof;
+            so.data          = oc.data;
+            so.mask          = oc.null_mask;
+            // offset of this output's quantiles in h_quantiles until uploaded
+            so.quantiles_dev = reinterpret_cast<const double*>(static_cast<uintptr_t>(h_quantiles.size()));
+            if (kind == GBX_AGG_MEDIAN) h_quantiles.push_back(0.5);
+            else if (kind == GBX_AGG_QUANTILE) h_quantiles.insert(h_quantiles.end(), ag.quantiles, ag.quantiles + nq);
+            sorted_outs.push_back(so);
+            sorted_out_index.push_back(op.nout);
+          }
           OutCol& o   = op.out[op.nout++];
-          o.data      = oc.data;
+          o.data      = is_sort_kind(kind) ? nullptr : oc.data;
           o.mask      = oc.null_mask;
           o.kind      = kind;
           o.ddof      = r.aggregations[k].ddof;
@@ -1300,10 +1373,51 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     GBX_CUDA(cudaMemsetAsync(d_nulls, 0, (kMaxKeyCols + kMaxOut) * 8, s));
     op.null_counts = d_nulls;
     GBX_CUDA(launch_finalize(plan, t, map, G, op, call.dev.num_sms, s));
+    if (!sorted_outs.empty() && G > 0 && call.n > 0) {
+      // ---- MEDIAN / QUANTILE / NUNIQUE / NTH_ELEMENT (gbx_sort.cu)
+      GBX_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int32_t), s));
+      double* d_q = nullptr;
+      if (!h_quantiles.empty()) {
+        d_q = static_cast<double*>(scratch.get(h_quantiles.size() * sizeof(double)));
+        GBX_CUDA(cudaMemcpyAsync(d_q, h_quantiles.data(), h_quantiles.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
+      }
+      SortedKindsArgs sa{};
+      sa.plan       = plan;
+      sa.table      = t;
+      sa.map        = map;
+      sa.num_groups = G;
+      sa.n          = call.n;
+      sa.max_probes = static_cast<uint32_t>(std::min<uint64_t>(cap, 1u << 12));
+      sa.scratch    = &scratch;
+      sa.status     = d_status;
+      sa.num_sms    = call.dev.num_sms;
+      sa.stream     = s;
+      for (size_t i = 0; i < sorted_outs.size(); ++i) {
+        SortedOut so     = sorted_outs[i];
+        so.quantiles_dev = d_q ? d_q + reinterpret_cast<uintptr_t>(so.quantiles_dev) : nullptr;
+        so.null_count    = d_nulls + kMaxKeyCols + sorted_out_index[i];
+        sa.outs.push_back(so);
+      }
+      // one sort of a channel's values serves all of its MEDIAN / QUANTILE /
+      // NUNIQUE outputs: those first, channel by channel, NTH_ELEMENT last
+      std::stable_sort(sa.outs.begin(), sa.outs.end(), [](const SortedOut& x, const SortedOut& y) {
+        const bool nx = x.kind == GBX_AGG_NTH_ELEMENT, ny = y.kind == GBX_AGG_NTH_ELEMENT;
+        if (nx != ny) return ny;
+        return x.chan < y.chan;
+      });
+      int sort_launches = 0;
+      sorted_kinds(sa, &sort_launches);
+      gb->stats.kernel_launches += sort_launches;
+    }
     timer.mark(5);
     std::vector<unsigned long long> h_nulls(kMaxKeyCols + kMaxOut, 0);
+    int32_t sort_status = 0;
     GBX_CUDA(cudaMemcpyAsync(h_nulls.data(), d_nulls, h_nulls.size() * 8, cudaMemcpyDeviceToHost, s));
+    if (!sorted_outs.empty())
+      GBX_CUDA(cudaMemcpyAsync(&sort_status, d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     GBX_CUDA(cudaStreamSynchronize(s));
+    if (sort_status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
     for (int c = 0; c < nkeys; ++c)
       if (res->keys[c].null_mask) res->keys[c].view.null_count = static_cast<int64_t>(h_nulls[c]);
     {
@@ -1312,6 +1426,13 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
         for (int k = 0; k < requests[q].num_aggregations; ++k, ++o) {
           gbx_column& oc = res->requests[q].results[k];
           if (oc.null_mask) oc.view.null_count = static_cast<int64_t>(h_nulls[kMaxKeyCols + o]);
+          if (requests[q].aggregations[k].kind == GBX_AGG_NTH_ELEMENT && oc.null_mask && oc.view.null_count == 0) {
+            // group_nth_element.cu: no mask without nulls
+            call.alloc.release(oc.null_mask, oc.mask_bytes);
+            oc.null_mask      = nullptr;
+            oc.mask_bytes     = 0;
+            oc.view.null_mask = nullptr;
+          }
         }
     }
     timer.read(gb->stats);
@@ -1346,6 +1467,12 @@ extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
     GBX_EXPECTS(gb != nullptr && num_groups != nullptr, "null argument");
     *num_groups = 0;
     validate(gb, requests, num_requests);
+    for (int q = 0; q < num_requests; ++q)
+      for (int k = 0; k < requests[q].num_aggregations; ++k)
+        if (is_sort_kind(requests[q].aggregations[k].kind))
+          fail(GBX_ERR_UNSUPPORTED,
+               "MEDIAN / QUANTILE / NUNIQUE / NTH_ELEMENT sort every row's value and need scratch in proportion "
+               "to the rows; use gbx_groupby_aggregate");
     const int nkeys = static_cast<int>(gb->keys.size());
     int nout        = 0;
     for (int q = 0; q < num_requests; ++q) nout += requests[q].num_aggregations;

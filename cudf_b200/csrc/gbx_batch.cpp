@@ -344,13 +344,15 @@ void build_schema(gbx_batch& b, const gbx_batch_instance* ins, int32_t ninst)
     }
     GBX_EXPECTS(b.nreq == 0 || in.requests != nullptr, "batch instance %d has no requests", i);
     validate_requests(in.requests, b.nreq, n);
-    // ARGMIN / ARGMAX index rows of the caller's column; the batched kernels
-    // address rows within their instance and do not provide them
+    // ARGMIN / ARGMAX index rows of the caller's column (the batched kernels
+    // address rows within their instance); M2 and the kinds that sort a
+    // group's values are computed by gbx_groupby_aggregate only
     for (int q = 0; q < b.nreq; ++q)
       for (int k = 0; k < in.requests[q].num_aggregations; ++k) {
         const int32_t kind = in.requests[q].aggregations[k].kind;
-        if (kind == GBX_AGG_ARGMIN || kind == GBX_AGG_ARGMAX)
-          fail(GBX_ERR_UNSUPPORTED, "ARGMIN/ARGMAX are not provided by the batched form; use gbx_groupby_aggregate");
+        if (!is_batch_kind(kind))
+          fail(GBX_ERR_UNSUPPORTED, "aggregation kind %d is not provided by the batched form; use gbx_groupby_aggregate",
+               kind);
       }
     std::vector<int> rc;
     std::vector<const gbx_column_view*> chans = collect_channels(in.requests, b.nreq, rc);

@@ -79,6 +79,10 @@ bool is_unsigned(int32_t t);
 int8_t phys_of(int32_t t);
 int32_t target_type(int32_t t, int32_t kind);
 bool is_hash_kind(int32_t k);
+// MEDIAN / QUANTILE / NUNIQUE / NTH_ELEMENT (computed by gbx_sort.cu)
+bool is_sort_kind(int32_t k);
+// the kinds the batched form computes
+bool is_batch_kind(int32_t k);
 int32_t value_type(const gbx_column_view& c);
 bool same_view(const gbx_column_view& a, const gbx_column_view& b);
 

@@ -239,9 +239,10 @@ __global__ void k_finalize(const __grid_constant__ Plan plan, const __grid_const
         }
       }
     }
-    // results
+    // results (an output without data belongs to a sorted kind, written later)
     for (int o = 0; o < op.nout; ++o) {
       const OutCol& oc  = op.out[o];
+      if (oc.data == nullptr) continue;
       const Channel& ch = plan.chan[oc.chan];
       bool valid        = false;
       uint64_t vbits    = 0;
@@ -312,9 +313,12 @@ __global__ void k_finalize(const __grid_constant__ Plan plan, const __grid_const
             break;
           }
           case GBX_AGG_VARIANCE:
-          case GBX_AGG_STD: {
+          case GBX_AGG_STD:
+          case GBX_AGG_M2: {
             int64_t nn = cnt;
-            if (nn == 0 || nn - oc.ddof <= 0) {
+            // M2 (group_m2.cu): the centred sum of squares itself, null without values
+            const int64_t ddof = oc.kind == GBX_AGG_M2 ? 0 : oc.ddof;
+            if (nn == 0 || nn - ddof <= 0) {
               valid = false;
               break;
             }
@@ -329,7 +333,7 @@ __global__ void k_finalize(const __grid_constant__ Plan plan, const __grid_const
                                       ch.a_s1 >= 0 ? ld_acc(t, ch.a_s1, s, 8) : 0, nn, K);
               double M2 = s2 - S1 * (S1 / static_cast<double>(nn));
               if (M2 < 0.0) M2 = 0.0;
-              var = M2 / static_cast<double>(nn - oc.ddof);
+              var = oc.kind == GBX_AGG_M2 ? M2 : M2 / static_cast<double>(nn - ddof);
             }
             if (oc.kind == GBX_AGG_STD) var = sqrt(var);
             vbits = static_cast<uint64_t>(__double_as_longlong(var));

@@ -229,11 +229,13 @@ __device__ __forceinline__ void fold_channel(const Plan& plan, const OutPlan& op
       if (oc.kind == GBX_AGG_MEAN && oc.out_ptype == P_F64) {
         valid = A.cnt > 0;
         v     = valid ? static_cast<uint64_t>(__double_as_longlong(mean)) : 0;
-      } else if (oc.kind == GBX_AGG_VARIANCE || oc.kind == GBX_AGG_STD) {
-        const int64_t nn = A.cnt;
-        valid            = nn > 0 && nn - oc.ddof > 0;
+      } else if (oc.kind == GBX_AGG_VARIANCE || oc.kind == GBX_AGG_STD || oc.kind == GBX_AGG_M2) {
+        // M2 (group_m2.cu): the centred sum of squares itself, null without values
+        const int64_t nn   = A.cnt;
+        const int64_t ddof = oc.kind == GBX_AGG_M2 ? 0 : oc.ddof;
+        valid              = nn > 0 && nn - ddof > 0;
         if (valid) {
-          double var = A.k == kShiftUnset ? m2 : m2 / static_cast<double>(nn - oc.ddof);
+          double var = A.k == kShiftUnset || oc.kind == GBX_AGG_M2 ? m2 : m2 / static_cast<double>(nn - ddof);
           if (oc.kind == GBX_AGG_STD) var = sqrt(var);
           v = static_cast<uint64_t>(__double_as_longlong(var));
         }

@@ -276,6 +276,8 @@ cudaError_t scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, void*
                               temp_bytes, st);
 }
 
+int scan_launches(int64_t n) { return n <= 0 ? 0 : n <= kScanTile ? 1 : 3; }
+
 cudaError_t compact_occupied(const TableRef& t, int nwords, uint32_t* map, int64_t* num_selected, int num_sms,
                              cudaStream_t st)
 {

@@ -17,4 +17,7 @@ cudaError_t scan_exclusive_u32(const uint32_t* in, uint32_t* out, int64_t n, voi
 cudaError_t scan_exclusive_i64(const int64_t* in, int64_t* out, int64_t n, void* temp, size_t* temp_bytes,
                                cudaStream_t st);
 
+// Kernels one scan of n values launches.
+int scan_launches(int64_t n);
+
 }  // namespace gbx

@@ -42,6 +42,7 @@ struct Job {
   std::vector<gbx_column_view> key_dicts;
   std::vector<gbx_request> reqs;
   std::vector<std::vector<gbx_aggregation>> aggs;
+  std::vector<std::vector<double>> quantiles;  // copies of QUANTILE arrays (aggs point here)
   std::vector<gbx_column_view> val_dicts;
   int64_t rows   = 0;
   int64_t charge = 0;
@@ -69,17 +70,20 @@ int64_t memory_charge(const Job& j)
     null_bits += k.null_mask ? 1 : 0;
   }
   const int64_t nw = (key_bytes * 8 + null_bits > 64) ? 16 : 8;  // packed key words
-  int64_t val_copy = 0, acc = 4, out = key_bytes + 1;
+  int64_t val_copy = 0, acc = 4, out = key_bytes + 1, sorted = 0;
   for (size_t q = 0; q < j.reqs.size(); ++q) {
     const int32_t vt = value_type(j.reqs[q].values);
     val_copy += type_width(vt) + 1;
     for (auto& a : j.aggs[q]) {
       acc += 16;  // at most two 8-byte accumulators per aggregation
-      out += std::max(4, type_width(target_type(vt, a.kind))) + 1;
+      const int64_t per_group = a.kind == GBX_AGG_QUANTILE ? std::max(a.num_quantiles, 1) : 1;
+      out += per_group * (std::max(4, type_width(target_type(vt, a.kind))) + 1);
+      // the sorted kinds: row labels, two record buffers and the flags
+      if (is_sort_kind(a.kind)) sorted = 44;
     }
   }
   const int64_t n = std::max<int64_t>(j.rows, 1);
-  return n * (nw + val_copy) + 4 * n * (nw + acc + 4) + n * out + (int64_t(32) << 20);
+  return n * (nw + val_copy + sorted) + 4 * n * (nw + acc + 4) + n * out + (int64_t(32) << 20);
 }
 
 std::string schema_of(const Job& j)
@@ -419,12 +423,22 @@ int gbx_server_submit(gbx_server* s, const gbx_table_view* keys, const gbx_reque
     j->reqs.assign(requests, requests + num_requests);
     j->aggs.resize(num_requests);
     j->val_dicts.resize(num_requests);
-    for (int q = 0; q < num_requests; ++q) {
-      // ARGMIN / ARGMAX run on the plain path only (the batched form lacks them)
+    size_t nquant = 0;
+    for (int q = 0; q < num_requests; ++q)
       for (int k = 0; k < requests[q].num_aggregations; ++k)
-        if (requests[q].aggregations[k].kind == GBX_AGG_ARGMIN || requests[q].aggregations[k].kind == GBX_AGG_ARGMAX)
-          j->mergeable = false;
+        nquant += requests[q].aggregations[k].kind == GBX_AGG_QUANTILE ? 1 : 0;
+    j->quantiles.reserve(nquant);  // no reallocation: aggs keep pointers into it
+    for (int q = 0; q < num_requests; ++q) {
+      // ARGMIN / ARGMAX, M2 and the sorted kinds run on the plain path only
+      // (the batched form lacks them)
+      for (int k = 0; k < requests[q].num_aggregations; ++k)
+        if (!is_batch_kind(requests[q].aggregations[k].kind)) j->mergeable = false;
       j->aggs[q].assign(requests[q].aggregations, requests[q].aggregations + requests[q].num_aggregations);
+      for (gbx_aggregation& a : j->aggs[q])
+        if (a.kind == GBX_AGG_QUANTILE) {
+          j->quantiles.emplace_back(a.quantiles, a.quantiles + a.num_quantiles);
+          a.quantiles = j->quantiles.back().data();
+        }
       j->reqs[q].aggregations = j->aggs[q].data();
       if (j->reqs[q].values.dict_keys) {
         j->val_dicts[q]             = *j->reqs[q].values.dict_keys;

@@ -1,0 +1,532 @@
+// gbx_sort.cu -- the kinds libcudf computes on its sort-based groupby
+// (MEDIAN, QUANTILE, NUNIQUE, NTH_ELEMENT), over the groups of the hash table.
+//
+// The reference sorts the keys, labels each row with its group and sorts a
+// request's values within their groups (groupby/sort/sort_helper.cu:251-272,
+// groupby/sort/aggregate.cpp:323-406, group_quantiles.cu, group_nunique.cu,
+// group_nth_element.cu).  Here the groups are already known from the hash
+// table: every row's label is the output row of its key (a probe of the
+// finished table), and only the (label, value) records of a request are put
+// in order, by an LSD radix sort of libgbx's own: 8-bit digits, each pass a
+// stable counting sort over 4,096-record tiles (tile histograms, one
+// exclusive scan over (digit, tile), ranks by warp-aggregated counts in tile
+// order).
+//
+// A record is (hi, lo): hi = label << 1 | null flag for a row with a key (a
+// larger sentinel for a row whose key is excluded), lo = the value's order key
+// (MEDIAN / QUANTILE / NUNIQUE) or the row index (NTH_ELEMENT, whose records
+// are sorted by hi alone, so that a group's rows stay in row order).  After
+// the sort each group's records are contiguous: valid values first, in
+// ascending order, then the nulls.
+#include <algorithm>
+#include <cmath>
+#include <utility>
+#include <vector>
+
+#include "gbx_host.hpp"
+#include "gbx_kernels.hpp"
+#include "gbx_scan.hpp"
+#include "gbx_sort.hpp"
+#include "gbx_warpcore.cuh"
+
+namespace gbx {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kSortBlock    = 256;
+constexpr int kSortWarps    = kSortBlock / 32;
+constexpr int kSortPerWarp  = 512;
+constexpr int kSortTile     = kSortWarps * kSortPerWarp;
+constexpr uint32_t kNoLabel = 0xffffffffu;
+
+// ------------------------------------------------------------ order keys
+
+// An unsigned key that orders the values of physical type pt as the
+// reference's sort does: equal for equal values (-0.0 and +0.0 one key, every
+// NaN one key), NaN after every number (the relational comparator of
+// table/experimental/row_operators.cuh).  A float's key takes the low 32
+// bits; k_sort_records keeps the row's own bits above it.
+__device__ __forceinline__ uint64_t order_key(uint64_t b, int pt)
+{
+  switch (pt) {
+    case P_I8: return static_cast<uint8_t>(static_cast<uint8_t>(b) ^ 0x80u);
+    case P_I16: return static_cast<uint16_t>(static_cast<uint16_t>(b) ^ 0x8000u);
+    case P_I32: return static_cast<uint32_t>(static_cast<uint32_t>(b) ^ 0x80000000u);
+    case P_I64: return b ^ 0x8000000000000000ULL;
+    case P_F32: {
+      uint32_t u    = static_cast<uint32_t>(b);
+      const float f = __uint_as_float(u);
+      if (f != f) u = 0x7fc00000u;
+      else if (f == 0.0f) u = 0;
+      return (u & 0x80000000u) ? static_cast<uint32_t>(~u) : (u | 0x80000000u);
+    }
+    case P_F64: {
+      uint64_t u     = b;
+      const double d = __longlong_as_double(static_cast<long long>(u));
+      if (d != d) u = 0x7ff8000000000000ULL;
+      else if (d == 0.0) u = 0;
+      return (u & 0x8000000000000000ULL) ? ~u : (u | 0x8000000000000000ULL);
+    }
+    case P_BOOL: return b != 0;
+    default: return b;  // unsigned
+  }
+}
+
+// The value bits of a sorted record's lo word.  A double's zero comes back
+// as +0.0 (its key holds no sign); every other value is the row's own.
+__device__ __forceinline__ uint64_t order_decode(uint64_t k, int pt)
+{
+  switch (pt) {
+    case P_I8: return static_cast<uint8_t>(static_cast<uint8_t>(k) ^ 0x80u);
+    case P_I16: return static_cast<uint16_t>(static_cast<uint16_t>(k) ^ 0x8000u);
+    case P_I32: return static_cast<uint32_t>(static_cast<uint32_t>(k) ^ 0x80000000u);
+    case P_I64: return k ^ 0x8000000000000000ULL;
+    case P_F32: return k >> 32;
+    case P_F64: return (k & 0x8000000000000000ULL) ? (k & 0x7fffffffffffffffULL) : ~k;
+    default: return k;
+  }
+}
+
+// ------------------------------------------------------------- labels
+
+// inv[map[g]] = g: each occupied slot's output row.
+__global__ void k_slot_rows(const uint32_t* __restrict__ map, int64_t G, uint32_t* __restrict__ inv)
+{
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    inv[map[g]] = static_cast<uint32_t>(g);
+}
+
+// labels[r] = the output row of row r's group (kNoLabel for a row whose key
+// is excluded); every key is in the table, so the probe only finds.
+template <int NW>
+__global__ void k_row_labels(const __grid_constant__ Plan plan, const __grid_constant__ TableRef t, int64_t n,
+                             const uint32_t* __restrict__ inv, uint32_t max_probes, uint32_t* __restrict__ labels)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint64_t k[NW];
+    uint32_t label = kNoLabel;
+    if (pack_key<NW>(plan.key, r, k)) {
+      const int64_t s = global_slot<NW>(t, k, max_probes);
+      if (s >= 0) label = inv[s];
+    }
+    labels[r] = label;
+  }
+}
+
+// --------------------------------------------------------------- records
+
+// The records of one request: values (lo = order key) or rows (lo = row
+// index; null values dropped when skip_nulls).
+__global__ void k_sort_records(const __grid_constant__ Channel ch, int64_t n, const uint32_t* __restrict__ labels,
+                               bool rows_mode, bool skip_nulls, uint32_t skip_hi, uint64_t* __restrict__ lo,
+                               uint32_t* __restrict__ hi, int32_t* status)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t label = labels[r];
+    uint64_t b           = 0;
+    bool valid           = false;
+    if (label != kNoLabel && bit_valid(ch.mask, r + ch.offset)) {
+      bool ok;
+      b     = value_bits(ch, r, ok);
+      valid = ok;
+      if (!ok) atomicOr(status, S_BAD_INDEX);
+    }
+    uint32_t h;
+    if (label == kNoLabel || (skip_nulls && !valid)) h = skip_hi;
+    else h = (label << 1) | ((rows_mode || valid) ? 0u : 1u);
+    uint64_t l = 0;
+    if (rows_mode) l = static_cast<uint64_t>(r);
+    else if (valid) {
+      l = order_key(b, ch.ptype);
+      // a float's own bits ride above its 32-bit key (not sorted on), so the
+      // value read back is the row's: -0.0 and NaN payloads kept
+      if (ch.ptype == P_F32) l |= b << 32;
+    }
+    hi[r] = h;
+    lo[r] = l;
+  }
+}
+
+// ------------------------------------------------------------- radix sort
+
+__device__ __forceinline__ uint32_t digit_at(uint64_t lo, uint32_t hi, int shift)
+{
+  return shift < 64 ? static_cast<uint32_t>(lo >> shift) & 0xffu : (hi >> (shift - 64)) & 0xffu;
+}
+
+// counts[d * ntiles + tile] = records of the tile with digit d.
+__global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint64_t* __restrict__ lo,
+                                                          const uint32_t* __restrict__ hi, int64_t n, int shift,
+                                                          int ntiles, uint32_t* __restrict__ counts)
+{
+  __shared__ uint32_t h[256];
+  for (int i = threadIdx.x; i < 256; i += kSortBlock) h[i] = 0;
+  __syncthreads();
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kSortTile;
+  for (int i = threadIdx.x; i < kSortTile; i += kSortBlock) {
+    const int64_t r = base + i;
+    if (r < n) atomicAdd(&h[digit_at(shift < 64 ? lo[r] : 0, hi[r], shift)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += kSortBlock) counts[static_cast<size_t>(i) * ntiles + blockIdx.x] = h[i];
+}
+
+// Stable scatter of one tile: the record at tile position (warp, batch,
+// lane) -- row order -- goes to offsets[d * ntiles + tile] plus its rank
+// among the tile's records of digit d.
+__global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __restrict__ lo_in,
+                                                             const uint32_t* __restrict__ hi_in, int64_t n,
+                                                             int shift, int ntiles,
+                                                             const uint32_t* __restrict__ offsets,
+                                                             uint64_t* __restrict__ lo_out,
+                                                             uint32_t* __restrict__ hi_out)
+{
+  __shared__ uint32_t cnt[kSortWarps][256];
+  const int lane     = threadIdx.x & 31;
+  const int warp     = threadIdx.x >> 5;
+  const uint32_t lt  = (1u << lane) - 1u;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kSortTile + warp * kSortPerWarp;
+  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortBlock) (&cnt[0][0])[i] = 0;
+  __syncthreads();
+  // each warp's digit counts
+  for (int j = 0; j < kSortPerWarp / 32; ++j) {
+    const int64_t r   = base + j * 32 + lane;
+    const bool act    = r < n;
+    const uint32_t d  = act ? digit_at(shift < 64 ? lo_in[r] : 0, hi_in[r], shift) : 0xffffffffu;
+    const uint32_t pe = __match_any_sync(0xffffffffu, d);
+    if (act && lane == __ffs(pe) - 1) cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: the tile's offset, then each warp's first position
+  for (int d = threadIdx.x; d < 256; d += kSortBlock) {
+    uint32_t run = offsets[static_cast<size_t>(d) * ntiles + blockIdx.x];
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = cnt[w][d];
+      cnt[w][d]        = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  for (int j = 0; j < kSortPerWarp / 32; ++j) {
+    const int64_t r = base + j * 32 + lane;
+    const bool act  = r < n;
+    uint64_t l      = 0;
+    uint32_t h      = 0;
+    if (act) {
+      l = lo_in[r];
+      h = hi_in[r];
+    }
+    const uint32_t d  = act ? digit_at(l, h, shift) : 0xffffffffu;
+    const uint32_t pe = __match_any_sync(0xffffffffu, d);
+    const uint32_t at = act ? cnt[warp][d] + static_cast<uint32_t>(__popc(pe & lt)) : 0u;
+    __syncwarp();
+    if (act && lane == __ffs(pe) - 1) cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
+    if (act) {
+      lo_out[at] = l;
+      hi_out[at] = h;
+    }
+    __syncwarp();
+  }
+}
+
+// --------------------------------------------------------------- bounds
+
+__device__ __forceinline__ int64_t lower_bound_hi(const uint32_t* hi, int64_t n, uint32_t v)
+{
+  int64_t a = 0, b = n;
+  while (a < b) {
+    const int64_t mid = a + ((b - a) >> 1);
+    if (hi[mid] < v) a = mid + 1;
+    else b = mid;
+  }
+  return a;
+}
+
+// bounds[3 g .. 3 g + 2] = group g's first record, first null record, end.
+__global__ void k_group_bounds(const uint32_t* __restrict__ hi, int64_t n, int64_t G, int64_t* __restrict__ bounds)
+{
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t key = static_cast<uint32_t>(g) << 1;
+    bounds[3 * g]      = lower_bound_hi(hi, n, key);
+    bounds[3 * g + 1]  = lower_bound_hi(hi, n, key | 1u);
+    bounds[3 * g + 2]  = lower_bound_hi(hi, n, key + 2u);
+  }
+}
+
+// --------------------------------------------------------------- results
+
+// interpolate::midpoint of two values as double (quantiles_util.hpp:56-72):
+// the int64 overload keeps the halves apart so that the sum cannot overflow
+__device__ __forceinline__ double midpoint_of(uint64_t a, uint64_t b, int pt)
+{
+  if (pt == P_I64) {
+    const int64_t x = static_cast<int64_t>(a), y = static_cast<int64_t>(b);
+    const int64_t half = x / 2 + y / 2;
+    const int64_t rest = x % 2 + y % 2;
+    return __dadd_rn(static_cast<double>(half), static_cast<double>(rest) * 0.5);
+  }
+  return __dadd_rn(__dmul_rn(as_f64(a, pt), 0.5), __dmul_rn(as_f64(b, pt), 0.5));
+}
+
+// QUANTILE (MEDIAN: {0.5}, LINEAR) of each group's valid values, with the
+// reference's quantile_index and interpolations (quantiles_util.hpp:92-190),
+// result row g * nq + j for group g and quantile j.
+__global__ void k_quantiles(const uint64_t* __restrict__ lo, const int64_t* __restrict__ bounds, int64_t G, int pt,
+                            const double* __restrict__ qs, int nq, int interp, double* __restrict__ out,
+                            uint32_t* __restrict__ mask, unsigned long long* null_count)
+{
+  const int lane      = threadIdx.x & 31;
+  const int64_t total = G * nq;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < total;
+       base += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i   = base + lane;
+    const bool active = i < total;
+    bool valid        = false;
+    if (active) {
+      const int64_t g     = i / nq;
+      const int64_t start = bounds[3 * g];
+      const int64_t count = bounds[3 * g + 1] - start;
+      double v            = 0.0;
+      valid               = count > 0;
+      if (valid) {
+        // plain double operations, each rounded on its own (no fused
+        // multiply-add), in the reference's order
+        const double q    = fmin(fmax(qs[i % nq], 0.0), 1.0);
+        const double val  = __dmul_rn(q, static_cast<double>(count - 1));
+        const int64_t lwr = static_cast<int64_t>(floor(val));
+        const int64_t hgr = static_cast<int64_t>(ceil(val));
+        const int64_t nst = static_cast<int64_t>(nearbyint(val));
+        const double frac = val - static_cast<double>(lwr);
+        const uint64_t a  = order_decode(lo[start + lwr], pt);
+        const uint64_t b  = order_decode(lo[start + hgr], pt);
+        switch (interp) {
+          case GBX_INTERP_LOWER: v = as_f64(a, pt); break;
+          case GBX_INTERP_HIGHER: v = as_f64(b, pt); break;
+          case GBX_INTERP_NEAREST: v = as_f64(order_decode(lo[start + nst], pt), pt); break;
+          case GBX_INTERP_MIDPOINT: v = midpoint_of(a, b, pt); break;
+          default: v = __dadd_rn(__dmul_rn(1.0 - frac, as_f64(a, pt)), __dmul_rn(frac, as_f64(b, pt))); break;
+        }
+      }
+      out[i] = v;
+    }
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    const uint32_t bal = __ballot_sync(0xffffffffu, active && valid);
+    if (lane == 0 && act != 0) {
+      // base stays a multiple of 32 (the stride is), so word base / 32 is
+      // this warp's alone
+      mask[base >> 5] = bal;
+      const uint32_t nulls = __popc(act & ~bal);
+      if (nulls) atomicAdd(null_count, static_cast<unsigned long long>(nulls));
+    }
+  }
+}
+
+// first[i] = 1 when record i holds a (group, value) pair not seen at i - 1;
+// only the order key's bits (`key_mask`) are compared.
+__global__ void k_distinct_flags(const uint64_t* __restrict__ lo, const uint32_t* __restrict__ hi, int64_t n,
+                                 uint64_t key_mask, uint32_t* __restrict__ first)
+{
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    first[i] = (i == 0 || hi[i] != hi[i - 1] || ((lo[i] ^ lo[i - 1]) & key_mask) != 0) ? 1u : 0u;
+}
+
+// NUNIQUE: the group's distinct valid values, plus one for its nulls under
+// INCLUDE (group_nunique.cu:63-72), from the exclusive scan of the flags.
+__global__ void k_nunique(const uint32_t* __restrict__ scanned, const int64_t* __restrict__ bounds, int64_t G,
+                          bool include_nulls, int32_t* __restrict__ out)
+{
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t s = bounds[3 * g], vend = bounds[3 * g + 1], e = bounds[3 * g + 2];
+    int32_t c       = static_cast<int32_t>(scanned[vend] - scanned[s]);
+    if (include_nulls && e > vend) ++c;
+    out[g] = c;
+  }
+}
+
+// NTH_ELEMENT: the n-th record of each group in row order (negative n from
+// the end); null when out of range or when that row's value is null
+// (group_nth_element.cu).
+__global__ void k_nth_element(const __grid_constant__ Channel ch, const uint64_t* __restrict__ lo,
+                              const int64_t* __restrict__ bounds, int64_t G, int64_t nth, int width,
+                              void* __restrict__ out, uint32_t* __restrict__ mask, unsigned long long* null_count,
+                              int32_t* status)
+{
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~int64_t(31); base < G;
+       base += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t g   = base + lane;
+    const bool active = g < G;
+    bool valid        = false;
+    if (active) {
+      uint64_t v        = 0;
+      const int64_t s   = bounds[3 * g];
+      const int64_t len = bounds[3 * g + 2] - s;
+      const int64_t idx = nth >= 0 ? nth : len + nth;
+      if (idx >= 0 && idx < len) {
+        const int64_t row = static_cast<int64_t>(lo[s + idx]);
+        if (bit_valid(ch.mask, row + ch.offset)) {
+          bool ok;
+          v     = value_bits(ch, row, ok);
+          valid = ok;
+          if (!ok) atomicOr(status, S_BAD_INDEX);
+        }
+      }
+      store_bits(out, g, width, valid ? v : 0);
+    }
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    const uint32_t bal = __ballot_sync(0xffffffffu, active && valid);
+    if (lane == 0 && act != 0) {
+      mask[base >> 5] = bal;
+      const uint32_t nulls = __popc(act & ~bal);
+      if (nulls) atomicAdd(null_count, static_cast<unsigned long long>(nulls));
+    }
+  }
+}
+
+int grid_of(int64_t work, int num_sms)
+{
+  const int64_t b = (work + 255) / 256;
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, int64_t(num_sms) * 8)));
+}
+
+int bits_for(uint64_t v)
+{
+  int b = 0;
+  while (b < 64 && (v >> b) != 0) ++b;
+  return b;
+}
+
+}  // namespace
+
+void sorted_kinds(const SortedKindsArgs& a, int* launches)
+{
+  const int64_t n = a.n;
+  const int64_t G = a.num_groups;
+  cudaStream_t s  = a.stream;
+  if (a.outs.empty() || n == 0 || G == 0) return;
+  if (G >= (int64_t(1) << 30)) fail(GBX_ERR_UNSUPPORTED, "sorted kinds over 2^30 groups or more");
+  Scratch& sc = *a.scratch;
+
+  // labels: each row's output row
+  auto* inv    = static_cast<uint32_t*>(sc.get((a.table.cap + 1) * sizeof(uint32_t)));
+  auto* labels = static_cast<uint32_t*>(sc.get(static_cast<size_t>(n) * sizeof(uint32_t)));
+  k_slot_rows<<<grid_of(G, a.num_sms), 256, 0, s>>>(a.map, G, inv);
+  GBX_CUDA(cudaGetLastError());
+  if (a.plan.key.nwords == 1)
+    k_row_labels<1><<<grid_of(n, a.num_sms), 256, 0, s>>>(a.plan, a.table, n, inv, a.max_probes, labels);
+  else
+    k_row_labels<2><<<grid_of(n, a.num_sms), 256, 0, s>>>(a.plan, a.table, n, inv, a.max_probes, labels);
+  GBX_CUDA(cudaGetLastError());
+  *launches += 2;
+
+  // records and their ping-pong copies, tile counts, scan scratch
+  const int ntiles    = static_cast<int>((n + kSortTile - 1) / kSortTile);
+  const size_t nrec   = static_cast<size_t>(n);
+  auto* lo0           = static_cast<uint64_t*>(sc.get(nrec * 8));
+  auto* lo1           = static_cast<uint64_t*>(sc.get(nrec * 8));
+  auto* hi0           = static_cast<uint32_t*>(sc.get(nrec * 4));
+  auto* hi1           = static_cast<uint32_t*>(sc.get(nrec * 4));
+  const int64_t items = static_cast<int64_t>(ntiles) * 256;
+  auto* counts        = static_cast<uint32_t*>(sc.get(static_cast<size_t>(items) * 4));
+  auto* offsets       = static_cast<uint32_t*>(sc.get(static_cast<size_t>(items) * 4));
+  size_t tb_items = 0, tb_flags = 0;
+  GBX_CUDA(scan_exclusive_u32(nullptr, nullptr, items, nullptr, &tb_items, s));
+  GBX_CUDA(scan_exclusive_u32(nullptr, nullptr, n + 1, nullptr, &tb_flags, s));
+  void* temp   = sc.get(std::max(tb_items, tb_flags));
+  auto* bounds = static_cast<int64_t*>(sc.get(static_cast<size_t>(G) * 3 * sizeof(int64_t)));
+  uint32_t* flags = nullptr;
+
+  // labels < 2^lbits; hi holds label << 1 | null, a skipped row 1 << (lbits + 1)
+  const int lbits       = std::max(1, bits_for(static_cast<uint64_t>(G)));
+  const uint32_t skiphi = 1u << (lbits + 1);
+  const int hi_bits     = lbits + 2;
+
+  // sorts (lo0, hi0) on the low lo_bits of lo, then on hi; returns the
+  // buffers holding the result and fills `bounds`
+  auto sort = [&](int lo_bits) {
+    uint64_t *li = lo0, *lout = lo1;
+    uint32_t *hin = hi0, *hout = hi1;
+    std::vector<int> shifts;
+    for (int b = 0; b < lo_bits; b += 8) shifts.push_back(b);
+    for (int b = 0; b < hi_bits; b += 8) shifts.push_back(64 + b);
+    for (int sh : shifts) {
+      k_sort_hist<<<ntiles, kSortBlock, 0, s>>>(li, hin, n, sh, ntiles, counts);
+      GBX_CUDA(cudaGetLastError());
+      size_t tb = std::max(tb_items, tb_flags);
+      GBX_CUDA(scan_exclusive_u32(counts, offsets, items, temp, &tb, s));
+      k_sort_scatter<<<ntiles, kSortBlock, 0, s>>>(li, hin, n, sh, ntiles, offsets, lout, hout);
+      GBX_CUDA(cudaGetLastError());
+      *launches += 2 + scan_launches(items);
+      std::swap(li, lout);
+      std::swap(hin, hout);
+    }
+    k_group_bounds<<<grid_of(G, a.num_sms), 256, 0, s>>>(hin, n, G, bounds);
+    GBX_CUDA(cudaGetLastError());
+    *launches += 1;
+    return std::make_pair(li, hin);
+  };
+
+  // one sort of a channel's values serves all of its MEDIAN / QUANTILE /
+  // NUNIQUE outputs (the caller lists them together)
+  int sorted_chan = -1;
+  int key_bits    = 64;
+  std::pair<uint64_t*, uint32_t*> sorted{nullptr, nullptr};
+  for (const SortedOut& o : a.outs) {
+    const Channel& ch = a.plan.chan[o.chan];
+    if (o.kind == GBX_AGG_NTH_ELEMENT) {
+      const bool skip = o.null_policy == GBX_NULL_EXCLUDE;
+      k_sort_records<<<grid_of(n, a.num_sms), 256, 0, s>>>(ch, n, labels, true, skip, skiphi, lo0, hi0, a.status);
+      GBX_CUDA(cudaGetLastError());
+      sorted_chan     = -1;  // the record buffers now hold rows
+      const auto recs = sort(0);
+      k_nth_element<<<grid_of(G, a.num_sms), 256, 0, s>>>(ch, recs.first, bounds, G, o.nth, o.out_width, o.data,
+                                                          o.mask, o.null_count, a.status);
+      GBX_CUDA(cudaGetLastError());
+      *launches += 2;
+      continue;
+    }
+    if (sorted_chan != o.chan) {
+      k_sort_records<<<grid_of(n, a.num_sms), 256, 0, s>>>(ch, n, labels, false, false, skiphi, lo0, hi0,
+                                                           a.status);
+      GBX_CUDA(cudaGetLastError());
+      *launches += 1;
+      key_bits    = 8 * pt_width(ch.ptype);
+      sorted      = sort(key_bits);
+      sorted_chan = o.chan;
+    }
+    if (o.kind == GBX_AGG_NUNIQUE) {
+      if (flags == nullptr) {
+        flags = static_cast<uint32_t*>(sc.get((nrec + 1) * 4));
+        GBX_CUDA(cudaMemsetAsync(flags + n, 0, 4, s));  // read by the scan, never counted
+      }
+      const uint64_t key_mask = key_bits >= 64 ? ~0ULL : ((1ULL << key_bits) - 1);
+      k_distinct_flags<<<grid_of(n, a.num_sms), 256, 0, s>>>(sorted.first, sorted.second, n, key_mask, flags);
+      GBX_CUDA(cudaGetLastError());
+      size_t tb = std::max(tb_items, tb_flags);
+      GBX_CUDA(scan_exclusive_u32(flags, flags, n + 1, temp, &tb, s));
+      k_nunique<<<grid_of(G, a.num_sms), 256, 0, s>>>(flags, bounds, G, o.null_policy == GBX_NULL_INCLUDE,
+                                                      static_cast<int32_t*>(o.data));
+      GBX_CUDA(cudaGetLastError());
+      *launches += 2 + scan_launches(n + 1);
+    } else {
+      const int nq = o.num_quantiles;
+      if (nq == 0) continue;
+      k_quantiles<<<grid_of(G * nq, a.num_sms), 256, 0, s>>>(sorted.first, bounds, G, ch.ptype, o.quantiles_dev,
+                                                             nq, o.interpolation, static_cast<double*>(o.data),
+                                                             o.mask, o.null_count);
+      GBX_CUDA(cudaGetLastError());
+      *launches += 1;
+    }
+  }
+}
+
+}  // namespace gbx

@@ -499,9 +499,12 @@ __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCo
       break;
     }
     case GBX_AGG_VARIANCE:
-    case GBX_AGG_STD: {
+    case GBX_AGG_STD:
+    case GBX_AGG_M2: {
       int64_t nn = cnt;
-      if (nn == 0 || nn - oc.ddof <= 0) {
+      // M2 (group_m2.cu): the centred sum of squares itself, null without values
+      const int64_t ddof = oc.kind == GBX_AGG_M2 ? 0 : oc.ddof;
+      if (nn == 0 || nn - ddof <= 0) {
         valid = false;
         break;
       }
@@ -515,7 +518,7 @@ __device__ __forceinline__ uint64_t finalize_from(const Channel& ch, const OutCo
         double S1 = shifted_sum(is_float, pt, V.sum(), V.s1(), nn, K);
         double M2 = s2 - S1 * (S1 / static_cast<double>(nn));
         if (M2 < 0.0) M2 = 0.0;
-        var = M2 / static_cast<double>(nn - oc.ddof);
+        var = oc.kind == GBX_AGG_M2 ? M2 : M2 / static_cast<double>(nn - ddof);
       }
       if (oc.kind == GBX_AGG_STD) var = sqrt(var);
       vbits = static_cast<uint64_t>(__double_as_longlong(var));

@@ -115,11 +115,8 @@ class GroupBy:
         for i, r in enumerate(requests):
             reqs[i].values = r.values.view()
             keep.append(r.values)
-            aggs = (_abi.gbx_aggregation * max(1, len(r.aggregations)))()
-            for j, a in enumerate(r.aggregations):
-                aggs[j].kind = int(a.kind)
-                aggs[j].ddof = int(a.ddof)
-            keep.append(aggs)
+            aggs, kept = _abi.aggregation_array(r.aggregations)
+            keep.append(kept)
             reqs[i].num_aggregations = len(r.aggregations)
             reqs[i].aggregations = C.cast(aggs, C.POINTER(_abi.gbx_aggregation))
         st = stream if stream is not None else torch.cuda.current_stream()

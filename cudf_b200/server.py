@@ -61,11 +61,8 @@ def request_array(requests: Sequence[GroupByRequest]):
     for q, r in enumerate(requests):
         reqs[q].values = r.values.view()
         keep.append(r.values)
-        aggs = (_abi.gbx_aggregation * max(1, len(r.aggregations)))()
-        for j, a in enumerate(r.aggregations):
-            aggs[j].kind = int(a.kind)
-            aggs[j].ddof = int(a.ddof)
-        keep.append(aggs)
+        aggs, kept = _abi.aggregation_array(r.aggregations)
+        keep.append(kept)
         reqs[q].num_aggregations = len(r.aggregations)
         reqs[q].aggregations = C.cast(aggs, C.POINTER(_abi.gbx_aggregation))
     return reqs, keep

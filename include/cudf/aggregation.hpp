@@ -1,5 +1,5 @@
 // cudf/aggregation.hpp -- aggregation kinds and factories with the reference's
-// names and enum values (cpp/include/cudf/aggregation.hpp:86-124, 199, 261-383).
+// names and enum values (cpp/include/cudf/aggregation.hpp:86-124, 199, 261-411).
 #pragma once
 
 #include <memory>
@@ -21,7 +21,10 @@ class aggregation {
   explicit aggregation(Kind a) : kind{a} {}
   virtual ~aggregation() = default;
   Kind kind;
-  size_type ddof{1};  // VARIANCE / STD
+  size_type ddof{1};                                    // VARIANCE / STD; n of NTH_ELEMENT
+  null_policy null_handling{null_policy::EXCLUDE};      // NUNIQUE / NTH_ELEMENT
+  interpolation interp{interpolation::LINEAR};          // QUANTILE
+  std::vector<double> quantiles;                        // QUANTILE
 };
 
 class groupby_aggregation : public virtual aggregation {
@@ -67,11 +70,33 @@ std::unique_ptr<Base> make_argmax_aggregation() { return detail::make_agg<Base>(
 template <typename Base = groupby_aggregation>
 std::unique_ptr<Base> make_argmin_aggregation() { return detail::make_agg<Base>(aggregation::ARGMIN); }
 template <typename Base = groupby_aggregation>
-std::unique_ptr<Base> make_median_aggregation() { return detail::make_agg<Base>(aggregation::MEDIAN); }
+std::unique_ptr<Base> make_m2_aggregation() { return detail::make_agg<Base>(aggregation::M2); }
 template <typename Base = groupby_aggregation>
-std::unique_ptr<Base> make_nth_element_aggregation(size_type n)
+std::unique_ptr<Base> make_median_aggregation() { return detail::make_agg<Base>(aggregation::MEDIAN); }
+// aggregation.hpp:364: num_groups * q.size() result rows, group by group
+template <typename Base = groupby_aggregation>
+std::unique_ptr<Base> make_quantile_aggregation(std::vector<double> const& q, interpolation i = interpolation::LINEAR)
 {
-  return detail::make_agg<Base>(aggregation::NTH_ELEMENT, n);
+  auto p       = detail::make_agg<Base>(aggregation::QUANTILE);
+  p->quantiles = q;
+  p->interp    = i;
+  return p;
+}
+// aggregation.hpp:397
+template <typename Base = groupby_aggregation>
+std::unique_ptr<Base> make_nunique_aggregation(null_policy null_handling = null_policy::EXCLUDE)
+{
+  auto p           = detail::make_agg<Base>(aggregation::NUNIQUE);
+  p->null_handling = null_handling;
+  return p;
+}
+// aggregation.hpp:410-411
+template <typename Base = groupby_aggregation>
+std::unique_ptr<Base> make_nth_element_aggregation(size_type n, null_policy null_handling = null_policy::INCLUDE)
+{
+  auto p           = detail::make_agg<Base>(aggregation::NTH_ELEMENT, n);
+  p->null_handling = null_handling;
+  return p;
 }
 
 }  // namespace cudf

@@ -81,7 +81,16 @@ class groupby {
     std::vector<std::vector<gbx_aggregation>> aggs(requests.size());
     for (std::size_t i = 0; i < requests.size(); ++i) {
       reqs[i].values = requests[i].values.to_gbx(&dict[i]);
-      for (auto const& a : requests[i].aggregations) aggs[i].push_back(gbx_aggregation{static_cast<int32_t>(a->kind), a->ddof});
+      for (auto const& a : requests[i].aggregations) {
+        gbx_aggregation g{};
+        g.kind          = static_cast<int32_t>(a->kind);
+        g.ddof          = a->ddof;
+        g.null_policy   = a->null_handling == null_policy::INCLUDE ? GBX_NULL_INCLUDE : GBX_NULL_EXCLUDE;
+        g.interpolation = static_cast<int32_t>(a->interp);
+        g.num_quantiles = static_cast<int32_t>(a->quantiles.size());
+        g.quantiles     = a->quantiles.data();
+        aggs[i].push_back(g);
+      }
       reqs[i].num_aggregations = static_cast<int32_t>(aggs[i].size());
       reqs[i].aggregations     = aggs[i].data();
     }

@@ -12,6 +12,7 @@ using size_type    = int32_t;   // types.hpp:95
 using bitmask_type = uint32_t;  // types.hpp:96
 
 enum class null_policy : bool { EXCLUDE, INCLUDE };  // types.hpp:126
+enum class interpolation : int32_t { LINEAR, LOWER, HIGHER, MIDPOINT, NEAREST };  // types.hpp:192-198
 enum class sorted : bool { NO, YES };                // types.hpp:167
 enum class order : bool { ASCENDING, DESCENDING };
 enum class null_order : bool { AFTER, BEFORE };

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define GBX_ABI_VERSION 3
+#define GBX_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define GBX_API __attribute__((visibility("default")))
@@ -42,7 +42,7 @@ typedef enum gbx_status {
   GBX_ERR_LOGIC       = 1, /* invalid argument: cudf::logic_error */
   GBX_ERR_CUDA        = 2, /* CUDA runtime failure: cudf::cuda_error */
   GBX_ERR_ALLOC       = 3, /* device allocation failed: rmm::bad_alloc */
-  GBX_ERR_UNSUPPORTED = 4, /* valid in libcudf, but only on its sort-based path (not provided) */
+  GBX_ERR_UNSUPPORTED = 4, /* valid in libcudf, but not provided here (a type or kind of its sort-based path) */
   GBX_ERR_DEVICE      = 5  /* a bounded device-side loop gave up (status word set by a kernel) */
 } gbx_status;
 
@@ -138,13 +138,34 @@ typedef struct gbx_table_view {
   const gbx_column_view* columns;
 } gbx_table_view;
 
+/* cudf::interpolation (types.hpp:192-198), for QUANTILE. */
+typedef enum gbx_interpolation {
+  GBX_INTERP_LINEAR   = 0,
+  GBX_INTERP_LOWER    = 1,
+  GBX_INTERP_HIGHER   = 2,
+  GBX_INTERP_MIDPOINT = 3,
+  GBX_INTERP_NEAREST  = 4
+} gbx_interpolation;
+
 /* One aggregation of a request (cudf::groupby_aggregation).  `ddof` is used by
- * VARIANCE/STD (make_variance_aggregation(ddof), aggregation.hpp:311-337).
- * COUNT's null_policy is encoded in the kind: COUNT_VALID (EXCLUDE) or
- * COUNT_ALL (INCLUDE), as make_count_aggregation does (aggregation.cpp:494-499). */
+ * VARIANCE/STD (make_variance_aggregation(ddof), aggregation.hpp:311-337) and
+ * holds n for NTH_ELEMENT (make_nth_element_aggregation(n, null_handling),
+ * aggregation.hpp:410-411).  COUNT's null_policy is encoded in the kind:
+ * COUNT_VALID (EXCLUDE) or COUNT_ALL (INCLUDE), as make_count_aggregation does
+ * (aggregation.cpp:494-499); NUNIQUE and NTH_ELEMENT carry theirs in
+ * `null_policy` (GBX_NULL_EXCLUDE / GBX_NULL_INCLUDE).  QUANTILE takes
+ * `num_quantiles` values from the host array `quantiles` (clamped to [0, 1])
+ * and an `interpolation` (make_quantile_aggregation, aggregation.hpp:364); its
+ * result column holds num_groups * num_quantiles rows, group by group.
+ * Fields a kind does not use are ignored (zero-initialise them). */
 typedef struct gbx_aggregation {
   int32_t kind;
   int32_t ddof;
+  int32_t null_policy;
+  int32_t interpolation;
+  int32_t num_quantiles;
+  int32_t reserved0;
+  const double* quantiles;
 } gbx_aggregation;
 
 /* cudf::groupby::aggregation_request (groupby.hpp:61-64). */
@@ -222,12 +243,17 @@ GBX_API int gbx_groupby_aggregate(gbx_groupby* gb,
 
 /* Whether every request is computable by the hash path
  * (can_use_hash_groupby, hash/groupby.cu:635-651).  Returns 1/0, or -1 with
- * gbx_last_error() set on malformed input. */
+ * gbx_last_error() set on malformed input.  A 0 does not mean that
+ * gbx_groupby_aggregate refuses the requests: M2, MEDIAN, QUANTILE, NUNIQUE
+ * and NTH_ELEMENT, which libcudf computes on its sort path, are computed
+ * here from the hash table's groups (the group order of the output is the
+ * hash path's either way). */
 GBX_API int gbx_can_use_hash_groupby(const gbx_request* requests, int32_t num_requests);
 
 /* Output type of aggregation `kind` over a column of `type_id`
- * (cudf::detail::target_type, detail/aggregation/aggregation.hpp:1212-1335);
- * returns GBX_TYPE_EMPTY when the combination is invalid. */
+ * (cudf::detail::target_type, detail/aggregation/aggregation.hpp:1212-1367)
+ * for the kinds gbx_groupby_aggregate computes; returns GBX_TYPE_EMPTY when
+ * the combination is invalid or the kind is not computed here. */
 GBX_API int32_t gbx_target_type(int32_t type_id, int32_t kind);
 
 GBX_API void gbx_result_release(gbx_result* result);
@@ -311,6 +337,8 @@ GBX_API int gbx_groupby_set_timing(gbx_groupby* gb, int32_t enable);
  * Limits: at most GBX_NOALLOC_MAX_GROUPS groups (more is rejected with
  * GBX_ERR_LOGIC after the aggregation pass, outputs untouched), and the
  * aggregations' per-group state must fit the array (else GBX_ERR_LOGIC).
+ * MEDIAN, QUANTILE, NUNIQUE and NTH_ELEMENT, which sort every row, are
+ * refused with GBX_ERR_UNSUPPORTED.
  *
  * Outputs: `out_keys` has one gbx_column per key column and `out_results` one
  * per aggregation of every request, in request order.  The caller sets each

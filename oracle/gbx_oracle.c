@@ -36,6 +36,18 @@
  * valid value of the group is NaN, in which case the result is NaN.
  * ARGMIN/ARGMAX ties resolve to the lowest row index, NaN handled the same way.
  *
+ * The kinds libcudf computes on its sort path are restated from there:
+ * M2 = sum((x - mean)^2) with MEAN's mask (groupby/sort/group_m2.cu);
+ * MEDIAN / QUANTILE select from each group's valid values sorted with NaN
+ * last, -0.0 == +0.0 and ties in row order (groupby/sort/sort_helper.cu:
+ * 251-272, group_quantiles.cu, quantiles/quantiles_util.hpp:39-190), in
+ * double arithmetic in the reference's order; NUNIQUE counts distinct valid
+ * values, NaNs equal, and the nulls as one value under INCLUDE
+ * (groupby/sort/group_nunique.cu:63-72); NTH_ELEMENT takes the n-th row of a
+ * group in row order, null values dropped first under EXCLUDE, null when out
+ * of range, without a mask when no output is null
+ * (groupby/sort/group_nth_element.cu).
+ *
  * Groups come out in first-occurrence order; callers sort by key to compare.
  */
 #define _GNU_SOURCE
@@ -138,8 +150,9 @@ static int is_duration(int32_t t)
 static int is_decimal(int32_t t) { return t == GBX_TYPE_DECIMAL32 || t == GBX_TYPE_DECIMAL64; }
 static int is_fixed_width(int32_t t) { return type_width(t) > 0 && t != GBX_TYPE_DICTIONARY32; }
 
-/* cudf::detail::target_type restated (detail/aggregation/aggregation.hpp:1212-1335),
- * restricted to what the hash path can compute (hash/groupby.cu:73-84, 635-651). */
+/* cudf::detail::target_type restated (detail/aggregation/aggregation.hpp:1212-1367)
+ * for the hash path's kinds (hash/groupby.cu:73-84, 635-651) and the sort
+ * path's M2, MEDIAN, QUANTILE, NUNIQUE and NTH_ELEMENT. */
 int32_t gbo_target_type(int32_t t, int32_t kind)
 {
   if (!is_fixed_width(t)) return GBX_TYPE_EMPTY;
@@ -167,6 +180,16 @@ int32_t gbo_target_type(int32_t t, int32_t kind)
     case GBX_AGG_STD:
       if (is_integral(t) || is_floating(t)) return GBX_TYPE_FLOAT64;
       return GBX_TYPE_EMPTY;
+    /* sort-path kinds (aggregation.hpp:1318-1367): M2 / MEDIAN / QUANTILE
+     * are double over arithmetic values, NUNIQUE a size_type count,
+     * NTH_ELEMENT the value's own type */
+    case GBX_AGG_M2:
+    case GBX_AGG_MEDIAN:
+    case GBX_AGG_QUANTILE:
+      if (is_integral(t) || is_floating(t)) return GBX_TYPE_FLOAT64;
+      return GBX_TYPE_EMPTY;
+    case GBX_AGG_NUNIQUE: return GBX_TYPE_INT32;
+    case GBX_AGG_NTH_ELEMENT: return t;
     default: return GBX_TYPE_EMPTY;
   }
 }
@@ -480,6 +503,7 @@ typedef struct {
   /* outputs */
   int64_t num_groups;
   int64_t* rep_row;   /* representative row per group */
+  int64_t* row_gid;   /* each row's group in this worker (-1: another worker's, or skipped) */
   accum** acc;        /* per request: num_groups accumulators */
   int status;
 } worker;
@@ -552,7 +576,7 @@ static void* run_worker(void* arg)
     int need_var = 0;
     for (int k = 0; k < w->requests[q].num_aggregations; ++k) {
       int32_t kind = w->requests[q].aggregations[k].kind;
-      if (kind == GBX_AGG_VARIANCE || kind == GBX_AGG_STD) need_var = 1;
+      if (kind == GBX_AGG_VARIANCE || kind == GBX_AGG_STD || kind == GBX_AGG_M2) need_var = 1;
     }
     if (need_var) {
       for (int64_t r = 0; r < n; ++r) {
@@ -569,7 +593,7 @@ static void* run_worker(void* arg)
     }
     w->acc[q] = a;
   }
-  free(row_gid);
+  w->row_gid    = row_gid;
   w->num_groups = ng;
   w->rep_row    = rep;
   w->status     = GBX_OK;
@@ -597,6 +621,10 @@ static int validate(const gbx_table_view* keys, const gbx_request* reqs, int32_t
     for (int k = 0; k < r->num_aggregations; ++k) {
       if (gbo_target_type(vt, r->aggregations[k].kind) == GBX_TYPE_EMPTY)
         return set_err(GBX_ERR_LOGIC, "Invalid type/aggregation combination.");
+      if (r->aggregations[k].kind == GBX_AGG_QUANTILE &&
+          (r->aggregations[k].num_quantiles < 0 ||
+           (r->aggregations[k].num_quantiles > 0 && r->aggregations[k].quantiles == NULL)))
+        return set_err(GBX_ERR_LOGIC, "invalid quantile array");
     }
   }
   return GBX_OK;
@@ -692,9 +720,182 @@ static void finalize_column(gbo_column* out,
         valid = 1;
         break;
       }
+      case GBX_AGG_M2:
+        /* sum((x - mean)^2) over the valid values, mean = SUM / COUNT_VALID,
+         * with MEAN's mask: nullable iff the values have nulls, null where
+         * the group has no valid value (group_m2.cu:37-52, 97-101) */
+        if (valid) ((double*)out->data)[g] = (double)a->m2;
+        break;
     }
     if (out->valid) out->valid[g] = (uint8_t)valid;
   }
+}
+
+/* ------------------------------------------------ sort-path kinds --- */
+
+static int is_sorted_kind(int32_t k)
+{
+  return k == GBX_AGG_MEDIAN || k == GBX_AGG_QUANTILE || k == GBX_AGG_NUNIQUE || k == GBX_AGG_NTH_ELEMENT;
+}
+
+typedef struct {
+  scalar v;
+  int64_t row;
+} sorted_value;
+
+/* The reference's value order: NaN after every number and NaNs equal;
+ * -0.0 == +0.0 (the `<` comparisons). */
+static int value_cmp(const scalar* a, const scalar* b)
+{
+  if (type_cat(a->type_id) == CAT_FLOAT) {
+    int na = isnan((double)a->f), nb = isnan((double)b->f);
+    if (na || nb) return na - nb;
+  }
+  if (scalar_less(a, b)) return -1;
+  if (scalar_less(b, a)) return 1;
+  return 0;
+}
+
+/* a stable sort by value: ties in row order */
+static int sorted_value_cmp(const void* x, const void* y)
+{
+  const sorted_value* a = (const sorted_value*)x;
+  const sorted_value* b = (const sorted_value*)y;
+  int c                 = value_cmp(&a->v, &b->v);
+  if (c) return c;
+  return (a->row > b->row) - (a->row < b->row);
+}
+
+/* convert_to_floating<double> (quantiles_util.hpp) */
+static double value_as_double(const scalar* a)
+{
+  switch (type_cat(a->type_id)) {
+    case CAT_SIGNED:
+    case CAT_BOOL: return (double)a->i;
+    case CAT_UNSIGNED: return (double)a->u;
+    default: return (double)a->f;
+  }
+}
+
+/* quantile_index and select_quantile_data (quantiles_util.hpp:92-190) over
+ * `count` sorted values, in double arithmetic in the reference's order. */
+static double select_quantile(const sorted_value* v, int64_t count, double q, int32_t interp)
+{
+  q               = q < 0.0 ? 0.0 : (q > 1.0 ? 1.0 : q);
+  double val      = q * (double)(count - 1);
+  int64_t lo      = (int64_t)floor(val);
+  int64_t hi      = (int64_t)ceil(val);
+  int64_t near    = (int64_t)nearbyint(val);
+  double frac     = val - (double)lo;
+  const scalar* a = &v[lo].v;
+  const scalar* b = &v[hi].v;
+  switch (interp) {
+    case GBX_INTERP_LOWER: return value_as_double(a);
+    case GBX_INTERP_HIGHER: return value_as_double(b);
+    case GBX_INTERP_NEAREST: return value_as_double(&v[near].v);
+    case GBX_INTERP_MIDPOINT:
+      if (a->type_id == GBX_TYPE_INT64) {
+        /* midpoint<double>(int64_t, int64_t), quantiles_util.hpp:65-72 */
+        int64_t half = a->i / 2 + b->i / 2;
+        int64_t rest = a->i % 2 + b->i % 2;
+        return (double)half + (double)rest * 0.5;
+      }
+      return value_as_double(a) / 2 + value_as_double(b) / 2;
+    default: {
+      double one_minus_frac = 1.0 - frac;
+      double x              = one_minus_frac * value_as_double(a);
+      double y              = frac * value_as_double(b);
+      return x + y;
+    }
+  }
+}
+
+/* MEDIAN / QUANTILE (group_quantiles.cu), NUNIQUE (group_nunique.cu) and
+ * NTH_ELEMENT (group_nth_element.cu) of one request over the groups' rows,
+ * rows[off[g] .. off[g+1]) in row order. */
+static void finalize_sorted(gbo_column* out, const gbx_request* req, const gbx_aggregation* agg, int64_t ng,
+                            const int64_t* off, const int64_t* rows)
+{
+  const gbx_column_view* col = &req->values;
+  int32_t vt                 = value_type(col);
+  int32_t tt                 = gbo_target_type(vt, agg->kind);
+  int64_t nq                 = agg->kind == GBX_AGG_QUANTILE ? agg->num_quantiles : 1;
+  out->type_id               = tt;
+  out->scale = is_decimal(tt) ? ((col->type_id == GBX_TYPE_DICTIONARY32) ? col->dict_keys->scale : col->scale) : 0;
+  out->size  = ng * nq;
+  out->data  = xcalloc((size_t)(ng * nq), (size_t)type_width(tt));
+  int64_t maxlen = 1;
+  for (int64_t g = 0; g < ng; ++g)
+    if (off[g + 1] - off[g] > maxlen) maxlen = off[g + 1] - off[g];
+  sorted_value* sv = (sorted_value*)xcalloc((size_t)maxlen, sizeof(sorted_value));
+
+  if (agg->kind == GBX_AGG_NTH_ELEMENT) {
+    uint8_t* valid = (uint8_t*)xcalloc((size_t)(ng ? ng : 1), 1);
+    int any_null   = 0;
+    int64_t nth    = agg->ddof;
+    for (int64_t g = 0; g < ng; ++g) {
+      /* the group's rows, null values dropped under EXCLUDE */
+      int64_t len = 0;
+      for (int64_t i = off[g]; i < off[g + 1]; ++i)
+        if (agg->null_policy == GBX_NULL_INCLUDE || col_valid(col, rows[i])) sv[len++].row = rows[i];
+      int64_t idx = nth < 0 ? len + nth : nth;
+      if (idx >= 0 && idx < len && col_valid(col, sv[idx].row)) {
+        scalar v  = read_value(col, sv[idx].row);
+        v.type_id = tt;
+        store_scalar(out->data, tt, g, &v);
+        valid[g] = 1;
+      } else any_null = 1;
+    }
+    if (any_null) out->valid = valid;
+    else free(valid);
+    free(sv);
+    return;
+  }
+
+  if (agg->kind == GBX_AGG_NUNIQUE) {
+    for (int64_t g = 0; g < ng; ++g) {
+      int64_t len = 0;
+      int nulls   = 0;
+      for (int64_t i = off[g]; i < off[g + 1]; ++i) {
+        if (!col_valid(col, rows[i])) {
+          nulls = 1;
+          continue;
+        }
+        sv[len].v   = read_value(col, rows[i]);
+        sv[len].row = rows[i];
+        ++len;
+      }
+      qsort(sv, (size_t)len, sizeof(sorted_value), sorted_value_cmp);
+      int32_t c = 0;
+      for (int64_t i = 0; i < len; ++i)
+        if (i == 0 || value_cmp(&sv[i].v, &sv[i - 1].v) != 0) ++c;
+      if (nulls && agg->null_policy == GBX_NULL_INCLUDE) ++c;
+      ((int32_t*)out->data)[g] = c;
+    }
+    free(sv);
+    return;
+  }
+
+  /* MEDIAN = QUANTILE {0.5}, LINEAR (aggregate.cpp:344-362); always nullable */
+  out->valid = (uint8_t*)xcalloc((size_t)(ng * nq > 0 ? ng * nq : 1), 1);
+  for (int64_t g = 0; g < ng; ++g) {
+    int64_t len = 0;
+    for (int64_t i = off[g]; i < off[g + 1]; ++i) {
+      if (!col_valid(col, rows[i])) continue;
+      sv[len].v   = read_value(col, rows[i]);
+      sv[len].row = rows[i];
+      ++len;
+    }
+    qsort(sv, (size_t)len, sizeof(sorted_value), sorted_value_cmp);
+    for (int64_t j = 0; j < nq; ++j) {
+      if (len == 0) continue;
+      double q       = agg->kind == GBX_AGG_MEDIAN ? 0.5 : agg->quantiles[j];
+      int32_t interp = agg->kind == GBX_AGG_MEDIAN ? GBX_INTERP_LINEAR : agg->interpolation;
+      ((double*)out->data)[g * nq + j] = select_quantile(sv, len, q, interp);
+      out->valid[g * nq + j]            = 1;
+    }
+  }
+  free(sv);
 }
 
 int gbo_groupby(const gbx_table_view* keys,
@@ -781,6 +982,33 @@ int gbo_groupby(const gbx_table_view* keys,
         for (int64_t g = 0; g < ng; ++g) oc->valid[g] = (uint8_t)col_valid(kc, rep[g]);
       }
     }
+    /* each group's rows in row order, for the sort-path kinds */
+    int64_t* goff  = NULL;
+    int64_t* grows = NULL;
+    int any_sorted = 0;
+    for (int q = 0; q < num_requests; ++q)
+      for (int k = 0; k < requests[q].num_aggregations; ++k)
+        any_sorted |= is_sorted_kind(requests[q].aggregations[k].kind);
+    if (any_sorted) {
+      int64_t* base = (int64_t*)xcalloc((size_t)threads, sizeof(int64_t));
+      for (int t = 1; t < threads; ++t) base[t] = base[t - 1] + ws[t - 1].num_groups;
+      int64_t* gid = (int64_t*)xcalloc((size_t)(n ? n : 1), sizeof(int64_t));
+      goff         = (int64_t*)xcalloc((size_t)(ng + 1), sizeof(int64_t));
+      for (int64_t row = 0; row < n; ++row) {
+        gid[row] = -1;
+        for (int t = 0; t < threads; ++t)
+          if (ws[t].row_gid[row] >= 0) gid[row] = base[t] + ws[t].row_gid[row];
+        if (gid[row] >= 0) goff[gid[row] + 1]++;
+      }
+      for (int64_t g = 0; g < ng; ++g) goff[g + 1] += goff[g];
+      grows        = (int64_t*)xcalloc((size_t)(goff[ng] ? goff[ng] : 1), sizeof(int64_t));
+      int64_t* pos = (int64_t*)xcalloc((size_t)(ng ? ng : 1), sizeof(int64_t));
+      for (int64_t row = 0; row < n; ++row)
+        if (gid[row] >= 0) grows[goff[gid[row]] + pos[gid[row]]++] = row;
+      free(pos);
+      free(gid);
+      free(base);
+    }
     r->num_results = (int32_t*)xcalloc((size_t)(num_requests ? num_requests : 1), sizeof(int32_t));
     r->results = (gbo_column**)xcalloc((size_t)(num_requests ? num_requests : 1), sizeof(gbo_column*));
     for (int q = 0; q < num_requests; ++q) {
@@ -788,9 +1016,14 @@ int gbo_groupby(const gbx_table_view* keys,
       r->num_results[q]     = rq->num_aggregations;
       r->results[q] = (gbo_column*)xcalloc((size_t)(rq->num_aggregations ? rq->num_aggregations : 1),
                                            sizeof(gbo_column));
-      for (int k = 0; k < rq->num_aggregations; ++k)
-        finalize_column(&r->results[q][k], rq, &rq->aggregations[k], ng, pg[q], rep);
+      for (int k = 0; k < rq->num_aggregations; ++k) {
+        if (is_sorted_kind(rq->aggregations[k].kind))
+          finalize_sorted(&r->results[q][k], rq, &rq->aggregations[k], ng, goff, grows);
+        else finalize_column(&r->results[q][k], rq, &rq->aggregations[k], ng, pg[q], rep);
+      }
     }
+    free(goff);
+    free(grows);
     for (int q = 0; q < num_requests; ++q) free(pg[q]);
     free(pg);
     free(rep);
@@ -801,6 +1034,7 @@ int gbo_groupby(const gbx_table_view* keys,
   }
   for (int t = 0; t < threads; ++t) {
     free(ws[t].rep_row);
+    free(ws[t].row_gid);
     if (ws[t].acc) {
       for (int q = 0; q < num_requests; ++q) free(ws[t].acc[q]);
       free(ws[t].acc);

@@ -17,7 +17,7 @@ from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from cudf_b200._abi import TypeId, gbx_aggregation, gbx_column_view, gbx_request, gbx_table_view
+from cudf_b200._abi import TypeId, aggregation_array, gbx_aggregation, gbx_column_view, gbx_request, gbx_table_view
 from cudf_b200.column import pack_mask, storage_dtype, type_of
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -147,7 +147,9 @@ def _np_of(col: gbo_column, n: int) -> Tuple[int, np.ndarray, Optional[np.ndarra
 
 def groupby(keys: Sequence[HostCol], requests: Sequence[Tuple[HostCol, Sequence[Tuple[int, int]]]],
             null_policy: int = 0, threads: int = 1) -> dict:
-    """Runs the oracle.  `requests` is [(values, [(kind, ddof), ...]), ...].
+    """Runs the oracle.  `requests` is [(values, [(kind, ddof[, extra]), ...]), ...]
+    (extra: a dict of null_policy / interpolation / quantiles, as
+    cudf_b200._abi.fill_aggregation reads it).
 
     Returns {"num_groups", "keys": [(type_id, values, valid)], "results": [[(type_id, values, valid)]]}.
     Raises RuntimeError carrying the gbx_status on invalid input."""
@@ -161,11 +163,8 @@ def groupby(keys: Sequence[HostCol], requests: Sequence[Tuple[HostCol, Sequence[
     keep = []
     for i, (vals, aggs) in enumerate(requests):
         reqs[i].values = vals.view()
-        arr = (gbx_aggregation * max(1, len(aggs)))()
-        for j, (kind, ddof) in enumerate(aggs):
-            arr[j].kind = int(kind)
-            arr[j].ddof = int(ddof)
-        keep.append(arr)
+        arr, kept = aggregation_array(aggs)
+        keep.append(kept)
         reqs[i].num_aggregations = len(aggs)
         reqs[i].aggregations = C.cast(arr, C.POINTER(gbx_aggregation))
     out = C.POINTER(gbo_result)()
@@ -181,7 +180,8 @@ def groupby(keys: Sequence[HostCol], requests: Sequence[Tuple[HostCol, Sequence[
         for c in range(r.num_key_columns):
             res["keys"].append(_np_of(r.keys[c], n))
         for q in range(r.num_requests):
-            res["results"].append([_np_of(r.results[q][k], n) for k in range(r.num_results[q])])
+            # a QUANTILE column holds num_quantiles rows per group
+            res["results"].append([_np_of(r.results[q][k], r.results[q][k].size) for k in range(r.num_results[q])])
         return res
     finally:
         lib().gbo_result_free(out)

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), f"{n} missing from libgbx.so"
         assert n in _abi.SIGNATURES, f"{n} has no ctypes signature"
-    assert lib.gbx_abi_version() == 3
+    assert lib.gbx_abi_version() == 4
 
 
 STRUCTS = ["gbx_column_view", "gbx_table_view", "gbx_aggregation", "gbx_request", "gbx_allocator",
@@ -65,11 +65,12 @@ def test_ctypes_layout_matches_c_header(tmp_path):
 
 def test_target_types_match_oracle():
     lib = _lib.lib()
-    hash_kinds = {Kind.SUM, Kind.PRODUCT, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.COUNT_ALL,
-                  Kind.SUM_OF_SQUARES, Kind.MEAN, Kind.VARIANCE, Kind.STD, Kind.ARGMIN, Kind.ARGMAX}
+    computed = {Kind.SUM, Kind.PRODUCT, Kind.MIN, Kind.MAX, Kind.COUNT_VALID, Kind.COUNT_ALL,
+                Kind.SUM_OF_SQUARES, Kind.MEAN, Kind.VARIANCE, Kind.STD, Kind.ARGMIN, Kind.ARGMAX,
+                Kind.M2, Kind.MEDIAN, Kind.QUANTILE, Kind.NUNIQUE, Kind.NTH_ELEMENT}
     for t in TypeId:
         for k in Kind:
-            want = orc.target_type(t, k) if k in hash_kinds else 0
+            want = orc.target_type(t, k) if k in computed else 0
             assert lib.gbx_target_type(int(t), int(k)) == want, (t.name, k.name)
 
 
@@ -111,19 +112,55 @@ def test_size_mismatch_is_logic_error():
     lib.gbx_groupby_destroy(h)
 
 
-@pytest.mark.parametrize("kind,status", [(Kind.NTH_ELEMENT, _abi.Status.ERR_UNSUPPORTED),
-                                         (Kind.MEDIAN, _abi.Status.ERR_UNSUPPORTED),
-                                         (Kind.QUANTILE, _abi.Status.ERR_UNSUPPORTED)])
-def test_sort_only_kinds_are_reported(kind, status):
+@pytest.mark.parametrize("kind", [Kind.ANY, Kind.ALL, 19, 30])
+def test_kinds_not_computed_are_reported(kind):
+    """ANY / ALL and libcudf's later kinds (ROW_NUMBER onwards) are not
+    computed here: UNSUPPORTED, before any device work."""
     lib = _lib.lib()
     tv, keep = _keys_view(3)
     h = C.c_void_p()
     assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == 0
     r, keep2 = _request(3, kind)
     out = C.POINTER(_abi.gbx_result)()
-    assert lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out)) == status
+    assert lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out)) == _abi.Status.ERR_UNSUPPORTED
     assert lib.gbx_can_use_hash_groupby(C.byref(r), 1) == 0
     lib.gbx_groupby_destroy(h)
+
+
+@pytest.mark.parametrize("kind", [Kind.M2, Kind.MEDIAN, Kind.QUANTILE, Kind.NUNIQUE, Kind.NTH_ELEMENT])
+def test_sort_path_kinds_are_not_hash_kinds(kind):
+    """can_use_hash_groupby (hash/groupby.cu:635-651) is false for the sort
+    path's kinds, which gbx_groupby_aggregate computes all the same."""
+    lib = _lib.lib()
+    r, keep = _request(3, kind)
+    assert lib.gbx_can_use_hash_groupby(C.byref(r), 1) == 0
+    assert lib.gbx_target_type(int(TypeId.INT32), int(kind)) != 0
+
+
+def _aggregate_status(agg_fields):
+    lib = _lib.lib()
+    tv, keep = _keys_view(3)
+    h = C.c_void_p()
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == 0
+    r, aggs = _request(3, agg_fields.pop("kind"))
+    for f, v in agg_fields.items():
+        setattr(aggs[0], f, v)
+    out = C.POINTER(_abi.gbx_result)()
+    st = lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out))
+    msg = lib.gbx_last_error()
+    lib.gbx_groupby_destroy(h)
+    return st, msg
+
+
+def test_quantile_arguments_are_checked():
+    """A QUANTILE without its array, or with an interpolation outside
+    cudf::interpolation, is a logic error before any device work."""
+    st, msg = _aggregate_status({"kind": Kind.QUANTILE, "num_quantiles": 2})
+    assert st == _abi.Status.ERR_LOGIC and b"quantile array" in msg
+    st, msg = _aggregate_status({"kind": Kind.QUANTILE, "interpolation": 7})
+    assert st == _abi.Status.ERR_LOGIC and b"interpolation" in msg
+    st, msg = _aggregate_status({"kind": Kind.NUNIQUE, "null_policy": 3})
+    assert st == _abi.Status.ERR_LOGIC and b"null_policy" in msg
 
 
 def test_invalid_type_agg_combination_is_logic_error():
@@ -222,4 +259,4 @@ def test_batch_rejects_argmin_argmax():
     for kind in (Kind.ARGMIN, Kind.ARGMAX):
         a, ka = _batch_instance(4, kind=kind)
         st, msg = _create_batch([a])
-        assert st == _abi.Status.ERR_UNSUPPORTED and b"ARGMIN/ARGMAX" in msg
+        assert st == _abi.Status.ERR_UNSUPPORTED and b"batched form" in msg

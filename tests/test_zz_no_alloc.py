@@ -67,15 +67,12 @@ class NoAllocCall:
         self.result_types = []
         for i, (col, aggs) in enumerate(requests):
             self.reqs[i].values = col.view()
-            arr = (_abi.gbx_aggregation * len(aggs))()
-            for j, (kind, ddof) in enumerate(aggs):
-                arr[j].kind = int(kind)
-                arr[j].ddof = int(ddof)
-            self._keep.append(arr)
+            arr, kept = _abi.aggregation_array(aggs)
+            self._keep.append(kept)
             self.reqs[i].num_aggregations = len(aggs)
             self.reqs[i].aggregations = C.cast(arr, C.POINTER(_abi.gbx_aggregation))
             vt = col.dict_keys.type_id if col.type_id == TypeId.DICTIONARY32 else col.type_id
-            self.result_types += [self.lib.gbx_target_type(int(vt), int(k)) for k, _ in aggs]
+            self.result_types += [self.lib.gbx_target_type(int(vt), int(a[0])) for a in aggs]
         self.aggs_per_req = [len(a) for _, a in requests]
 
     def outputs(self, capacity):
