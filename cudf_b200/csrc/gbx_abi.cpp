@@ -1418,6 +1418,8 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
       GBX_CUDA(cudaMemcpyAsync(&sort_status, d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     GBX_CUDA(cudaStreamSynchronize(s));
     if (sort_status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
+    if (sort_status & (S_TABLE_FULL | S_SPIN_LIMIT))
+      fail(GBX_ERR_DEVICE, "sorted kinds: a row's key was not found in the finished table (status 0x%x)", sort_status);
     for (int c = 0; c < nkeys; ++c)
       if (res->keys[c].null_mask) res->keys[c].view.null_count = static_cast<int64_t>(h_nulls[c]);
     {

@@ -18,6 +18,9 @@ Tolerances (stated here, used by every float comparison):
     rounding of their conversion to double, 4 * 2^-52 * max|x| * range.
     STD's bound is VAR's divided by 2 std (or its square root near 0);
   * MIN/MAX: bit-exact (values are selected, not computed), NaN == NaN.
+  * M2: VAR's bound times the group's valid count (M2 = n VAR_pop);
+  * MEDIAN/QUANTILE: equal to the oracle (the same double operations in the
+    same order), NaN == NaN, +0.0 == -0.0; NUNIQUE / NTH_ELEMENT bit-exact.
 """
 from __future__ import annotations
 
@@ -36,14 +39,28 @@ KAT_RTOL = 1e-12  # known answers are exact rationals
 
 
 def device_column(h: HostCol):
-    """HostCol -> cudf_b200.Column on cuda:0 (same bytes)."""
+    """HostCol -> cudf_b200.Column on cuda:0 (same bytes, same offset and size)."""
     from cudf_b200 import Column
 
     if h.dict_keys is not None:
         idx = Column.from_numpy(h.values, h.valid)
         keys = device_column(h.dict_keys)
-        return Column.dictionary(idx, keys)
-    return Column.from_numpy(h.values, h.valid, type_id=h.type_id, scale=h.scale)
+        col = Column.dictionary(idx, keys)
+    else:
+        col = Column.from_numpy(h.values, h.valid, type_id=h.type_id, scale=h.scale)
+    if h.offset != 0 or h.size != len(h.values):
+        col = col.slice(h.offset, h.offset + h.size)
+    return col
+
+
+def _aggregation(a):
+    """(kind, ddof[, extra]) -> cudf_b200.aggregation.Aggregation; extra holds
+    null_policy / interpolation / quantiles."""
+    from cudf_b200.aggregation import Aggregation
+
+    extra = a[2] if len(a) > 2 else {}
+    return Aggregation(Kind(a[0]), int(a[1]), null_policy=NullPolicy(extra.get("null_policy", 0)),
+                       interpolation=extra.get("interpolation", 0), quantiles=tuple(extra.get("quantiles", ())))
 
 
 def run_gpu(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, strategy=None):
@@ -55,7 +72,7 @@ def run_gpu(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, s
     gb = GroupBy(Table(kcols), null_handling=null_policy)
     if strategy is not None:
         gb.set_strategy(strategy)
-    reqs = [GroupByRequest(device_column(v), [Aggregation(Kind(k), d) for k, d in aggs]) for v, aggs in requests]
+    reqs = [GroupByRequest(device_column(v), [_aggregation(a) for a in aggs]) for v, aggs in requests]
     ktab, results = gb.aggregate(reqs)
     out = {"num_groups": ktab.num_rows() if ktab.num_columns() else 0, "keys": [], "results": [], "stats": gb.last_stats()}
     for c in ktab.columns():
@@ -90,6 +107,15 @@ def sort_order(keys) -> np.ndarray:
     return np.lexsort(seq)
 
 
+def rows_of_groups(order: np.ndarray, per_group: int) -> np.ndarray:
+    """Result rows in the group order `order` when each group has
+    `per_group` consecutive result rows (QUANTILE)."""
+    order = np.asarray(order, dtype=np.int64)
+    if per_group == 1:
+        return order
+    return (order[:, None] * per_group + np.arange(per_group)[None, :]).reshape(-1)
+
+
 def _valid_or_all(valid, n):
     return np.ones(n, dtype=bool) if valid is None else np.asarray(valid, dtype=bool)
 
@@ -112,7 +138,9 @@ def compare_keys(got_keys, want_keys, go, wo):
             assert np.array_equal(a, b), "keys differ"
 
 
-def compare_values(kind, got, want, go, wo, scale=None, var_scale=None, ctx=""):
+def compare_values(kind, got, want, go, wo, scale=None, var_scale=None, ctx="", exact=False):
+    """Compares result columns row by row in the orders go / wo.  `exact`
+    asks for equal floating values (NaN where NaN; +0.0 == -0.0)."""
     gt, gv, gm = got
     wt, wv, wm = want
     assert gt == wt, f"{ctx}: result type {TypeId(gt).name} != {TypeId(wt).name}"
@@ -132,10 +160,14 @@ def compare_values(kind, got, want, go, wo, scale=None, var_scale=None, ctx=""):
     nan_ok = np.isnan(a64) == np.isnan(b64)
     assert nan_ok.all(), f"{ctx}: NaN placement differs"
     fin = ~np.isnan(b64)
+    if exact:
+        bad = np.nonzero(a64[fin] != b64[fin])[0]
+        assert len(bad) == 0, f"{ctx}: {len(bad)} results differ, first {a64[fin][bad[:3]]} vs {b64[fin][bad[:3]]}"
+        return
     if kind in (Kind.MIN, Kind.MAX):
         assert np.array_equal(a64[fin], b64[fin]), f"{ctx}: min/max differ"
         return
-    if kind in (Kind.VARIANCE, Kind.STD) and var_scale is not None:
+    if kind in (Kind.VARIANCE, Kind.STD, Kind.M2) and var_scale is not None:
         vtol = np.asarray(var_scale)[wo][wmask][fin] + 1e-300
         tol = vtol
         if kind == Kind.STD:
@@ -230,11 +262,13 @@ def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCL
         vt = vals.dict_keys.type_id if vals.dict_keys is not None else vals.type_id
         is_float = vt in (TypeId.FLOAT32, TypeId.FLOAT64)
         sc = None
-        for k, (kind, ddof) in enumerate(aggs):
-            kind = Kind(kind)
+        for k, agg in enumerate(aggs):
+            kind = Kind(agg[0])
+            extra = agg[2] if len(agg) > 2 else {}
             ctx = f"request {q} agg {kind.name}"
             s = v = None
-            if kind in (Kind.VARIANCE, Kind.STD) or (is_float and kind in (Kind.SUM, Kind.MEAN, Kind.SUM_OF_SQUARES)):
+            if kind in (Kind.VARIANCE, Kind.STD, Kind.M2) or (
+                    is_float and kind in (Kind.SUM, Kind.MEAN, Kind.SUM_OF_SQUARES)):
                 if sc is None:
                     sc = group_scales(keys, vals, null_policy, threads)
                 if kind == Kind.SUM:
@@ -243,7 +277,15 @@ def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCL
                     s = sc["abs"] / np.maximum(sc["cnt"], 1)
                 elif kind == Kind.SUM_OF_SQUARES:
                     s = sc["sq"]
+                elif kind == Kind.M2:
+                    # M2 = (n - ddof) VAR: the VAR bound times the group's count
+                    v = sc["var"] * np.maximum(sc["cnt"], 1)
                 else:
                     v = sc["var"]
-            compare_values(kind, got["results"][q][k], want["results"][q][k], go, wo, s, v, ctx)
+            # QUANTILE: num_quantiles result rows per group
+            nq = len(extra.get("quantiles", ())) if kind == Kind.QUANTILE else 1
+            # MEDIAN / QUANTILE: the same double operations in the same order
+            # as the oracle, so equal results
+            compare_values(kind, got["results"][q][k], want["results"][q][k], rows_of_groups(go, nq),
+                           rows_of_groups(wo, nq), s, v, ctx, exact=kind in (Kind.MEDIAN, Kind.QUANTILE))
     return got, want

@@ -41,13 +41,17 @@ def sum_type(v):
 
 def _case(cid, ktype, keys, vtype, vals, kind, expect_keys, expect, *, kvalid=None, vvalid=None, evalid=None,
           ekvalid=None, ddof=0, null_policy=NullPolicy.EXCLUDE, rtype=None, vdict=False, kdict=False,
-          float_expect=False):
+          float_expect=False, extra=None, offset=0, size=None):
+    """`null_policy` is the groupby's; `extra` holds an aggregation's own
+    null_policy / interpolation / quantiles; `offset` and `size` slice both
+    columns (a column view of rows offset .. offset + size)."""
     return dict(
         id=cid, key_type=ktype, keys=keys, key_valid=kvalid, key_dict=kdict,
         value_type=vtype, values=vals, value_valid=vvalid, value_dict=vdict,
         kind=kind, ddof=ddof, null_policy=null_policy,
         expect_keys=expect_keys, expect_key_valid=ekvalid,
         expect=expect, expect_valid=evalid, result_type=rtype, float_expect=float_expect,
+        extra=extra or {}, offset=offset, size=size,
     )
 
 
@@ -245,6 +249,163 @@ def cases():
     # sorted dictionary keys, values summed per dictionary entry.
     out.append(_case("keys_tests.cpp:338-365 dictionary_keys basic", T.INT32, [0, 1, 2, 0, 1, 1, 0, 2, 2, 1], T.INT32,
                      V10, Kind.SUM, [0, 1, 2], [9, 19, 17], rtype=T.INT64, kdict=True))
+    out += sort_path_cases()
+    return out
+
+
+# The kinds libcudf computes on its sort path.  Groups come out in hash order
+# here, so, like the cases above, they are compared sorted by key.
+ALL_TYPES = INTS + UINTS + FLOATS + [T.BOOL8] + DURATIONS + TIMESTAMPS + [T.DECIMAL32, T.DECIMAL64]
+K14 = [1, 2, 3, 3, 1, 2, 2, 1, 3, 3, 2, 4, 4, 2]
+K14_VALID = [1, 1, 1, 1, 1, 1, 1, 1, 0, 1, 1, 1, 1, 1]
+V14 = [0, 1, 2, 2, 3, 4, 5, 6, 7, 8, 9, 4, 4, 2]
+V14_VALID_NUNIQUE = [0, 1, 1, 1, 1, 1, 0, 1, 1, 1, 1, 0, 0, 0]   # nunique_tests.cpp:154-155
+V14_VALID_NTH = [0, 1, 1, 1, 1, 1, 0, 1, 1, 1, 1, 1, 0, 0]       # nth_element_tests.cpp:215-216
+
+
+def _q(quantiles, interp=0):
+    return {"quantiles": list(quantiles), "interpolation": interp}
+
+
+def sort_path_cases():
+    out = []
+    K = T.INT32
+    F = T.FLOAT64
+    # ---- median_tests.cpp and quantile_tests.cpp (int8..int64, float, double)
+    for v in INTS + FLOATS:
+        for tag, kind, ex, lines in (("median", Kind.MEDIAN, None, (35, 55, 71, 87, 103, 124)),
+                                     ("quantile", Kind.QUANTILE, _q([0.5]), (36, 56, 72, 88, 104, 194))):
+            b, e, zk, zv, nk, d = lines
+            out += [
+                _case(f"{tag}_tests.cpp:{b} basic[{v.name}]", K, K10, v, V10, kind, [1, 2, 3], [3.0, 4.5, 7.0],
+                      rtype=F, extra=ex),
+                _case(f"{tag}_tests.cpp:{e} empty_cols[{v.name}]", K, [], v, [], kind, [], [], rtype=F, extra=ex),
+                _case(f"{tag}_tests.cpp:{zk} zero_valid_keys[{v.name}]", K, [1, 2, 3], v, [3, 4, 5], kind, [], [],
+                      kvalid=[0, 0, 0], rtype=F, extra=ex),
+                _case(f"{tag}_tests.cpp:{zv} zero_valid_values[{v.name}]", K, [1, 1, 1], v, [3, 4, 5], kind, [1],
+                      [0.0], vvalid=[0, 0, 0], evalid=[0], rtype=F, extra=ex),
+                _case(f"{tag}_tests.cpp:{nk} null_keys_and_values[{v.name}]", K, K11, v, V11, kind, [1, 2, 3, 4],
+                      [4.5, 4.0, 5.0, 0.0], kvalid=K11_VALID, vvalid=V11_VALID_A, evalid=[1, 1, 1, 0], rtype=F,
+                      extra=ex),
+                _case(f"{tag}_tests.cpp:{d} dictionary[{v.name}]", K, K10, v, V10, kind, [1, 2, 3], [3.0, 4.5, 7.0],
+                      rtype=F, vdict=True, extra=ex),
+            ]
+        out.append(_case(f"quantile_tests.cpp:125 multiple_quantile[{v.name}]", K, K10, v, V10, Kind.QUANTILE,
+                         [1, 2, 3], [1.5, 4.5, 3.25, 6.0, 4.5, 7.5], rtype=F, extra=_q([0.25, 0.75])))
+        k9, v9 = [1, 2, 3, 1, 2, 2, 1, 3, 2], [0, 1, 2, 3, 4, 5, 6, 7, 9]
+        for interp, name, want in ((0, "LINEAR", [2.4, 4.2, 4.0]), (4, "NEAREST", [3, 4, 2]), (1, "LOWER", [0, 4, 2]),
+                                   (2, "HIGHER", [3, 5, 7]), (3, "MIDPOINT", [1.5, 4.5, 4.5])):
+            out.append(_case(f"quantile_tests.cpp:155 interpolation_types {name}[{v.name}]", K, k9, v, v9,
+                             Kind.QUANTILE, [1, 2, 3], [float(x) for x in want], rtype=F, extra=_q([0.4], interp)))
+
+    # ---- nunique_tests.cpp (AllTypes); bool values collapse to two
+    for v in ALL_TYPES:
+        is_b = v == T.BOOL8
+        R = T.INT32
+        out += [
+            _case(f"nunique_tests.cpp:31 basic[{v.name}]", K, K10, v, V10, Kind.NUNIQUE, [1, 2, 3],
+                  [2, 1, 1] if is_b else [3, 4, 3], rtype=R),
+            _case(f"nunique_tests.cpp:54 empty_cols[{v.name}]", K, [], v, [], Kind.NUNIQUE, [], [], rtype=R),
+            _case(f"nunique_tests.cpp:70 basic_duplicates[{v.name}]", K, K10, v, [0, 1, 2, 3, 4, 5, 3, 2, 2, 9],
+                  Kind.NUNIQUE, [1, 2, 3], [2, 1, 1] if is_b else [2, 4, 1], rtype=R),
+            _case(f"nunique_tests.cpp:90 zero_valid_keys[{v.name}]", K, [0, 0, 0], v, [3, 4, 5], Kind.NUNIQUE, [], [],
+                  kvalid=[0, 0, 0], rtype=R),
+            _case(f"nunique_tests.cpp:106 zero_valid_values[{v.name}]", K, [1, 1, 1], v, [0, 0, 0], Kind.NUNIQUE, [1],
+                  [0], vvalid=[0, 0, 0], rtype=R),
+            _case(f"nunique_tests.cpp:122 null_keys_and_values[{v.name}]", K, K11, v, V11, Kind.NUNIQUE,
+                  [1, 2, 3, 4], [1, 1, 1, 0] if is_b else [2, 3, 2, 0], kvalid=K11_VALID, vvalid=V11_VALID_A, rtype=R),
+            _case(f"nunique_tests.cpp:148 null_keys_and_values_with_duplicates[{v.name}]", K, K14, v, V14,
+                  Kind.NUNIQUE, [1, 2, 3, 4], [1, 1, 1, 0] if is_b else [2, 3, 2, 0], kvalid=K14_VALID,
+                  vvalid=V14_VALID_NUNIQUE, rtype=R),
+            _case(f"nunique_tests.cpp:175 include_nulls[{v.name}]", K, K14, v, V14, Kind.NUNIQUE, [1, 2, 3, 4],
+                  [2, 2, 1, 1] if is_b else [3, 4, 2, 1], kvalid=K14_VALID, vvalid=V14_VALID_NUNIQUE, rtype=R,
+                  extra={"null_policy": NullPolicy.INCLUDE}),
+        ]
+        if v in INTS + FLOATS:
+            out.append(_case(f"nunique_tests.cpp:202 dictionary[{v.name}]", K, [1, 2, 3, 3, 1, 2, 2, 1, 0, 3, 2, 4, 4, 2],
+                             v, [0, 1, 2, 2, 3, 4, 0, 6, 7, 8, 9, 0, 0, 0], Kind.NUNIQUE, [1, 2, 3, 4], [3, 4, 2, 1],
+                             kvalid=K14_VALID, vvalid=V14_VALID_NUNIQUE, rtype=R, vdict=True,
+                             extra={"null_policy": NullPolicy.INCLUDE}))
+
+    # ---- nth_element_tests.cpp (AllTypes); the result has the value's type,
+    # null positions are written 0 (the reference's -1 placeholders)
+    for v in ALL_TYPES:
+        def nth(line, name, keys, vals, n, want, *, wvalid=None, kvalid=None, vvalid=None, policy=NullPolicy.INCLUDE,
+                ekeys=(1, 2, 3)):
+            if v == T.BOOL8:
+                want = [int(bool(w)) for w in want]
+            want = [0 if (wvalid is not None and not ok) else w for w, ok in zip(want, wvalid or [1] * len(want))]
+            return _case(f"nth_element_tests.cpp:{line} {name}[{v.name}]", K, keys, v, vals, Kind.NTH_ELEMENT,
+                         list(ekeys), want, evalid=wvalid, kvalid=kvalid, vvalid=vvalid, ddof=n, rtype=v,
+                         extra={"null_policy": policy})
+        vdup = [0, 1, 2, 3, 4, 5, 3, 2, 2, 9]
+        out += [
+            nth(35, "basic n=0", K10, V10, 0, [0, 1, 2]),
+            nth(35, "basic n=1", K10, V10, 1, [3, 4, 7]),
+            nth(35, "basic n=2", K10, V10, 2, [6, 5, 8]),
+            nth(62, "empty_cols", [], [], 0, [], ekeys=()),
+            nth(78, "basic_out_of_bounds", K10, vdup, 3, [0, 9, 0], wvalid=[0, 1, 0]),
+            nth(94, "negative n=-1", K10, V10, -1, [6, 9, 8]),
+            nth(94, "negative n=-2", K10, V10, -2, [3, 5, 7]),
+            nth(94, "negative n=-3", K10, V10, -3, [0, 4, 2]),
+            nth(121, "negative_out_of_bounds", K10, vdup, -4, [0, 1, 0], wvalid=[0, 1, 0]),
+            nth(137, "zero_valid_keys", [1, 2, 3], [3, 4, 5], 0, [], kvalid=[0, 0, 0], ekeys=()),
+            nth(153, "zero_valid_values", [1, 1, 1], [3, 4, 5], 0, [3], wvalid=[0], vvalid=[0, 0, 0], ekeys=(1,)),
+            nth(169, "null_keys_and_values", K11, V11, 0, [-1, 1, 2, -1], wvalid=[0, 1, 1, 0], kvalid=K11_VALID,
+                vvalid=V11_VALID_A, ekeys=(1, 2, 3, 4)),
+            nth(189, "null_keys_and_values_out_of_bounds", K11, V11, 2, [6, -1, -1, -1], wvalid=[1, 0, 0, 0],
+                kvalid=K11_VALID, vvalid=V11_VALID_A, ekeys=(1, 2, 3, 4)),
+        ]
+        for line, name, n, policy, want, wvalid in (
+            (209, "exclude_nulls INCLUDE n=0", 0, NullPolicy.INCLUDE, [-1, 1, 2, 4], [0, 1, 1, 1]),
+            (209, "exclude_nulls INCLUDE n=1", 1, NullPolicy.INCLUDE, [3, 4, 2, -1], [1, 1, 1, 0]),
+            (209, "exclude_nulls INCLUDE n=2", 2, NullPolicy.INCLUDE, [6, -1, 8, -1], [1, 0, 1, 0]),
+            (209, "exclude_nulls EXCLUDE n=0", 0, NullPolicy.EXCLUDE, [3, 1, 2, 4], None),
+            (209, "exclude_nulls EXCLUDE n=1", 1, NullPolicy.EXCLUDE, [6, 4, 2, -1], [1, 1, 1, 0]),
+            (209, "exclude_nulls EXCLUDE n=2", 2, NullPolicy.EXCLUDE, [-1, 9, 8, -1], [0, 1, 1, 0]),
+            (251, "exclude_nulls_negative_index INCLUDE n=-1", -1, NullPolicy.INCLUDE, [6, -1, 8, -1], [1, 0, 1, 0]),
+            (251, "exclude_nulls_negative_index INCLUDE n=-2", -2, NullPolicy.INCLUDE, [3, 9, 2, 4], None),
+            (251, "exclude_nulls_negative_index INCLUDE n=-3", -3, NullPolicy.INCLUDE, [-1, -1, 2, -1], [0, 0, 1, 0]),
+            (251, "exclude_nulls_negative_index EXCLUDE n=-1", -1, NullPolicy.EXCLUDE, [6, 9, 8, 4], None),
+            (251, "exclude_nulls_negative_index EXCLUDE n=-2", -2, NullPolicy.EXCLUDE, [3, 4, 2, -1], [1, 1, 1, 0]),
+            (251, "exclude_nulls_negative_index EXCLUDE n=-3", -3, NullPolicy.EXCLUDE, [-1, 1, 2, -1], [0, 1, 1, 0]),
+        ):
+            out.append(nth(line, name, K14, V14, n, want, wvalid=wvalid, kvalid=K14_VALID, vvalid=V14_VALID_NTH,
+                           policy=policy, ekeys=(1, 2, 3, 4)))
+
+    # ---- m2_tests.cpp (int8..int64, float, double as both key and value type)
+    nan = math.nan
+    for t in INTS + FLOATS:
+        out += [
+            _case(f"m2_tests.cpp:62 EmptyInput[{t.name}]", t, [], t, [], Kind.M2, [], [], rtype=F),
+            _case(f"m2_tests.cpp:77 AllNullKeysInput[{t.name}]", t, [1, 2, 3], t, [3, 4, 5], Kind.M2, [], [],
+                  kvalid=[0, 0, 0], rtype=F),
+            _case(f"m2_tests.cpp:93 AllNullValuesInput[{t.name}]", t, [1, 2, 3], t, [3, 4, 5], Kind.M2, [1, 2, 3],
+                  [0.0, 0.0, 0.0], vvalid=[0, 0, 0], evalid=[0, 0, 0], rtype=F),
+            _case(f"m2_tests.cpp:108 SimpleInput[{t.name}]", t, K10, t, V10, Kind.M2, [1, 2, 3],
+                  [18.0, 32.75, 20.0 + 2.0 / 3.0], rtype=F),
+            _case(f"m2_tests.cpp:127 SimpleInputHavingNegativeValues[{t.name}]", t, K10, t,
+                  [0, 1, -2, 3, -4, -5, -6, 7, -8, 9], Kind.M2, [1, 2, 3], [42.0, 122.75, 114.0], rtype=F),
+            _case(f"m2_tests.cpp:146 ValuesHaveNulls[{t.name}]", t, [1, 2, 3, 4, 5, 2, 3, 2], t,
+                  [0, 0, 2, 3, 0, 5, 6, 7], Kind.M2, [1, 2, 3, 4, 5], [0.0, 2.0, 8.0, 0.0, 0.0],
+                  vvalid=[1, 0, 1, 1, 0, 1, 1, 1], evalid=[1, 1, 1, 1, 0], rtype=F),
+            _case(f"m2_tests.cpp:162 KeysAndValuesHaveNulls[{t.name}]", t, [1, 2, 3, 1, 2, 2, 1, 0, 3, 2, 4], t,
+                  [0, 1, 2, 3, 4, 0, 6, 7, 8, 9, 0], Kind.M2, [1, 2, 3, 4], [4.5, 32.0 + 2.0 / 3.0, 18.0, 0.0],
+                  kvalid=[1, 1, 1, 1, 1, 1, 1, 0, 1, 1, 1], vvalid=[0, 1, 1, 1, 1, 0, 1, 1, 1, 1, 0],
+                  evalid=[1, 1, 1, 0], rtype=F),
+            _case(f"m2_tests.cpp:182 InputHaveNullsAndNaNs[{t.name}]", t, [4, 3, 1, 2, 3, 1, 2, 2, 1, 0, 3, 2, 4, 4],
+                  T.FLOAT64, [0.0, 0.0, 0.0, 1.0, 2.0, 3.0, 4.0, nan, 6.0, 7.0, 8.0, 9.0, 10.0, nan], Kind.M2,
+                  [1, 2, 3, 4], [18.0, nan, 18.0, nan], kvalid=[1] * 9 + [0] + [1] * 4,
+                  vvalid=[0, 0] + [1] * 12, rtype=F),
+            _case(f"m2_tests.cpp:204 SlicedColumnsInput[{t.name}]", t,
+                  [1, 2, 3, 4, 5, 1, 2, 3, 4, 5] + [4, 3, 1, 2, 3, 1, 2, 2, 1, 0, 3, 2, 4, 4]
+                  + [1, 2, 3, 4, 5, 1, 2, 3, 4, 5], T.FLOAT64,
+                  [3.0, 2.0, 5.0, 4.0, 6.0, 9.0, 1.0, 0.0, 1.0, 7.0]
+                  + [0.0, 0.0, 0.0, 1.0, 2.0, 3.0, 4.0, nan, 6.0, 7.0, 8.0, 9.0, 10.0, nan]
+                  + [9.0, 10.0, 11.0, 12.0, 0.0, 5.0, 1.0, 20.0, 19.0, 15.0], Kind.M2,
+                  [1, 2, 3, 4], [18.0, nan, 18.0, nan], kvalid=[1] * 19 + [0] + [1] * 14,
+                  vvalid=[1] * 10 + [0, 0] + [1] * 22, rtype=F, offset=10, size=14),
+        ]
     return out
 
 

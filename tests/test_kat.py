@@ -16,7 +16,7 @@ from tests.golden import reference_kats as KAT
 CASES = KAT.cases()
 
 
-def _host(vals, valid, tid, scale=0, as_dict=False):
+def _host(vals, valid, tid, scale=0, as_dict=False, offset=0, size=None):
     tid = TypeId(tid)
     if tid == TypeId.BOOL8:
         arr = np.array([bool(v) for v in vals], dtype=np.uint8)
@@ -26,8 +26,8 @@ def _host(vals, valid, tid, scale=0, as_dict=False):
     if as_dict:
         uniq, idx = np.unique(arr, return_inverse=True)
         keys = HostCol(uniq, None, type_id=tid, scale=scale)
-        return HostCol(idx.astype(np.int32), vm, dict_keys=keys)
-    return HostCol(arr, vm, type_id=tid, scale=scale)
+        return HostCol(idx.astype(np.int32), vm, dict_keys=keys, offset=offset, size=size)
+    return HostCol(arr, vm, type_id=tid, scale=scale, offset=offset, size=size)
 
 
 def build(case):
@@ -36,10 +36,10 @@ def build(case):
         keys = HostCol(np.array(case["keys"], dtype=np.int32), None if case["key_valid"] is None
                        else np.array(case["key_valid"], bool), dict_keys=placeholder)
     else:
-        keys = _host(case["keys"], case["key_valid"], case["key_type"])
+        keys = _host(case["keys"], case["key_valid"], case["key_type"], offset=case["offset"], size=case["size"])
     vals = _host(case["values"], case["value_valid"], case["value_type"], case.get("value_scale", 0),
-                 as_dict=case["value_dict"])
-    return [keys], [(vals, [(case["kind"], case["ddof"])])]
+                 as_dict=case["value_dict"], offset=case["offset"], size=case["size"])
+    return [keys], [(vals, [(case["kind"], case["ddof"], case["extra"])])]
 
 
 def expected(case):
@@ -62,6 +62,9 @@ def check_against_expected(got, case):
     go = T.sort_order(got["keys"])
     wo = T.sort_order(want["keys"])
     T.compare_keys(got["keys"], want["keys"], go, wo)
+    # a QUANTILE result holds num_quantiles rows per group, group by group
+    nq = len(case["extra"].get("quantiles", ())) if Kind(case["kind"]) == Kind.QUANTILE else 1
+    go, wo = T.rows_of_groups(go, nq), T.rows_of_groups(wo, nq)
     T.compare_values(Kind(case["kind"]), got["results"][0][0], want["results"][0][0], go, wo, ctx=case["id"])
 
 
