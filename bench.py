@@ -24,7 +24,9 @@ per groupby) are larger than L2 (126 MB), so no L2 flush is needed.
 
 Further sections in the same JSON line: config1 (10M rows, 1e3 groups, with
 the oracle, pandas and pyarrow over the same rows), config3 (200M rows,
-Zipf(1.2) composite key with null keys), batched (4,096 instances in one
+Zipf(1.2) composite key with null keys), sorted (the sort-path kinds MEDIAN,
+QUANTILE, NUNIQUE, NTH_ELEMENT and M2 over the 100M-row columns at 1e4
+groups), batched (4,096 instances in one
 graph launch against a plain loop and an async 4-stream plain loop) and
 served (Poisson arrivals at three rates, plus each form's capacity).
 
@@ -79,9 +81,10 @@ def parse_args(argv=None):
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--c3-rows", type=int, default=200_000_000)
-    p.add_argument("--sections", type=str, default="plain,config1,config3,batched,served",
+    p.add_argument("--sections", type=str, default="plain,config1,config3,sorted,batched,served",
                    help="comma list of: plain (the headline line), config1 (10M rows, 1e3 groups), config3 "
-                        "(200M rows, Zipf composite key), batched (4,096-instance batch), served (Poisson "
+                        "(200M rows, Zipf composite key), sorted (MEDIAN / QUANTILE / NUNIQUE / NTH_ELEMENT / "
+                        "M2 over the 100M-row columns), batched (4,096-instance batch), served (Poisson "
                         "request stream)")
     p.add_argument("--batch-instances", type=int, default=4096)
     p.add_argument("--batch-tune", choices=["off", "cached", "missing", "all"], default="missing")
@@ -396,8 +399,8 @@ def run_ours(args, rank, world, local):
     torch.cuda.empty_cache()
     sections = args.sections.split(",")
     extra = {}
-    for name, fn in (("config1", run_config1), ("config3", run_config3), ("batched", run_batched),
-                     ("served", run_served)):
+    for name, fn in (("config1", run_config1), ("config3", run_config3), ("sorted", run_sorted),
+                     ("batched", run_batched), ("served", run_served)):
         if name not in sections:
             continue
         if name == "served":
@@ -699,6 +702,92 @@ def run_config3(args, rank, world, device, stream, alloc):
         cpu = _cpu_baselines(keys, [(HostCol(d.values[0]), a2)], a2, rows, {"v0": ["sum", "mean"]},
                              [("v0", "sum"), ("v0", "mean")])
         cpu["sample"] = f"{rows} rows of the same distribution (numpy seed)"
+        out["cpu_baseline"] = cpu
+    return out
+
+
+# --------------------------------------------------- sort-path kinds (plain)
+
+SORTED_CARD = 10_000
+SORTED_QS = (0.25, 0.5, 0.75)
+
+
+def run_sorted(args, rank, world, device, stream, alloc):
+    """The kinds libcudf computes on its sort path, over the 100M-row
+    workload's columns at 1e4 groups: MEDIAN, QUANTILE {.25, .5, .75} and
+    NUNIQUE of the int64 column a, NTH_ELEMENT(0) and M2 of the float32
+    column b (10% nulls).  Checks at full size: QUANTILE 0.5 equals MEDIAN,
+    quantiles ascend within a group, NUNIQUE <= the group's row count."""
+    import numpy as np
+    import torch
+
+    from cudf_b200 import GroupBy, GroupByRequest, Table
+    from cudf_b200 import aggregation as agg
+    from cudf_b200 import workloads as W
+    from cudf_b200._abi import Kind, NullPolicy
+    from oracle.oracle import HostCol
+
+    n = args.rows
+    k, a, b = W.plain_100m_device(SORTED_CARD, n, W.SEED0 + 11 + rank, device)
+    gb = GroupBy(Table([k]))
+    gb.set_timing(True)
+    reqs = [GroupByRequest(a, [agg.median(), agg.quantile(SORTED_QS), agg.nunique(), agg.count()]),
+            GroupByRequest(b, [agg.nth_element(0), agg.m2()])]
+    with ClockSampler(device.index) as clk:
+        ms, st, groups = _time_calls(gb, reqs, stream, alloc, max(args.warmup, 3), max(args.steps, 5))
+    kt, res = gb.aggregate(reqs, stream=stream, allocator=alloc)
+    med = res[0].columns()[0].to_numpy()[0]
+    qv = res[0].columns()[1].to_numpy()[0].reshape(-1, len(SORTED_QS))
+    nu = res[0].columns()[2].to_numpy()[0]
+    cnt = res[0].columns()[3].to_numpy()[0]
+    checks = {"groups": int(kt.num_rows()),
+              "median_equals_quantile_0.5": bool(np.array_equal(med, qv[:, 1])),
+              "quantiles_ascend": bool(np.all(np.diff(qv, axis=1) >= 0)),
+              "nunique_le_rows": bool(np.all((nu >= 1) & (nu <= cnt))),
+              "rows_total": int(cnt.sum()) == n}
+    del kt, res
+    peaks = _load_peaks()
+    alg = n * (8 + 8 + 4 + 0.125) + groups * (8 + 8 + 8 * len(SORTED_QS) + 4 + 4 + 4 + 8)
+    out = {"metric": "groupby rows/s (100M rows, int64 key, 1e4 groups; MEDIAN, QUANTILE x3, NUNIQUE, "
+                     "NTH_ELEMENT, M2)",
+           "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_call": ms, "groups": groups,
+           "strategy": STRATEGY_NAMES.get(st["strategy"], st["strategy"]),
+           "kernel_launches": st["kernel_launches"],
+           "phases_ms": {p: st[p] for p in ("sample_ms", "init_ms", "aggregate_ms", "compact_ms", "finalize_ms")},
+           "hbm_frac_whole_call": alg / (ms / 1e3) / 1e9 / peaks["hbm_gbs"],
+           "checks": checks,
+           "config": {"rows": n, "key": "int64 U[0, 1e4)", "values": ["int64 U[-1e6,1e6]", "float32 N(0,1) 10% nulls"],
+                      "aggregations": ["MEDIAN(a)", "QUANTILE(a, .25/.5/.75, LINEAR)", "NUNIQUE(a)", "COUNT(a)",
+                                       "NTH_ELEMENT(b, 0)", "M2(b)"],
+                      "note": "finalize_ms holds the labels, the radix sorts of (group, value) records and the "
+                              "selections"},
+           "clocks": clk.summary()}
+    del gb, reqs, k, a, b
+    if rank == 0 and not args.no_cpu:
+        rows = min(args.cpu_sample_rows, 2_000_000)
+        d = W.plain_100m(SORTED_CARD, n=rows)
+        aggs_a = [(Kind.MEDIAN, 0), (Kind.QUANTILE, 0, {"quantiles": list(SORTED_QS)}), (Kind.NUNIQUE, 0),
+                  (Kind.COUNT_VALID, 0)]
+        aggs_b = [(Kind.NTH_ELEMENT, 0, {"null_policy": NullPolicy.INCLUDE}), (Kind.M2, 0)]
+        from oracle import oracle as orc
+
+        t0 = time.perf_counter()
+        orc.groupby([HostCol(d.keys[0])], [(HostCol(d.values[0]), aggs_a),
+                                            (HostCol(d.values[1], d.value_valid[1]), aggs_b)])
+        cpu = {"value": rows / (time.perf_counter() - t0), "unit": "rows/s", "cores": 1, "kind": "port",
+               "sample": f"{rows} rows of the same distribution (numpy seed)"}
+        try:
+            import pandas as pd
+
+            df = pd.DataFrame({"k": d.keys[0], "a": d.values[0],
+                               "b": np.where(d.value_valid[1], d.values[1], np.nan)})
+            t0 = time.perf_counter()
+            g = df.groupby("k", sort=False)
+            g["a"].median(), g["a"].quantile(list(SORTED_QS)), g["a"].nunique(), g["a"].count()
+            g["b"].nth(0), g["b"].var(ddof=0)
+            cpu["pandas_rows_per_s"] = rows / (time.perf_counter() - t0)
+        except Exception as e:  # pragma: no cover
+            cpu["pandas_error"] = str(e)
         out["cpu_baseline"] = cpu
     return out
 
