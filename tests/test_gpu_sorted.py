@@ -142,3 +142,30 @@ def test_null_keys_are_excluded_from_sorted_kinds():
     kv = rng.random(n) >= 0.3
     v = rng.integers(0, 10, n).astype(np.int64)
     T.assert_parity([HostCol(k, kv)], [(HostCol(v), sorted_aggs())], NullPolicy.EXCLUDE)
+
+
+@pytest.mark.parametrize("case", ["int64_full_range", "float64_unit_interval", "float32_no_neg_zero",
+                                  "float64_wide", "constant_values", "tiny_range_many_groups"])
+def test_record_formats(case):
+    """Values whose range fits one 64-bit record beside the group label take
+    the packed records, the others (full-range int64, wide float64, float32
+    with -0.0) the split ones: both must give the oracle's results."""
+    rng = np.random.default_rng(18)
+    n, card = 150_000, 2_000
+    if case == "int64_full_range":
+        v = rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64)
+    elif case == "float64_unit_interval":
+        v = 1.0 + rng.random(n)
+    elif case == "float32_no_neg_zero":
+        v = rng.normal(0, 1, n).astype(np.float32)
+        v[v == 0] = 1.0
+    elif case == "float64_wide":
+        v = rng.normal(0, 1e300, n)
+    elif case == "constant_values":
+        v = np.full(n, 7, np.int32)
+    else:
+        card = 60_000
+        v = rng.integers(0, 3, n).astype(np.int16)
+    k = rng.integers(0, card, n).astype(np.int32)
+    valid = rng.random(n) >= 0.1
+    T.assert_parity([HostCol(k)], [(HostCol(v, valid), sorted_aggs())])
