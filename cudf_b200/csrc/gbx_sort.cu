@@ -294,9 +294,24 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint64_t* __rest
   for (int i = threadIdx.x; i < 256; i += kSortBlock) counts[static_cast<size_t>(i) * ntiles + blockIdx.x] = h[i];
 }
 
+// Lanes of the warp whose 8-bit digit equals this lane's (`act` lanes only):
+// one ballot per digit bit (the match of lanes by digit from ballots).
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t act)
+{
+  uint32_t peers = act;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const uint32_t v = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+    peers &= ((d >> b) & 1u) ? v : ~v;
+  }
+  return peers;
+}
+
 // Stable scatter of one tile: the record at tile position (warp, batch,
 // lane) -- row order -- goes to offsets[d * ntiles + tile] plus its rank
-// among the tile's records of digit d.
+// among the tile's records of digit d.  Each lane keeps its 16 records and
+// their ranks within the warp in registers, so the ranking runs once: ranks
+// by warp, then per digit the warps' bases, then the writes.
 template <bool kSplit>
 __global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __restrict__ lo_in,
                                                              const uint32_t* __restrict__ hi_in, int64_t n,
@@ -305,21 +320,36 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __r
                                                              uint64_t* __restrict__ lo_out,
                                                              uint32_t* __restrict__ hi_out)
 {
+  constexpr int kBatches = kSortPerWarp / 32;
   __shared__ uint32_t cnt[kSortWarps][256];
   const int lane     = threadIdx.x & 31;
   const int warp     = threadIdx.x >> 5;
   const uint32_t lt  = (1u << lane) - 1u;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kSortTile + warp * kSortPerWarp;
-  const bool use_hi  = kSplit && shift >= 64;
   for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortBlock) (&cnt[0][0])[i] = 0;
+  uint64_t l[kBatches];
+  uint32_t h[kBatches];
+  uint32_t rank[kBatches];
+#pragma unroll
+  for (int j = 0; j < kBatches; ++j) {
+    const int64_t r = base + j * 32 + lane;
+    l[j]            = r < n ? lo_in[r] : 0;
+    h[j]            = 0;
+    if constexpr (kSplit) h[j] = r < n ? hi_in[r] : 0;
+  }
   __syncthreads();
-  // each warp's digit counts
-  for (int j = 0; j < kSortPerWarp / 32; ++j) {
-    const int64_t r   = base + j * 32 + lane;
-    const bool act    = r < n;
-    const uint32_t d  = act ? digit_at<kSplit>(use_hi ? 0 : lo_in[r], use_hi ? hi_in[r] : 0, shift) : 0xffffffffu;
-    const uint32_t pe = __match_any_sync(0xffffffffu, d);
-    if (act && lane == __ffs(pe) - 1) cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
+  // ranks within the warp, digit by digit in row order
+#pragma unroll
+  for (int j = 0; j < kBatches; ++j) {
+    const int64_t r     = base + j * 32 + lane;
+    const uint32_t act  = __ballot_sync(0xffffffffu, r < n);
+    const uint32_t d    = digit_at<kSplit>(l[j], h[j], shift);
+    const uint32_t pe   = digit_peers(d, act);
+    const bool mine     = (act >> lane) & 1u;
+    const uint32_t prev = mine ? cnt[warp][d] : 0u;
+    rank[j]             = prev + static_cast<uint32_t>(__popc(pe & lt));
+    __syncwarp();
+    if (mine && (pe & lt) == 0) cnt[warp][d] = prev + static_cast<uint32_t>(__popc(pe));
     __syncwarp();
   }
   __syncthreads();
@@ -333,25 +363,14 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __r
     }
   }
   __syncthreads();
-  for (int j = 0; j < kSortPerWarp / 32; ++j) {
+#pragma unroll
+  for (int j = 0; j < kBatches; ++j) {
     const int64_t r = base + j * 32 + lane;
-    const bool act  = r < n;
-    uint64_t l      = 0;
-    uint32_t h      = 0;
-    if (act) {
-      l = lo_in[r];
-      if constexpr (kSplit) h = hi_in[r];
+    if (r < n) {
+      const uint32_t at = cnt[warp][digit_at<kSplit>(l[j], h[j], shift)] + rank[j];
+      lo_out[at]        = l[j];
+      if constexpr (kSplit) hi_out[at] = h[j];
     }
-    const uint32_t d  = act ? digit_at<kSplit>(l, h, shift) : 0xffffffffu;
-    const uint32_t pe = __match_any_sync(0xffffffffu, d);
-    const uint32_t at = act ? cnt[warp][d] + static_cast<uint32_t>(__popc(pe & lt)) : 0u;
-    __syncwarp();
-    if (act && lane == __ffs(pe) - 1) cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
-    if (act) {
-      lo_out[at] = l;
-      if constexpr (kSplit) hi_out[at] = h;
-    }
-    __syncwarp();
   }
 }
 
