@@ -310,8 +310,10 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t act)
 // Stable scatter of one tile: the record at tile position (warp, batch,
 // lane) -- row order -- goes to offsets[d * ntiles + tile] plus its rank
 // among the tile's records of digit d.  Each lane keeps its 16 records and
-// their ranks within the warp in registers, so the ranking runs once: ranks
-// by warp, then per digit the warps' bases, then the writes.
+// their ranks within the warp in registers (the ranking runs once); the tile
+// is then laid out in shared memory in digit order and written out digit run
+// by digit run with consecutive threads on consecutive rows, so that a warp's
+// stores cover whole sectors.
 template <bool kSplit>
 __global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __restrict__ lo_in,
                                                              const uint32_t* __restrict__ hi_in, int64_t n,
@@ -321,11 +323,21 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __r
                                                              uint32_t* __restrict__ hi_out)
 {
   constexpr int kBatches = kSortPerWarp / 32;
+  static_assert(kSortBlock == 256, "one thread per digit");
   __shared__ uint32_t cnt[kSortWarps][256];
-  const int lane     = threadIdx.x & 31;
-  const int warp     = threadIdx.x >> 5;
-  const uint32_t lt  = (1u << lane) - 1u;
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * kSortTile + warp * kSortPerWarp;
+  __shared__ uint32_t dstart[256];   // the digit's first position in the tile
+  __shared__ uint32_t gstart[256];   // the digit run's first output row
+  __shared__ uint32_t wsum[kSortWarps];
+  // the staged tile (dynamic shared memory: scatter_smem_bytes)
+  extern __shared__ __align__(16) unsigned char sort_stage[];
+  uint64_t* stage_lo = reinterpret_cast<uint64_t*>(sort_stage);
+  uint32_t* stage_hi = reinterpret_cast<uint32_t*>(sort_stage + kSortTile * sizeof(uint64_t));
+  const int lane      = threadIdx.x & 31;
+  const int warp      = threadIdx.x >> 5;
+  const uint32_t lt   = (1u << lane) - 1u;
+  const int64_t tile0 = static_cast<int64_t>(blockIdx.x) * kSortTile;
+  const int64_t base  = tile0 + warp * kSortPerWarp;
+  const int tile_n    = static_cast<int>(n - tile0 < kSortTile ? n - tile0 : kSortTile);
   for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortBlock) (&cnt[0][0])[i] = 0;
   uint64_t l[kBatches];
   uint32_t h[kBatches];
@@ -353,25 +365,58 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __r
     __syncwarp();
   }
   __syncthreads();
-  // per digit: the tile's offset, then each warp's first position
-  for (int d = threadIdx.x; d < 256; d += kSortBlock) {
-    uint32_t run = offsets[static_cast<size_t>(d) * ntiles + blockIdx.x];
+  // thread d: the warps' bases within digit d, the digit's tile count, then
+  // an exclusive scan of the counts over the digits (kSortBlock == 256)
+  {
+    const int d   = threadIdx.x;
+    uint32_t tot  = 0;
     for (int w = 0; w < kSortWarps; ++w) {
       const uint32_t c = cnt[w][d];
-      cnt[w][d]        = run;
-      run += c;
+      cnt[w][d]        = tot;
+      tot += c;
     }
+    uint32_t x = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += wsum[w];
+    dstart[d] = before + x - tot;
+    gstart[d] = offsets[static_cast<size_t>(d) * ntiles + blockIdx.x];
   }
   __syncthreads();
+  // the tile in digit order in shared memory
 #pragma unroll
   for (int j = 0; j < kBatches; ++j) {
     const int64_t r = base + j * 32 + lane;
     if (r < n) {
-      const uint32_t at = cnt[warp][digit_at<kSplit>(l[j], h[j], shift)] + rank[j];
-      lo_out[at]        = l[j];
-      if constexpr (kSplit) hi_out[at] = h[j];
+      const uint32_t d  = digit_at<kSplit>(l[j], h[j], shift);
+      const uint32_t at = dstart[d] + cnt[warp][d] + rank[j];
+      stage_lo[at]      = l[j];
+      if constexpr (kSplit) stage_hi[at] = h[j];
     }
   }
+  __syncthreads();
+  // digit runs out: position i of the tile is record i - dstart[d] of digit d
+  for (int i = threadIdx.x; i < tile_n; i += kSortBlock) {
+    const uint64_t v  = stage_lo[i];
+    uint32_t hv       = 0;
+    if constexpr (kSplit) hv = stage_hi[i];
+    const uint32_t d  = digit_at<kSplit>(v, hv, shift);
+    const uint32_t at = gstart[d] + static_cast<uint32_t>(i) - dstart[d];
+    lo_out[at]        = v;
+    if constexpr (kSplit) hi_out[at] = hv;
+  }
+}
+
+// Dynamic shared memory of k_sort_scatter: the staged tile.
+constexpr size_t scatter_smem_bytes(bool split)
+{
+  return kSortTile * sizeof(uint64_t) + (split ? kSortTile * sizeof(uint32_t) : 0);
 }
 
 // --------------------------------------------------------------- bounds
@@ -612,6 +657,11 @@ void sorted_kinds(const SortedKindsArgs& a, int* launches)
   const int pbits = bits_for(static_cast<uint64_t>(G));  // bits of the largest packed label, G
   const int rbits = std::max(1, bits_for(static_cast<uint64_t>(n - 1)));
 
+  GBX_CUDA(cudaFuncSetAttribute(k_sort_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(scatter_smem_bytes(true))));
+  GBX_CUDA(cudaFuncSetAttribute(k_sort_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(scatter_smem_bytes(false))));
+
   // sorts the records on bits [from, to) (split: lo's low lo_bits, then hi's
   // label bits); returns where the result lies and fills `bounds`
   auto sort = [&](bool split, int from, int to, int lo_bits, const Fmt& f) {
@@ -630,12 +680,14 @@ void sorted_kinds(const SortedKindsArgs& a, int* launches)
         k_sort_hist<true><<<ntiles, kSortBlock, 0, s>>>(li, hin, n, sh, ntiles, counts);
         GBX_CUDA(cudaGetLastError());
         GBX_CUDA(scan_exclusive_u32(counts, offsets, items, temp, &tbx, s));
-        k_sort_scatter<true><<<ntiles, kSortBlock, 0, s>>>(li, hin, n, sh, ntiles, offsets, lout, hout);
+        k_sort_scatter<true><<<ntiles, kSortBlock, scatter_smem_bytes(true), s>>>(li, hin, n, sh, ntiles, offsets,
+                                                                                  lout, hout);
       } else {
         k_sort_hist<false><<<ntiles, kSortBlock, 0, s>>>(li, nullptr, n, sh, ntiles, counts);
         GBX_CUDA(cudaGetLastError());
         GBX_CUDA(scan_exclusive_u32(counts, offsets, items, temp, &tbx, s));
-        k_sort_scatter<false><<<ntiles, kSortBlock, 0, s>>>(li, nullptr, n, sh, ntiles, offsets, lout, nullptr);
+        k_sort_scatter<false><<<ntiles, kSortBlock, scatter_smem_bytes(false), s>>>(li, nullptr, n, sh, ntiles,
+                                                                                   offsets, lout, nullptr);
       }
       GBX_CUDA(cudaGetLastError());
       *launches += 2 + scan_launches(items);
