@@ -444,5 +444,20 @@ __device__ __forceinline__ int64_t find_or_insert(typename Space::addr_t keys,
   return -1;
 }
 
+// Lanes of the warp (among `act`) whose digit of `width` (<= 8) bits equals
+// this lane's: one ballot per digit bit.  The same lane sets as a match on
+// the digit, on the ALU instead of the pipe that serialises matches.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, int width, uint32_t act)
+{
+  uint32_t peers = act;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    if (b >= width) break;
+    const uint32_t v = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+    peers &= ((d >> b) & 1u) ? v : ~v;
+  }
+  return peers;
+}
+
 }  // namespace dev
 }  // namespace gbx

@@ -184,10 +184,16 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
     }
 #pragma unroll
     for (int u = 0; u < kLoadGroup; ++u) {
-      const uint32_t d  = act[u] ? digit_of<NW>(k[u], dg) : 0xffffffffu;
-      const uint32_t pe = __match_any_sync(kFull, d);
-      if (act[u] && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
-      sm.lpos[warp * kRowsPerWarp + (j0 + u) * 32 + lane] = static_cast<uint16_t>(act[u] ? d : 0xffffu);
+      const int row       = warp * kRowsPerWarp + (j0 + u) * 32 + lane;
+      const uint32_t d    = act[u] ? digit_of<NW>(k[u], dg) : 0u;
+      const uint32_t pe   = digit_peers(d, dg.width, __ballot_sync(kFull, act[u]));
+      const uint32_t prev = act[u] ? sm.cnt[warp][d] : 0u;
+      // the row's rank among its warp's rows of its digit, and the digit
+      // (in vstage, unused until the columns are staged)
+      sm.lpos[row]   = static_cast<uint16_t>(act[u] ? prev + static_cast<uint32_t>(__popc(pe & lt)) : 0xffffu);
+      sm.vstage[row] = static_cast<uint8_t>(d);
+      __syncwarp();
+      if (act[u] && (pe & lt) == 0) sm.cnt[warp][d] = prev + static_cast<uint32_t>(__popc(pe));
       __syncwarp();
     }
   }
@@ -233,17 +239,18 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
     }
   }
   __syncthreads();
-  // local positions (the digits come back from lpos, which then takes the
-  // position) and the output row of each; key word 0 staged on the way
+  // local positions (the rank comes back from lpos, which then takes the
+  // position, the digit from vstage) and the output row of each; key word 0
+  // staged on the way
   for (int j0 = 0; j0 < kRowsPerWarp / 32; j0 += kLoadGroup) {
     uint64_t k0[kLoadGroup];
-    uint32_t dd[kLoadGroup];
+    uint32_t rr[kLoadGroup];
 #pragma unroll
     for (int u = 0; u < kLoadGroup; ++u) {
       const int row = warp * kRowsPerWarp + (j0 + u) * 32 + lane;
-      dd[u]         = sm.lpos[row];
+      rr[u]         = sm.lpos[row];
       k0[u]         = 0;
-      if (dd[u] != 0xffffu) {
+      if (rr[u] != 0xffffu) {
         uint64_t k[NW];
         src.key(base + (j0 + u) * 32 + lane, k);
         k0[u] = k[0];
@@ -251,18 +258,14 @@ __global__ void __launch_bounds__(kRadixBlock, 3) k_radix_scatter(const __grid_c
     }
 #pragma unroll
     for (int u = 0; u < kLoadGroup; ++u) {
-      const bool act    = dd[u] != 0xffffu;
-      const uint32_t d  = act ? dd[u] : 0xffffffffu;
-      const uint32_t pe = __match_any_sync(kFull, d);
-      const uint32_t lp = act ? sm.cnt[warp][d] + static_cast<uint32_t>(__popc(pe & lt)) : 0xffffu;
-      __syncwarp();
-      if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
-      sm.lpos[warp * kRowsPerWarp + (j0 + u) * 32 + lane] = static_cast<uint16_t>(lp);
-      if (act) {
-        sm.gp[lp]    = sm.goff[d] + (lp - sm.tstart[d]);
-        sm.stage[lp] = k0[u];
+      const int row = warp * kRowsPerWarp + (j0 + u) * 32 + lane;
+      if (rr[u] != 0xffffu) {
+        const uint32_t d  = sm.vstage[row];
+        const uint32_t lp = sm.cnt[warp][d] + rr[u];
+        sm.lpos[row]      = static_cast<uint16_t>(lp);
+        sm.gp[lp]         = sm.goff[d] + (lp - sm.tstart[d]);
+        sm.stage[lp]      = k0[u];
       }
-      __syncwarp();
     }
   }
   __syncthreads();
@@ -335,6 +338,7 @@ struct BulkSmem {
   uint32_t gp[kTileRows];                // output row of local position i
   uint16_t src[kTileRows];               // tile row at local position i
   uint8_t dig[kTileRows];                // digit of tile row r
+  uint16_t rk[kTileRows];                // rank of tile row r among its warp's rows of its digit
   uint32_t cnt[kRadixWarps][kMaxRadix];  // per warp: rows of each digit, then its first local position
   uint32_t tstart[kMaxRadix];            // first local position of each digit in the tile
   uint32_t goff[kMaxRadix];              // first output row of the tile's rows of each digit
@@ -549,17 +553,23 @@ __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __g
     return;
   }
 
-  // per warp: rows of each digit; each row's digit kept
+  // per warp: rows of each digit; each row's digit and its rank among the
+  // warp's rows of that digit kept (stable: batch, then lane order)
   for (int j0 = 0; j0 < kRowsPerWarp / 32; ++j0) {
     const int r    = warp * kRowsPerWarp + j0 * 32 + lane;
     const bool act = r < nrows;
     uint64_t k[NW];
 #pragma unroll
     for (int w = 0; w < NW; ++w) k[w] = act ? sm.raw[w][r] : 0;
-    const uint32_t d  = act ? digit_of<NW>(k, dg) : 0xffffffffu;
-    const uint32_t pe = __match_any_sync(kFull, d);
-    if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
-    if (act) sm.dig[r] = static_cast<uint8_t>(d);
+    const uint32_t d    = act ? digit_of<NW>(k, dg) : 0u;
+    const uint32_t pe   = digit_peers(d, dg.width, __ballot_sync(kFull, act));
+    const uint32_t prev = act ? sm.cnt[warp][d] : 0u;
+    if (act) {
+      sm.dig[r] = static_cast<uint8_t>(d);
+      sm.rk[r]  = static_cast<uint16_t>(prev + static_cast<uint32_t>(__popc(pe & lt)));
+    }
+    __syncwarp();
+    if (act && (pe & lt) == 0) sm.cnt[warp][d] = prev + static_cast<uint32_t>(__popc(pe));
     __syncwarp();
   }
   __syncthreads();
@@ -605,18 +615,13 @@ __global__ void __launch_bounds__(kRadixBlock, 2) k_radix_scatter_bulk(const __g
   // local position of every row (stable: warp, batch, lane order), with the
   // tile row and the output row stored at it
   for (int j0 = 0; j0 < kRowsPerWarp / 32; ++j0) {
-    const int r       = warp * kRowsPerWarp + j0 * 32 + lane;
-    const bool act    = r < nrows;
-    const uint32_t d  = act ? sm.dig[r] : 0xffffffffu;
-    const uint32_t pe = __match_any_sync(kFull, d);
-    const uint32_t lp = act ? sm.cnt[warp][d] + static_cast<uint32_t>(__popc(pe & lt)) : 0u;
-    __syncwarp();
-    if (act && lane == __ffs(pe) - 1) sm.cnt[warp][d] += static_cast<uint32_t>(__popc(pe));
-    if (act) {
-      sm.src[lp] = static_cast<uint16_t>(r);
-      sm.gp[lp]  = sm.goff[d] + (lp - sm.tstart[d]);
+    const int r = warp * kRowsPerWarp + j0 * 32 + lane;
+    if (r < nrows) {
+      const uint32_t d  = sm.dig[r];
+      const uint32_t lp = sm.cnt[warp][d] + sm.rk[r];
+      sm.src[lp]        = static_cast<uint16_t>(r);
+      sm.gp[lp]         = sm.goff[d] + (lp - sm.tstart[d]);
     }
-    __syncwarp();
   }
   __syncthreads();
 

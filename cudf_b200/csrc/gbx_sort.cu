@@ -294,19 +294,6 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint64_t* __rest
   for (int i = threadIdx.x; i < 256; i += kSortBlock) counts[static_cast<size_t>(i) * ntiles + blockIdx.x] = h[i];
 }
 
-// Lanes of the warp whose 8-bit digit equals this lane's (`act` lanes only):
-// one ballot per digit bit (the match of lanes by digit from ballots).
-__device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t act)
-{
-  uint32_t peers = act;
-#pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const uint32_t v = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-    peers &= ((d >> b) & 1u) ? v : ~v;
-  }
-  return peers;
-}
-
 // Stable scatter of one tile: the record at tile position (warp, batch,
 // lane) -- row order -- goes to offsets[d * ntiles + tile] plus its rank
 // among the tile's records of digit d.  Each lane keeps its 16 records and
@@ -356,7 +343,7 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __r
     const int64_t r     = base + j * 32 + lane;
     const uint32_t act  = __ballot_sync(0xffffffffu, r < n);
     const uint32_t d    = digit_at<kSplit>(l[j], h[j], shift);
-    const uint32_t pe   = digit_peers(d, act);
+    const uint32_t pe   = digit_peers(d, 8, act);
     const bool mine     = (act >> lane) & 1u;
     const uint32_t prev = mine ? cnt[warp][d] : 0u;
     rank[j]             = prev + static_cast<uint32_t>(__popc(pe & lt));
