@@ -138,6 +138,29 @@ class gbx_table_view(C.Structure):
     ]
 
 
+class NullEquality(enum.IntEnum):
+    """cudf::null_equality (types.hpp:151-154)."""
+
+    EQUAL = 0
+    UNEQUAL = 1
+
+
+class NanEquality(enum.IntEnum):
+    """cudf::nan_equality (types.hpp:143-146)."""
+
+    ALL_EQUAL = 0
+    UNEQUAL = 1
+
+
+class DuplicateKeep(enum.IntEnum):
+    """cudf::duplicate_keep_option (stream_compaction.hpp:225-230)."""
+
+    KEEP_ANY = 0
+    KEEP_FIRST = 1
+    KEEP_LAST = 2
+    KEEP_NONE = 3
+
+
 class Interpolation(enum.IntEnum):
     """cudf::interpolation (types.hpp:192-198), for QUANTILE."""
 
@@ -414,6 +437,15 @@ SIGNATURES = {
     "gbx_groupby_set_strategy": (C.c_int, [C.c_void_p, C.c_int32]),
     "gbx_groupby_last_stats": (C.c_int, [C.c_void_p, C.POINTER(gbx_stats)]),
     "gbx_groupby_set_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "gbx_distinct_count": (
+        C.c_int, [C.POINTER(gbx_table_view), C.c_int32, C.c_void_p, C.POINTER(gbx_allocator), C.POINTER(C.c_int64)]),
+    "gbx_distinct_indices": (
+        C.c_int, [C.POINTER(gbx_table_view), C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(gbx_allocator),
+                  C.POINTER(gbx_column)]),
+    "gbx_distinct_join": (
+        C.c_int, [C.POINTER(gbx_table_view), C.POINTER(gbx_table_view), C.c_int32, C.c_int32, C.c_void_p,
+                  C.POINTER(gbx_allocator), C.POINTER(gbx_column), C.POINTER(gbx_column)]),
+    "gbx_column_release": (None, [C.POINTER(gbx_column), C.POINTER(gbx_allocator), C.c_void_p]),
     "gbx_groupby_aggregate_noalloc": (
         C.c_int,
         [C.c_void_p, C.POINTER(gbx_request), C.c_int32, C.c_void_p, C.POINTER(gbx_column), C.POINTER(gbx_column),

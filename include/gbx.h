@@ -561,6 +561,54 @@ GBX_API int gbx_server_last_stats(const gbx_server* server, gbx_server_stats* ou
 /* Finishes the admitted requests, fails the waiting ones, and frees the server. */
 GBX_API void gbx_server_destroy(gbx_server* server);
 
+/* ---- distinct rows and a distinct-key hash join on the same tables --------
+ * cudf::null_equality / nan_equality (types.hpp:143-154) and
+ * duplicate_keep_option (stream_compaction.hpp:225-230). */
+#define GBX_NULLS_EQUAL 0
+#define GBX_NULLS_UNEQUAL 1
+#define GBX_NANS_EQUAL 0   /* nan_equality::ALL_EQUAL */
+#define GBX_NANS_UNEQUAL 1
+typedef enum gbx_duplicate_keep {
+  GBX_KEEP_ANY   = 0,
+  GBX_KEEP_FIRST = 1,
+  GBX_KEEP_LAST  = 2,
+  GBX_KEEP_NONE  = 3
+} gbx_duplicate_keep;
+
+/* cudf::distinct_count(table_view, null_equality) (stream_compaction.hpp:422-424):
+ * the number of distinct rows of `keys` (NaNs equal, -0.0 == +0.0; under
+ * GBX_NULLS_UNEQUAL every row holding a null is distinct).  Synchronises
+ * `stream`. */
+GBX_API int gbx_distinct_count(const gbx_table_view* keys, int32_t nulls_equal, void* stream,
+                               const gbx_allocator* mr, int64_t* out);
+
+/* cudf::distinct_indices(table_view, keep, nulls_equal, nans_equal)
+ * (stream_compaction.hpp:311-317): an INT32 column of the row indices kept,
+ * one per distinct row (KEEP_ANY / FIRST / LAST: the first / first / last
+ * row of each; KEEP_NONE: rows whose key occurs once), in no particular
+ * order, allocated from `mr`.  Release it with gbx_column_release. */
+GBX_API int gbx_distinct_indices(const gbx_table_view* keys, int32_t keep, int32_t nulls_equal, int32_t nans_equal,
+                                 void* stream, const gbx_allocator* mr, gbx_column* out);
+
+/* cudf::distinct_hash_join(build, probe, has_nulls, compare_nulls)
+ * (join.hpp:494-533), the build side's keys distinct:
+ *   join_kind 0 (inner_join): `build_indices` / `probe_indices` INT32 columns
+ *     of the matching row pairs, in no particular order;
+ *   join_kind 1 (left_join): `build_indices` holds, for every probe row, its
+ *     build row or INT32_MIN (JoinNoneValue) and `probe_indices` is left
+ *     empty.
+ * Key columns must agree in count and type; dictionary keys are refused.
+ * NaN keys match NaN keys.  Under GBX_NULLS_UNEQUAL a key holding a null
+ * matches nothing.  A build key that occurs more than once answers its
+ * first row.  Columns are allocated from `mr`. */
+GBX_API int gbx_distinct_join(const gbx_table_view* build, const gbx_table_view* probe, int32_t compare_nulls,
+                              int32_t join_kind, void* stream, const gbx_allocator* mr, gbx_column* build_indices,
+                              gbx_column* probe_indices);
+
+/* Frees a column returned by gbx_distinct_indices / gbx_distinct_join with
+ * the allocator that made it. */
+GBX_API void gbx_column_release(gbx_column* col, const gbx_allocator* mr, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
