@@ -16,7 +16,8 @@ enum class interpolation : int32_t { LINEAR, LOWER, HIGHER, MIDPOINT, NEAREST };
 enum class sorted : bool { NO, YES };                // types.hpp:167
 enum class order : bool { ASCENDING, DESCENDING };
 enum class null_order : bool { AFTER, BEFORE };
-enum class null_equality : bool { EQUAL, UNEQUAL };
+enum class null_equality : bool { EQUAL, UNEQUAL };  // types.hpp:151-154
+enum class nan_equality { ALL_EQUAL, UNEQUAL };      // types.hpp:143-146
 
 enum class type_id : int32_t {
   EMPTY = GBX_TYPE_EMPTY,

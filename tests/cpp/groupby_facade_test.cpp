@@ -4,6 +4,8 @@
 // results are sorted by key before comparing, as groupby_test_util.cpp:89-96
 // does.  Prints one line per case and exits non-zero on any failure.
 #include <cudf/groupby.hpp>
+#include <cudf/join.hpp>
+#include <cudf/stream_compaction.hpp>
 
 #include <cuda_runtime_api.h>
 
@@ -12,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -267,6 +270,47 @@ int main()
     run_single(col(type_id::INT32, std::vector<int32_t>{}), col(type_id::INT32, std::vector<int32_t>{}),
                cudf::make_sum_aggregation<cudf::groupby_aggregation>(), k, kv, v, vv);
     CHECK(k.empty() && v.empty(), "empty result");
+  });
+  run("median / quantile / nunique / nth_element: median_tests.cpp:35 basic, quantile_tests.cpp:125, "
+      "nunique_tests.cpp:31, nth_element_tests.cpp:94", [] {
+    std::vector<int32_t> kk{1, 2, 3, 1, 2, 2, 1, 3, 3, 2};
+    std::vector<int32_t> vv{0, 1, 2, 3, 4, 5, 6, 7, 8, 9};
+    std::vector<int32_t> k; std::vector<int> kv, rv; std::vector<double> r;
+    run_single(col(type_id::INT32, kk), col(type_id::INT32, vv),
+               cudf::make_median_aggregation<cudf::groupby_aggregation>(), k, kv, r, rv);
+    expect_near(r, {3., 4.5, 7.}, rv);
+    std::vector<int32_t> nu; std::vector<int> nuv;
+    run_single(col(type_id::INT32, kk), col(type_id::INT32, vv),
+               cudf::make_nunique_aggregation<cudf::groupby_aggregation>(), k, kv, nu, nuv);
+    expect_equal(nu, std::vector<int32_t>{3, 4, 3}, "nunique");
+    std::vector<int32_t> nth; std::vector<int> nthv;
+    run_single(col(type_id::INT32, kk), col(type_id::INT32, vv),
+               cudf::make_nth_element_aggregation<cudf::groupby_aggregation>(-1), k, kv, nth, nthv);
+    expect_equal(nth, std::vector<int32_t>{6, 9, 8}, "nth_element(-1)");
+  });
+  run("distinct_count_tests.cpp:279 TableWithSomeNull; distinct_tests.cpp:219 NoNullsTable", [] {
+    auto c1 = col(type_id::INT32, std::vector<int32_t>{1, 2, 3, 4, 5, 6}, {1, 0, 1, 0, 1, 0});
+    auto c2 = col(type_id::INT32, std::vector<int32_t>{1, 1, 1, 1, 1, 1});
+    CHECK(cudf::distinct_count(cudf::table_view({c1, c2}), cudf::null_equality::EQUAL) == 4, "EQUAL");
+    CHECK(cudf::distinct_count(cudf::table_view({c1, c2}), cudf::null_equality::UNEQUAL) == 6, "UNEQUAL");
+    auto k1 = col(type_id::INT32, std::vector<int32_t>{20, 20, 20, 20, 19, 21, 9});
+    auto k2 = col(type_id::INT32, std::vector<int32_t>{19, 19, 19, 20, 20, 9, 21});
+    auto idx = cudf::distinct_indices(cudf::table_view({k1, k2}), cudf::duplicate_keep_option::KEEP_LAST);
+    auto got = host_values<int32_t>(idx->view());
+    std::sort(got.begin(), got.end());
+    expect_equal(got, std::vector<int32_t>{2, 3, 4, 5, 6}, "KEEP_LAST rows");
+  });
+  run("distinct_join_tests.cpp:406 LeftJoinWithNulls (string keys as codes)", [] {
+    auto b0 = col(type_id::INT32, std::vector<int32_t>{2, 2, 0, 4, 3});
+    auto b1 = col(type_id::INT32, std::vector<int32_t>{1, 0, 1, 2, 1});
+    auto p0 = col(type_id::INT32, std::vector<int32_t>{3, 1, 2, 0, 2});
+    auto p1 = col(type_id::INT32, std::vector<int32_t>{1, 1, 0, 4, 0}, {1, 1, 0, 1, 1});
+    cudf::distinct_hash_join join(cudf::table_view({b0, b1}), cudf::table_view({p0, p1}));
+    auto left = host_values<int32_t>(join.left_join()->view());
+    int32_t const none = std::numeric_limits<int32_t>::min();
+    expect_equal(left, std::vector<int32_t>{4, none, none, none, 1}, "left join");
+    auto [bi, pi] = join.inner_join();
+    CHECK(bi->size() == 2 && pi->size() == 2, "two pairs");
   });
   for (auto p : g_buffers) cudaFree(p);
   std::printf("%d failure(s)\n", g_failures);
