@@ -128,6 +128,30 @@ class Column:
                    indices.offset, null_count if mask is not None else indices._null_count,
                    dict_keys=keys, index_type_id=indices.type_id)
 
+    @classmethod
+    def from_strings(cls, values, valid: Optional[np.ndarray] = None, device="cuda") -> "Column":
+        """STRING column: UTF-8 characters in `data`, an INT32 offsets child
+        (held in `dict_keys`, as the C ABI passes it) and an optional mask
+        (None entries of `values` are nulls too)."""
+        vals = list(values)
+        ok = np.array([v is not None for v in vals], dtype=bool)
+        if valid is not None:
+            ok &= np.asarray(valid, dtype=bool)
+        enc = [(v if v is not None else "").encode("utf-8") for v in vals]
+        lens = np.array([len(b) for b in enc], dtype=np.int64)
+        offs = np.zeros(len(vals) + 1, dtype=np.int64)
+        np.cumsum(lens, out=offs[1:])
+        ow = np.int32 if offs[-1] < 2 ** 31 else np.int64
+        chars = np.frombuffer(b"".join(enc), dtype=np.uint8) if offs[-1] else np.zeros(1, np.uint8)
+        offsets = cls.from_numpy(offs.astype(ow), device=device)
+        data = _to_device(chars, device, False)
+        mask = None
+        nulls = 0
+        if not ok.all():
+            nulls = int(len(ok) - ok.sum())
+            mask = _to_device(pack_mask(ok), device, False)
+        return cls(TypeId.STRING, len(vals), data, mask, 0, nulls, dict_keys=offsets)
+
     def slice(self, begin: int, end: int) -> "Column":
         """A view of rows [begin, end) sharing this column's buffers (cudf::slice)."""
         return Column(self.type_id, end - begin, self.data, self.mask, self.offset + begin, None,
@@ -164,7 +188,17 @@ class Column:
 
     # ---- host conversion
     def to_numpy(self):
-        """(values, valid) on the host; valid is None when the column has no mask."""
+        """(values, valid) on the host; valid is None when the column has no mask.
+        A STRING column's values are a numpy object array of str."""
+        if self.type_id == TypeId.STRING:
+            offs = self.dict_keys.to_numpy()[0].astype(np.int64)
+            raw = self.data.detach().cpu().numpy().view(np.uint8).tobytes() if self.data is not None else b""
+            o = offs[self.offset: self.offset + self.size + 1]
+            vals = np.array([raw[o[i]:o[i + 1]].decode("utf-8") for i in range(self.size)], dtype=object)
+            valid = None
+            if self.mask is not None:
+                valid = unpack_mask(self.mask.detach().cpu().numpy(), self.size, self.offset)
+            return vals, valid
         if self.type_id == TypeId.DICTIONARY32:
             dt = storage_dtype(self.index_type_id)
         else:

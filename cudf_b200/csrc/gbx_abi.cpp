@@ -644,9 +644,17 @@ int gbx_groupby_create(const gbx_table_view* keys, int32_t null_policy, int32_t 
           k.dict_keys      = &gb->dict_keys[c];
           int32_t it       = k.index_type_id ? k.index_type_id : GBX_TYPE_INT32;
           GBX_EXPECTS(is_integral(it) && it != GBX_TYPE_BOOL8, "dictionary indices must be integers");
+        } else if (k.type_id == GBX_TYPE_STRING) {
+          // characters in `data`, the offsets column in `dict_keys`
+          GBX_EXPECTS(k.dict_keys != nullptr && (k.dict_keys->type_id == GBX_TYPE_INT32 ||
+                                                 k.dict_keys->type_id == GBX_TYPE_INT64),
+                      "a STRING key column needs its INT32 / INT64 offsets column");
+          GBX_EXPECTS(k.size == 0 || k.dict_keys->size >= k.offset + k.size + 1, "offsets column too short");
+          gb->dict_keys[c] = *k.dict_keys;
+          k.dict_keys      = &gb->dict_keys[c];
         } else if (!is_fixed_width(k.type_id)) {
-          fail(GBX_ERR_UNSUPPORTED,
-               "key type %d (string / list / struct / decimal128) is not supported by this library", k.type_id);
+          fail(GBX_ERR_UNSUPPORTED, "key type %d (list / struct / decimal128) is not supported by this library",
+               k.type_id);
         }
         GBX_EXPECTS(k.size >= 0 && k.offset >= 0, "negative size or offset");
         GBX_EXPECTS(k.size <= INT32_MAX, "row count exceeds cudf::size_type");
@@ -717,6 +725,8 @@ void gbx_result_release(gbx_result* r)
     }
   };
   for (int c = 0; c < r->num_key_columns; ++c) free_col(r->keys[c]);
+  if (in)
+    for (auto& b : in->extra) in->alloc.release(b.first, b.second);
   for (int q = 0; q < r->num_requests; ++q) {
     for (int k = 0; k < r->requests[q].num_results; ++k) free_col(r->requests[q].results[k]);
     delete[] r->requests[q].results;
@@ -740,6 +750,13 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     *out = nullptr;
     validate(gb, requests, num_requests);
 
+    if (keys_need_representatives(gb->keys, gb->null_policy)) {
+      // STRING keys, or keys beyond two packed 64-bit words (gbx_rep.cu)
+      gb->stats = gbx_stats{};
+      aggregate_by_representatives(gb, gb->keys, gb->null_policy, requests, num_requests, stream, mr, &res,
+                                   &gb->stats);
+      return;
+    }
     Call call{gb, requests, num_requests};
     call.alloc.st = static_cast<cudaStream_t>(stream);
     if (mr && mr->allocate && mr->deallocate) {
@@ -1469,6 +1486,9 @@ extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
     GBX_EXPECTS(gb != nullptr && num_groups != nullptr, "null argument");
     *num_groups = 0;
     validate(gb, requests, num_requests);
+    if (keys_need_representatives(gb->keys, gb->null_policy))
+      fail(GBX_ERR_UNSUPPORTED, "STRING keys and keys beyond 128 packed bits need scratch in proportion to the rows; "
+                                "use gbx_groupby_aggregate");
     for (int q = 0; q < num_requests; ++q)
       for (int k = 0; k < requests[q].num_aggregations; ++k)
         if (is_sort_kind(requests[q].aggregations[k].kind))

@@ -239,6 +239,26 @@ KeyPlan plan_keys(const gbx_table_view* keys, int32_t policy, const std::vector<
   return plan;
 }
 
+// The key columns as k_split_alone reads them (data, mask, offset, width,
+// float or not), whatever their packed width.
+KeyPlan key_columns(const gbx_table_view* keys)
+{
+  KeyPlan kp{};
+  kp.ncols = keys->num_columns;
+  for (int c = 0; c < keys->num_columns; ++c) {
+    const gbx_column_view& col = keys->columns[c];
+    const int32_t t = col.type_id == GBX_TYPE_DICTIONARY32 ? (col.index_type_id ? col.index_type_id : GBX_TYPE_INT32)
+                                                           : col.type_id;
+    KeyCol& kc  = kp.cols[c];
+    kc.data     = col.data;
+    kc.mask     = col.null_mask;
+    kc.offset   = col.offset;
+    kc.width    = static_cast<int8_t>(type_width(t));
+    kc.is_float = is_floating(t) ? 1 : 0;
+  }
+  return kp;
+}
+
 bool any_float_key(const gbx_table_view* keys)
 {
   for (int c = 0; c < keys->num_columns; ++c)
@@ -296,9 +316,7 @@ int gbx_distinct_count(const gbx_table_view* keys, int32_t nulls_equal, void* st
       // every row holding a null is a distinct row of its own
       Alloc a = make_alloc(mr, s);
       Scratch sc(&a);
-      std::vector<bool> nullable(keys->num_columns);
-      for (int c = 0; c < keys->num_columns; ++c) nullable[c] = keys->columns[c].null_mask != nullptr;
-      const KeyPlan kp = plan_keys(keys, GBX_NULL_INCLUDE, nullable);
+      const KeyPlan kp = key_columns(keys);
       auto* cnt        = static_cast<unsigned long long*>(sc.get(8));
       GBX_CUDA(cudaMemsetAsync(cnt, 0, 8, s));
       k_split_alone<<<grid_for_rows(n, current_device().num_sms), kBlock, 0, s>>>(kp, n, true, false, nullptr,
@@ -347,9 +365,7 @@ int gbx_distinct_indices(const gbx_table_view* keys, int32_t keep, int32_t nulls
     unsigned long long* nalone = nullptr;
     unsigned long long h_alone = 0;
     if (nulls_apart || nans_apart) {
-      std::vector<bool> nullable(nk);
-      for (int c = 0; c < nk; ++c) nullable[c] = keys->columns[c].null_mask != nullptr;
-      const KeyPlan kp = plan_keys(keys, GBX_NULL_INCLUDE, nullable);
+      const KeyPlan kp = key_columns(keys);
       nalone           = static_cast<unsigned long long*>(sc.get(8));
       GBX_CUDA(cudaMemsetAsync(nalone, 0, 8, s));
       if (nulls_apart) {

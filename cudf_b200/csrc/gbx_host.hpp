@@ -11,6 +11,7 @@
 #include <new>
 #include <string>
 #include <utility>
+#include <deque>
 #include <vector>
 
 #include "../../include/gbx.h"
@@ -145,6 +146,10 @@ void alloc_column(Alloc& a, gbx_column& c, int32_t type_id, int32_t scale, int64
 // (gbx_result_release).
 struct ResultInternal {
   gbx::Alloc alloc;
+  // buffers beyond the columns' own (STRING keys' offsets) and the child
+  // views the columns point at
+  std::vector<std::pair<void*, size_t>> extra;
+  std::deque<gbx_column_view> children;
 };
 
 namespace gbx {
@@ -154,6 +159,14 @@ namespace gbx {
 // verify_valid_requests (groupby.cu:176-192) and the size check of
 // groupby::aggregate (groupby.cu:210-214) for keys of `n` rows.
 void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n);
+
+// Keys that do not pack into two 64-bit words (STRING columns, or more than
+// 128 bits with the null bits) and the groupby over them: rows labelled by a
+// representative-row table, the groupby run on the label (gbx_rep.cu).
+bool keys_need_representatives(const std::vector<gbx_column_view>& keys, int32_t null_policy);
+int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
+                                 const gbx_request* requests, int32_t num_requests, void* stream,
+                                 const gbx_allocator* mr, gbx_result** out, gbx_stats* stats);
 
 // Null count of a column when known without a kernel (0 without a mask), else -1.
 int64_t exact_null_count_or_neg(const gbx_column_view& c);

@@ -1,0 +1,496 @@
+// gbx_rep.cu -- groupby over keys that do not pack into two 64-bit words:
+// STRING key columns, or fixed-width columns beyond 128 bits with their null
+// bits.
+//
+// Each row is labelled with the first row inserted of its key -- a table of
+// row indices probed by a hash of every key column and resolved by comparing
+// the rows' columns themselves, as the reference's set of representative rows
+// does for every key (hash/groupby.cu:571-593, row_operators.cuh:1339-1365,
+// 1429-1447).  The label is a plain INT32 key, so the groupby proper then runs
+// on it with every strategy of the packed-key path; the output keys are the
+// original key columns gathered at the representative rows.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <vector>
+
+#include "../../include/gbx.h"
+#include "gbx_host.hpp"
+#include "gbx_device.cuh"
+#include "gbx_kernels.hpp"
+#include "gbx_scan.hpp"
+
+namespace gbx {
+
+using namespace dev;
+
+namespace {
+
+constexpr int kRepBlock  = 256;
+constexpr int kKindFixed = 0, kKindF32 = 1, kKindF64 = 2, kKindBool = 3, kKindString = 4;
+
+// One key column as the representative table reads it.
+struct RepCol {
+  const void* data;      // fixed width: elements; STRING: characters
+  const uint32_t* mask;  // validity (nullptr: all valid)
+  int64_t offset;        // the view's first row
+  const void* offs;      // STRING: offsets (element offset + row)
+  int64_t offs_offset;   // STRING: the offsets view's own offset
+  int32_t width;         // fixed width: bytes; STRING: bytes of an offset (4 or 8)
+  int32_t kind;
+};
+
+struct RepKeys {
+  int32_t ncols;
+  int32_t exclude_nulls;  // EXCLUDE: a row with a null key takes no label
+  RepCol cols[kMaxKeyCols];
+};
+
+__device__ __forceinline__ uint64_t load_width(const void* p, int64_t i, int w)
+{
+  switch (w) {
+    case 1: return reinterpret_cast<const uint8_t*>(p)[i];
+    case 2: return reinterpret_cast<const uint16_t*>(p)[i];
+    case 4: return reinterpret_cast<const uint32_t*>(p)[i];
+    default: return reinterpret_cast<const uint64_t*>(p)[i];
+  }
+}
+
+// The value bits that decide equality: -0.0 and +0.0 one value, every NaN one
+// value (row_operators.cuh:1285-1312), booleans 0 / 1.
+__device__ __forceinline__ uint64_t norm_bits(const RepCol& c, int64_t r)
+{
+  const int64_t i  = r + c.offset;
+  const uint64_t b = load_width(c.data, i, c.width);
+  if (c.kind == kKindF32) {
+    const float f = __uint_as_float(static_cast<uint32_t>(b));
+    if (f != f) return 0x7fc00000u;
+    return f == 0.0f ? 0u : b;
+  }
+  if (c.kind == kKindF64) {
+    const double d = __longlong_as_double(static_cast<long long>(b));
+    if (d != d) return 0x7ff8000000000000ULL;
+    return d == 0.0 ? 0u : b;
+  }
+  if (c.kind == kKindBool) return b != 0;
+  return b;
+}
+
+__device__ __forceinline__ void str_span(const RepCol& c, int64_t r, int64_t& begin, int64_t& len)
+{
+  const int64_t i = r + c.offset + c.offs_offset;
+  const int64_t a = static_cast<int64_t>(load_width(c.offs, i, c.width));
+  const int64_t b = static_cast<int64_t>(load_width(c.offs, i + 1, c.width));
+  begin           = a;
+  len             = b - a;
+}
+
+// 64-bit hash of a row's key (a null contributes a marker of its own).
+__device__ __forceinline__ uint64_t rep_hash(const RepKeys& k, int64_t r)
+{
+  uint64_t h = 0x2545f4914f6cdd1dULL;
+  for (int c = 0; c < k.ncols; ++c) {
+    const RepCol& col = k.cols[c];
+    uint64_t v;
+    if (!bit_valid(col.mask, r + col.offset)) {
+      v = 0x9e3779b97f4a7c15ULL;
+    } else if (col.kind == kKindString) {
+      int64_t begin, len;
+      str_span(col, r, begin, len);
+      const auto* s = static_cast<const unsigned char*>(col.data) + begin;
+      uint64_t f    = 0xcbf29ce484222325ULL ^ static_cast<uint64_t>(len);  // FNV-1a over the bytes
+      for (int64_t j = 0; j < len; ++j) f = (f ^ s[j]) * 0x100000001b3ULL;
+      v = f;
+    } else {
+      v = norm_bits(col, r);
+    }
+    h = fmix64(h ^ (v + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2)));
+  }
+  return h;
+}
+
+__device__ __forceinline__ bool rep_equal(const RepKeys& k, int64_t a, int64_t b)
+{
+  for (int c = 0; c < k.ncols; ++c) {
+    const RepCol& col = k.cols[c];
+    const bool va     = bit_valid(col.mask, a + col.offset);
+    const bool vb     = bit_valid(col.mask, b + col.offset);
+    if (va != vb) return false;
+    if (!va) continue;  // nulls are equal (hash/groupby.cu:558)
+    if (col.kind == kKindString) {
+      int64_t ba, la, bb, lb;
+      str_span(col, a, ba, la);
+      str_span(col, b, bb, lb);
+      if (la != lb) return false;
+      const auto* s = static_cast<const unsigned char*>(col.data);
+      for (int64_t j = 0; j < la; ++j)
+        if (s[ba + j] != s[bb + j]) return false;
+    } else if (norm_bits(col, a) != norm_bits(col, b)) {
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool any_null(const RepKeys& k, int64_t r)
+{
+  for (int c = 0; c < k.ncols; ++c)
+    if (!bit_valid(k.cols[c].mask, r + k.cols[c].offset)) return true;
+  return false;
+}
+
+// rep[r] = the representative row of row r's key (-1: a null key under
+// EXCLUDE); `slots` holds row indices (-1: empty), probed linearly at most
+// cap times (S_TABLE_FULL beyond).
+__global__ void k_rep_insert(const __grid_constant__ RepKeys k, int64_t n, int32_t* __restrict__ slots, uint64_t cap,
+                             int32_t* __restrict__ rep, int32_t* status)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (k.exclude_nulls && any_null(k, r)) {
+      rep[r] = -1;
+      continue;
+    }
+    uint64_t s  = rep_hash(k, r) & (cap - 1);
+    int32_t out = -1;
+    for (uint64_t p = 0; p < cap; ++p) {
+      int32_t cur = slots[s];
+      if (cur < 0) {
+        const int32_t old = atomicCAS(slots + s, -1, static_cast<int32_t>(r));
+        if (old < 0) {
+          out = static_cast<int32_t>(r);
+          break;
+        }
+        cur = old;
+      }
+      if (rep_equal(k, cur, r)) {
+        out = cur;
+        break;
+      }
+      s = (s + 1) & (cap - 1);
+    }
+    if (out < 0) atomicOr(status, S_TABLE_FULL);
+    rep[r] = out;
+  }
+}
+
+// Validity words of the label column: rep >= 0.
+__global__ void k_rep_mask(const int32_t* __restrict__ rep, int64_t n, uint32_t* __restrict__ mask)
+{
+  const int lane       = threadIdx.x & 31;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t n_up   = (n + 31) & ~int64_t(31);
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n_up; r += stride) {
+    const uint32_t bal = __ballot_sync(0xffffffffu, r < n && rep[r] >= 0);
+    if (lane == 0) mask[r >> 5] = bal;
+  }
+}
+
+// Output key column c: element g = source row rows[g] (and its validity).
+__global__ void k_gather_fixed(const void* __restrict__ src, int64_t src_offset, const uint32_t* __restrict__ src_mask,
+                               int width, const int32_t* __restrict__ rows, int64_t G, void* __restrict__ dst,
+                               uint32_t* __restrict__ dst_mask, unsigned long long* nulls)
+{
+  const int lane       = threadIdx.x & 31;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t g_up   = (G + 31) & ~int64_t(31);
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < g_up; g += stride) {
+    bool valid = false;
+    if (g < G) {
+      const int64_t r = rows[g];
+      valid           = bit_valid(src_mask, r + src_offset);
+      const uint64_t v = load_width(src, r + src_offset, width);
+      switch (width) {
+        case 1: reinterpret_cast<uint8_t*>(dst)[g] = static_cast<uint8_t>(v); break;
+        case 2: reinterpret_cast<uint16_t*>(dst)[g] = static_cast<uint16_t>(v); break;
+        case 4: reinterpret_cast<uint32_t*>(dst)[g] = static_cast<uint32_t>(v); break;
+        default: reinterpret_cast<uint64_t*>(dst)[g] = v; break;
+      }
+    }
+    const uint32_t act = __ballot_sync(0xffffffffu, g < G);
+    const uint32_t bal = __ballot_sync(0xffffffffu, g < G && valid);
+    if (dst_mask != nullptr && lane == 0 && act) {
+      dst_mask[g >> 5] = bal;
+      const uint32_t nn = __popc(act & ~bal);
+      if (nn) atomicAdd(nulls, static_cast<unsigned long long>(nn));
+    }
+  }
+}
+
+// Validity words of a gathered column (null counts added to *nulls).
+__global__ void k_gather_valid(const uint32_t* __restrict__ src_mask, int64_t src_offset,
+                               const int32_t* __restrict__ rows, int64_t G, uint32_t* __restrict__ dst_mask,
+                               unsigned long long* nulls)
+{
+  const int lane       = threadIdx.x & 31;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t g_up   = (G + 31) & ~int64_t(31);
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < g_up; g += stride) {
+    const bool valid   = g < G && bit_valid(src_mask, rows[g] + src_offset);
+    const uint32_t act = __ballot_sync(0xffffffffu, g < G);
+    const uint32_t bal = __ballot_sync(0xffffffffu, valid);
+    if (lane == 0 && act) {
+      dst_mask[g >> 5] = bal;
+      const uint32_t nn = __popc(act & ~bal);
+      if (nn) atomicAdd(nulls, static_cast<unsigned long long>(nn));
+    }
+  }
+}
+
+// STRING output: lengths of the gathered rows (0 for a null row).
+__global__ void k_gather_str_len(const __grid_constant__ RepCol c, const int32_t* __restrict__ rows, int64_t G,
+                                 int64_t* __restrict__ len)
+{
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = rows[g];
+    int64_t b = 0, l = 0;
+    if (bit_valid(c.mask, r + c.offset)) str_span(c, r, b, l);
+    len[g] = l;
+  }
+}
+
+// STRING output: one warp copies each row's characters to its new offset.
+__global__ void k_gather_str_copy(const __grid_constant__ RepCol c, const int32_t* __restrict__ rows, int64_t G,
+                                  const int64_t* __restrict__ out_offs, unsigned char* __restrict__ out_chars)
+{
+  const int lane  = threadIdx.x & 31;
+  const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t g = w; g < G; g += nw) {
+    const int64_t r = rows[g];
+    if (!bit_valid(c.mask, r + c.offset)) continue;
+    int64_t b, l;
+    str_span(c, r, b, l);
+    const auto* s = static_cast<const unsigned char*>(c.data) + b;
+    unsigned char* d = out_chars + out_offs[g];
+    for (int64_t j = lane; j < l; j += 32) d[j] = s[j];
+  }
+}
+
+__global__ void k_offsets_out(const int64_t* __restrict__ excl, const int64_t* __restrict__ len, int64_t G,
+                              int width, void* __restrict__ out)
+{
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g <= G;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t v = g < G ? excl[g] : (G > 0 ? excl[G - 1] + len[G - 1] : 0);
+    if (width == 4) reinterpret_cast<int32_t*>(out)[g] = static_cast<int32_t>(v);
+    else reinterpret_cast<int64_t*>(out)[g] = v;
+  }
+}
+
+__global__ void k_fill_i32(int32_t* p, int32_t v, int64_t n)
+{
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+
+int grid_of(int64_t n, int num_sms)
+{
+  const int64_t b = (n + kRepBlock - 1) / kRepBlock;
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, int64_t(num_sms) * 8)));
+}
+
+RepKeys rep_keys(const std::vector<gbx_column_view>& keys, int32_t null_policy)
+{
+  RepKeys k{};
+  k.ncols         = static_cast<int32_t>(keys.size());
+  k.exclude_nulls = null_policy == GBX_NULL_EXCLUDE ? 1 : 0;
+  for (size_t c = 0; c < keys.size(); ++c) {
+    const gbx_column_view& v = keys[c];
+    RepCol& rc               = k.cols[c];
+    rc.mask                  = v.null_count == 0 ? nullptr : v.null_mask;
+    rc.offset                = v.offset;
+    rc.data                  = v.data;
+    if (v.type_id == GBX_TYPE_STRING) {
+      rc.kind        = kKindString;
+      rc.offs        = v.dict_keys->data;
+      rc.offs_offset = v.dict_keys->offset;
+      rc.width       = type_width(v.dict_keys->type_id);
+    } else {
+      const int32_t t = v.type_id == GBX_TYPE_DICTIONARY32 ? (v.index_type_id ? v.index_type_id : GBX_TYPE_INT32)
+                                                           : v.type_id;
+      rc.width = type_width(t);
+      rc.kind  = t == GBX_TYPE_FLOAT32 ? kKindF32 : t == GBX_TYPE_FLOAT64 ? kKindF64 : t == GBX_TYPE_BOOL8 ? kKindBool
+                                                                                                         : kKindFixed;
+    }
+  }
+  return k;
+}
+
+}  // namespace
+
+bool keys_need_representatives(const std::vector<gbx_column_view>& keys, int32_t null_policy)
+{
+  for (const auto& k : keys)
+    if (k.type_id == GBX_TYPE_STRING) return true;
+  bool ok = true;
+  (void)make_key_plan(keys.data(), static_cast<int>(keys.size()), null_policy,
+                      std::vector<int64_t>(keys.size(), -1), ok);
+  return !ok;
+}
+
+int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
+                                 const gbx_request* requests, int32_t num_requests, void* stream,
+                                 const gbx_allocator* mr, gbx_result** out, gbx_stats* stats)
+{
+  (void)gb;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Alloc a;
+  a.st = s;
+  if (mr && mr->allocate && mr->deallocate) {
+    a.user     = *mr;
+    a.has_user = true;
+  }
+  const int64_t n   = keys.empty() ? 0 : keys[0].size;
+  const int num_sms = current_device().num_sms;
+  Scratch sc(&a);
+
+  // labels: each row's representative row
+  const RepKeys rk  = rep_keys(keys, null_policy);
+  const uint64_t cap = next_pow2(std::max<uint64_t>(2 * static_cast<uint64_t>(n) + 2, 64));
+  auto* slots  = static_cast<int32_t*>(sc.get(cap * 4));
+  auto* rep    = static_cast<int32_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(n, 1)) * 4));
+  auto* status = static_cast<int32_t*>(sc.get(8));
+  auto* mask   = static_cast<uint32_t*>(sc.get(static_cast<size_t>((n + 31) / 32) * 4 + 64));
+  GBX_CUDA(cudaMemsetAsync(status, 0, 8, s));
+  k_fill_i32<<<grid_of(static_cast<int64_t>(cap), num_sms), kRepBlock, 0, s>>>(slots, -1, static_cast<int64_t>(cap));
+  GBX_CUDA(cudaGetLastError());
+  if (n > 0) {
+    k_rep_insert<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rk, n, slots, cap, rep, status);
+    GBX_CUDA(cudaGetLastError());
+    if (rk.exclude_nulls) {
+      k_rep_mask<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, mask);
+      GBX_CUDA(cudaGetLastError());
+    }
+  }
+  int32_t h_status = 0;
+  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaStreamSynchronize(s));
+  if (h_status & S_TABLE_FULL) fail(GBX_ERR_DEVICE, "representative table overflow (status 0x%x)", h_status);
+
+  // the groupby on the label
+  gbx_column_view label{};
+  label.type_id    = GBX_TYPE_INT32;
+  label.size       = n;
+  label.data       = rep;
+  label.null_mask  = rk.exclude_nulls ? mask : nullptr;
+  label.null_count = rk.exclude_nulls ? -1 : 0;
+  gbx_table_view tv{1, 0, &label};
+  gbx_groupby* inner = nullptr;
+  gbx_result* ir     = nullptr;
+  int st             = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
+  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &ir);
+  if (st == GBX_OK && stats) gbx_groupby_last_stats(inner, stats);
+  if (inner) gbx_groupby_destroy(inner);
+  if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+
+  // the result: the inner results, and the key columns gathered at the labels
+  const int64_t G     = ir->num_groups;
+  const auto* rows    = static_cast<const int32_t*>(ir->keys[0].data);
+  const int nkeys     = static_cast<int>(keys.size());
+  auto* res           = new gbx_result();
+  std::memset(res, 0, sizeof(*res));
+  auto* internal      = new ResultInternal{a, {}, {}};
+  res->internal        = internal;
+  res->num_key_columns = nkeys;
+  res->num_requests    = ir->num_requests;
+  res->num_groups      = G;
+  res->keys            = new gbx_column[nkeys > 0 ? nkeys : 1]();
+  res->requests        = ir->requests;  // the inner result's request columns move over
+  ir->requests         = nullptr;
+  ir->num_requests     = 0;
+  // the same allocator made them: the outer result releases them
+  auto* nulls = static_cast<unsigned long long*>(sc.get(8 * kMaxKeyCols));
+  GBX_CUDA(cudaMemsetAsync(nulls, 0, 8 * kMaxKeyCols, s));
+  for (int c = 0; c < nkeys; ++c) {
+    const gbx_column_view& kv = keys[c];
+    gbx_column& oc            = res->keys[c];
+    const bool with_mask      = kv.null_mask != nullptr && kv.null_count != 0 && null_policy == GBX_NULL_INCLUDE;
+    if (kv.type_id == GBX_TYPE_STRING) {
+      alloc_column(a, oc, GBX_TYPE_STRING, 0, 0, false);
+      const RepCol& rc = rk.cols[c];
+      auto* len        = static_cast<int64_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 8));
+      auto* excl       = static_cast<int64_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 8));
+      int64_t total    = 0;
+      if (G > 0) {
+        k_gather_str_len<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(rc, rows, G, len);
+        GBX_CUDA(cudaGetLastError());
+        size_t tb = 0;
+        GBX_CUDA(scan_exclusive_i64(nullptr, nullptr, G, nullptr, &tb, s));
+        void* temp = sc.get(tb);
+        GBX_CUDA(scan_exclusive_i64(len, excl, G, temp, &tb, s));
+        int64_t last[2] = {0, 0};
+        GBX_CUDA(cudaMemcpyAsync(&last[0], excl + G - 1, 8, cudaMemcpyDeviceToHost, s));
+        GBX_CUDA(cudaMemcpyAsync(&last[1], len + G - 1, 8, cudaMemcpyDeviceToHost, s));
+        GBX_CUDA(cudaStreamSynchronize(s));
+        total = last[0] + last[1];
+      }
+      const int ow          = total < (int64_t(1) << 31) ? 4 : 8;
+      const size_t ob       = static_cast<size_t>(G + 1) * ow;
+      void* offs_buf        = a.allocate(ob);
+      internal->extra.emplace_back(offs_buf, ob);
+      oc.data_bytes         = static_cast<size_t>(std::max<int64_t>(total, 1));
+      oc.data               = a.allocate(oc.data_bytes);
+      k_offsets_out<<<grid_of(G + 1, num_sms), kRepBlock, 0, s>>>(excl, len, G, ow, offs_buf);
+      GBX_CUDA(cudaGetLastError());
+      if (total > 0) {
+        k_gather_str_copy<<<grid_of(G * 32, num_sms), kRepBlock, 0, s>>>(rc, rows, G, excl,
+                                                                         static_cast<unsigned char*>(oc.data));
+        GBX_CUDA(cudaGetLastError());
+      }
+      gbx_column_view ov{};
+      ov.type_id    = ow == 4 ? GBX_TYPE_INT32 : GBX_TYPE_INT64;
+      ov.size       = G + 1;
+      ov.data       = offs_buf;
+      internal->children.push_back(ov);
+      oc.view.type_id   = GBX_TYPE_STRING;
+      oc.view.size      = G;
+      oc.view.data      = oc.data;
+      oc.view.dict_keys = &internal->children.back();
+      if (with_mask) {
+        const size_t words = static_cast<size_t>((G + 31) / 32);
+        oc.mask_bytes      = ((words * 4 + 63) / 64) * 64;
+        oc.null_mask       = G > 0 ? static_cast<uint32_t*>(a.allocate(oc.mask_bytes)) : nullptr;
+        oc.view.null_mask  = oc.null_mask;
+        if (G > 0) {
+          k_gather_valid<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(kv.null_mask, kv.offset, rows, G, oc.null_mask,
+                                                                   nulls + c);
+          GBX_CUDA(cudaGetLastError());
+        }
+      }
+    } else {
+      alloc_column(a, oc, kv.type_id, kv.scale, G, with_mask);
+      if (kv.type_id == GBX_TYPE_DICTIONARY32) {
+        const int32_t it = kv.index_type_id ? kv.index_type_id : GBX_TYPE_INT32;
+        oc.view.index_type_id = it;
+        oc.view.dict_keys     = kv.dict_keys;
+        if (type_width(it) != 4) {
+          a.release(oc.data, oc.data_bytes);
+          oc.data_bytes = static_cast<size_t>(G) * type_width(it);
+          oc.data       = G > 0 ? a.allocate(oc.data_bytes) : nullptr;
+          oc.view.data  = oc.data;
+        }
+      }
+      if (G > 0) {
+        k_gather_fixed<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(kv.data, kv.offset, with_mask ? kv.null_mask : nullptr,
+                                                                  rk.cols[c].width, rows, G, oc.data, oc.null_mask,
+                                                                  nulls + c);
+        GBX_CUDA(cudaGetLastError());
+      }
+    }
+  }
+  unsigned long long h_nulls[kMaxKeyCols] = {};
+  GBX_CUDA(cudaMemcpyAsync(h_nulls, nulls, 8 * kMaxKeyCols, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaStreamSynchronize(s));
+  for (int c = 0; c < nkeys; ++c)
+    res->keys[c].view.null_count = res->keys[c].null_mask ? static_cast<int64_t>(h_nulls[c]) : 0;
+  gbx_result_release(ir);
+  *out = res;
+  return GBX_OK;
+}
+
+}  // namespace gbx

@@ -415,7 +415,7 @@ int gbx_server_submit(gbx_server* s, const gbx_table_view* keys, const gbx_reque
         j->key_dicts[c]      = *j->keys[c].dict_keys;
         j->keys[c].dict_keys = &j->key_dicts[c];
       }
-      if (j->keys[c].type_id == GBX_TYPE_DICTIONARY32) j->mergeable = false;
+      if (j->keys[c].type_id == GBX_TYPE_DICTIONARY32 || j->keys[c].type_id == GBX_TYPE_STRING) j->mergeable = false;
       GBX_EXPECTS(j->keys[c].size == j->keys[0].size, "key columns differ in size");
     }
     j->rows = j->keys[0].size;

@@ -71,6 +71,12 @@ def _result_column(col: _abi.gbx_column, alloc: TorchAllocator, keys_of=None) ->
     if mask is not None:
         mask = mask.view(torch.int32)
     nc = v.null_count if v.null_count >= 0 else None
+    if v.type_id == _abi.TypeId.STRING:
+        # the characters, and the offsets child the result also owns
+        ov = v.dict_keys.contents
+        offs = alloc.take(ov.data)
+        offsets = Column(ov.type_id, ov.size, offs, None, 0, 0)
+        return Column(_abi.TypeId.STRING, v.size, data, mask, 0, nc, dict_keys=offsets)
     return Column(v.type_id, v.size, data, mask, 0, nc, dict_keys=keys_of,
                   index_type_id=v.index_type_id if v.type_id == _abi.TypeId.DICTIONARY32 else _abi.TypeId.INT32,
                   scale=v.scale)

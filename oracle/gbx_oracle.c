@@ -289,11 +289,31 @@ static uint64_t fmix64(uint64_t k)
   return k;
 }
 
+/* STRING element `row`: its bytes and length (the offsets child in dict_keys). */
+static const unsigned char* str_at(const gbx_column_view* c, int64_t row, int64_t* len)
+{
+  const gbx_column_view* o = c->dict_keys;
+  int w                    = type_width(o->type_id);
+  int64_t i                = row + c->offset + o->offset;
+  int64_t a                = w == 4 ? ((const int32_t*)o->data)[i] : ((const int64_t*)o->data)[i];
+  int64_t b                = w == 4 ? ((const int32_t*)o->data)[i + 1] : ((const int64_t*)o->data)[i + 1];
+  *len                     = b - a;
+  return (const unsigned char*)c->data + a;
+}
+
 /* Normalised bits of a key element: -0.0 -> +0.0 and every NaN -> one NaN,
  * as normalize_nans_and_zeros does before hashing (hash_functions.cuh:41-47). */
 static uint64_t key_bits(const gbx_column_view* c, int64_t row)
 {
   if (c->type_id == GBX_TYPE_DICTIONARY32) return (uint64_t)dict_index(c, row);
+  if (c->type_id == GBX_TYPE_STRING) {
+    /* a hash of the bytes (equality compares the bytes themselves) */
+    int64_t len;
+    const unsigned char* s = str_at(c, row, &len);
+    uint64_t h             = 1469598103934665603ULL ^ (uint64_t)len;
+    for (int64_t j = 0; j < len; ++j) h = (h ^ s[j]) * 1099511628211ULL;
+    return h;
+  }
   scalar s = read_fixed(c, row);
   switch (type_cat(c->type_id)) {
     case CAT_SIGNED:
@@ -337,6 +357,13 @@ static int row_equal(const row_ops* ops, int64_t a, int64_t b)
       int va = col_valid(col, a), vb = col_valid(col, b);
       if (!va && !vb) continue;
       if (va != vb) return 0;
+    }
+    if (col->type_id == GBX_TYPE_STRING) {
+      int64_t la, lb;
+      const unsigned char* sa = str_at(col, a, &la);
+      const unsigned char* sb = str_at(col, b, &lb);
+      if (la != lb || (la > 0 && memcmp(sa, sb, (size_t)la) != 0)) return 0;
+      continue;
     }
     if (key_bits(col, a) != key_bits(col, b)) return 0;
   }
@@ -609,6 +636,8 @@ static int validate(const gbx_table_view* keys, const gbx_request* reqs, int32_t
     if (k->size != n) return set_err(GBX_ERR_LOGIC, "key columns differ in size");
     if (k->type_id == GBX_TYPE_DICTIONARY32) {
       if (!k->dict_keys) return set_err(GBX_ERR_LOGIC, "dictionary key column without keys");
+    } else if (k->type_id == GBX_TYPE_STRING) {
+      if (!k->dict_keys) return set_err(GBX_ERR_LOGIC, "STRING key column without offsets");
     } else if (!is_fixed_width(k->type_id)) {
       return set_err(GBX_ERR_UNSUPPORTED, "key type %d not supported", k->type_id);
     }
@@ -970,6 +999,24 @@ int gbo_groupby(const gbx_table_view* keys,
       if (kc->type_id == GBX_TYPE_DICTIONARY32) {
         oc->data = xcalloc((size_t)ng, 4);
         for (int64_t g = 0; g < ng; ++g) ((int32_t*)oc->data)[g] = (int32_t)dict_index(kc, rep[g]);
+      } else if (kc->type_id == GBX_TYPE_STRING) {
+        /* the representative rows' strings (a null key's is empty) */
+        oc->str_offsets = (int64_t*)xcalloc((size_t)ng + 1, sizeof(int64_t));
+        int64_t total   = 0;
+        for (int64_t g = 0; g < ng; ++g) {
+          int64_t len = 0;
+          if (col_valid(kc, rep[g])) (void)str_at(kc, rep[g], &len);
+          oc->str_offsets[g] = total;
+          total += len;
+        }
+        oc->str_offsets[ng] = total;
+        oc->data            = xcalloc((size_t)(total ? total : 1), 1);
+        for (int64_t g = 0; g < ng; ++g) {
+          int64_t len = 0;
+          if (!col_valid(kc, rep[g])) continue;
+          const unsigned char* s = str_at(kc, rep[g], &len);
+          if (len) memcpy((unsigned char*)oc->data + oc->str_offsets[g], s, (size_t)len);
+        }
       } else {
         oc->data = xcalloc((size_t)ng, (size_t)type_width(kc->type_id));
         for (int64_t g = 0; g < ng; ++g) {
@@ -1052,6 +1099,7 @@ void gbo_result_free(gbo_result* r)
   for (int c = 0; c < r->num_key_columns; ++c) {
     free(r->keys[c].data);
     free(r->keys[c].valid);
+    free(r->keys[c].str_offsets);
   }
   free(r->keys);
   for (int q = 0; q < r->num_requests; ++q) {

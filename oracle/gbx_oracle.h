@@ -27,7 +27,10 @@ typedef struct gbo_column {
   int64_t size;
   void* data;
   uint8_t* valid;
-  /* DICTIONARY32 output keys: data holds int32 indices into the input's keys */
+  /* DICTIONARY32 output keys: data holds int32 indices into the input's keys;
+   * STRING output keys: data holds the characters and str_offsets the
+   * size + 1 offsets into them */
+  int64_t* str_offsets;
 } gbo_column;
 
 typedef struct gbo_result {

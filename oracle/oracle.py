@@ -38,6 +38,7 @@ class gbo_column(C.Structure):
         ("size", C.c_int64),
         ("data", C.c_void_p),
         ("valid", C.POINTER(C.c_uint8)),
+        ("str_offsets", C.POINTER(C.c_int64)),
     ]
 
 
@@ -86,6 +87,21 @@ class HostCol:
     _keep: list = field(default_factory=list, repr=False)
 
     def __post_init__(self):
+        if self.type_id == TypeId.STRING:
+            # str (or None: null) values; UTF-8 characters and int64 offsets for the view
+            self.values = np.array(list(self.values), dtype=object)
+            ok = np.array([v is not None for v in self.values], dtype=bool)
+            if self.valid is not None:
+                ok &= np.asarray(self.valid, dtype=bool)
+            self.valid = None if ok.all() else ok
+            enc = [(v if v is not None else "").encode("utf-8") for v in self.values]
+            offs = np.zeros(len(enc) + 1, dtype=np.int64)
+            np.cumsum([len(b) for b in enc], out=offs[1:])
+            self._chars = np.frombuffer(b"".join(enc) or b"\0", dtype=np.uint8).copy()
+            self.dict_keys = HostCol(offs)
+            if self.size is None:
+                self.size = len(self.values) - self.offset
+            return
         self.values = np.asarray(self.values)
         if self.dict_keys is not None:
             self.type_id = TypeId.DICTIONARY32
@@ -110,7 +126,10 @@ class HostCol:
         v.scale = self.scale
         v.size = self.size
         v.offset = self.offset
-        vals = np.ascontiguousarray(self.values)
+        if self.type_id == TypeId.STRING:
+            vals = self._chars
+        else:
+            vals = np.ascontiguousarray(self.values)
         self._keep = [vals]
         v.data = vals.ctypes.data if len(vals) else None
         if self.valid is not None:
@@ -125,12 +144,20 @@ class HostCol:
             kv = self.dict_keys.view()
             self._keep.append(kv)
             v.dict_keys = C.pointer(kv)
-            v.index_type_id = int(self.index_type)
+            v.index_type_id = int(self.index_type) if self.type_id == TypeId.DICTIONARY32 else 0
         return v
 
 
 def _np_of(col: gbo_column, n: int) -> Tuple[int, np.ndarray, Optional[np.ndarray]]:
     tid = TypeId(col.type_id)
+    if tid == TypeId.STRING:
+        offs = np.ctypeslib.as_array(col.str_offsets, shape=(n + 1,)).copy() if col.str_offsets else np.zeros(1, np.int64)
+        raw = bytes((C.c_uint8 * int(offs[-1])).from_address(col.data)) if offs[-1] else b""
+        vals = np.array([raw[offs[i]:offs[i + 1]].decode("utf-8") for i in range(n)], dtype=object)
+        valid = None
+        if col.valid:
+            valid = np.ctypeslib.as_array(col.valid, shape=(n,)).astype(bool).copy() if n else np.zeros(0, bool)
+        return int(tid), vals, valid
     dt = np.dtype(np.int32) if tid == TypeId.DICTIONARY32 else storage_dtype(tid)
     if n == 0 or not col.data:
         vals = np.zeros(0, dtype=dt)

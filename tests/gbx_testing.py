@@ -42,7 +42,9 @@ def device_column(h: HostCol):
     """HostCol -> cudf_b200.Column on cuda:0 (same bytes, same offset and size)."""
     from cudf_b200 import Column
 
-    if h.dict_keys is not None:
+    if h.type_id == TypeId.STRING:
+        col = Column.from_strings(h.values, h.valid)
+    elif h.dict_keys is not None:
         idx = Column.from_numpy(h.values, h.valid)
         keys = device_column(h.dict_keys)
         col = Column.dictionary(idx, keys)
@@ -91,6 +93,10 @@ def _sort_key_columns(keys):
             v = np.where(np.isnan(v), np.inf, v)  # NaN keys sort last
             v = np.where(v == 0, 0.0, v)
         nul = np.zeros(len(v), dtype=np.int8) if valid is None else (~valid).astype(np.int8)
+        if v.dtype == object:  # strings: nulls as ""
+            vv = np.array(["" if n else x for x, n in zip(v, nul)], dtype=object)
+            cols.append((nul, vv))
+            continue
         vv = np.where(nul == 1, np.zeros(1, dtype=v.dtype), v)
         cols.append((nul, vv))
     return cols

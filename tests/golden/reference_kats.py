@@ -250,6 +250,10 @@ def cases():
     out.append(_case("keys_tests.cpp:338-365 dictionary_keys basic", T.INT32, [0, 1, 2, 0, 1, 1, 0, 2, 2, 1], T.INT32,
                      V10, Kind.SUM, [0, 1, 2], [9, 19, 17], rtype=T.INT64, kdict=True))
     out += sort_path_cases()
+    # keys_tests.cpp:318-333 groupby_string_keys_test basic: STRING keys
+    out.append(_case("keys_tests.cpp:318-333 string_keys basic", T.STRING,
+                     ["aaa", "año", "₹1", "aaa", "año", "año", "aaa", "₹1", "₹1", "año"], T.INT32, V10, Kind.SUM,
+                     ["aaa", "año", "₹1"], [9, 19, 17], rtype=T.INT64))
     return out
 
 

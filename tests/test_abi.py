@@ -177,12 +177,24 @@ def test_invalid_type_agg_combination_is_logic_error():
     lib.gbx_groupby_destroy(h)
 
 
-def test_create_rejects_string_keys_and_bad_policy():
+def test_create_checks_key_columns_and_policy():
+    """A STRING key needs its offsets child; list / struct keys are refused."""
     lib = _lib.lib()
     tv, keep = _keys_view(3)
     h = C.c_void_p()
     assert lib.gbx_groupby_create(C.byref(tv), 7, 0, C.byref(h)) == _abi.Status.ERR_LOGIC
     keep[1][0].type_id = TypeId.STRING
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == _abi.Status.ERR_LOGIC
+    assert b"offsets" in lib.gbx_last_error()
+    offs = np.array([0, 1, 2, 3], dtype=np.int32)
+    ov = _abi.gbx_column_view()
+    ov.type_id = TypeId.INT32
+    ov.size = 4
+    ov.data = offs.ctypes.data
+    keep[1][0].dict_keys = C.pointer(ov)
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == _abi.Status.OK
+    lib.gbx_groupby_destroy(h)
+    keep[1][0].type_id = TypeId.LIST
     assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == _abi.Status.ERR_UNSUPPORTED
 
 

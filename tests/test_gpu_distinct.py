@@ -41,14 +41,6 @@ def nan_eq(b):
 def test_distinct_count_kat(case):
     cid, spec, eq, uneq = case
     t = dev_table(spec)
-    if "TableMixedTypes" in cid:
-        # int32 + float64 + uint32 values and three null bits: 131 packed
-        # bits, beyond the two 64-bit table words (refused, not mis-answered)
-        from cudf_b200 import UnsupportedError
-
-        with pytest.raises(UnsupportedError, match="128 packed bits"):
-            sc.distinct_count(t, NullEquality.EQUAL)
-        return
     assert sc.distinct_count(t, NullEquality.EQUAL) == eq
     assert sc.distinct_count(t, NullEquality.UNEQUAL) == uneq
 

@@ -88,16 +88,14 @@ def test_two_word_keys_with_nulls_include():
     T.assert_parity([hc(a, va), hc(b, vb)], [(hc(v), ALL6)], NullPolicy.EXCLUDE)
 
 
-def test_keys_wider_than_128_bits_are_reported():
-    """Two int64 keys plus their null bits need 130 packed bits: a clear
-    UNSUPPORTED error, not a wrong answer."""
-    from cudf_b200 import UnsupportedError
-
+def test_keys_wider_than_128_bits():
+    """Two nullable int64 keys need 130 packed bits: the rows are labelled
+    by a representative-row table and grouped on the label."""
     n = 1000
-    a = np.arange(n, dtype=np.int64)
+    a = np.arange(n, dtype=np.int64) % 37
     va = np.arange(n) % 3 > 0
-    with pytest.raises(UnsupportedError, match="128 packed bits"):
-        T.run_gpu([hc(a, va), hc(a, va)], [(hc(a), [(Kind.SUM, 0)])], NullPolicy.INCLUDE)
+    for policy in (NullPolicy.EXCLUDE, NullPolicy.INCLUDE):
+        T.assert_parity([hc(a, va), hc(a * 3, va)], [(hc(a), [(Kind.SUM, 0)])], policy)
 
 
 def test_all_distinct_and_all_equal_keys():

@@ -18,6 +18,9 @@ CASES = KAT.cases()
 
 def _host(vals, valid, tid, scale=0, as_dict=False, offset=0, size=None):
     tid = TypeId(tid)
+    if tid == TypeId.STRING:
+        return HostCol(list(vals), None if valid is None else np.array(valid, bool), type_id=tid, offset=offset,
+                       size=size)
     if tid == TypeId.BOOL8:
         arr = np.array([bool(v) for v in vals], dtype=np.uint8)
     else:
@@ -44,7 +47,10 @@ def build(case):
 
 def expected(case):
     kt = TypeId.INT32 if case["key_dict"] else TypeId(case["key_type"])
-    ek = np.array(case["expect_keys"], dtype=storage_dtype(kt)) if case["expect_keys"] else np.zeros(0, storage_dtype(kt))
+    if kt == TypeId.STRING:
+        ek = np.array(case["expect_keys"], dtype=object)
+    else:
+        ek = np.array(case["expect_keys"], dtype=storage_dtype(kt)) if case["expect_keys"] else np.zeros(0, storage_dtype(kt))
     ekv = None if case["expect_key_valid"] is None else np.array(case["expect_key_valid"], bool)
     rt = TypeId(case["result_type"])
     if rt == TypeId.BOOL8:
