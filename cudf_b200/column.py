@@ -142,7 +142,7 @@ class Column:
         offs = np.zeros(len(vals) + 1, dtype=np.int64)
         np.cumsum(lens, out=offs[1:])
         ow = np.int32 if offs[-1] < 2 ** 31 else np.int64
-        chars = np.frombuffer(b"".join(enc), dtype=np.uint8) if offs[-1] else np.zeros(1, np.uint8)
+        chars = np.frombuffer(b"".join(enc), dtype=np.uint8).copy() if offs[-1] else np.zeros(1, np.uint8)
         offsets = cls.from_numpy(offs.astype(ow), device=device)
         data = _to_device(chars, device, False)
         mask = None

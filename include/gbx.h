@@ -117,6 +117,10 @@ typedef enum gbx_agg_kind {
  * For DICTIONARY32 columns `data` holds the indices (of integer type
  * `index_type_id`, default INT32) and `dict_keys` the dictionary's keys column;
  * `null_mask` is the dictionary's own mask.  DECIMAL32/64 carry `scale`.
+ * For STRING key columns `data` holds the UTF-8 characters and `dict_keys`
+ * the offsets column (INT32 or INT64, at least offset + size + 1 rows; row r's
+ * characters are data[offsets[offset + r]] up to offsets[offset + r + 1]), as
+ * a cudf strings column holds its offsets child.
  * `null_count` may be -1 (unknown): the library then counts nulls itself.
  */
 typedef struct gbx_column_view {
