@@ -745,6 +745,7 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
                           gbx_result** out)
 {
   gbx_result* res = nullptr;
+  bool pack_args  = false;
   int st          = guarded([&] {
     GBX_EXPECTS(gb != nullptr && out != nullptr, "null argument");
     *out = nullptr;
@@ -959,8 +960,16 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     // only the kernels that read the caller's rows in place (the privatised
     // shared table, untiled, and the global table) do
     const bool arg_kinds = plan_has_arg(plan);
-    if (arg_kinds && strategy != GBX_STRATEGY_PRIVATIZED && strategy != GBX_STRATEGY_GLOBAL)
+    if (arg_kinds && strategy != GBX_STRATEGY_PRIVATIZED && strategy != GBX_STRATEGY_GLOBAL) {
+      if (args_packable(requests, num_requests)) {
+        // values of up to 32 bits: the ARG kinds become MIN / MAX of packed
+        // words that every strategy computes (gbx_args.cu); this call is
+        // redone with those requests
+        pack_args = true;
+        return;
+      }
       strategy = est * 2.0 <= static_cast<double>(s_max) ? GBX_STRATEGY_PRIVATIZED : GBX_STRATEGY_GLOBAL;
+    }
     // MEDIAN / QUANTILE / NUNIQUE / NTH_ELEMENT label each row by a probe of
     // the finished global table, which the partitioned path does not build
     bool has_sorted = false;
@@ -1457,6 +1466,13 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     timer.read(gb->stats);
     // scratch is released stream-ordered by ~Scratch
   });
+  if (st == GBX_OK && pack_args) {
+    if (res) gbx_result_release(res);
+    res = nullptr;
+    st  = guarded([&] {
+      aggregate_with_packed_args(gb, gb->keys.empty() ? 0 : gb->keys[0].size, requests, num_requests, stream, mr, &res);
+    });
+  }
   if (st != GBX_OK) {
     if (res) gbx_result_release(res);
     return st;

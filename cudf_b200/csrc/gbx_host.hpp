@@ -168,6 +168,14 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
                                  const gbx_request* requests, int32_t num_requests, void* stream,
                                  const gbx_allocator* mr, gbx_result** out, gbx_stats* stats);
 
+// ARGMIN / ARGMAX over values of up to 32 bits as MIN / MAX of packed words
+// (gbx_args.cu): whether the requests hold such kinds only, and the groupby
+// with them rewritten.
+bool args_packable(const gbx_request* requests, int32_t num_requests);
+int aggregate_with_packed_args(gbx_groupby* gb, int64_t n, const gbx_request* requests, int32_t num_requests,
+                               void* stream, const gbx_allocator* mr, gbx_result** out);
+int8_t phys_of(int32_t t);
+
 // Null count of a column when known without a kernel (0 without a mask), else -1.
 int64_t exact_null_count_or_neg(const gbx_column_view& c);
 

@@ -5,9 +5,11 @@ Every result is a row index (INT32), so parity is exact.  The reference's CAS
 loop leaves ties and NaN order-dependent; this library and the oracle both
 fix one order: the lowest row wins a tie, -0.0 ties +0.0, and NaN loses to
 every number (an all-NaN group answers its first NaN row).  Values here are
-drawn from small ranges so that ties are common.  Only the row-preserving
-strategies (privatised shared table, global table) compute these kinds; a
-call that forces another strategy runs on one of those two.
+drawn from small ranges so that ties are common.  Values of up to 32 bits
+take every strategy (the ARG kinds become MIN / MAX of packed (order key, row)
+words, gbx_args.cu); with a 64-bit value among them only the row-preserving
+strategies (privatised shared table, global table) compute them, and a call
+that forces another strategy runs on one of those two.
 """
 from __future__ import annotations
 
@@ -52,7 +54,10 @@ def test_value_types_and_strategies(tid, strategy):
     valid = rng.random(n) > 0.15
     got, _ = T.assert_parity([HostCol(k)], [(HostCol(v, valid, type_id=tid), ARGS + [(Kind.MIN, 0)]),
                                             (HostCol(v, type_id=tid), ARGS)], strategy=strategy)
-    assert got["stats"]["strategy"] in ROW_PRESERVING
+    if storage_dtype(tid).itemsize == 8:
+        assert got["stats"]["strategy"] in ROW_PRESERVING
+    elif strategy in (Strategy.PARTITIONED, Strategy.BUCKETED, Strategy.GLOBAL, Strategy.PRIVATIZED):
+        assert got["stats"]["strategy"] == int(strategy)
 
 
 @pytest.mark.parametrize("dt", [np.float32, np.float64])
@@ -86,6 +91,23 @@ def test_high_cardinality_with_every_other_kind(strategy):
             (Kind.VARIANCE, 1)] + ARGS
     got, _ = T.assert_parity([HostCol(k)], [(HostCol(a), aggs), (HostCol(b, bv), aggs)], strategy=strategy)
     assert got["stats"]["strategy"] == int(Strategy.GLOBAL)
+
+
+@pytest.mark.parametrize("strategy", [Strategy.AUTO, Strategy.PARTITIONED, Strategy.BUCKETED], ids=lambda s: s.name)
+def test_high_cardinality_packed_args_partition(strategy):
+    """Only 32-bit-or-narrower values: ARGMIN / ARGMAX ride the radix
+    partitions as MIN / MAX of packed words (AUTO partitions at 3e5 groups)."""
+    rng = np.random.default_rng(712)
+    n = 2_000_000
+    k = rng.integers(0, 600_000, size=n, dtype=np.int64)
+    b = rng.integers(-50, 50, size=n).astype(np.float32)
+    b[::101] = np.nan
+    bv = rng.random(n) >= 0.10
+    c = rng.integers(0, 7, size=n).astype(np.int16)
+    aggs = [(Kind.SUM, 0), (Kind.COUNT_VALID, 0), (Kind.MIN, 0)] + ARGS
+    got, _ = T.assert_parity([HostCol(k)], [(HostCol(b, bv), aggs), (HostCol(c), ARGS + [(Kind.MAX, 0)])],
+                             strategy=strategy)
+    assert got["stats"]["strategy"] == int(Strategy.PARTITIONED if strategy == Strategy.AUTO else strategy)
 
 
 def test_few_groups_many_ties():
