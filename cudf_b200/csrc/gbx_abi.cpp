@@ -246,6 +246,8 @@ struct gbx_groupby {
   }
 };
 
+int32_t gbx::groupby_strategy(const gbx_groupby* gb) { return gb->strategy; }
+
 namespace gbx {
 namespace {
 
@@ -629,6 +631,7 @@ int gbx_groupby_create(const gbx_table_view* keys, int32_t null_policy, int32_t 
     GBX_EXPECTS(keys != nullptr && keys->num_columns >= 0 && (keys->num_columns == 0 || keys->columns),
                 "invalid keys table");
     GBX_EXPECTS(null_policy == GBX_NULL_EXCLUDE || null_policy == GBX_NULL_INCLUDE, "invalid null_policy");
+    GBX_EXPECTS(keys_are_sorted == 0 || keys_are_sorted == 1, "invalid keys_are_sorted");
     auto* gb            = new gbx_groupby();
     gb->null_policy     = null_policy;
     gb->keys_are_sorted = keys_are_sorted;
@@ -751,6 +754,12 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     *out = nullptr;
     validate(gb, requests, num_requests);
 
+    if (gb->keys_are_sorted) {
+      // keys the caller declares sorted group by runs (gbx_rep.cu)
+      gb->stats = gbx_stats{};
+      aggregate_presorted(gb, gb->keys, gb->null_policy, requests, num_requests, stream, mr, &res, &gb->stats);
+      return;
+    }
     if (keys_need_representatives(gb->keys, gb->null_policy)) {
       // STRING keys, or keys beyond two packed 64-bit words (gbx_rep.cu)
       gb->stats = gbx_stats{};
@@ -1502,6 +1511,9 @@ extern "C" int gbx_groupby_aggregate_noalloc(gbx_groupby* gb,
     GBX_EXPECTS(gb != nullptr && num_groups != nullptr, "null argument");
     *num_groups = 0;
     validate(gb, requests, num_requests);
+    if (gb->keys_are_sorted)
+      fail(GBX_ERR_UNSUPPORTED, "keys declared sorted group by runs, which need scratch in proportion to the rows; "
+                                "use gbx_groupby_aggregate");
     if (keys_need_representatives(gb->keys, gb->null_policy))
       fail(GBX_ERR_UNSUPPORTED, "STRING keys and keys beyond 128 packed bits need scratch in proportion to the rows; "
                                 "use gbx_groupby_aggregate");

@@ -167,6 +167,14 @@ bool keys_need_representatives(const std::vector<gbx_column_view>& keys, int32_t
 int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
                                  const gbx_request* requests, int32_t num_requests, void* stream,
                                  const gbx_allocator* mr, gbx_result** out, gbx_stats* stats);
+// The strategy set on a groupby (a groupby run on labels inherits it).
+int32_t groupby_strategy(const gbx_groupby* gb);
+// Keys the caller declares sorted: groups are the runs of equal adjacent rows
+// in row order; under EXCLUDE with null keys, one group per key ordered by
+// its first row (gbx_rep.cu).
+int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
+                        const gbx_request* requests, int32_t num_requests, void* stream, const gbx_allocator* mr,
+                        gbx_result** out, gbx_stats* stats);
 
 // ARGMIN / ARGMAX over values of up to 32 bits as MIN / MAX of packed words
 // (gbx_args.cu): whether the requests hold such kinds only, and the groupby

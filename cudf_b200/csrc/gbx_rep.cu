@@ -9,6 +9,13 @@
 // 1429-1447).  The label is a plain INT32 key, so the groupby proper then runs
 // on it with every strategy of the packed-key path; the output keys are the
 // original key columns gathered at the representative rows.
+//
+// Keys the caller declares sorted take the same route with another label:
+// the reference's sort path then groups runs of equal adjacent rows in row
+// order (sort_helper.cu:96-104, 141-179), or, under EXCLUDE with null keys,
+// sorts the rows again (sort_helper.cu:64-71).  Here the label is the run's
+// index, or the rank of the key's first row; the groupby runs on it and its
+// output is put in label order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -188,9 +195,11 @@ __global__ void k_rep_mask(const int32_t* __restrict__ rep, int64_t n, uint32_t*
   }
 }
 
-// Output key column c: element g = source row rows[g] (and its validity).
+// Output column: element g = source element rows[g] (per == 1), or element
+// rows[g / per] * per + g % per of a column of `per` elements a group; and
+// its validity (null counts added to *nulls).
 __global__ void k_gather_fixed(const void* __restrict__ src, int64_t src_offset, const uint32_t* __restrict__ src_mask,
-                               int width, const int32_t* __restrict__ rows, int64_t G, void* __restrict__ dst,
+                               int width, int per, const int32_t* __restrict__ rows, int64_t G, void* __restrict__ dst,
                                uint32_t* __restrict__ dst_mask, unsigned long long* nulls)
 {
   const int lane       = threadIdx.x & 31;
@@ -199,7 +208,7 @@ __global__ void k_gather_fixed(const void* __restrict__ src, int64_t src_offset,
   for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < g_up; g += stride) {
     bool valid = false;
     if (g < G) {
-      const int64_t r = rows[g];
+      const int64_t r = per == 1 ? rows[g] : static_cast<int64_t>(rows[g / per]) * per + g % per;
       valid           = bit_valid(src_mask, r + src_offset);
       const uint64_t v = load_width(src, r + src_offset, width);
       switch (width) {
@@ -288,6 +297,81 @@ __global__ void k_fill_i32(int32_t* p, int32_t v, int64_t n)
     p[i] = v;
 }
 
+
+// ------------------------------------------- keys the caller declares sorted
+
+// start[r] = 1 when row r begins a run: its key differs from row r-1's
+// (nulls equal, NaNs equal, sort_helper.cu:141-179).
+__global__ void k_run_starts(const __grid_constant__ RepKeys k, int64_t n, uint32_t* __restrict__ start)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    start[r] = (r == 0 || !rep_equal(k, r - 1, r)) ? 1u : 0u;
+}
+
+// label[r] = the run of row r (the inclusive scan of the starts, less one);
+// first[run] = its first row.
+__global__ void k_run_labels(const uint32_t* __restrict__ start, const uint32_t* __restrict__ excl, int64_t n,
+                             int32_t* __restrict__ label, int32_t* __restrict__ first)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t id = excl[r] + start[r] - 1u;
+    label[r]          = static_cast<int32_t>(id);
+    if (start[r]) first[id] = static_cast<int32_t>(r);
+  }
+}
+
+// fmin[rep] = the smallest row of each representative's key.
+__global__ void k_key_first_row(const int32_t* __restrict__ rep, int64_t n, int32_t* __restrict__ fmin)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    if (rep[r] >= 0) atomicMin(fmin + rep[r], static_cast<int32_t>(r));
+}
+
+// mark[r] = 1 when row r is the first row of its key.
+__global__ void k_key_first_mark(const int32_t* __restrict__ rep, const int32_t* __restrict__ fmin, int64_t n,
+                                 uint32_t* __restrict__ mark)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    mark[r] = (rep[r] >= 0 && fmin[rep[r]] == static_cast<int32_t>(r)) ? 1u : 0u;
+}
+
+// label[r] = the rank of the first row of row r's key among the keys' first
+// rows (rows with no key keep their label; the mask drops them);
+// first[rank] = that row.
+__global__ void k_key_labels(const int32_t* __restrict__ rep, const int32_t* __restrict__ fmin,
+                             const uint32_t* __restrict__ mark, const uint32_t* __restrict__ excl, int64_t n,
+                             int32_t* __restrict__ label, int32_t* __restrict__ first)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (rep[r] < 0) {
+      label[r] = 0;
+      continue;
+    }
+    label[r] = static_cast<int32_t>(excl[fmin[rep[r]]]);
+    if (mark[r]) first[excl[r]] = static_cast<int32_t>(r);
+  }
+}
+
+// inv[label of group g] = g: the inner result row of each ordered group.
+__global__ void k_order_inverse(const int32_t* __restrict__ labels, int64_t G, int32_t* __restrict__ inv,
+                                int32_t* status)
+{
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < G;
+       g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t l = labels[g];
+    if (l < 0 || l >= G) {
+      atomicOr(status, S_BAD_INDEX);
+      continue;
+    }
+    inv[l] = static_cast<int32_t>(g);
+  }
+}
+
 int grid_of(int64_t n, int num_sms)
 {
   const int64_t b = (n + kRepBlock - 1) / kRepBlock;
@@ -321,89 +405,20 @@ RepKeys rep_keys(const std::vector<gbx_column_view>& keys, int32_t null_policy)
   return k;
 }
 
-}  // namespace
-
-bool keys_need_representatives(const std::vector<gbx_column_view>& keys, int32_t null_policy)
+// A result whose key columns are `keys` gathered at `rows` (G of them, a null
+// key kept only under INCLUDE); the caller adds the request columns.
+gbx_result* result_with_keys(Alloc& a, Scratch& sc, const std::vector<gbx_column_view>& keys,
+                             int32_t null_policy, const RepKeys& rk, const int32_t* rows, int64_t G, int num_sms,
+                             cudaStream_t s)
 {
-  for (const auto& k : keys)
-    if (k.type_id == GBX_TYPE_STRING) return true;
-  bool ok = true;
-  (void)make_key_plan(keys.data(), static_cast<int>(keys.size()), null_policy,
-                      std::vector<int64_t>(keys.size(), -1), ok);
-  return !ok;
-}
-
-int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
-                                 const gbx_request* requests, int32_t num_requests, void* stream,
-                                 const gbx_allocator* mr, gbx_result** out, gbx_stats* stats)
-{
-  (void)gb;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  Alloc a;
-  a.st = s;
-  if (mr && mr->allocate && mr->deallocate) {
-    a.user     = *mr;
-    a.has_user = true;
-  }
-  const int64_t n   = keys.empty() ? 0 : keys[0].size;
-  const int num_sms = current_device().num_sms;
-  Scratch sc(&a);
-
-  // labels: each row's representative row
-  const RepKeys rk  = rep_keys(keys, null_policy);
-  const uint64_t cap = next_pow2(std::max<uint64_t>(2 * static_cast<uint64_t>(n) + 2, 64));
-  auto* slots  = static_cast<int32_t*>(sc.get(cap * 4));
-  auto* rep    = static_cast<int32_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(n, 1)) * 4));
-  auto* status = static_cast<int32_t*>(sc.get(8));
-  auto* mask   = static_cast<uint32_t*>(sc.get(static_cast<size_t>((n + 31) / 32) * 4 + 64));
-  GBX_CUDA(cudaMemsetAsync(status, 0, 8, s));
-  k_fill_i32<<<grid_of(static_cast<int64_t>(cap), num_sms), kRepBlock, 0, s>>>(slots, -1, static_cast<int64_t>(cap));
-  GBX_CUDA(cudaGetLastError());
-  if (n > 0) {
-    k_rep_insert<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rk, n, slots, cap, rep, status);
-    GBX_CUDA(cudaGetLastError());
-    if (rk.exclude_nulls) {
-      k_rep_mask<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, mask);
-      GBX_CUDA(cudaGetLastError());
-    }
-  }
-  int32_t h_status = 0;
-  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
-  GBX_CUDA(cudaStreamSynchronize(s));
-  if (h_status & S_TABLE_FULL) fail(GBX_ERR_DEVICE, "representative table overflow (status 0x%x)", h_status);
-
-  // the groupby on the label
-  gbx_column_view label{};
-  label.type_id    = GBX_TYPE_INT32;
-  label.size       = n;
-  label.data       = rep;
-  label.null_mask  = rk.exclude_nulls ? mask : nullptr;
-  label.null_count = rk.exclude_nulls ? -1 : 0;
-  gbx_table_view tv{1, 0, &label};
-  gbx_groupby* inner = nullptr;
-  gbx_result* ir     = nullptr;
-  int st             = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
-  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &ir);
-  if (st == GBX_OK && stats) gbx_groupby_last_stats(inner, stats);
-  if (inner) gbx_groupby_destroy(inner);
-  if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
-
-  // the result: the inner results, and the key columns gathered at the labels
-  const int64_t G     = ir->num_groups;
-  const auto* rows    = static_cast<const int32_t*>(ir->keys[0].data);
   const int nkeys     = static_cast<int>(keys.size());
   auto* res           = new gbx_result();
   std::memset(res, 0, sizeof(*res));
   auto* internal      = new ResultInternal{a, {}, {}};
   res->internal        = internal;
   res->num_key_columns = nkeys;
-  res->num_requests    = ir->num_requests;
   res->num_groups      = G;
   res->keys            = new gbx_column[nkeys > 0 ? nkeys : 1]();
-  res->requests        = ir->requests;  // the inner result's request columns move over
-  ir->requests         = nullptr;
-  ir->num_requests     = 0;
-  // the same allocator made them: the outer result releases them
   auto* nulls = static_cast<unsigned long long*>(sc.get(8 * kMaxKeyCols));
   GBX_CUDA(cudaMemsetAsync(nulls, 0, 8 * kMaxKeyCols, s));
   for (int c = 0; c < nkeys; ++c) {
@@ -477,7 +492,7 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
       }
       if (G > 0) {
         k_gather_fixed<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(kv.data, kv.offset, with_mask ? kv.null_mask : nullptr,
-                                                                  rk.cols[c].width, rows, G, oc.data, oc.null_mask,
+                                                                  rk.cols[c].width, 1, rows, G, oc.data, oc.null_mask,
                                                                   nulls + c);
         GBX_CUDA(cudaGetLastError());
       }
@@ -488,6 +503,218 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
   GBX_CUDA(cudaStreamSynchronize(s));
   for (int c = 0; c < nkeys; ++c)
     res->keys[c].view.null_count = res->keys[c].null_mask ? static_cast<int64_t>(h_nulls[c]) : 0;
+  return res;
+}
+
+}  // namespace
+
+bool keys_need_representatives(const std::vector<gbx_column_view>& keys, int32_t null_policy)
+{
+  for (const auto& k : keys)
+    if (k.type_id == GBX_TYPE_STRING) return true;
+  bool ok = true;
+  (void)make_key_plan(keys.data(), static_cast<int>(keys.size()), null_policy,
+                      std::vector<int64_t>(keys.size(), -1), ok);
+  return !ok;
+}
+
+int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
+                                 const gbx_request* requests, int32_t num_requests, void* stream,
+                                 const gbx_allocator* mr, gbx_result** out, gbx_stats* stats)
+{
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Alloc a;
+  a.st = s;
+  if (mr && mr->allocate && mr->deallocate) {
+    a.user     = *mr;
+    a.has_user = true;
+  }
+  const int64_t n   = keys.empty() ? 0 : keys[0].size;
+  const int num_sms = current_device().num_sms;
+  Scratch sc(&a);
+
+  // labels: each row's representative row
+  const RepKeys rk  = rep_keys(keys, null_policy);
+  const uint64_t cap = next_pow2(std::max<uint64_t>(2 * static_cast<uint64_t>(n) + 2, 64));
+  auto* slots  = static_cast<int32_t*>(sc.get(cap * 4));
+  auto* rep    = static_cast<int32_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(n, 1)) * 4));
+  auto* status = static_cast<int32_t*>(sc.get(8));
+  auto* mask   = static_cast<uint32_t*>(sc.get(static_cast<size_t>((n + 31) / 32) * 4 + 64));
+  GBX_CUDA(cudaMemsetAsync(status, 0, 8, s));
+  k_fill_i32<<<grid_of(static_cast<int64_t>(cap), num_sms), kRepBlock, 0, s>>>(slots, -1, static_cast<int64_t>(cap));
+  GBX_CUDA(cudaGetLastError());
+  if (n > 0) {
+    k_rep_insert<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rk, n, slots, cap, rep, status);
+    GBX_CUDA(cudaGetLastError());
+    if (rk.exclude_nulls) {
+      k_rep_mask<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, mask);
+      GBX_CUDA(cudaGetLastError());
+    }
+  }
+  int32_t h_status = 0;
+  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaStreamSynchronize(s));
+  if (h_status & S_TABLE_FULL) fail(GBX_ERR_DEVICE, "representative table overflow (status 0x%x)", h_status);
+
+  // the groupby on the label
+  gbx_column_view label{};
+  label.type_id    = GBX_TYPE_INT32;
+  label.size       = n;
+  label.data       = rep;
+  label.null_mask  = rk.exclude_nulls ? mask : nullptr;
+  label.null_count = rk.exclude_nulls ? -1 : 0;
+  gbx_table_view tv{1, 0, &label};
+  gbx_groupby* inner = nullptr;
+  gbx_result* ir     = nullptr;
+  int st             = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
+  if (st == GBX_OK) st = gbx_groupby_set_strategy(inner, groupby_strategy(gb));
+  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &ir);
+  if (st == GBX_OK && stats) gbx_groupby_last_stats(inner, stats);
+  if (inner) gbx_groupby_destroy(inner);
+  if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+
+  // the result: the key columns gathered at the labels; the inner result's
+  // request columns move over (the same allocator made them)
+  const int64_t G  = ir->num_groups;
+  const auto* rows = static_cast<const int32_t*>(ir->keys[0].data);
+  gbx_result* res  = result_with_keys(a, sc, keys, null_policy, rk, rows, G, num_sms, s);
+  res->num_requests = ir->num_requests;
+  res->requests     = ir->requests;
+  ir->requests      = nullptr;
+  ir->num_requests  = 0;
+  gbx_result_release(ir);
+  *out = res;
+  return GBX_OK;
+}
+
+int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
+                        const gbx_request* requests, int32_t num_requests, void* stream, const gbx_allocator* mr,
+                        gbx_result** out, gbx_stats* stats)
+{
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Alloc a;
+  a.st = s;
+  if (mr && mr->allocate && mr->deallocate) {
+    a.user     = *mr;
+    a.has_user = true;
+  }
+  const int64_t n   = keys.empty() ? 0 : keys[0].size;
+  const int num_sms = current_device().num_sms;
+  Scratch sc(&a);
+  const RepKeys rk = rep_keys(keys, null_policy);
+  bool null_keys   = false;
+  for (const auto& k : keys) null_keys = null_keys || (k.null_mask != nullptr && k.null_count != 0);
+  // EXCLUDE with null keys: the reference sorts the rows again
+  // (sort_helper.cu:64-71), so equal keys form one group wherever they sit
+  const bool by_key = rk.exclude_nulls && null_keys;
+
+  const size_t nb = static_cast<size_t>(std::max<int64_t>(n, 1)) * 4;
+  auto* label     = static_cast<int32_t*>(sc.get(nb));
+  auto* first     = static_cast<int32_t*>(sc.get(nb));
+  auto* flags     = static_cast<uint32_t*>(sc.get(nb));
+  auto* excl      = static_cast<uint32_t*>(sc.get(nb));
+  auto* status    = static_cast<int32_t*>(sc.get(8));
+  uint32_t* mask  = nullptr;
+  GBX_CUDA(cudaMemsetAsync(status, 0, 8, s));
+  size_t tb = 0;
+  GBX_CUDA(scan_exclusive_u32(nullptr, nullptr, n, nullptr, &tb, s));
+  void* temp = sc.get(std::max<size_t>(tb, 1));
+  if (!by_key) {
+    // runs of equal adjacent rows, in row order
+    if (n > 0) {
+      k_run_starts<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rk, n, flags);
+      GBX_CUDA(cudaGetLastError());
+      GBX_CUDA(scan_exclusive_u32(flags, excl, n, temp, &tb, s));
+      k_run_labels<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(flags, excl, n, label, first);
+      GBX_CUDA(cudaGetLastError());
+    }
+  } else {
+    // one group per key, ordered by the key's first row
+    const uint64_t cap = next_pow2(std::max<uint64_t>(2 * static_cast<uint64_t>(n) + 2, 64));
+    auto* slots        = static_cast<int32_t*>(sc.get(cap * 4));
+    auto* rep          = static_cast<int32_t*>(sc.get(nb));
+    auto* fmin         = static_cast<int32_t*>(sc.get(nb));
+    mask               = static_cast<uint32_t*>(sc.get(static_cast<size_t>((n + 31) / 32) * 4 + 64));
+    k_fill_i32<<<grid_of(static_cast<int64_t>(cap), num_sms), kRepBlock, 0, s>>>(slots, -1, static_cast<int64_t>(cap));
+    GBX_CUDA(cudaGetLastError());
+    if (n > 0) {
+      k_fill_i32<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(fmin, INT32_MAX, n);
+      k_rep_insert<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rk, n, slots, cap, rep, status);
+      k_rep_mask<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, mask);
+      k_key_first_row<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, fmin);
+      k_key_first_mark<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, fmin, n, flags);
+      GBX_CUDA(cudaGetLastError());
+      GBX_CUDA(scan_exclusive_u32(flags, excl, n, temp, &tb, s));
+      k_key_labels<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, fmin, flags, excl, n, label, first);
+      GBX_CUDA(cudaGetLastError());
+    }
+  }
+  int32_t h_status = 0;
+  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaStreamSynchronize(s));
+  if (h_status & S_TABLE_FULL) fail(GBX_ERR_DEVICE, "representative table overflow (status 0x%x)", h_status);
+
+  // the groupby on the label: group g of the ordered output has label g
+  gbx_column_view lv{};
+  lv.type_id    = GBX_TYPE_INT32;
+  lv.size       = n;
+  lv.data       = label;
+  lv.null_mask  = mask;
+  lv.null_count = mask ? -1 : 0;
+  gbx_table_view tv{1, 0, &lv};
+  gbx_groupby* inner = nullptr;
+  gbx_result* ir     = nullptr;
+  int st             = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
+  if (st == GBX_OK) st = gbx_groupby_set_strategy(inner, groupby_strategy(gb));
+  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &ir);
+  if (st == GBX_OK && stats) gbx_groupby_last_stats(inner, stats);
+  if (inner) gbx_groupby_destroy(inner);
+  if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+
+  // every request column put in label order
+  const int64_t G = ir->num_groups;
+  auto* inv       = static_cast<int32_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 4));
+  auto* nulls     = static_cast<unsigned long long*>(sc.get(8));
+  if (G > 0) {
+    k_order_inverse<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(static_cast<const int32_t*>(ir->keys[0].data), G, inv,
+                                                               status);
+    GBX_CUDA(cudaGetLastError());
+  }
+  for (int q = 0; q < ir->num_requests && G > 0; ++q)
+    for (int k = 0; k < ir->requests[q].num_results; ++k) {
+      gbx_column& c = ir->requests[q].results[k];
+      const int64_t rows = c.view.size;
+      if (rows == 0 || c.data == nullptr) continue;
+      GBX_EXPECTS(rows % G == 0, "result column of %lld rows over %lld groups", static_cast<long long>(rows),
+                  static_cast<long long>(G));
+      const int32_t et = c.view.type_id == GBX_TYPE_DICTIONARY32
+                             ? (c.view.index_type_id ? c.view.index_type_id : GBX_TYPE_INT32)
+                             : c.view.type_id;
+      void* data      = a.allocate(c.data_bytes);
+      uint32_t* vmask = c.null_mask ? static_cast<uint32_t*>(a.allocate(c.mask_bytes)) : nullptr;
+      k_gather_fixed<<<grid_of(rows, num_sms), kRepBlock, 0, s>>>(c.data, 0, c.null_mask, type_width(et),
+                                                                   static_cast<int>(rows / G), inv, rows, data, vmask,
+                                                                   nulls);
+      GBX_CUDA(cudaGetLastError());
+      a.release(c.data, c.data_bytes);
+      if (c.null_mask) a.release(c.null_mask, c.mask_bytes);
+      c.data      = data;
+      c.view.data = data;
+      if (c.null_mask) {
+        c.null_mask      = vmask;
+        c.view.null_mask = vmask;
+      }
+    }
+  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaStreamSynchronize(s));
+  if (h_status & S_BAD_INDEX) fail(GBX_ERR_DEVICE, "group label out of range (status 0x%x)", h_status);
+
+  // the key columns at each group's first row
+  gbx_result* res   = result_with_keys(a, sc, keys, null_policy, rk, first, G, num_sms, s);
+  res->num_requests = ir->num_requests;
+  res->requests     = ir->requests;
+  ir->requests      = nullptr;
+  ir->num_requests  = 0;
   gbx_result_release(ir);
   *out = res;
   return GBX_OK;

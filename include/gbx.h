@@ -224,8 +224,15 @@ typedef struct gbx_groupby gbx_groupby;
 
 /* cudf::groupby::groupby::groupby (groupby.hpp:128-132, groupby.cu:53-64).
  * Copies the key descriptors (not the data: the caller keeps `keys` alive, as
- * with the reference).  `keys_are_sorted` is accepted for API parity; the hash
- * path is used either way and group order is unspecified. */
+ * with the reference).  `keys_are_sorted` 0 (sorted::NO): one group per key,
+ * in no particular order.  1 (sorted::YES): the caller declares the rows
+ * sorted by key, and groups follow the reference's sort path
+ * (sort_helper.cu:64-71, 96-104, 141-179): each run of equal adjacent rows is
+ * a group (nulls equal, NaNs equal; under INCLUDE a null run between runs is
+ * a group of its own), output in row order; under EXCLUDE with null keys the
+ * reference sorts the rows again, and here every key is one group, output in
+ * the order of each key's first row (the same order when the keys are
+ * ascending).  Any other value fails with GBX_ERR_LOGIC. */
 GBX_API int gbx_groupby_create(const gbx_table_view* keys,
                        int32_t null_policy,
                        int32_t keys_are_sorted,
@@ -341,8 +348,10 @@ GBX_API int gbx_groupby_set_timing(gbx_groupby* gb, int32_t enable);
  * Limits: at most GBX_NOALLOC_MAX_GROUPS groups (more is rejected with
  * GBX_ERR_LOGIC after the aggregation pass, outputs untouched), and the
  * aggregations' per-group state must fit the array (else GBX_ERR_LOGIC).
- * MEDIAN, QUANTILE, NUNIQUE and NTH_ELEMENT, which sort every row, are
- * refused with GBX_ERR_UNSUPPORTED.
+ * MEDIAN, QUANTILE, NUNIQUE and NTH_ELEMENT, which sort every row, STRING
+ * keys and keys beyond 128 packed bits, and a groupby created with
+ * keys_are_sorted 1, which label every row first, are refused with
+ * GBX_ERR_UNSUPPORTED.
  *
  * Outputs: `out_keys` has one gbx_column per key column and `out_results` one
  * per aggregation of every request, in request order.  The caller sets each

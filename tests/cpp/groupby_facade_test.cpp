@@ -156,6 +156,22 @@ int main()
     expect_equal(k, std::vector<int32_t>{1, 2, 3}, "keys");
     expect_equal(v, std::vector<int64_t>{9, 19, 17}, "sums");
   });
+  run("keys_tests.cpp:199-225 pre_sorted_keys_nulls_before_include_nulls (sorted::YES, row order)", [] {
+    std::vector<cudf::groupby::aggregation_request> requests(1);
+    auto keys      = col(type_id::INT32, std::vector<int32_t>{1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4},
+                         {1, 1, 1, 0, 0, 1, 1, 0, 1, 1, 1});
+    auto vals      = col(type_id::INT32, std::vector<int32_t>{0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 4});
+    requests[0].values = vals;
+    requests[0].aggregations.push_back(cudf::make_sum_aggregation<cudf::groupby_aggregation>());
+    cudf::groupby::groupby gb(cudf::table_view({keys}), cudf::null_policy::INCLUDE, cudf::sorted::YES);
+    auto result = gb.aggregate(requests);
+    auto kview  = result.first->view().column(0);
+    expect_equal(host_valid(kview), std::vector<int>{1, 0, 1, 0, 1, 1}, "key validity");
+    auto k = host_values<int32_t>(kview);
+    expect_equal(std::vector<int32_t>{k[0], k[2], k[4], k[5]}, std::vector<int32_t>{1, 2, 3, 4}, "keys");
+    expect_equal(host_values<int64_t>(result.second[0].results[0]->view()), std::vector<int64_t>{3, 7, 11, 7, 17, 4},
+                 "sums");
+  });
   run("sum_tests.cpp:110-132 null_keys_and_values", [] {
     std::vector<int32_t> k; std::vector<int> kv, vv; std::vector<double> v;
     run_single(col(type_id::INT32, K11, K11V),

@@ -32,6 +32,7 @@ import numpy as np
 from cudf_b200._abi import Kind, NullPolicy, TypeId
 from oracle.oracle import HostCol
 from oracle import oracle as orc
+from oracle import presorted as orc_sorted
 
 FLOAT_RTOL = 1e-12
 VAR_EPS = 16.0 * 2.0 ** -52
@@ -65,13 +66,15 @@ def _aggregation(a):
                        interpolation=extra.get("interpolation", 0), quantiles=tuple(extra.get("quantiles", ())))
 
 
-def run_gpu(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, strategy=None):
+def run_gpu(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, strategy=None,
+            keys_are_sorted=False):
     """Runs libgbx; returns the same structure as oracle.groupby."""
     from cudf_b200 import GroupBy, GroupByRequest, Table
-    from cudf_b200.aggregation import Aggregation
+    from cudf_b200._abi import Sorted
 
     kcols = [device_column(k) for k in keys]
-    gb = GroupBy(Table(kcols), null_handling=null_policy)
+    gb = GroupBy(Table(kcols), null_handling=null_policy,
+                 keys_are_sorted=Sorted.YES if keys_are_sorted else Sorted.NO)
     if strategy is not None:
         gb.set_strategy(strategy)
     reqs = [GroupByRequest(device_column(v), [_aggregation(a) for a in aggs]) for v, aggs in requests]
@@ -256,13 +259,21 @@ def sorted_group_scales(key: np.ndarray, x: np.ndarray, valid: Optional[np.ndarr
 
 
 def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, strategy=None, gpu=None,
-                  threads: int = 1):
-    """Full parity check of libgbx against the oracle on the same inputs."""
-    want = orc.groupby(keys, requests, null_policy, threads)
-    got = gpu if gpu is not None else run_gpu(keys, requests, null_policy, strategy)
+                  threads: int = 1, keys_are_sorted=False):
+    """Full parity check of libgbx against the oracle on the same inputs.
+    With keys_are_sorted the groups are the reference's sort-path groups
+    (oracle/presorted.py) and must come out in its order."""
+    if keys_are_sorted:
+        want = orc_sorted.groupby(keys, requests, null_policy, threads)
+    else:
+        want = orc.groupby(keys, requests, null_policy, threads)
+    got = gpu if gpu is not None else run_gpu(keys, requests, null_policy, strategy, keys_are_sorted)
     assert got["num_groups"] == want["num_groups"], f"groups {got['num_groups']} != {want['num_groups']}"
-    go = sort_order(got["keys"])
-    wo = sort_order(want["keys"])
+    if keys_are_sorted:
+        go = wo = np.arange(want["num_groups"])
+    else:
+        go = sort_order(got["keys"])
+        wo = sort_order(want["keys"])
     compare_keys(got["keys"], want["keys"], go, wo)
     for q, (vals, aggs) in enumerate(requests):
         vt = vals.dict_keys.type_id if vals.dict_keys is not None else vals.type_id
@@ -275,7 +286,11 @@ def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCL
             s = v = None
             if kind in (Kind.VARIANCE, Kind.STD, Kind.M2) or (
                     is_float and kind in (Kind.SUM, Kind.MEAN, Kind.SUM_OF_SQUARES)):
-                if sc is None:
+                if sc is None and keys_are_sorted:
+                    # the scales of the label groups, in output order
+                    sc = group_scales([want["label"]], vals, NullPolicy.EXCLUDE, threads)
+                    sc = {name: a[want["perm"]] for name, a in sc.items()}
+                elif sc is None:
                     sc = group_scales(keys, vals, null_policy, threads)
                 if kind == Kind.SUM:
                     s = sc["abs"]

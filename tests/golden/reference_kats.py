@@ -41,17 +41,18 @@ def sum_type(v):
 
 def _case(cid, ktype, keys, vtype, vals, kind, expect_keys, expect, *, kvalid=None, vvalid=None, evalid=None,
           ekvalid=None, ddof=0, null_policy=NullPolicy.EXCLUDE, rtype=None, vdict=False, kdict=False,
-          float_expect=False, extra=None, offset=0, size=None):
+          float_expect=False, extra=None, offset=0, size=None, keys_are_sorted=False):
     """`null_policy` is the groupby's; `extra` holds an aggregation's own
     null_policy / interpolation / quantiles; `offset` and `size` slice both
-    columns (a column view of rows offset .. offset + size)."""
+    columns (a column view of rows offset .. offset + size);
+    `keys_are_sorted` is the groupby's sorted::YES."""
     return dict(
         id=cid, key_type=ktype, keys=keys, key_valid=kvalid, key_dict=kdict,
         value_type=vtype, values=vals, value_valid=vvalid, value_dict=vdict,
         kind=kind, ddof=ddof, null_policy=null_policy,
         expect_keys=expect_keys, expect_key_valid=ekvalid,
         expect=expect, expect_valid=evalid, result_type=rtype, float_expect=float_expect,
-        extra=extra or {}, offset=offset, size=size,
+        extra=extra or {}, offset=offset, size=size, keys_are_sorted=keys_are_sorted,
     )
 
 
@@ -232,18 +233,20 @@ def cases():
             _case(f"keys_tests.cpp:94-120 include_null_keys[{kt.name}]", kt, K11, V, V11, Kind.SUM, [1, 2, 3, 4, 3],
                   [9, 19, 10, 4, 7], kvalid=K11_VALID, ekvalid=[1, 1, 1, 1, 0], null_policy=NullPolicy.INCLUDE,
                   rtype=T.INT64),
-            # pre-sorted cases run the sort path in the reference; values are order-independent
+            # sorted::YES: groups are the runs of equal adjacent rows (under
+            # INCLUDE a null run between two runs is a group of its own)
             _case(f"keys_tests.cpp:122-145 pre_sorted_keys[{kt.name}]", kt, [1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4], V,
-                  V11, Kind.SUM, [1, 2, 3, 4], [3, 18, 24, 4], rtype=T.INT64),
+                  V11, Kind.SUM, [1, 2, 3, 4], [3, 18, 24, 4], rtype=T.INT64, keys_are_sorted=True),
             _case(f"keys_tests.cpp:147-171 pre_sorted_keys_descending[{kt.name}]", kt,
-                  [4, 3, 3, 3, 2, 2, 2, 2, 1, 1, 1], V, V11, Kind.SUM, [4, 3, 2, 1], [0, 6, 22, 21], rtype=T.INT64),
+                  [4, 3, 3, 3, 2, 2, 2, 2, 1, 1, 1], V, V11, Kind.SUM, [4, 3, 2, 1], [0, 6, 22, 21], rtype=T.INT64,
+                  keys_are_sorted=True),
             _case(f"keys_tests.cpp:173-197 pre_sorted_keys_nullable[{kt.name}]", kt,
                   [1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4], V, V11, Kind.SUM, [1, 2, 3, 4], [3, 15, 17, 4],
-                  kvalid=[1, 1, 1, 0, 1, 1, 1, 0, 1, 1, 1], rtype=T.INT64),
+                  kvalid=[1, 1, 1, 0, 1, 1, 1, 0, 1, 1, 1], rtype=T.INT64, keys_are_sorted=True),
             _case(f"keys_tests.cpp:199-225 pre_sorted_keys_nulls_before_include_nulls[{kt.name}]", kt,
-                  [1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4], V, V11, Kind.SUM, [1, 2, 3, 4, 2],
-                  [3, 11, 17, 4, 14], kvalid=[1, 1, 1, 0, 0, 1, 1, 0, 1, 1, 1], ekvalid=[1, 1, 1, 1, 0],
-                  null_policy=NullPolicy.INCLUDE, rtype=T.INT64),
+                  [1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4], V, V11, Kind.SUM, [1, 2, 2, 3, 3, 4],
+                  [3, 7, 11, 7, 17, 4], kvalid=[1, 1, 1, 0, 0, 1, 1, 0, 1, 1, 1], ekvalid=[1, 0, 1, 0, 1, 1],
+                  null_policy=NullPolicy.INCLUDE, rtype=T.INT64, keys_are_sorted=True),
         ]
     # keys_tests.cpp:338-365: dictionary keys {"aaa","año","₹1"}; indices into the
     # sorted dictionary keys, values summed per dictionary entry.

@@ -1,6 +1,8 @@
 """Known-answer tests: the reference gtests' vectors (tests/golden/reference_kats.py)
 checked against the oracle (CPU) and against libgbx (GPU), sorted by key as
-the reference harness does (cpp/tests/groupby/groupby_test_util.cpp:89-96)."""
+the reference harness does (cpp/tests/groupby/groupby_test_util.cpp:89-96).
+Cases with sorted::YES keys go through oracle/presorted.py and libgbx's
+keys_are_sorted path."""
 from __future__ import annotations
 
 import numpy as np
@@ -9,6 +11,7 @@ import pytest
 from cudf_b200._abi import Kind, TypeId
 from cudf_b200.column import storage_dtype
 from oracle import oracle as orc
+from oracle import presorted as orc_sorted
 from oracle.oracle import HostCol
 from tests import gbx_testing as T
 from tests.golden import reference_kats as KAT
@@ -77,7 +80,10 @@ def check_against_expected(got, case):
 @pytest.mark.parametrize("case", CASES, ids=[c["id"] for c in CASES])
 def test_oracle_matches_reference_kat(case):
     keys, reqs = build(case)
-    got = orc.groupby(keys, reqs, case["null_policy"])
+    if case["keys_are_sorted"]:
+        got = orc_sorted.groupby(keys, reqs, case["null_policy"])
+    else:
+        got = orc.groupby(keys, reqs, case["null_policy"])
     check_against_expected(got, case)
 
 
@@ -85,7 +91,7 @@ def test_oracle_matches_reference_kat(case):
 @pytest.mark.parametrize("case", CASES, ids=[c["id"] for c in CASES])
 def test_gpu_matches_reference_kat(case):
     keys, reqs = build(case)
-    got = T.run_gpu(keys, reqs, case["null_policy"])
+    got = T.run_gpu(keys, reqs, case["null_policy"], keys_are_sorted=case["keys_are_sorted"])
     check_against_expected(got, case)
 
 
