@@ -676,9 +676,16 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
   auto* inv       = static_cast<int32_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 4));
   auto* nulls     = static_cast<unsigned long long*>(sc.get(8));
   if (G > 0) {
+    k_fill_i32<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(inv, 0, G);
     k_order_inverse<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(static_cast<const int32_t*>(ir->keys[0].data), G, inv,
                                                                status);
     GBX_CUDA(cudaGetLastError());
+    GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
+    GBX_CUDA(cudaStreamSynchronize(s));
+    if (h_status & S_BAD_INDEX) {
+      gbx_result_release(ir);
+      fail(GBX_ERR_DEVICE, "group label out of range (status 0x%x)", h_status);
+    }
   }
   for (int q = 0; q < ir->num_requests && G > 0; ++q)
     for (int k = 0; k < ir->requests[q].num_results; ++k) {
@@ -705,10 +712,6 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
         c.view.null_mask = vmask;
       }
     }
-  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
-  GBX_CUDA(cudaStreamSynchronize(s));
-  if (h_status & S_BAD_INDEX) fail(GBX_ERR_DEVICE, "group label out of range (status 0x%x)", h_status);
-
   // the key columns at each group's first row
   gbx_result* res   = result_with_keys(a, sc, keys, null_policy, rk, first, G, num_sms, s);
   res->num_requests = ir->num_requests;
