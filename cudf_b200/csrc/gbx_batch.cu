@@ -58,11 +58,28 @@ struct BatchSource {
 
 __device__ __forceinline__ uint32_t probe_limit(uint64_t cap) { return static_cast<uint32_t>(cap < 4096 ? cap : 4096); }
 
+// A row whose value bits were loaded ahead (RowVals), read through the
+// row-source interface of accumulate_row_from.
+template <int NCH>
+struct LoadedRow {
+  const RowVals<NCH>* v;
+  __device__ __forceinline__ bool value(int c, int64_t, uint64_t& b, int32_t*) const
+  {
+    // selected with constant indices, so that the values stay in registers
+    b = 0;
+#pragma unroll
+    for (int i = 0; i < NCH; ++i)
+      if (i == c) b = v->bits[i];
+    return (v->valid >> c) & 1u;
+  }
+};
+
+
 // --------------------------------------------------------- per-item modes
 
 // CTA-shared table with shared-memory atomics; rows whose key finds no room
 // go to the global table; the table is merged into the global one at the end.
-template <int NW, int BLOCK>
+template <int NW, int NCH, int BLOCK>
 __device__ __forceinline__ void item_shared(const Plan& plan, const BatchInst& I, unsigned char* smem,
                                             uint32_t& s_special, int64_t begin, int64_t end)
 {
@@ -89,22 +106,38 @@ __device__ __forceinline__ void item_shared(const Plan& plan, const BatchInst& I
   const uint32_t keys        = base + sl.keys_off;
   const uint32_t smem_probes = S < 32 ? S : 32;
   const uint32_t max_probes  = probe_limit(I.t.cap);
-  for (int64_t r = begin + threadIdx.x; r < end; r += BLOCK) {
-    uint64_t k[NW];
-    if (!src.key<NW>(r, k)) continue;
-    int64_t s;
-    if (key_is_empty<NW>(k)) {
-      s = S;
-      if (s_special == 0) s_special = 1;
-    } else {
-      s = find_or_insert<Shared, NW>(keys, S - 1, k, hash_key<NW>(k), smem_probes);
+  // the next row's key and values load while this row is applied
+  int64_t r = begin + threadIdx.x;
+  uint64_t k[NW];
+  bool act = r < end && src.key<NW>(r, k);
+  RowVals<NCH> v;
+  load_row_values(plan, src, act, r, v, I.t.status);
+  for (; r < end; r += BLOCK) {
+    const int64_t rn = r + BLOCK;
+    uint64_t kn[NW];
+    const bool actn = rn < end && src.key<NW>(rn, kn);
+    RowVals<NCH> vn;
+    load_row_values(plan, src, actn, rn, vn, I.t.status);
+    if (act) {
+      int64_t s;
+      if (key_is_empty<NW>(k)) {
+        s = S;
+        if (s_special == 0) s_special = 1;
+      } else {
+        s = find_or_insert<Shared, NW>(keys, S - 1, k, hash_key<NW>(k), smem_probes);
+      }
+      const LoadedRow<NCH> lr{&v};
+      if (s >= 0) {
+        accumulate_row_from<Shared>(plan, lr, L, s, r, I.t.status);
+      } else {
+        const int64_t g = global_slot<NW>(I.t, k, max_probes);
+        if (g >= 0) accumulate_row_from<Global>(plan, lr, G, g, r, I.t.status);
+      }
     }
-    if (s >= 0) {
-      accumulate_row_from<Shared>(plan, src, L, s, r, I.t.status);
-    } else {
-      const int64_t g = global_slot<NW>(I.t, k, max_probes);
-      if (g >= 0) accumulate_row_from<Global>(plan, src, G, g, r, I.t.status);
-    }
+    act = actn;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) k[w] = kn[w];
+    v = vn;
   }
   __syncthreads();
 
@@ -183,17 +216,31 @@ __device__ __forceinline__ void item_warp(const Plan& plan, const BatchInst& I, 
 }
 
 // Every row updates the instance's global table.
-template <int NW, int BLOCK>
+template <int NW, int NCH, int BLOCK>
 __device__ __forceinline__ void item_global(const Plan& plan, const BatchInst& I, int64_t begin, int64_t end)
 {
   const BatchSource src{&plan, &I.cols};
   const Level<Global> G{&I.t};
   const uint32_t max_probes = probe_limit(I.t.cap);
-  for (int64_t r = begin + threadIdx.x; r < end; r += BLOCK) {
-    uint64_t k[NW];
-    if (!src.key<NW>(r, k)) continue;
-    const int64_t g = global_slot<NW>(I.t, k, max_probes);
-    if (g >= 0) accumulate_row_from<Global>(plan, src, G, g, r, I.t.status);
+  int64_t r = begin + threadIdx.x;
+  uint64_t k[NW];
+  bool act = r < end && src.key<NW>(r, k);
+  RowVals<NCH> v;
+  load_row_values(plan, src, act, r, v, I.t.status);
+  for (; r < end; r += BLOCK) {
+    const int64_t rn = r + BLOCK;
+    uint64_t kn[NW];
+    const bool actn = rn < end && src.key<NW>(rn, kn);
+    RowVals<NCH> vn;
+    load_row_values(plan, src, actn, rn, vn, I.t.status);
+    if (act) {
+      const int64_t g = global_slot<NW>(I.t, k, max_probes);
+      if (g >= 0) accumulate_row_from<Global>(plan, LoadedRow<NCH>{&v}, G, g, r, I.t.status);
+    }
+    act = actn;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) k[w] = kn[w];
+    v = vn;
   }
 }
 
@@ -226,9 +273,9 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_batch_agg(const __grid_c
     if (threadIdx.x == 0) s_special = 0;
     __syncthreads();
     switch (s_inst.mode) {
-      case BM_SHARED: item_shared<NW, BLOCK>(plan, s_inst, smem, s_special, item.begin, item.end); break;
+      case BM_SHARED: item_shared<NW, NCH, BLOCK>(plan, s_inst, smem, s_special, item.begin, item.end); break;
       case BM_WARP: item_warp<NW, NCH, BLOCK>(plan, s_inst, smem, item.begin, item.end); break;
-      default: item_global<NW, BLOCK>(plan, s_inst, item.begin, item.end); break;
+      default: item_global<NW, NCH, BLOCK>(plan, s_inst, item.begin, item.end); break;
     }
     __syncthreads();  // s_inst and the shared tables are rewritten by the next item
   }
