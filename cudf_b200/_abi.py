@@ -125,7 +125,7 @@ gbx_column_view._fields_ = [
     ("null_mask", C.c_void_p),
     ("null_count", C.c_int64),
     ("index_type_id", C.c_int32),
-    ("reserved0", C.c_int32),
+    ("num_children", C.c_int32),
     ("dict_keys", C.POINTER(gbx_column_view)),
 ]
 

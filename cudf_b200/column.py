@@ -89,8 +89,10 @@ class Column:
         dict_keys: Optional["Column"] = None,
         index_type_id: int = TypeId.INT32,
         scale: int = 0,
+        children: Optional[Sequence["Column"]] = None,
     ):
         self.type_id = TypeId(type_id)
+        self.children = list(children) if children is not None else []
         self.size = int(size)
         self.data = data
         self.mask = mask
@@ -152,10 +154,24 @@ class Column:
             mask = _to_device(pack_mask(ok), device, False)
         return cls(TypeId.STRING, len(vals), data, mask, 0, nulls, dict_keys=offsets)
 
+    @classmethod
+    def struct(cls, members: Sequence["Column"], valid: Optional[np.ndarray] = None, device="cuda") -> "Column":
+        """STRUCT column of `members` (equal sizes; fixed-width, STRING or
+        STRUCT), with an optional validity of its own."""
+        members = list(members)
+        n = members[0].size if members else 0
+        mask = None
+        nulls = 0
+        if valid is not None:
+            valid = np.asarray(valid, dtype=bool)
+            nulls = int(len(valid) - valid.sum())
+            mask = _to_device(pack_mask(valid), device, False)
+        return cls(TypeId.STRUCT, n, None, mask, 0, nulls, children=members)
+
     def slice(self, begin: int, end: int) -> "Column":
         """A view of rows [begin, end) sharing this column's buffers (cudf::slice)."""
         return Column(self.type_id, end - begin, self.data, self.mask, self.offset + begin, None,
-                      self.dict_keys, self.index_type_id, self.scale)
+                      self.dict_keys, self.index_type_id, self.scale, self.children)
 
     # ---- properties
     @property
@@ -183,13 +199,28 @@ class Column:
         if self.dict_keys is not None:
             self._kview = self.dict_keys.view()
             v.dict_keys = C.pointer(self._kview)
+        if self.type_id == TypeId.STRUCT:
+            # the members' views, as an array the view points at
+            self._members = (gbx_column_view * max(1, len(self.children)))()
+            for i, m in enumerate(self.children):
+                self._members[i] = m.view()
+            v.num_children = len(self.children)
+            v.dict_keys = C.cast(self._members, C.POINTER(gbx_column_view))
         self._view = v
         return v
 
     # ---- host conversion
     def to_numpy(self):
         """(values, valid) on the host; valid is None when the column has no mask.
-        A STRING column's values are a numpy object array of str."""
+        A STRING column's values are a numpy object array of str; a STRUCT
+        column's values are the list of its members' (values, valid) over
+        this column's rows."""
+        if self.type_id == TypeId.STRUCT:
+            vals = [m.slice(self.offset, self.offset + self.size).to_numpy() for m in self.children]
+            valid = None
+            if self.mask is not None:
+                valid = unpack_mask(self.mask.detach().cpu().numpy(), self.size, self.offset)
+            return vals, valid
         if self.type_id == TypeId.STRING:
             offs = self.dict_keys.to_numpy()[0].astype(np.int64)
             raw = self.data.detach().cpu().numpy().view(np.uint8).tobytes() if self.data is not None else b""

@@ -234,6 +234,7 @@ struct gbx_groupby {
   std::vector<gbx_column_view> dict_keys;  // copies of each key column's dictionary keys
   int32_t null_policy = GBX_NULL_EXCLUDE;
   int32_t keys_are_sorted = 0;
+  std::deque<std::vector<gbx_column_view>> members;  // copies of STRUCT keys' member views (and their offsets)
   int32_t strategy = GBX_STRATEGY_AUTO;
   int32_t timing = 0;
   cudaEvent_t events[6] = {};  // phase boundaries when timing is on
@@ -247,6 +248,44 @@ struct gbx_groupby {
 };
 
 int32_t gbx::groupby_strategy(const gbx_groupby* gb) { return gb->strategy; }
+
+namespace {
+
+constexpr int kMaxStructDepth = 4;
+
+// Checks a STRUCT key column's members and points the view at copies of
+// their descriptors held by the groupby (recursively, with STRING members'
+// offsets), as the plain key descriptors are copied.
+void adopt_struct_key(gbx_groupby* gb, gbx_column_view& v, int depth)
+{
+  GBX_EXPECTS(depth < kMaxStructDepth, "struct keys nested deeper than %d levels", kMaxStructDepth);
+  GBX_EXPECTS(v.num_children > 0 && v.dict_keys != nullptr, "a STRUCT key column needs its members");
+  gb->members.emplace_back(v.dict_keys, v.dict_keys + v.num_children);
+  std::vector<gbx_column_view>& m = gb->members.back();
+  for (gbx_column_view& c : m) {
+    GBX_EXPECTS(c.offset >= 0 && c.size >= v.offset + v.size, "a struct member is shorter than its struct");
+    if (c.type_id == GBX_TYPE_STRUCT) {
+      adopt_struct_key(gb, c, depth + 1);
+    } else if (c.type_id == GBX_TYPE_STRING) {
+      GBX_EXPECTS(c.dict_keys != nullptr && (c.dict_keys->type_id == GBX_TYPE_INT32 ||
+                                             c.dict_keys->type_id == GBX_TYPE_INT64),
+                  "a STRING struct member needs its INT32 / INT64 offsets column");
+      GBX_EXPECTS(c.dict_keys->size >= c.offset + v.offset + v.size + 1, "offsets column too short");
+      gb->members.emplace_back(1, *c.dict_keys);
+      c.dict_keys = gb->members.back().data();
+    } else if (!is_fixed_width(c.type_id) || c.type_id == GBX_TYPE_DICTIONARY32) {
+      fail(GBX_ERR_UNSUPPORTED, "struct member type %d (list / dictionary / decimal128) is not supported",
+           c.type_id);
+    } else {
+      c.num_children = 0;
+      c.dict_keys    = nullptr;
+    }
+  }
+  v.data      = nullptr;
+  v.dict_keys = m.data();
+}
+
+}  // namespace
 
 namespace gbx {
 namespace {
@@ -655,9 +694,10 @@ int gbx_groupby_create(const gbx_table_view* keys, int32_t null_policy, int32_t 
           GBX_EXPECTS(k.size == 0 || k.dict_keys->size >= k.offset + k.size + 1, "offsets column too short");
           gb->dict_keys[c] = *k.dict_keys;
           k.dict_keys      = &gb->dict_keys[c];
+        } else if (k.type_id == GBX_TYPE_STRUCT) {
+          adopt_struct_key(gb, k, 0);
         } else if (!is_fixed_width(k.type_id)) {
-          fail(GBX_ERR_UNSUPPORTED, "key type %d (list / struct / decimal128) is not supported by this library",
-               k.type_id);
+          fail(GBX_ERR_UNSUPPORTED, "key type %d (list / decimal128) is not supported by this library", k.type_id);
         }
         GBX_EXPECTS(k.size >= 0 && k.offset >= 0, "negative size or offset");
         GBX_EXPECTS(k.size <= INT32_MAX, "row count exceeds cudf::size_type");

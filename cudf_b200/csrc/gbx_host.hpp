@@ -146,10 +146,11 @@ void alloc_column(Alloc& a, gbx_column& c, int32_t type_id, int32_t scale, int64
 // (gbx_result_release).
 struct ResultInternal {
   gbx::Alloc alloc;
-  // buffers beyond the columns' own (STRING keys' offsets) and the child
-  // views the columns point at
+  // buffers beyond the columns' own (STRING keys' offsets, STRUCT keys'
+  // members) and the child views the columns point at
   std::vector<std::pair<void*, size_t>> extra;
   std::deque<gbx_column_view> children;
+  std::deque<std::vector<gbx_column_view>> arrays;  // STRUCT members
 };
 
 namespace gbx {

@@ -36,24 +36,44 @@ using namespace dev;
 namespace {
 
 constexpr int kRepBlock  = 256;
-constexpr int kKindFixed = 0, kKindF32 = 1, kKindF64 = 2, kKindBool = 3, kKindString = 4;
+constexpr int kKindFixed = 0, kKindF32 = 1, kKindF64 = 2, kKindBool = 3, kKindString = 4, kKindValidity = 5;
+// leaves of one key (a STRUCT key is its own validity and its members'
+// leaves) and the enclosing structs a leaf inherits nulls from
+constexpr int kRepMaxLeaves = 32;
+constexpr int kRepMaxDepth  = 4;
 
-// One key column as the representative table reads it.
+// One leaf of the key as the representative table reads it: a fixed-width or
+// STRING column, or the validity of a STRUCT column (kKindValidity).
 struct RepCol {
   const void* data;      // fixed width: elements; STRING: characters
-  const uint32_t* mask;  // validity (nullptr: all valid)
-  int64_t offset;        // the view's first row
+  const uint32_t* mask;  // own validity (nullptr: all valid)
+  int64_t offset;        // element of row 0 (every enclosing struct's offset included)
   const void* offs;      // STRING: offsets (element offset + row)
   int64_t offs_offset;   // STRING: the offsets view's own offset
   int32_t width;         // fixed width: bytes; STRING: bytes of an offset (4 or 8)
   int32_t kind;
+  int32_t top;           // a key column itself, not a struct member: EXCLUDE drops rows where it is null
+  int32_t nanc;          // enclosing structs with a validity mask
+  const uint32_t* anc_mask[kRepMaxDepth];
+  int64_t anc_offset[kRepMaxDepth];
 };
 
 struct RepKeys {
-  int32_t ncols;
-  int32_t exclude_nulls;  // EXCLUDE: a row with a null key takes no label
-  RepCol cols[kMaxKeyCols];
+  int32_t ncols;          // leaves
+  int32_t exclude_nulls;  // EXCLUDE: a row with a null key column takes no label
+  RepCol cols[kRepMaxLeaves];
 };
+
+// A leaf is null where it, or a struct enclosing it, is null: a null struct
+// row's members read as nulls (the nested comparator compares a struct's
+// validity before its members, row_operators.cuh:1456-1500).
+__device__ __forceinline__ bool leaf_valid(const RepCol& c, int64_t r)
+{
+  if (!bit_valid(c.mask, r + c.offset)) return false;
+  for (int j = 0; j < c.nanc; ++j)
+    if (!bit_valid(c.anc_mask[j], r + c.anc_offset[j])) return false;
+  return true;
+}
 
 __device__ __forceinline__ uint64_t load_width(const void* p, int64_t i, int w)
 {
@@ -101,8 +121,10 @@ __device__ __forceinline__ uint64_t rep_hash(const RepKeys& k, int64_t r)
   for (int c = 0; c < k.ncols; ++c) {
     const RepCol& col = k.cols[c];
     uint64_t v;
-    if (!bit_valid(col.mask, r + col.offset)) {
+    if (!leaf_valid(col, r)) {
       v = 0x9e3779b97f4a7c15ULL;
+    } else if (col.kind == kKindValidity) {
+      v = 1;
     } else if (col.kind == kKindString) {
       int64_t begin, len;
       str_span(col, r, begin, len);
@@ -122,10 +144,10 @@ __device__ __forceinline__ bool rep_equal(const RepKeys& k, int64_t a, int64_t b
 {
   for (int c = 0; c < k.ncols; ++c) {
     const RepCol& col = k.cols[c];
-    const bool va     = bit_valid(col.mask, a + col.offset);
-    const bool vb     = bit_valid(col.mask, b + col.offset);
+    const bool va     = leaf_valid(col, a);
+    const bool vb     = leaf_valid(col, b);
     if (va != vb) return false;
-    if (!va) continue;  // nulls are equal (hash/groupby.cu:558)
+    if (!va || col.kind == kKindValidity) continue;  // nulls are equal (hash/groupby.cu:558)
     if (col.kind == kKindString) {
       int64_t ba, la, bb, lb;
       str_span(col, a, ba, la);
@@ -141,10 +163,12 @@ __device__ __forceinline__ bool rep_equal(const RepKeys& k, int64_t a, int64_t b
   return true;
 }
 
+// A null key column (EXCLUDE drops the row: the AND of the key columns' own
+// masks, hash/groupby.cu:560-567; a null struct member does not count).
 __device__ __forceinline__ bool any_null(const RepKeys& k, int64_t r)
 {
   for (int c = 0; c < k.ncols; ++c)
-    if (!bit_valid(k.cols[c].mask, r + k.cols[c].offset)) return true;
+    if (k.cols[c].top && !bit_valid(k.cols[c].mask, r + k.cols[c].offset)) return true;
   return false;
 }
 
@@ -228,16 +252,16 @@ __global__ void k_gather_fixed(const void* __restrict__ src, int64_t src_offset,
   }
 }
 
-// Validity words of a gathered column (null counts added to *nulls).
-__global__ void k_gather_valid(const uint32_t* __restrict__ src_mask, int64_t src_offset,
-                               const int32_t* __restrict__ rows, int64_t G, uint32_t* __restrict__ dst_mask,
-                               unsigned long long* nulls)
+// Validity words of a gathered leaf (its own and its enclosing structs'
+// nulls; null counts added to *nulls).
+__global__ void k_gather_leaf_valid(const __grid_constant__ RepCol c, const int32_t* __restrict__ rows, int64_t G,
+                                    uint32_t* __restrict__ dst_mask, unsigned long long* nulls)
 {
   const int lane       = threadIdx.x & 31;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   const int64_t g_up   = (G + 31) & ~int64_t(31);
   for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < g_up; g += stride) {
-    const bool valid   = g < G && bit_valid(src_mask, rows[g] + src_offset);
+    const bool valid   = g < G && leaf_valid(c, rows[g]);
     const uint32_t act = __ballot_sync(0xffffffffu, g < G);
     const uint32_t bal = __ballot_sync(0xffffffffu, valid);
     if (lane == 0 && act) {
@@ -256,7 +280,7 @@ __global__ void k_gather_str_len(const __grid_constant__ RepCol c, const int32_t
        g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t r = rows[g];
     int64_t b = 0, l = 0;
-    if (bit_valid(c.mask, r + c.offset)) str_span(c, r, b, l);
+    if (leaf_valid(c, r)) str_span(c, r, b, l);
     len[g] = l;
   }
 }
@@ -270,7 +294,7 @@ __global__ void k_gather_str_copy(const __grid_constant__ RepCol c, const int32_
   const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   for (int64_t g = w; g < G; g += nw) {
     const int64_t r = rows[g];
-    if (!bit_valid(c.mask, r + c.offset)) continue;
+    if (!leaf_valid(c, r)) continue;
     int64_t b, l;
     str_span(c, r, b, l);
     const auto* s = static_cast<const unsigned char*>(c.data) + b;
@@ -378,59 +402,126 @@ int grid_of(int64_t n, int num_sms)
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, int64_t(num_sms) * 8)));
 }
 
-RepKeys rep_keys(const std::vector<gbx_column_view>& keys, int32_t null_policy)
+// The key as a tree of columns (STRUCT columns hold their members) and the
+// leaves the kernels read.
+struct KeyNode {
+  const gbx_column_view* v;
+  int leaf;               // its leaf (a STRUCT's validity)
+  std::vector<int> kids;  // STRUCT: member nodes
+};
+
+struct KeyTree {
+  RepKeys rk{};
+  std::vector<KeyNode> nodes;
+  std::vector<int> roots;  // one node per key column
+};
+
+int add_key_node(KeyTree& t, const gbx_column_view& v, int64_t base, const RepCol& parent, bool top)
 {
-  RepKeys k{};
-  k.ncols         = static_cast<int32_t>(keys.size());
-  k.exclude_nulls = null_policy == GBX_NULL_EXCLUDE ? 1 : 0;
-  for (size_t c = 0; c < keys.size(); ++c) {
-    const gbx_column_view& v = keys[c];
-    RepCol& rc               = k.cols[c];
-    rc.mask                  = v.null_count == 0 ? nullptr : v.null_mask;
-    rc.offset                = v.offset;
-    rc.data                  = v.data;
-    if (v.type_id == GBX_TYPE_STRING) {
-      rc.kind        = kKindString;
-      rc.offs        = v.dict_keys->data;
-      rc.offs_offset = v.dict_keys->offset;
-      rc.width       = type_width(v.dict_keys->type_id);
-    } else {
-      const int32_t t = v.type_id == GBX_TYPE_DICTIONARY32 ? (v.index_type_id ? v.index_type_id : GBX_TYPE_INT32)
-                                                           : v.type_id;
-      rc.width = type_width(t);
-      rc.kind  = t == GBX_TYPE_FLOAT32 ? kKindF32 : t == GBX_TYPE_FLOAT64 ? kKindF64 : t == GBX_TYPE_BOOL8 ? kKindBool
-                                                                                                         : kKindFixed;
-    }
+  GBX_EXPECTS(t.rk.ncols < kRepMaxLeaves, "a key of more than %d columns and struct members", kRepMaxLeaves);
+  const int leaf = t.rk.ncols++;
+  RepCol rc{};
+  rc.mask   = v.null_count == 0 ? nullptr : v.null_mask;
+  rc.offset = base + v.offset;
+  rc.data   = v.data;
+  rc.top    = top ? 1 : 0;
+  rc.nanc   = parent.nanc;
+  for (int j = 0; j < parent.nanc; ++j) {
+    rc.anc_mask[j]   = parent.anc_mask[j];
+    rc.anc_offset[j] = parent.anc_offset[j];
   }
-  return k;
+  KeyNode node{&v, leaf, {}};
+  if (v.type_id == GBX_TYPE_STRUCT) {
+    rc.kind = kKindValidity;
+    // members inherit this struct's nulls; their rows start at its offset
+    RepCol inherit = rc;
+    if (rc.mask != nullptr) {
+      GBX_EXPECTS(inherit.nanc < kRepMaxDepth, "struct keys nested deeper than %d levels", kRepMaxDepth);
+      inherit.anc_mask[inherit.nanc]   = rc.mask;
+      inherit.anc_offset[inherit.nanc] = rc.offset;
+      ++inherit.nanc;
+    }
+    t.rk.cols[leaf] = rc;
+    for (int32_t m = 0; m < v.num_children; ++m)
+      node.kids.push_back(add_key_node(t, v.dict_keys[m], rc.offset, inherit, false));
+  } else if (v.type_id == GBX_TYPE_STRING) {
+    rc.kind        = kKindString;
+    rc.offs        = v.dict_keys->data;
+    rc.offs_offset = v.dict_keys->offset;
+    rc.width       = type_width(v.dict_keys->type_id);
+    t.rk.cols[leaf] = rc;
+  } else {
+    const int32_t ty = v.type_id == GBX_TYPE_DICTIONARY32 ? (v.index_type_id ? v.index_type_id : GBX_TYPE_INT32)
+                                                          : v.type_id;
+    rc.width = type_width(ty);
+    rc.kind  = ty == GBX_TYPE_FLOAT32 ? kKindF32 : ty == GBX_TYPE_FLOAT64 ? kKindF64 : ty == GBX_TYPE_BOOL8 ? kKindBool
+                                                                                                       : kKindFixed;
+    t.rk.cols[leaf] = rc;
+  }
+  t.nodes.push_back(std::move(node));
+  return static_cast<int>(t.nodes.size()) - 1;
 }
 
-// A result whose key columns are `keys` gathered at `rows` (G of them, a null
-// key kept only under INCLUDE); the caller adds the request columns.
-gbx_result* result_with_keys(Alloc& a, Scratch& sc, const std::vector<gbx_column_view>& keys,
-                             int32_t null_policy, const RepKeys& rk, const int32_t* rows, int64_t G, int num_sms,
-                             cudaStream_t s)
+KeyTree key_tree(const std::vector<gbx_column_view>& keys, int32_t null_policy)
 {
-  const int nkeys     = static_cast<int>(keys.size());
-  auto* res           = new gbx_result();
-  std::memset(res, 0, sizeof(*res));
-  auto* internal      = new ResultInternal{a, {}, {}};
-  res->internal        = internal;
-  res->num_key_columns = nkeys;
-  res->num_groups      = G;
-  res->keys            = new gbx_column[nkeys > 0 ? nkeys : 1]();
-  auto* nulls = static_cast<unsigned long long*>(sc.get(8 * kMaxKeyCols));
-  GBX_CUDA(cudaMemsetAsync(nulls, 0, 8 * kMaxKeyCols, s));
-  for (int c = 0; c < nkeys; ++c) {
-    const gbx_column_view& kv = keys[c];
-    gbx_column& oc            = res->keys[c];
-    const bool with_mask      = kv.null_mask != nullptr && kv.null_count != 0 && null_policy == GBX_NULL_INCLUDE;
-    if (kv.type_id == GBX_TYPE_STRING) {
-      alloc_column(a, oc, GBX_TYPE_STRING, 0, 0, false);
-      const RepCol& rc = rk.cols[c];
-      auto* len        = static_cast<int64_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 8));
-      auto* excl       = static_cast<int64_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 8));
-      int64_t total    = 0;
+  KeyTree t;
+  t.rk.exclude_nulls = null_policy == GBX_NULL_EXCLUDE ? 1 : 0;
+  const RepCol none{};
+  for (const auto& k : keys) t.roots.push_back(add_key_node(t, k, 0, none, true));
+  return t;
+}
+
+// One gathered key column (or struct member): its view and the buffers it
+// owns, taken from the result's allocator.
+struct Gathered {
+  gbx_column_view view{};
+  void* data        = nullptr;
+  size_t data_bytes = 0;
+  uint32_t* mask    = nullptr;
+  size_t mask_bytes = 0;
+};
+
+struct KeyGather {
+  Alloc& a;
+  Scratch& sc;
+  ResultInternal* internal;
+  const KeyTree& t;
+  const int32_t* rows;
+  int64_t G;
+  int num_sms;
+  cudaStream_t s;
+  bool include;
+  unsigned long long* nulls;  // one counter per node
+
+  // Node `i` gathered at the rows; a key column keeps a mask under INCLUDE
+  // only (EXCLUDE dropped its null rows), a struct member whenever it or an
+  // enclosing struct may be null (a null struct's members come back null,
+  // as a gather of a struct column gives them).
+  Gathered node(int i)
+  {
+    const KeyNode& kn = t.nodes[static_cast<size_t>(i)];
+    const RepCol& rc  = t.rk.cols[kn.leaf];
+    const gbx_column_view& kv = *kn.v;
+    Gathered out;
+    out.view.type_id = kv.type_id;
+    out.view.scale   = kv.scale;
+    out.view.size    = G;
+    const bool with_mask = rc.top ? (rc.mask != nullptr && include) : (rc.mask != nullptr || rc.nanc > 0);
+    if (kv.type_id == GBX_TYPE_STRUCT) {
+      internal->arrays.emplace_back();
+      auto& members = internal->arrays.back();
+      for (int k : kn.kids) {
+        Gathered m = node(k);
+        if (m.data) internal->extra.emplace_back(m.data, m.data_bytes);
+        if (m.mask) internal->extra.emplace_back(m.mask, m.mask_bytes);
+        members.push_back(m.view);
+      }
+      out.view.num_children = static_cast<int32_t>(members.size());
+      out.view.dict_keys    = members.data();
+    } else if (kv.type_id == GBX_TYPE_STRING) {
+      auto* len     = static_cast<int64_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 8));
+      auto* excl    = static_cast<int64_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 8));
+      int64_t total = 0;
       if (G > 0) {
         k_gather_str_len<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(rc, rows, G, len);
         GBX_CUDA(cudaGetLastError());
@@ -444,65 +535,99 @@ gbx_result* result_with_keys(Alloc& a, Scratch& sc, const std::vector<gbx_column
         GBX_CUDA(cudaStreamSynchronize(s));
         total = last[0] + last[1];
       }
-      const int ow          = total < (int64_t(1) << 31) ? 4 : 8;
-      const size_t ob       = static_cast<size_t>(G + 1) * ow;
-      void* offs_buf        = a.allocate(ob);
+      const int ow    = total < (int64_t(1) << 31) ? 4 : 8;
+      const size_t ob = static_cast<size_t>(G + 1) * ow;
+      void* offs_buf  = a.allocate(ob);
       internal->extra.emplace_back(offs_buf, ob);
-      oc.data_bytes         = static_cast<size_t>(std::max<int64_t>(total, 1));
-      oc.data               = a.allocate(oc.data_bytes);
+      out.data_bytes = static_cast<size_t>(std::max<int64_t>(total, 1));
+      out.data       = a.allocate(out.data_bytes);
       k_offsets_out<<<grid_of(G + 1, num_sms), kRepBlock, 0, s>>>(excl, len, G, ow, offs_buf);
       GBX_CUDA(cudaGetLastError());
       if (total > 0) {
         k_gather_str_copy<<<grid_of(G * 32, num_sms), kRepBlock, 0, s>>>(rc, rows, G, excl,
-                                                                         static_cast<unsigned char*>(oc.data));
+                                                                         static_cast<unsigned char*>(out.data));
         GBX_CUDA(cudaGetLastError());
       }
       gbx_column_view ov{};
-      ov.type_id    = ow == 4 ? GBX_TYPE_INT32 : GBX_TYPE_INT64;
-      ov.size       = G + 1;
-      ov.data       = offs_buf;
+      ov.type_id = ow == 4 ? GBX_TYPE_INT32 : GBX_TYPE_INT64;
+      ov.size    = G + 1;
+      ov.data    = offs_buf;
       internal->children.push_back(ov);
-      oc.view.type_id   = GBX_TYPE_STRING;
-      oc.view.size      = G;
-      oc.view.data      = oc.data;
-      oc.view.dict_keys = &internal->children.back();
-      if (with_mask) {
-        const size_t words = static_cast<size_t>((G + 31) / 32);
-        oc.mask_bytes      = ((words * 4 + 63) / 64) * 64;
-        oc.null_mask       = G > 0 ? static_cast<uint32_t*>(a.allocate(oc.mask_bytes)) : nullptr;
-        oc.view.null_mask  = oc.null_mask;
-        if (G > 0) {
-          k_gather_valid<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(kv.null_mask, kv.offset, rows, G, oc.null_mask,
-                                                                   nulls + c);
-          GBX_CUDA(cudaGetLastError());
-        }
-      }
+      out.view.data      = out.data;
+      out.view.dict_keys = &internal->children.back();
     } else {
-      alloc_column(a, oc, kv.type_id, kv.scale, G, with_mask);
+      int32_t et = kv.type_id;
       if (kv.type_id == GBX_TYPE_DICTIONARY32) {
-        const int32_t it = kv.index_type_id ? kv.index_type_id : GBX_TYPE_INT32;
-        oc.view.index_type_id = it;
-        oc.view.dict_keys     = kv.dict_keys;
-        if (type_width(it) != 4) {
-          a.release(oc.data, oc.data_bytes);
-          oc.data_bytes = static_cast<size_t>(G) * type_width(it);
-          oc.data       = G > 0 ? a.allocate(oc.data_bytes) : nullptr;
-          oc.view.data  = oc.data;
-        }
+        et                     = kv.index_type_id ? kv.index_type_id : GBX_TYPE_INT32;
+        out.view.index_type_id = et;
+        out.view.dict_keys     = kv.dict_keys;
       }
+      out.data_bytes = static_cast<size_t>(std::max<int64_t>(G, 1)) * type_width(et);
+      out.data       = a.allocate(out.data_bytes);
+      out.view.data  = out.data;
       if (G > 0) {
-        k_gather_fixed<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(kv.data, kv.offset, with_mask ? kv.null_mask : nullptr,
-                                                                  rk.cols[c].width, 1, rows, G, oc.data, oc.null_mask,
-                                                                  nulls + c);
+        k_gather_fixed<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(kv.data, rc.offset, nullptr, rc.width, 1, rows, G,
+                                                                  out.data, nullptr, nulls + i);
         GBX_CUDA(cudaGetLastError());
       }
     }
+    if (with_mask) {
+      const size_t words = static_cast<size_t>((G + 31) / 32);
+      out.mask_bytes     = std::max<size_t>(((words * 4 + 63) / 64) * 64, 64);
+      out.mask           = static_cast<uint32_t*>(a.allocate(out.mask_bytes));
+      out.view.null_mask = out.mask;
+      out.view.null_count = -1;  // counted below
+      if (G > 0) {
+        k_gather_leaf_valid<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(rc, rows, G, out.mask, nulls + i);
+        GBX_CUDA(cudaGetLastError());
+      }
+    }
+    return out;
   }
-  unsigned long long h_nulls[kMaxKeyCols] = {};
-  GBX_CUDA(cudaMemcpyAsync(h_nulls, nulls, 8 * kMaxKeyCols, cudaMemcpyDeviceToHost, s));
+};
+
+// Sets the null count of a gathered view and its members from the nodes'
+// counters.
+void set_null_counts(gbx_column_view& v, const unsigned long long* h, const KeyTree& t, int node)
+{
+  const KeyNode& kn = t.nodes[static_cast<size_t>(node)];
+  if (v.type_id == GBX_TYPE_STRUCT)
+    for (size_t m = 0; m < kn.kids.size(); ++m)
+      set_null_counts(const_cast<gbx_column_view&>(v.dict_keys[m]), h, t, kn.kids[m]);
+  v.null_count = v.null_mask ? static_cast<int64_t>(h[node]) : 0;
+}
+
+// A result whose key columns are `keys` gathered at `rows` (G of them, a null
+// key kept only under INCLUDE); the caller adds the request columns.
+gbx_result* result_with_keys(Alloc& a, Scratch& sc, const std::vector<gbx_column_view>& keys,
+                             int32_t null_policy, const KeyTree& t, const int32_t* rows, int64_t G, int num_sms,
+                             cudaStream_t s)
+{
+  const int nkeys = static_cast<int>(keys.size());
+  auto* res       = new gbx_result();
+  std::memset(res, 0, sizeof(*res));
+  auto* internal       = new ResultInternal{a, {}, {}, {}};
+  res->internal        = internal;
+  res->num_key_columns = nkeys;
+  res->num_groups      = G;
+  res->keys            = new gbx_column[nkeys > 0 ? nkeys : 1]();
+  const size_t nn      = std::max<size_t>(t.nodes.size(), 1);
+  auto* nulls          = static_cast<unsigned long long*>(sc.get(8 * nn));
+  GBX_CUDA(cudaMemsetAsync(nulls, 0, 8 * nn, s));
+  KeyGather kg{a, sc, internal, t, rows, G, num_sms, s, null_policy == GBX_NULL_INCLUDE, nulls};
+  for (int c = 0; c < nkeys; ++c) {
+    Gathered g        = kg.node(t.roots[static_cast<size_t>(c)]);
+    gbx_column& oc    = res->keys[c];
+    oc.view           = g.view;
+    oc.data           = g.data;
+    oc.data_bytes     = g.data_bytes;
+    oc.null_mask      = g.mask;
+    oc.mask_bytes     = g.mask_bytes;
+  }
+  std::vector<unsigned long long> h(nn, 0);
+  GBX_CUDA(cudaMemcpyAsync(h.data(), nulls, 8 * nn, cudaMemcpyDeviceToHost, s));
   GBX_CUDA(cudaStreamSynchronize(s));
-  for (int c = 0; c < nkeys; ++c)
-    res->keys[c].view.null_count = res->keys[c].null_mask ? static_cast<int64_t>(h_nulls[c]) : 0;
+  for (int c = 0; c < nkeys; ++c) set_null_counts(res->keys[c].view, h.data(), t, t.roots[static_cast<size_t>(c)]);
   return res;
 }
 
@@ -511,7 +636,7 @@ gbx_result* result_with_keys(Alloc& a, Scratch& sc, const std::vector<gbx_column
 bool keys_need_representatives(const std::vector<gbx_column_view>& keys, int32_t null_policy)
 {
   for (const auto& k : keys)
-    if (k.type_id == GBX_TYPE_STRING) return true;
+    if (k.type_id == GBX_TYPE_STRING || k.type_id == GBX_TYPE_STRUCT) return true;
   bool ok = true;
   (void)make_key_plan(keys.data(), static_cast<int>(keys.size()), null_policy,
                       std::vector<int64_t>(keys.size(), -1), ok);
@@ -534,7 +659,8 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
   Scratch sc(&a);
 
   // labels: each row's representative row
-  const RepKeys rk  = rep_keys(keys, null_policy);
+  const KeyTree tree = key_tree(keys, null_policy);
+  const RepKeys& rk   = tree.rk;
   const uint64_t cap = next_pow2(std::max<uint64_t>(2 * static_cast<uint64_t>(n) + 2, 64));
   auto* slots  = static_cast<int32_t*>(sc.get(cap * 4));
   auto* rep    = static_cast<int32_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(n, 1)) * 4));
@@ -577,7 +703,7 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
   // request columns move over (the same allocator made them)
   const int64_t G  = ir->num_groups;
   const auto* rows = static_cast<const int32_t*>(ir->keys[0].data);
-  gbx_result* res  = result_with_keys(a, sc, keys, null_policy, rk, rows, G, num_sms, s);
+  gbx_result* res  = result_with_keys(a, sc, keys, null_policy, tree, rows, G, num_sms, s);
   res->num_requests = ir->num_requests;
   res->requests     = ir->requests;
   ir->requests      = nullptr;
@@ -601,7 +727,8 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
   const int64_t n   = keys.empty() ? 0 : keys[0].size;
   const int num_sms = current_device().num_sms;
   Scratch sc(&a);
-  const RepKeys rk = rep_keys(keys, null_policy);
+  const KeyTree tree = key_tree(keys, null_policy);
+  const RepKeys& rk   = tree.rk;
   bool null_keys   = false;
   for (const auto& k : keys) null_keys = null_keys || (k.null_mask != nullptr && k.null_count != 0);
   // EXCLUDE with null keys: the reference sorts the rows again
@@ -713,7 +840,7 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
       }
     }
   // the key columns at each group's first row
-  gbx_result* res   = result_with_keys(a, sc, keys, null_policy, rk, first, G, num_sms, s);
+  gbx_result* res   = result_with_keys(a, sc, keys, null_policy, tree, first, G, num_sms, s);
   res->num_requests = ir->num_requests;
   res->requests     = ir->requests;
   ir->requests      = nullptr;

@@ -411,6 +411,8 @@ int gbx_server_submit(gbx_server* s, const gbx_table_view* keys, const gbx_reque
     j->keys.assign(keys->columns, keys->columns + keys->num_columns);
     j->key_dicts.resize(j->keys.size());
     for (size_t c = 0; c < j->keys.size(); ++c) {
+      if (j->keys[c].type_id == GBX_TYPE_STRUCT)
+        fail(GBX_ERR_UNSUPPORTED, "STRUCT keys are not served; use gbx_groupby_aggregate");
       if (j->keys[c].dict_keys) {
         j->key_dicts[c]      = *j->keys[c].dict_keys;
         j->keys[c].dict_keys = &j->key_dicts[c];

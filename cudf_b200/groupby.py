@@ -64,6 +64,23 @@ class GroupByRequest:
         self.aggregations = list(aggregations)
 
 
+def _member_column(v: _abi.gbx_column_view, alloc: TorchAllocator) -> Column:
+    """A STRUCT result's member (its buffers taken from the allocator)."""
+    data = alloc.take(v.data) if v.data else None
+    mask = alloc.take(v.null_mask) if v.null_mask else None
+    if mask is not None:
+        mask = mask.view(torch.int32)
+    nc = v.null_count if v.null_count >= 0 else None
+    if v.type_id == _abi.TypeId.STRUCT:
+        return Column(_abi.TypeId.STRUCT, v.size, None, mask, 0, nc,
+                      children=[_member_column(v.dict_keys[i], alloc) for i in range(v.num_children)])
+    if v.type_id == _abi.TypeId.STRING:
+        ov = v.dict_keys.contents
+        offsets = Column(ov.type_id, ov.size, alloc.take(ov.data), None, 0, 0)
+        return Column(_abi.TypeId.STRING, v.size, data, mask, 0, nc, dict_keys=offsets)
+    return Column(v.type_id, v.size, data, mask, 0, nc, scale=v.scale)
+
+
 def _result_column(col: _abi.gbx_column, alloc: TorchAllocator, keys_of=None) -> Column:
     v = col.view
     data = alloc.take(col.data) if col.data else None
@@ -71,6 +88,9 @@ def _result_column(col: _abi.gbx_column, alloc: TorchAllocator, keys_of=None) ->
     if mask is not None:
         mask = mask.view(torch.int32)
     nc = v.null_count if v.null_count >= 0 else None
+    if v.type_id == _abi.TypeId.STRUCT:
+        return Column(_abi.TypeId.STRUCT, v.size, None, mask, 0, nc,
+                      children=[_member_column(v.dict_keys[i], alloc) for i in range(v.num_children)])
     if v.type_id == _abi.TypeId.STRING:
         # the characters, and the offsets child the result also owns
         ov = v.dict_keys.contents

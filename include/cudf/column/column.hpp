@@ -16,9 +16,12 @@ class column {
   column(column const&) = delete;
   column& operator=(column const&) = delete;
 
-  // Adopts a result column produced by libgbx.
-  column(gbx_column const& c, gbx_allocator const* mr, cudaStream_t stream, column_view dict_keys = {})
-    : _c(c), _has_mr(mr != nullptr), _stream(stream), _dict_keys(dict_keys)
+  // Adopts a result column produced by libgbx.  `keep` holds what the
+  // column's children point into (a STRING key's offsets, a STRUCT key's
+  // members: buffers the libgbx result owns).
+  column(gbx_column const& c, gbx_allocator const* mr, cudaStream_t stream, column_view dict_keys = {},
+         std::shared_ptr<void> keep = {})
+    : _c(c), _has_mr(mr != nullptr), _stream(stream), _dict_keys(dict_keys), _keep(std::move(keep))
   {
     if (mr) _mr = *mr;
   }
@@ -42,6 +45,12 @@ class column {
       column_view indices(it, size(), _c.data);
       return column_view(t, size(), nullptr, _c.null_mask, null_count(), 0, {indices, _dict_keys});
     }
+    if (t.id() == type_id::STRING || t.id() == type_id::STRUCT) {
+      gbx_column_view v = _c.view;
+      v.data            = _c.data;
+      v.null_mask       = _c.null_mask;
+      return column_view::from_gbx(v);
+    }
     return column_view(t, size(), _c.data, _c.null_mask, null_count());
   }
   operator column_view() const { return view(); }
@@ -60,6 +69,7 @@ class column {
   bool _has_mr{false};
   cudaStream_t _stream{nullptr};
   column_view _dict_keys{};
+  std::shared_ptr<void> _keep{};
 };
 
 }  // namespace cudf

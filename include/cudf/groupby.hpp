@@ -52,8 +52,7 @@ class groupby {
     (void)column_order;
     (void)null_precedence;
     _kviews.resize(keys.num_columns());
-    _kdict.resize(keys.num_columns());
-    for (size_type i = 0; i < keys.num_columns(); ++i) _kviews[i] = keys.column(i).to_gbx(&_kdict[i]);
+    for (size_type i = 0; i < keys.num_columns(); ++i) _kviews[i] = keys.column(i).to_gbx(_kstore);
     gbx_table_view tv{};
     tv.num_columns = keys.num_columns();
     tv.columns     = _kviews.data();
@@ -98,10 +97,14 @@ class groupby {
     detail::throw_on_gbx_error(gbx_groupby_aggregate(_gb, reqs.data(), static_cast<int32_t>(reqs.size()),
                                                      stream.value(), mr.allocator, &res));
     // move every buffer into its own owning column, then free the shell
+    // (kept while a STRING / STRUCT key column points into it)
+    std::shared_ptr<void> shell(res, [](void* r) { gbx_result_release(static_cast<gbx_result*>(r)); });
     std::vector<std::unique_ptr<column>> key_cols;
     for (int c = 0; c < res->num_key_columns; ++c) {
       column_view dk = _keys.column(c).type().id() == type_id::DICTIONARY32 ? _keys.column(c).child(1) : column_view{};
-      key_cols.push_back(std::make_unique<column>(res->keys[c], mr.allocator, stream.value(), dk));
+      const auto kt  = _keys.column(c).type().id();
+      key_cols.push_back(std::make_unique<column>(res->keys[c], mr.allocator, stream.value(), dk,
+                                                  kt == type_id::STRING || kt == type_id::STRUCT ? shell : nullptr));
       res->keys[c].data      = nullptr;
       res->keys[c].null_mask = nullptr;
     }
@@ -114,14 +117,13 @@ class groupby {
         gc.null_mask = nullptr;
       }
     }
-    gbx_result_release(res);
     return {std::make_unique<table>(std::move(key_cols)), std::move(out)};
   }
 
  private:
   table_view _keys;
   std::vector<gbx_column_view> _kviews;
-  std::vector<gbx_column_view> _kdict;
+  std::deque<std::vector<gbx_column_view>> _kstore;
   gbx_groupby* _gb{nullptr};
 };
 

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define GBX_ABI_VERSION 4
+#define GBX_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define GBX_API __attribute__((visibility("default")))
@@ -121,6 +121,12 @@ typedef enum gbx_agg_kind {
  * the offsets column (INT32 or INT64, at least offset + size + 1 rows; row r's
  * characters are data[offsets[offset + r]] up to offsets[offset + r + 1]), as
  * a cudf strings column holds its offsets child.
+ * For STRUCT key columns `dict_keys` points to an array of `num_children`
+ * member views (fixed-width, STRING or STRUCT; not DICTIONARY32) and `data`
+ * is unused; row r of the struct is row offset + r of every member (each
+ * member applying its own offset too), as a cudf structs column holds its
+ * children; members hold at least offset + size rows.  `num_children` is 0
+ * for every other type.
  * `null_count` may be -1 (unknown): the library then counts nulls itself.
  */
 typedef struct gbx_column_view {
@@ -132,7 +138,7 @@ typedef struct gbx_column_view {
   const uint32_t* null_mask;
   int64_t null_count;
   int32_t index_type_id;
-  int32_t reserved0;
+  int32_t num_children;
   const struct gbx_column_view* dict_keys;
 } gbx_column_view;
 

@@ -84,9 +84,18 @@ class HostCol:
     dict_keys: Optional["HostCol"] = None
     offset: int = 0
     size: Optional[int] = None
+    children: Optional[list] = None  # STRUCT: member HostCols (row r is row offset + r of each)
     _keep: list = field(default_factory=list, repr=False)
 
     def __post_init__(self):
+        if self.type_id == TypeId.STRUCT:
+            n = self.children[0].size if self.children else 0
+            self.values = np.zeros(0, dtype=np.uint8)
+            if self.valid is not None:
+                self.valid = np.asarray(self.valid, dtype=bool)
+            if self.size is None:
+                self.size = n - self.offset
+            return
         if self.type_id == TypeId.STRING:
             # str (or None: null) values; UTF-8 characters and int64 offsets for the view
             self.values = np.array(list(self.values), dtype=object)
@@ -126,7 +135,15 @@ class HostCol:
         v.scale = self.scale
         v.size = self.size
         v.offset = self.offset
-        if self.type_id == TypeId.STRING:
+        if self.type_id == TypeId.STRUCT:
+            vals = np.zeros(0, dtype=np.uint8)
+            members = (gbx_column_view * max(1, len(self.children)))()
+            for i, m in enumerate(self.children):
+                members[i] = m.view()
+            v.num_children = len(self.children)
+            v.dict_keys = C.cast(members, C.POINTER(gbx_column_view))
+            self._members = members
+        elif self.type_id == TypeId.STRING:
             vals = self._chars
         else:
             vals = np.ascontiguousarray(self.values)

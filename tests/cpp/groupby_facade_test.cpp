@@ -172,6 +172,47 @@ int main()
     expect_equal(host_values<int64_t>(result.second[0].results[0]->view()), std::vector<int64_t>{3, 7, 11, 7, 17, 4},
                  "sums");
   });
+  run("structs_tests.cpp:124-148 structs_with_null_rows (STRUCT key with a STRING member)", [] {
+    // members: int32 {1,2,3,1,2,2,1,3,3,2} and strings "11" / "22" / "33"; struct rows 0 and 3 null
+    std::vector<int32_t> m0{1, 2, 3, 1, 2, 2, 1, 3, 3, 2};
+    std::vector<std::string> m2{"11", "22", "33", "11", "22", "22", "11", "33", "33", "22"};
+    std::string chars;
+    std::vector<int32_t> offs{0};
+    for (auto const& x : m2) {
+      chars += x;
+      offs.push_back(static_cast<int32_t>(chars.size()));
+    }
+    auto offsets = col(type_id::INT32, offs);
+    cudf::column_view strings(cudf::data_type{type_id::STRING}, 10,
+                              to_device(std::vector<char>(chars.begin(), chars.end())), nullptr, 0, 0, {offsets});
+    std::vector<int> sv{0, 1, 1, 0, 1, 1, 1, 1, 1, 1};
+    cudf::column_view key(cudf::data_type{type_id::STRUCT}, 10, nullptr, mask_of(sv), 2, 0,
+                          {col(type_id::INT32, m0), strings});
+    std::vector<cudf::groupby::aggregation_request> requests(1);
+    requests[0].values = col(type_id::INT32, std::vector<int32_t>{0, 1, 2, 3, 4, 5, 6, 7, 8, 9});
+    requests[0].aggregations.push_back(cudf::make_sum_aggregation<cudf::groupby_aggregation>());
+    cudf::groupby::groupby gb(cudf::table_view({key}), cudf::null_policy::INCLUDE);
+    auto result = gb.aggregate(requests);
+    auto kv     = result.first->view().column(0);
+    CHECK(kv.type().id() == type_id::STRUCT && kv.num_children() == 2, "a STRUCT key of two members");
+    auto valid = host_valid(kv);
+    auto sums  = host_values<int64_t>(result.second[0].results[0]->view());
+    auto ints  = host_values<int32_t>(kv.child(0));
+    auto ivld  = host_valid(kv.child(0));
+    auto soffs = host_values<int32_t>(kv.child(1).child(0));
+    std::vector<char> sch(static_cast<size_t>(soffs.back()));
+    if (!sch.empty()) cudaMemcpy(sch.data(), kv.child(1).head(), sch.size(), cudaMemcpyDeviceToHost);
+    CHECK(sums.size() == 4, "four groups");
+    for (size_t g = 0; g < sums.size(); ++g) {
+      if (!valid[g]) {
+        CHECK(sums[g] == 3 && !ivld[g], "the null struct rows: sum 3, members null");
+        continue;
+      }
+      const std::string s(sch.begin() + soffs[g], sch.begin() + soffs[g + 1]);
+      const int64_t want = ints[g] == 1 ? 6 : ints[g] == 2 ? 19 : 17;
+      CHECK(sums[g] == want && s == std::to_string(ints[g] * 11), "group %d", ints[g]);
+    }
+  });
   run("sum_tests.cpp:110-132 null_keys_and_values", [] {
     std::vector<int32_t> k; std::vector<int> kv, vv; std::vector<double> v;
     run_single(col(type_id::INT32, K11, K11V),

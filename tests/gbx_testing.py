@@ -33,6 +33,7 @@ from cudf_b200._abi import Kind, NullPolicy, TypeId
 from oracle.oracle import HostCol
 from oracle import oracle as orc
 from oracle import presorted as orc_sorted
+from oracle import structs as orc_structs
 
 FLOAT_RTOL = 1e-12
 VAR_EPS = 16.0 * 2.0 ** -52
@@ -43,6 +44,13 @@ def device_column(h: HostCol):
     """HostCol -> cudf_b200.Column on cuda:0 (same bytes, same offset and size)."""
     from cudf_b200 import Column
 
+    if h.type_id == TypeId.STRUCT:
+        n = h.children[0].size if h.children else 0
+        valid = None if h.valid is None else np.asarray(h.valid, dtype=bool)[:n]
+        col = Column.struct([device_column(m) for m in h.children], valid)
+        if h.offset != 0 or h.size != n:
+            col = col.slice(h.offset, h.offset + h.size)
+        return col
     if h.type_id == TypeId.STRING:
         col = Column.from_strings(h.values, h.valid)
     elif h.dict_keys is not None:
@@ -81,11 +89,20 @@ def run_gpu(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCLUDE, s
     ktab, results = gb.aggregate(reqs)
     out = {"num_groups": ktab.num_rows() if ktab.num_columns() else 0, "keys": [], "results": [], "stats": gb.last_stats()}
     for c in ktab.columns():
-        v, m = c.to_numpy()
-        out["keys"].append((int(c.type_id), v, m))
+        out["keys"].append(_host_of(c))
     for t in results:
         out["results"].append([(int(c.type_id),) + tuple(c.to_numpy()) for c in t.columns()])
     return out
+
+
+def _host_of(c):
+    """(type_id, values, valid) of a result column; a STRUCT column's values
+    are its members' (type_id, values, valid) over its rows."""
+    if c.type_id == TypeId.STRUCT:
+        _, valid = c.to_numpy()
+        return (int(c.type_id), [_host_of(m.slice(c.offset, c.offset + c.size)) for m in c.children], valid)
+    v, m = c.to_numpy()
+    return (int(c.type_id), v, m)
 
 
 def _sort_key_columns(keys):
@@ -263,18 +280,27 @@ def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCL
     """Full parity check of libgbx against the oracle on the same inputs.
     With keys_are_sorted the groups are the reference's sort-path groups
     (oracle/presorted.py) and must come out in its order."""
+    struct_keys = any(k.type_id == TypeId.STRUCT for k in keys)
     if keys_are_sorted:
         want = orc_sorted.groupby(keys, requests, null_policy, threads)
+    elif struct_keys:
+        want = orc_structs.groupby(keys, requests, null_policy, threads)
     else:
         want = orc.groupby(keys, requests, null_policy, threads)
     got = gpu if gpu is not None else run_gpu(keys, requests, null_policy, strategy, keys_are_sorted)
     assert got["num_groups"] == want["num_groups"], f"groups {got['num_groups']} != {want['num_groups']}"
+    got_keys, want_keys = got["keys"], want["keys"]
+    if struct_keys:
+        # leaf by leaf (oracle/structs.py)
+        got_keys = [leaf for k in got["keys"] for leaf in orc_structs.flatten_output(*k)]
+        if keys_are_sorted:
+            want_keys = [leaf for k in want["keys"] for leaf in orc_structs.flatten_output(*k)]
     if keys_are_sorted:
         go = wo = np.arange(want["num_groups"])
     else:
-        go = sort_order(got["keys"])
-        wo = sort_order(want["keys"])
-    compare_keys(got["keys"], want["keys"], go, wo)
+        go = sort_order(got_keys)
+        wo = sort_order(want_keys)
+    compare_keys(got_keys, want_keys, go, wo)
     for q, (vals, aggs) in enumerate(requests):
         vt = vals.dict_keys.type_id if vals.dict_keys is not None else vals.type_id
         is_float = vt in (TypeId.FLOAT32, TypeId.FLOAT64)
@@ -290,6 +316,8 @@ def assert_parity(keys: Sequence[HostCol], requests, null_policy=NullPolicy.EXCL
                     # the scales of the label groups, in output order
                     sc = group_scales([want["label"]], vals, NullPolicy.EXCLUDE, threads)
                     sc = {name: a[want["perm"]] for name, a in sc.items()}
+                elif sc is None and struct_keys:
+                    sc = group_scales(want["enc"], vals, NullPolicy.EXCLUDE, threads)
                 elif sc is None:
                     sc = group_scales(keys, vals, null_policy, threads)
                 if kind == Kind.SUM:

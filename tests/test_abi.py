@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), f"{n} missing from libgbx.so"
         assert n in _abi.SIGNATURES, f"{n} has no ctypes signature"
-    assert lib.gbx_abi_version() == 4
+    assert lib.gbx_abi_version() == 5
 
 
 STRUCTS = ["gbx_column_view", "gbx_table_view", "gbx_aggregation", "gbx_request", "gbx_allocator",
