@@ -152,6 +152,17 @@ class NanEquality(enum.IntEnum):
     UNEQUAL = 1
 
 
+class JoinKind(enum.IntEnum):
+    """gbx_join_kind: the joins of cudf::inner_join / left_join / full_join /
+    left_semi_join / left_anti_join (join.hpp:107-260)."""
+
+    INNER = 0
+    LEFT = 1
+    FULL = 2
+    LEFT_SEMI = 3
+    LEFT_ANTI = 4
+
+
 class DuplicateKeep(enum.IntEnum):
     """cudf::duplicate_keep_option (stream_compaction.hpp:225-230)."""
 
@@ -443,6 +454,9 @@ SIGNATURES = {
         C.c_int, [C.POINTER(gbx_table_view), C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(gbx_allocator),
                   C.POINTER(gbx_column)]),
     "gbx_distinct_join": (
+        C.c_int, [C.POINTER(gbx_table_view), C.POINTER(gbx_table_view), C.c_int32, C.c_int32, C.c_void_p,
+                  C.POINTER(gbx_allocator), C.POINTER(gbx_column), C.POINTER(gbx_column)]),
+    "gbx_hash_join": (
         C.c_int, [C.POINTER(gbx_table_view), C.POINTER(gbx_table_view), C.c_int32, C.c_int32, C.c_void_p,
                   C.POINTER(gbx_allocator), C.POINTER(gbx_column), C.POINTER(gbx_column)]),
     "gbx_column_release": (None, [C.POINTER(gbx_column), C.POINTER(gbx_allocator), C.c_void_p]),

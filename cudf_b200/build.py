@@ -13,9 +13,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgbx.so")
 
 SOURCES = ["gbx_kernels.cu", "gbx_warp.cu", "gbx_part.cu", "gbx_radix.cu", "gbx_tiled.cu", "gbx_batch.cu",
-           "gbx_scan.cu", "gbx_stream.cu", "gbx_sort.cu", "gbx_distinct.cu", "gbx_rep.cu", "gbx_args.cu", "gbx_abi.cpp", "gbx_batch.cpp", "gbx_server.cpp", "gbx_noalloc.cu"]
+           "gbx_scan.cu", "gbx_stream.cu", "gbx_sort.cu", "gbx_distinct.cu", "gbx_rep.cu", "gbx_join.cu", "gbx_args.cu", "gbx_abi.cpp", "gbx_batch.cpp", "gbx_server.cpp", "gbx_noalloc.cu"]
 HEADERS = ["gbx_plan.hpp", "gbx_host.hpp", "gbx_device.cuh", "gbx_table.cuh", "gbx_warpcore.cuh", "gbx_kernels.hpp",
-           "gbx_batch.hpp", "gbx_scan.hpp", "gbx_sort.hpp", os.path.join("..", "..", "include", "gbx.h")]
+           "gbx_batch.hpp", "gbx_scan.hpp", "gbx_sort.hpp", "gbx_rep.cuh", os.path.join("..", "..", "include", "gbx.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

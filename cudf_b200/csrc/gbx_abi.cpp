@@ -270,7 +270,7 @@ void adopt_struct_key(gbx_groupby* gb, gbx_column_view& v, int depth)
       GBX_EXPECTS(c.dict_keys != nullptr && (c.dict_keys->type_id == GBX_TYPE_INT32 ||
                                              c.dict_keys->type_id == GBX_TYPE_INT64),
                   "a STRING struct member needs its INT32 / INT64 offsets column");
-      GBX_EXPECTS(c.dict_keys->size >= c.offset + v.offset + v.size + 1, "offsets column too short");
+      GBX_EXPECTS(c.dict_keys->size >= c.offset + c.size + 1, "offsets column too short");
       gb->members.emplace_back(1, *c.dict_keys);
       c.dict_keys = gb->members.back().data();
     } else if (!is_fixed_width(c.type_id) || c.type_id == GBX_TYPE_DICTIONARY32) {

@@ -3,6 +3,7 @@
 // 225-230, 311-317, 422-424), implemented over libgbx's C ABI (include/gbx.h).
 #pragma once
 
+#include <deque>
 #include <memory>
 #include <vector>
 
@@ -19,11 +20,12 @@ enum class duplicate_keep_option { KEEP_ANY = 0, KEEP_FIRST, KEEP_LAST, KEEP_NON
 
 namespace detail {
 struct gbx_table_holder {
-  std::vector<gbx_column_view> views, dicts;
+  std::vector<gbx_column_view> views;
+  std::deque<std::vector<gbx_column_view>> store;  // dictionary keys, STRING offsets, STRUCT members
   gbx_table_view tv{};
-  explicit gbx_table_holder(table_view const& t) : views(t.num_columns()), dicts(t.num_columns())
+  explicit gbx_table_holder(table_view const& t) : views(t.num_columns())
   {
-    for (size_type i = 0; i < t.num_columns(); ++i) views[i] = t.column(i).to_gbx(&dicts[i]);
+    for (size_type i = 0; i < t.num_columns(); ++i) views[i] = t.column(i).to_gbx(store);
     tv.num_columns = t.num_columns();
     tv.columns     = views.data();
   }

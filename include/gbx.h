@@ -624,7 +624,32 @@ GBX_API int gbx_distinct_join(const gbx_table_view* build, const gbx_table_view*
                               int32_t join_kind, void* stream, const gbx_allocator* mr, gbx_column* build_indices,
                               gbx_column* probe_indices);
 
-/* Frees a column returned by gbx_distinct_indices / gbx_distinct_join with
+/* Hash joins (cudf::inner_join / left_join / full_join, join.hpp:107-190;
+ * cudf::left_semi_join / left_anti_join, join.hpp:200-260).  `left` and
+ * `right` have the same key columns (type, scale; STRUCT members alike):
+ * fixed-width, STRING or STRUCT, not DICTIONARY32.  Returns INT32 gather maps
+ * in no particular order (as the reference's): INNER the matching (left,
+ * right) row pairs; LEFT every left row with each matching right row, or
+ * GBX_JOIN_NONE; FULL the left join's pairs and then (GBX_JOIN_NONE, right
+ * row) for every right row that matched nothing; LEFT_SEMI / LEFT_ANTI the
+ * left rows with / without a match in `left_indices` (`right_indices` empty).
+ * compare_nulls GBX_NULLS_EQUAL: nulls are equal, at every nesting level;
+ * GBX_NULLS_UNEQUAL: a row holding a null anywhere in its key matches no
+ * row.  NaNs are equal, -0.0 == +0.0.  Free both outputs with
+ * gbx_column_release. */
+typedef enum gbx_join_kind {
+  GBX_JOIN_INNER     = 0,
+  GBX_JOIN_LEFT      = 1,
+  GBX_JOIN_FULL      = 2,
+  GBX_JOIN_LEFT_SEMI = 3,
+  GBX_JOIN_LEFT_ANTI = 4
+} gbx_join_kind;
+#define GBX_JOIN_NONE INT32_MIN /* cudf::JoinNoneValue */
+GBX_API int gbx_hash_join(const gbx_table_view* left, const gbx_table_view* right, int32_t compare_nulls,
+                          int32_t join_kind, void* stream, const gbx_allocator* mr, gbx_column* left_indices,
+                          gbx_column* right_indices);
+
+/* Frees a column returned by gbx_distinct_indices / gbx_distinct_join / gbx_hash_join with
  * the allocator that made it. */
 GBX_API void gbx_column_release(gbx_column* col, const gbx_allocator* mr, void* stream);
 

@@ -17,6 +17,7 @@
 #include <limits>
 #include <numeric>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace {
@@ -368,6 +369,34 @@ int main()
     expect_equal(left, std::vector<int32_t>{4, none, none, none, 1}, "left join");
     auto [bi, pi] = join.inner_join();
     CHECK(bi->size() == 2 && pi->size() == 2, "two pairs");
+  });
+  run("join_tests.cpp:701-744 InnerJoinNoNulls (INT32 + STRING keys)", [] {
+    auto strings = [](std::vector<std::string> const& v) {
+      std::string chars;
+      std::vector<int32_t> offs{0};
+      for (auto const& x : v) {
+        chars += x;
+        offs.push_back(static_cast<int32_t>(chars.size()));
+      }
+      return cudf::column_view(cudf::data_type{type_id::STRING}, static_cast<cudf::size_type>(v.size()),
+                               to_device(std::vector<char>(chars.begin(), chars.end())), nullptr, 0, 0,
+                               {col(type_id::INT32, offs)});
+    };
+    auto l0 = col(type_id::INT32, std::vector<int32_t>{3, 1, 2, 0, 2});
+    auto l1 = strings({"s1", "s1", "s0", "s4", "s0"});
+    auto r0 = col(type_id::INT32, std::vector<int32_t>{2, 2, 0, 4, 3});
+    auto r1 = strings({"s1", "s0", "s1", "s2", "s1"});
+    auto [li, ri] = cudf::inner_join(cudf::table_view({l0, l1}), cudf::table_view({r0, r1}));
+    auto a = host_values<int32_t>(li->view());
+    auto b = host_values<int32_t>(ri->view());
+    std::vector<std::pair<int32_t, int32_t>> pairs;
+    for (size_t i = 0; i < a.size(); ++i) pairs.emplace_back(a[i], b[i]);
+    std::sort(pairs.begin(), pairs.end());
+    CHECK((pairs == std::vector<std::pair<int32_t, int32_t>>{{0, 4}, {2, 1}, {4, 1}}), "the matching pairs");
+    auto semi = host_values<int32_t>(cudf::left_semi_join(cudf::table_view({l0, l1}),
+                                                          cudf::table_view({r0, r1}))->view());
+    std::sort(semi.begin(), semi.end());
+    expect_equal(semi, std::vector<int32_t>{0, 2, 4}, "semi join");
   });
   for (auto p : g_buffers) cudaFree(p);
   std::printf("%d failure(s)\n", g_failures);
