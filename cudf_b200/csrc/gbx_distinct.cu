@@ -302,8 +302,13 @@ int gbx_distinct_count(const gbx_table_view* keys, int32_t nulls_equal, void* st
   return guarded([&] {
     GBX_EXPECTS(out != nullptr, "out is null");
     *out = 0;
-    check_keys(keys);
     GBX_EXPECTS(nulls_equal == GBX_NULLS_EQUAL || nulls_equal == GBX_NULLS_UNEQUAL, "invalid null_equality");
+    if (keys_are_nested_or_strings(keys)) {
+      // STRING / STRUCT keys: representative rows (NaNs equal, as here)
+      *out = distinct_by_representatives(keys, GBX_KEEP_ANY, nulls_equal, GBX_NANS_EQUAL, stream, mr, nullptr);
+      return;
+    }
+    check_keys(keys);
     cudaStream_t s  = static_cast<cudaStream_t>(stream);
     const int64_t n = keys->columns[0].size;
     if (n == 0) return;
@@ -337,10 +342,15 @@ int gbx_distinct_indices(const gbx_table_view* keys, int32_t keep, int32_t nulls
   return guarded([&] {
     GBX_EXPECTS(out != nullptr, "out is null");
     std::memset(out, 0, sizeof(*out));
-    check_keys(keys);
     GBX_EXPECTS(keep >= GBX_KEEP_ANY && keep <= GBX_KEEP_NONE, "invalid duplicate_keep_option");
     GBX_EXPECTS(nulls_equal == GBX_NULLS_EQUAL || nulls_equal == GBX_NULLS_UNEQUAL, "invalid null_equality");
     GBX_EXPECTS(nans_equal == GBX_NANS_EQUAL || nans_equal == GBX_NANS_UNEQUAL, "invalid nan_equality");
+    if (keys_are_nested_or_strings(keys)) {
+      // STRING / STRUCT keys: representative rows
+      (void)distinct_by_representatives(keys, keep, nulls_equal, nans_equal, stream, mr, out);
+      return;
+    }
+    check_keys(keys);
     cudaStream_t s  = static_cast<cudaStream_t>(stream);
     Alloc a         = make_alloc(mr, s);
     const int64_t n = keys->columns[0].size;

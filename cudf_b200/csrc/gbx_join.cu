@@ -141,6 +141,49 @@ __global__ void k_append_unmatched(const uint32_t* __restrict__ flag, const uint
   }
 }
 
+// ------------------------------------------------- distinct rows, any keys
+
+// Per key (indexed by its representative row): first and last row, rows.
+__global__ void k_rep_stats(const int32_t* __restrict__ rep, int64_t n, int32_t* __restrict__ fmin,
+                            int32_t* __restrict__ fmax, uint32_t* __restrict__ cnt)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t k = rep[r];
+    if (k < 0) continue;
+    atomicMin(fmin + k, static_cast<int32_t>(r));
+    atomicMax(fmax + k, static_cast<int32_t>(r));
+    atomicAdd(cnt + k, 1u);
+  }
+}
+
+// flag[r] = 1 when row r is kept: a row distinct on its own (no label), or
+// its key's row by the keep option (KEEP_ANY: the representative).
+__global__ void k_rep_keep(const int32_t* __restrict__ rep, int64_t n, const int32_t* __restrict__ fmin,
+                           const int32_t* __restrict__ fmax, const uint32_t* __restrict__ cnt, int32_t keep,
+                           uint32_t* __restrict__ flag)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t k = rep[r];
+    bool kept;
+    if (k < 0) kept = true;
+    else if (keep == GBX_KEEP_FIRST) kept = fmin[k] == r;
+    else if (keep == GBX_KEEP_LAST) kept = fmax[k] == r;
+    else if (keep == GBX_KEEP_NONE) kept = k == r && cnt[k] == 1;
+    else kept = k == r;
+    flag[r] = kept ? 1u : 0u;
+  }
+}
+
+__global__ void k_compact_rows(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos, int64_t n,
+                               int32_t* __restrict__ out)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    if (flag[r]) out[pos[r]] = static_cast<int32_t>(r);
+}
+
 // Both key tables must have the same columns: type, scale and, for STRUCT
 // columns, the same members.
 void check_join_keys(const gbx_column_view& a, const gbx_column_view& b)
@@ -180,6 +223,80 @@ void check_table(const gbx_table_view* t)
 }
 
 }  // namespace
+
+bool keys_are_nested_or_strings(const gbx_table_view* keys)
+{
+  if (keys == nullptr || keys->columns == nullptr) return false;
+  for (int c = 0; c < keys->num_columns; ++c)
+    if (keys->columns[c].type_id == GBX_TYPE_STRING || keys->columns[c].type_id == GBX_TYPE_STRUCT) return true;
+  return false;
+}
+
+int64_t distinct_by_representatives(const gbx_table_view* keys, int32_t keep, int32_t nulls_equal,
+                                    int32_t nans_equal, void* stream, const gbx_allocator* mr, gbx_column* out)
+{
+  check_table(keys);
+  for (int c = 0; c < keys->num_columns; ++c) check_join_keys(keys->columns[c], keys->columns[c]);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Alloc a;
+  a.st = s;
+  if (mr && mr->allocate && mr->deallocate) {
+    a.user     = *mr;
+    a.has_user = true;
+  }
+  const int64_t n = keys->columns[0].size;
+  if (n == 0) {
+    if (out) alloc_column(a, *out, GBX_TYPE_INT32, 0, 0, false);
+    return 0;
+  }
+  const int num_sms = current_device().num_sms;
+  const std::vector<gbx_column_view> cols(keys->columns, keys->columns + keys->num_columns);
+  KeyTree t          = key_tree(cols, GBX_NULL_INCLUDE);
+  t.rk.exclude_nulls = nulls_equal == GBX_NULLS_UNEQUAL ? kExcludeAnyNull : 0;
+  t.rk.nan_alone     = nans_equal == GBX_NANS_UNEQUAL ? 1 : 0;
+
+  Scratch sc(&a);
+  const size_t n4    = static_cast<size_t>(n) * 4;
+  const uint64_t cap = next_pow2(std::max<uint64_t>(2 * static_cast<uint64_t>(n) + 2, 64));
+  auto* slots  = static_cast<int32_t*>(sc.get(cap * 4));
+  auto* rep    = static_cast<int32_t*>(sc.get(n4));
+  auto* fmin   = static_cast<int32_t*>(sc.get(n4));
+  auto* fmax   = static_cast<int32_t*>(sc.get(n4));
+  auto* cnt    = static_cast<uint32_t*>(sc.get(n4));
+  auto* flag   = static_cast<uint32_t*>(sc.get(n4));
+  auto* pos    = static_cast<uint32_t*>(sc.get(n4));
+  auto* status = static_cast<int32_t*>(sc.get(8));
+  GBX_CUDA(cudaMemsetAsync(status, 0, 8, s));
+  GBX_CUDA(cudaMemsetAsync(cnt, 0, n4, s));
+  k_fill_i32<<<grid_of(static_cast<int64_t>(cap), num_sms), kRepBlock, 0, s>>>(slots, -1, static_cast<int64_t>(cap));
+  k_fill_i32<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(fmin, INT32_MAX, n);
+  k_fill_i32<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(fmax, -1, n);
+  k_rep_insert<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(t.rk, n, slots, cap, rep, status);
+  k_rep_stats<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, fmin, fmax, cnt);
+  k_rep_keep<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, fmin, fmax, cnt, keep, flag);
+  GBX_CUDA(cudaGetLastError());
+  size_t tb = 0;
+  GBX_CUDA(scan_exclusive_u32(nullptr, nullptr, n, nullptr, &tb, s));
+  void* temp = sc.get(std::max<size_t>(tb, 1));
+  GBX_CUDA(scan_exclusive_u32(flag, pos, n, temp, &tb, s));
+  uint32_t last[2] = {0, 0};
+  int32_t h_status = 0;
+  GBX_CUDA(cudaMemcpyAsync(&last[0], pos + n - 1, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaMemcpyAsync(&last[1], flag + n - 1, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaStreamSynchronize(s));
+  if (h_status & S_TABLE_FULL) fail(GBX_ERR_DEVICE, "representative table overflow (status 0x%x)", h_status);
+  const int64_t kept = static_cast<int64_t>(last[0]) + last[1];
+  if (out) {
+    alloc_column(a, *out, GBX_TYPE_INT32, 0, kept, false);
+    if (kept > 0) {
+      k_compact_rows<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(flag, pos, n, static_cast<int32_t*>(out->data));
+      GBX_CUDA(cudaGetLastError());
+    }
+    GBX_CUDA(cudaStreamSynchronize(s));
+  }
+  return kept;
+}
 
 }  // namespace gbx
 

@@ -45,6 +45,7 @@ struct RepCol {
 struct RepKeys {
   int32_t ncols;          // leaves
   int32_t exclude_nulls;  // rows that take no label (any_null)
+  int32_t nan_alone;      // distinct rows with NaNs unequal: a row holding a NaN takes no label
   RepCol cols[kRepMaxLeaves];
 };
 
@@ -172,6 +173,21 @@ __device__ __forceinline__ bool any_null(const RepKeys& k, int64_t r)
   return false;
 }
 
+// A valid floating leaf of the row holds a NaN.
+__device__ __forceinline__ bool any_nan(const RepKeys& k, int64_t r)
+{
+  for (int c = 0; c < k.ncols; ++c) {
+    const RepCol& col = k.cols[c];
+    if ((col.kind != kKindF32 && col.kind != kKindF64) || !leaf_valid(col, r)) continue;
+    const uint64_t b = load_width(col.data, r + col.offset, col.width);
+    if (col.kind == kKindF32 ? (__uint_as_float(static_cast<uint32_t>(b)) != __uint_as_float(static_cast<uint32_t>(b)))
+                             : (__longlong_as_double(static_cast<long long>(b)) !=
+                                __longlong_as_double(static_cast<long long>(b))))
+      return true;
+  }
+  return false;
+}
+
 // rep[r] = the representative row of row r's key (-1: a null key under
 // EXCLUDE); `slots` holds row indices (-1: empty), probed linearly at most
 // cap times (S_TABLE_FULL beyond).
@@ -180,7 +196,7 @@ __global__ void k_rep_insert(const __grid_constant__ RepKeys k, int64_t n, int32
 {
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
        r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    if (k.exclude_nulls && any_null(k, r)) {
+    if ((k.exclude_nulls && any_null(k, r)) || (k.nan_alone && any_nan(k, r))) {
       rep[r] = -1;
       continue;
     }

@@ -77,3 +77,24 @@ JOIN = [
      [([3, 1, 2, 0, 2], None, "int32"), ([1, 1, 0, 4, 0], [1, 1, 0, 1, 1], "int32")],
      True, None, [4, None, None, None, 1]),
 ]
+
+
+# STRING and STRUCT keys (column forms of tests/golden/struct_kats.py).
+# distinct_tests.cpp:80-123 DistinctKeepFirstLastNone.StringKeyColumn: the
+# kept rows of the key column {"all", "new", "new", "all", NULL, "the",
+# "strings"} (nulls equal) per keep option.
+STRING_KEY_COLUMN = ([("string", ["all", "new", "new", "all", "", "the", "strings"], [1, 1, 1, 1, 0, 1, 1])],
+                     {1: [0, 1, 4, 5, 6], 2: [2, 3, 4, 5, 6], 3: [4, 5, 6]})
+# distinct_tests.cpp:1204-1255 DistinctKeepAny.StructsOfStructs: s1{s2{a, b}, c}
+# with s2 null at rows 2, 3, 7 and s1 null at rows 4, 5; KEEP_ANY keeps one row
+# of each class: {0, 6}, {1}, {2}, {3, 7}, {4, 5}, {8} with nulls equal, and
+# under nulls unequal every row holding a null stands alone.
+_X = 0  # a placeholder under a null
+STRUCTS_OF_STRUCTS = (
+    [("struct", [("struct", [("fixed", "int32", [1, 1, _X, _X, _X, _X, 1, _X, 2], None),
+                             ("fixed", "int32", [1, 2, _X, _X, _X, _X, 1, _X, 1], None)],
+                  [1, 1, 0, 0, 1, 1, 1, 0, 1]),
+                 ("fixed", "int32", [5, 4, 6, 4, _X, _X, 5, 4, 5], None)],
+      [1, 1, 1, 1, 0, 0, 1, 1, 1])],
+    {"equal": [[0, 6], [1], [2], [3, 7], [4, 5], [8]],
+     "unequal": [[0, 6], [1], [2], [3], [7], [4], [5], [8]]})

@@ -112,8 +112,12 @@ def test_abi_checks_before_device_work():
     assert lib.gbx_distinct_join(C.byref(tv1), C.byref(tvf), 0, 0, None, None, C.byref(b1),
                                  C.byref(b2)) == _abi.Status.ERR_LOGIC
     assert b"data types" in lib.gbx_last_error()
+    # a STRING key needs its offsets; list keys are not taken
     tvs, keeps = _tv([(a, TypeId.STRING)])
-    assert lib.gbx_distinct_count(C.byref(tvs), 0, None, None, C.byref(out)) == _abi.Status.ERR_UNSUPPORTED
+    assert lib.gbx_distinct_count(C.byref(tvs), 0, None, None, C.byref(out)) == _abi.Status.ERR_LOGIC
+    assert b"offsets" in lib.gbx_last_error()
+    tvl, keepl = _tv([(a, TypeId.LIST)])
+    assert lib.gbx_distinct_count(C.byref(tvl), 0, None, None, C.byref(out)) == _abi.Status.ERR_UNSUPPORTED
 
 
 def test_abi_empty_input_needs_no_device():
