@@ -355,7 +355,14 @@ void alloc_column(Alloc& a, gbx_column& c, int32_t type_id, int32_t scale, int64
   c.view.null_count = with_mask ? -1 : 0;
 }
 
-void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n)
+bool is_count_kind(int32_t kind) { return kind == GBX_AGG_COUNT_VALID || kind == GBX_AGG_COUNT_ALL; }
+
+bool counted_only(int32_t vt)
+{
+  return vt == GBX_TYPE_STRING || vt == GBX_TYPE_LIST || vt == GBX_TYPE_STRUCT || vt == GBX_TYPE_DECIMAL128;
+}
+
+void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n, bool count_any)
 {
   GBX_EXPECTS(nreq >= 0 && (nreq == 0 || reqs != nullptr), "invalid request array");
   for (int32_t q = 0; q < nreq; ++q) {
@@ -388,9 +395,12 @@ void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n)
       if (kind == GBX_AGG_NUNIQUE || kind == GBX_AGG_NTH_ELEMENT)
         GBX_EXPECTS(ag.null_policy == GBX_NULL_EXCLUDE || ag.null_policy == GBX_NULL_INCLUDE,
                     "invalid null_policy %d", ag.null_policy);
-      if (vt == GBX_TYPE_STRING || vt == GBX_TYPE_LIST || vt == GBX_TYPE_STRUCT || vt == GBX_TYPE_DECIMAL128)
+      if (counted_only(vt)) {
+        // COUNT reads only the rows' validity: any column type (hash/groupby.cu:73-84 with a size_type target)
+        if (count_any && is_count_kind(kind)) continue;
         fail(GBX_ERR_UNSUPPORTED,
              "value type %d is aggregated by libcudf's sort-based groupby, which this library does not provide", vt);
+      }
       GBX_EXPECTS(target_type(vt, kind) != GBX_TYPE_EMPTY, "Invalid type/aggregation combination.");
     }
   }
@@ -643,9 +653,9 @@ struct Call {
   int64_t n = 0;
 };
 
-void validate(const gbx_groupby* gb, const gbx_request* reqs, int32_t nreq)
+void validate(const gbx_groupby* gb, const gbx_request* reqs, int32_t nreq, bool count_any = false)
 {
-  gbx::validate_requests(reqs, nreq, gb->keys.empty() ? 0 : gb->keys[0].size);
+  gbx::validate_requests(reqs, nreq, gb->keys.empty() ? 0 : gb->keys[0].size, count_any);
 }
 
 }  // namespace
@@ -792,8 +802,14 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
   int st          = guarded([&] {
     GBX_EXPECTS(gb != nullptr && out != nullptr, "null argument");
     *out = nullptr;
-    validate(gb, requests, num_requests);
+    validate(gb, requests, num_requests, true);
 
+    if (needs_count_stand_ins(requests, num_requests)) {
+      // COUNT of STRING / LIST / STRUCT / DECIMAL128 values (gbx_args.cu)
+      aggregate_with_count_stand_ins(gb, gb->keys.empty() ? 0 : gb->keys[0].size, requests, num_requests, stream,
+                                     mr, &res);
+      return;
+    }
     if (gb->keys_are_sorted) {
       // keys the caller declares sorted group by runs (gbx_rep.cu)
       gb->stats = gbx_stats{};

@@ -13,6 +13,7 @@
 // hash/groupby.cu:73-84, aggregation.cuh:436-491).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -218,6 +219,50 @@ int aggregate_with_packed_args(gbx_groupby* gb, int64_t n, const gbx_request* re
   GBX_CUDA(cudaStreamSynchronize(s));
   gbx_result_release(ir);
   *out = res;
+  return GBX_OK;
+}
+
+bool needs_count_stand_ins(const gbx_request* requests, int32_t num_requests)
+{
+  for (int q = 0; q < num_requests; ++q)
+    if (counted_only(requests[q].values.type_id)) return true;
+  return false;
+}
+
+// COUNT_VALID / COUNT_ALL over a column the kernels do not read (STRING,
+// LIST, STRUCT, DECIMAL128): only its rows' validity matters, so the request
+// runs over an INT8 column of zeros with the same offset, size and mask.
+int aggregate_with_count_stand_ins(gbx_groupby* gb, int64_t n, const gbx_request* requests, int32_t num_requests,
+                                   void* stream, const gbx_allocator* mr, gbx_result** out)
+{
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Alloc a;
+  a.st = s;
+  if (mr && mr->allocate && mr->deallocate) {
+    a.user     = *mr;
+    a.has_user = true;
+  }
+  int64_t bytes = 1;
+  for (int q = 0; q < num_requests; ++q)
+    if (counted_only(requests[q].values.type_id)) bytes = std::max(bytes, requests[q].values.offset + n);
+  Scratch sc(&a);
+  void* zeros = sc.get(static_cast<size_t>(bytes));
+  GBX_CUDA(cudaMemsetAsync(zeros, 0, static_cast<size_t>(bytes), s));
+  std::vector<gbx_request> reqs(requests, requests + num_requests);
+  for (gbx_request& r : reqs) {
+    if (!counted_only(r.values.type_id)) continue;
+    gbx_column_view v{};
+    v.type_id    = GBX_TYPE_INT8;
+    v.size       = r.values.size;
+    v.offset     = r.values.offset;
+    v.data       = zeros;
+    v.null_mask  = r.values.null_mask;
+    v.null_count = r.values.null_count;
+    r.values     = v;
+  }
+  const int st = gbx_groupby_aggregate(gb, reqs.data(), num_requests, stream, mr, out);
+  if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+  // the stand-in's release is stream-ordered after the call's kernels
   return GBX_OK;
 }
 

@@ -159,7 +159,10 @@ namespace gbx {
 
 // verify_valid_requests (groupby.cu:176-192) and the size check of
 // groupby::aggregate (groupby.cu:210-214) for keys of `n` rows.
-void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n);
+// count_any: COUNT_VALID / COUNT_ALL are accepted over any value type (the
+// plain entry point answers them through stand-in columns).
+void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n, bool count_any = false);
+bool counted_only(int32_t value_type);
 
 // Keys that do not pack into two 64-bit words (STRING columns, or more than
 // 128 bits with the null bits) and the groupby over them: rows labelled by a
@@ -187,6 +190,12 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
 // (gbx_args.cu): whether the requests hold such kinds only, and the groupby
 // with them rewritten.
 bool args_packable(const gbx_request* requests, int32_t num_requests);
+// Requests whose values only COUNT can read (STRING, LIST, STRUCT,
+// DECIMAL128): answered over an INT8 stand-in with the same rows and
+// validity (gbx_args.cu).
+bool needs_count_stand_ins(const gbx_request* requests, int32_t num_requests);
+int aggregate_with_count_stand_ins(gbx_groupby* gb, int64_t n, const gbx_request* requests, int32_t num_requests,
+                                   void* stream, const gbx_allocator* mr, gbx_result** out);
 int aggregate_with_packed_args(gbx_groupby* gb, int64_t n, const gbx_request* requests, int32_t num_requests,
                                void* stream, const gbx_allocator* mr, gbx_result** out);
 int8_t phys_of(int32_t t);

@@ -112,6 +112,29 @@ def test_size_mismatch_is_logic_error():
     lib.gbx_groupby_destroy(h)
 
 
+@pytest.mark.parametrize("vtype", [TypeId.STRING, TypeId.STRUCT, TypeId.LIST, TypeId.DECIMAL128])
+def test_values_only_counted(vtype):
+    """STRING / STRUCT / LIST / DECIMAL128 values: COUNT is computed (through
+    a stand-in, on the device), any other kind is UNSUPPORTED before device
+    work; the no-allocation entry point refuses them all."""
+    lib = _lib.lib()
+    tv, keep = _keys_view(3)
+    h = C.c_void_p()
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 0, C.byref(h)) == 0
+    for kind in (Kind.SUM, Kind.MIN, Kind.MEAN):
+        r, keep2 = _request(3, kind)
+        r.values.type_id = int(vtype)
+        out = C.POINTER(_abi.gbx_result)()
+        assert lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out)) == _abi.Status.ERR_UNSUPPORTED
+    r, keep2 = _request(3, Kind.COUNT_VALID)
+    r.values.type_id = int(vtype)
+    res = (_abi.gbx_column * 1)()
+    ng = C.c_int64()
+    assert lib.gbx_groupby_aggregate_noalloc(h, C.byref(r), 1, None, None, res, 8, C.byref(ng)) == \
+        _abi.Status.ERR_UNSUPPORTED
+    lib.gbx_groupby_destroy(h)
+
+
 @pytest.mark.parametrize("kind", [Kind.ANY, Kind.ALL, 19, 30])
 def test_kinds_not_computed_are_reported(kind):
     """ANY / ALL and libcudf's later kinds (ROW_NUMBER onwards) are not
