@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint64_t* __rest
 // by digit run with consecutive threads on consecutive rows, so that a warp's
 // stores cover whole sectors.
 template <bool kSplit>
-__global__ void __launch_bounds__(kSortBlock) k_sort_scatter(const uint64_t* __restrict__ lo_in,
+__global__ void __launch_bounds__(kSortBlock, kSplit ? 2 : 3) k_sort_scatter(const uint64_t* __restrict__ lo_in,
                                                              const uint32_t* __restrict__ hi_in, int64_t n,
                                                              int shift, int ntiles,
                                                              const uint32_t* __restrict__ offsets,
