@@ -300,7 +300,10 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_hist(const uint64_t* __rest
 // their ranks within the warp in registers (the ranking runs once); the tile
 // is then laid out in shared memory in digit order and written out digit run
 // by digit run with consecutive threads on consecutive rows, so that a warp's
-// stores cover whole sectors.
+// stores cover whole sectors.  The pass mostly waits on its tile's loads, so
+// the packed-record form is held to three CTAs an SM (80 registers, a few
+// spilled): the extra resident warps hide more of that wait than the spills
+// cost.
 template <bool kSplit>
 __global__ void __launch_bounds__(kSortBlock, kSplit ? 2 : 3) k_sort_scatter(const uint64_t* __restrict__ lo_in,
                                                              const uint32_t* __restrict__ hi_in, int64_t n,
