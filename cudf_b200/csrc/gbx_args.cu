@@ -174,12 +174,15 @@ int aggregate_with_packed_args(gbx_groupby* gb, int64_t n, const gbx_request* re
   if (h_status & S_BAD_INDEX) fail(GBX_ERR_LOGIC, "dictionary index out of range");
 
   // the groupby with the rewritten requests (no ARG kind left)
-  gbx_result* ir = nullptr;
-  const int st   = gbx_groupby_aggregate(gb, reqs.data(), static_cast<int32_t>(reqs.size()), stream, mr, &ir);
+  ResultHold inner_res;
+  const int st = gbx_groupby_aggregate(gb, reqs.data(), static_cast<int32_t>(reqs.size()), stream, mr, &inner_res.r);
   if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+  gbx_result* ir = inner_res.r;
 
   // the result in the caller's request order
-  auto* res = new gbx_result();
+  ResultHold out_res;
+  out_res.r = new gbx_result();
+  auto* res = out_res.r;
   std::memset(res, 0, sizeof(*res));
   res->internal        = ir->internal;  // the same allocator made every column
   ir->internal         = nullptr;
@@ -217,8 +220,7 @@ int aggregate_with_packed_args(gbx_groupby* gb, int64_t n, const gbx_request* re
     std::memset(&src, 0, sizeof(src));
   }
   GBX_CUDA(cudaStreamSynchronize(s));
-  gbx_result_release(ir);
-  *out = res;
+  *out = out_res.take();
   return GBX_OK;
 }
 

@@ -144,6 +144,22 @@ void alloc_column(Alloc& a, gbx_column& c, int32_t type_id, int32_t scale, int64
 
 // gbx_result::internal: the allocator the result's buffers go back to
 // (gbx_result_release).
+// Releases a result when it goes out of scope unless taken: the error paths
+// of the calls that build one result from another.
+struct ResultHold {
+  gbx_result* r = nullptr;
+  ResultHold() = default;
+  ResultHold(const ResultHold&) = delete;
+  ResultHold& operator=(const ResultHold&) = delete;
+  ~ResultHold() { if (r) gbx_result_release(r); }
+  gbx_result* take()
+  {
+    gbx_result* t = r;
+    r             = nullptr;
+    return t;
+  }
+};
+
 struct ResultInternal {
   gbx::Alloc alloc;
   // buffers beyond the columns' own (STRING keys' offsets, STRUCT keys'

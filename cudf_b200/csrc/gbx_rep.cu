@@ -340,7 +340,9 @@ gbx_result* result_with_keys(Alloc& a, Scratch& sc, const std::vector<gbx_column
                              cudaStream_t s)
 {
   const int nkeys = static_cast<int>(keys.size());
-  auto* res       = new gbx_result();
+  ResultHold hold;
+  hold.r    = new gbx_result();
+  auto* res = hold.r;
   std::memset(res, 0, sizeof(*res));
   auto* internal       = new ResultInternal{a, {}, {}, {}};
   res->internal        = internal;
@@ -364,7 +366,7 @@ gbx_result* result_with_keys(Alloc& a, Scratch& sc, const std::vector<gbx_column
   GBX_CUDA(cudaMemcpyAsync(h.data(), nulls, 8 * nn, cudaMemcpyDeviceToHost, s));
   GBX_CUDA(cudaStreamSynchronize(s));
   for (int c = 0; c < nkeys; ++c) set_null_counts(res->keys[c].view, h.data(), t, t.roots[static_cast<size_t>(c)]);
-  return res;
+  return hold.take();
 }
 
 }  // namespace
@@ -427,13 +429,14 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
   label.null_count = rk.exclude_nulls ? -1 : 0;
   gbx_table_view tv{1, 0, &label};
   gbx_groupby* inner = nullptr;
-  gbx_result* ir     = nullptr;
-  int st             = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
+  ResultHold inner_res;
+  int st = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
   if (st == GBX_OK) st = gbx_groupby_set_strategy(inner, groupby_strategy(gb));
-  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &ir);
+  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &inner_res.r);
   if (st == GBX_OK && stats) gbx_groupby_last_stats(inner, stats);
   if (inner) gbx_groupby_destroy(inner);
   if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+  gbx_result* ir = inner_res.r;
 
   // the result: the key columns gathered at the labels; the inner result's
   // request columns move over (the same allocator made them)
@@ -444,7 +447,6 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
   res->requests     = ir->requests;
   ir->requests      = nullptr;
   ir->num_requests  = 0;
-  gbx_result_release(ir);
   *out = res;
   return GBX_OK;
 }
@@ -526,13 +528,14 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
   lv.null_count = mask ? -1 : 0;
   gbx_table_view tv{1, 0, &lv};
   gbx_groupby* inner = nullptr;
-  gbx_result* ir     = nullptr;
-  int st             = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
+  ResultHold inner_res;
+  int st = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
   if (st == GBX_OK) st = gbx_groupby_set_strategy(inner, groupby_strategy(gb));
-  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &ir);
+  if (st == GBX_OK) st = gbx_groupby_aggregate(inner, requests, num_requests, stream, mr, &inner_res.r);
   if (st == GBX_OK && stats) gbx_groupby_last_stats(inner, stats);
   if (inner) gbx_groupby_destroy(inner);
   if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+  gbx_result* ir = inner_res.r;
 
   // every request column put in label order
   const int64_t G = ir->num_groups;
@@ -545,10 +548,7 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
     GBX_CUDA(cudaGetLastError());
     GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
     GBX_CUDA(cudaStreamSynchronize(s));
-    if (h_status & S_BAD_INDEX) {
-      gbx_result_release(ir);
-      fail(GBX_ERR_DEVICE, "group label out of range (status 0x%x)", h_status);
-    }
+    if (h_status & S_BAD_INDEX) fail(GBX_ERR_DEVICE, "group label out of range (status 0x%x)", h_status);
   }
   for (int q = 0; q < ir->num_requests && G > 0; ++q)
     for (int k = 0; k < ir->requests[q].num_results; ++k) {
@@ -581,7 +581,6 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
   res->requests     = ir->requests;
   ir->requests      = nullptr;
   ir->num_requests  = 0;
-  gbx_result_release(ir);
   *out = res;
   return GBX_OK;
 }
