@@ -51,27 +51,60 @@ def distinct_indices(table: Table, keep: DuplicateKeep = DuplicateKeep.KEEP_ANY,
 
 
 def gather(col: Column, indices: Column) -> Column:
-    """Rows `indices` of a fixed-width column (torch gather; a dictionary
-    column keeps its keys)."""
-    idx = torch.as_tensor(indices.to_numpy()[0], dtype=torch.int64, device=col.data.device if col.data is not None
-                          else "cuda")
-    tid = col.index_type_id if col.type_id == _abi.TypeId.DICTIONARY32 else col.type_id
+    """Rows `indices` of a column (cudf::gather with in-bounds indices):
+    fixed-width (a dictionary column keeps its keys), STRING (characters and
+    offsets rebuilt) and STRUCT (members gathered, the struct's own mask
+    kept).  Plumbing around the library's index outputs, in torch."""
+    import numpy as np
+
+    return _gather(col, np.asarray(indices.to_numpy()[0], dtype=np.int64))
+
+
+def _gathered_mask(col: Column, idx, device):
+    if col.mask is None:
+        return None, 0
+    from .column import pack_mask, unpack_mask
+
+    valid = unpack_mask(col.mask.cpu().numpy(), col.size, col.offset)[idx]
+    return torch.from_numpy(pack_mask(valid)).to(device), int(len(valid) - valid.sum())
+
+
+def _gather(col: Column, idx) -> Column:
+    import numpy as np
+
     from .column import storage_dtype
 
+    if col.type_id == _abi.TypeId.STRUCT:
+        members = [_gather(m.slice(col.offset, col.offset + col.size), idx) for m in col.children]
+        device = col.mask.device if col.mask is not None else "cpu"
+        mask, nulls = _gathered_mask(col, idx, device)
+        return Column(_abi.TypeId.STRUCT, len(idx), None, mask, 0, nulls, children=members)
+    if col.type_id == _abi.TypeId.STRING:
+        offs = col.dict_keys.to_numpy()[0].astype(np.int64)[col.offset:col.offset + col.size + 1]
+        starts, lens = offs[:-1][idx], (offs[1:] - offs[:-1])[idx]
+        new_offs = np.zeros(len(idx) + 1, dtype=np.int64)
+        np.cumsum(lens, out=new_offs[1:])
+        total = int(new_offs[-1])
+        device = col.data.device if col.data is not None else "cpu"
+        pos = np.repeat(starts - new_offs[:-1], lens) + np.arange(total, dtype=np.int64)
+        if total:
+            chars = col.data.view(torch.uint8).index_select(0, torch.from_numpy(pos).to(device)).clone()
+        else:
+            chars = torch.zeros(1, dtype=torch.uint8, device=device)
+        ow = np.int32 if total < 2 ** 31 else np.int64
+        offsets = Column.from_numpy(new_offs.astype(ow), device=device)
+        mask, nulls = _gathered_mask(col, idx, device)
+        return Column(_abi.TypeId.STRING, len(idx), chars, mask, 0, nulls, dict_keys=offsets)
+    device = col.data.device if col.data is not None else "cuda"
+    t_idx = torch.as_tensor(idx, dtype=torch.int64, device=device)
+    tid = col.index_type_id if col.type_id == _abi.TypeId.DICTIONARY32 else col.type_id
     dt = storage_dtype(tid)
     w = dt.itemsize
     data = None
     if col.data is not None and len(idx):
         elems = col.data.view(torch.uint8)[col.offset * w:(col.offset + col.size) * w].view(-1, w)
-        data = elems.index_select(0, idx).reshape(-1).clone()
-    mask = None
-    nulls = 0
-    if col.mask is not None:
-        from .column import pack_mask, unpack_mask
-
-        valid = unpack_mask(col.mask.cpu().numpy(), col.size, col.offset)[idx.cpu().numpy()]
-        nulls = int(len(valid) - valid.sum())
-        mask = torch.from_numpy(pack_mask(valid)).to(idx.device)
+        data = elems.index_select(0, t_idx).reshape(-1).clone()
+    mask, nulls = _gathered_mask(col, idx, device)
     return Column(col.type_id, len(idx), data, mask, 0, nulls, dict_keys=col.dict_keys,
                   index_type_id=col.index_type_id, scale=col.scale)
 

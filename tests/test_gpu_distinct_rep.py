@@ -89,3 +89,22 @@ def test_counts_and_empty():
     e = [HostCol([], type_id=TypeId.STRING)]
     assert sc.distinct_count(dev(e)) == 0
     assert len(sc.distinct_indices(dev(e)).to_numpy()[0]) == 0
+
+
+def test_distinct_table_with_string_and_struct_columns():
+    """cudf::distinct over a STRING key: the kept rows of every column,
+    gathered (distinct_tests.cpp:80-123 inputs, KEEP_FIRST)."""
+    from cudf_b200 import Column
+
+    keys = Column.from_strings(["all", "new", "new", "all", None, "the", "strings"])
+    col = Column.from_numpy(np.array([0, 1, 2, 3, 4, 5, 6], np.int32), np.array([1, 0, 1, 1, 1, 1, 1], bool))
+    st = Column.struct([col], np.array([1, 1, 1, 0, 1, 1, 1], bool))
+    out = sc.distinct(Table([col, keys, st]), [1], DuplicateKeep.KEEP_FIRST)
+    vals, valid = out[0].to_numpy()
+    kv, kvalid = out[1].to_numpy()
+    order = np.argsort(vals)
+    assert list(vals[order]) == [0, 1, 4, 5, 6]
+    assert list(kv[order]) == ["all", "new", "", "the", "strings"]
+    assert list(kvalid[order]) == [True, True, False, True, True]
+    members, svalid = out[2].to_numpy()
+    assert list(members[0][0][order]) == [0, 1, 4, 5, 6]
