@@ -398,6 +398,15 @@ void validate_requests(const gbx_request* reqs, int32_t nreq, int64_t n, bool co
       if (counted_only(vt)) {
         // COUNT reads only the rows' validity: any column type (hash/groupby.cu:73-84 with a size_type target)
         if (count_any && is_count_kind(kind)) continue;
+        // MIN / MAX of strings: libcudf's sort path; here a best row per group
+        if (count_any && vt == GBX_TYPE_STRING && (kind == GBX_AGG_MIN || kind == GBX_AGG_MAX)) {
+          GBX_EXPECTS(r.values.dict_keys != nullptr && (r.values.dict_keys->type_id == GBX_TYPE_INT32 ||
+                                                        r.values.dict_keys->type_id == GBX_TYPE_INT64),
+                      "a STRING value column needs its INT32 / INT64 offsets column");
+          GBX_EXPECTS(r.values.size == 0 || r.values.dict_keys->size >= r.values.offset + r.values.size + 1,
+                      "offsets column too short");
+          continue;
+        }
         fail(GBX_ERR_UNSUPPORTED,
              "value type %d is aggregated by libcudf's sort-based groupby, which this library does not provide", vt);
       }
@@ -804,6 +813,14 @@ int gbx_groupby_aggregate(gbx_groupby* gb,
     *out = nullptr;
     validate(gb, requests, num_requests, true);
 
+    if (needs_string_extrema(requests, num_requests)) {
+      // MIN / MAX of STRING values (gbx_rep.cu)
+      if (gb->keys_are_sorted)
+        fail(GBX_ERR_UNSUPPORTED, "MIN / MAX of STRING values with keys declared sorted are not provided");
+      gb->stats = gbx_stats{};
+      aggregate_string_extrema(gb, gb->keys, gb->null_policy, requests, num_requests, stream, mr, &res, &gb->stats);
+      return;
+    }
     if (needs_count_stand_ins(requests, num_requests)) {
       // COUNT of STRING / LIST / STRUCT / DECIMAL128 values (gbx_args.cu)
       aggregate_with_count_stand_ins(gb, gb->keys.empty() ? 0 : gb->keys[0].size, requests, num_requests, stream,

@@ -193,6 +193,13 @@ int aggregate_by_representatives(gbx_groupby* gb, const std::vector<gbx_column_v
 bool keys_are_nested_or_strings(const gbx_table_view* keys);
 int64_t distinct_by_representatives(const gbx_table_view* keys, int32_t keep, int32_t nulls_equal,
                                     int32_t nans_equal, void* stream, const gbx_allocator* mr, gbx_column* out);
+// MIN / MAX of STRING values (gbx_rep.cu): each group's least / greatest
+// string by a compare-and-swap of its best row, the other requests by the
+// groupby on the key's representative-row label.
+bool needs_string_extrema(const gbx_request* requests, int32_t num_requests);
+int aggregate_string_extrema(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
+                             const gbx_request* requests, int32_t num_requests, void* stream,
+                             const gbx_allocator* mr, gbx_result** out, gbx_stats* stats);
 // The strategy set on a groupby (a groupby run on labels inherits it).
 int32_t groupby_strategy(const gbx_groupby* gb);
 // Keys the caller declares sorted: groups are the runs of equal adjacent rows

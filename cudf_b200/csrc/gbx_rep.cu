@@ -70,7 +70,7 @@ __global__ void k_gather_fixed(const void* __restrict__ src, int64_t src_offset,
 }
 
 // Validity words of a gathered leaf (its own and its enclosing structs'
-// nulls; null counts added to *nulls).
+// nulls; a negative row is null; null counts added to *nulls).
 __global__ void k_gather_leaf_valid(const __grid_constant__ RepCol c, const int32_t* __restrict__ rows, int64_t G,
                                     uint32_t* __restrict__ dst_mask, unsigned long long* nulls)
 {
@@ -78,7 +78,7 @@ __global__ void k_gather_leaf_valid(const __grid_constant__ RepCol c, const int3
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   const int64_t g_up   = (G + 31) & ~int64_t(31);
   for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < g_up; g += stride) {
-    const bool valid   = g < G && leaf_valid(c, rows[g]);
+    const bool valid   = g < G && rows[g] >= 0 && leaf_valid(c, rows[g]);
     const uint32_t act = __ballot_sync(0xffffffffu, g < G);
     const uint32_t bal = __ballot_sync(0xffffffffu, valid);
     if (lane == 0 && act) {
@@ -89,7 +89,8 @@ __global__ void k_gather_leaf_valid(const __grid_constant__ RepCol c, const int3
   }
 }
 
-// STRING output: lengths of the gathered rows (0 for a null row).
+// STRING output: lengths of the gathered rows (0 for a null row, or a
+// negative one).
 __global__ void k_gather_str_len(const __grid_constant__ RepCol c, const int32_t* __restrict__ rows, int64_t G,
                                  int64_t* __restrict__ len)
 {
@@ -97,7 +98,7 @@ __global__ void k_gather_str_len(const __grid_constant__ RepCol c, const int32_t
        g += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t r = rows[g];
     int64_t b = 0, l = 0;
-    if (leaf_valid(c, r)) str_span(c, r, b, l);
+    if (r >= 0 && leaf_valid(c, r)) str_span(c, r, b, l);
     len[g] = l;
   }
 }
@@ -111,7 +112,7 @@ __global__ void k_gather_str_copy(const __grid_constant__ RepCol c, const int32_
   const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   for (int64_t g = w; g < G; g += nw) {
     const int64_t r = rows[g];
-    if (!leaf_valid(c, r)) continue;
+    if (r < 0 || !leaf_valid(c, r)) continue;
     int64_t b, l;
     str_span(c, r, b, l);
     const auto* s = static_cast<const unsigned char*>(c.data) + b;
@@ -132,6 +133,59 @@ __global__ void k_offsets_out(const int64_t* __restrict__ excl, const int64_t* _
 }
 
 
+
+// ---------------------------------------------- MIN / MAX of STRING values
+
+// Lexicographic byte comparison of rows a and b of a STRING leaf (a prefix
+// sorts first): <0, 0 or >0, as libcudf compares strings.
+__device__ __forceinline__ int str_compare(const RepCol& c, int64_t a, int64_t b)
+{
+  int64_t ba, la, bb, lb;
+  str_span(c, a, ba, la);
+  str_span(c, b, bb, lb);
+  const auto* s   = static_cast<const unsigned char*>(c.data);
+  const int64_t m = la < lb ? la : lb;
+  for (int64_t j = 0; j < m; ++j)
+    if (s[ba + j] != s[bb + j]) return s[ba + j] < s[bb + j] ? -1 : 1;
+  return la < lb ? -1 : (la > lb ? 1 : 0);
+}
+
+constexpr int kStrSpin = 1 << 16;
+
+// best[g] = the row of group g's least (greatest) valid string: a row
+// replaces the held row by compare-and-swap while its string is strictly
+// smaller (greater); bounded (S_SPIN_LIMIT beyond).
+__global__ void k_str_extreme(const __grid_constant__ RepCol c, const int32_t* __restrict__ label, int64_t n,
+                              bool for_min, int32_t* __restrict__ best, int32_t* status)
+{
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t g = label[r];
+    if (g < 0 || !leaf_valid(c, r)) continue;
+    int32_t cur = best[g];
+    int it      = 0;
+    for (; it < kStrSpin; ++it) {
+      if (cur >= 0) {
+        const int cmp = str_compare(c, r, cur);
+        if (for_min ? cmp >= 0 : cmp <= 0) break;
+      }
+      const int32_t old = atomicCAS(best + g, cur, static_cast<int32_t>(r));
+      if (old == cur) break;
+      cur = old;
+    }
+    if (it == kStrSpin) atomicOr(status, S_SPIN_LIMIT);
+  }
+}
+
+// rows[j] = best[labels[j]]: the row whose string each output group takes
+// (-1: a group without valid values).
+__global__ void k_pick_rows(const int32_t* __restrict__ labels, int64_t G, const int32_t* __restrict__ best,
+                            int32_t* __restrict__ rows)
+{
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < G;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    rows[j] = best[labels[j]];
+}
 
 // ------------------------------------------- keys the caller declares sorted
 
@@ -228,6 +282,7 @@ struct KeyGather {
   cudaStream_t s;
   bool include;
   unsigned long long* nulls;  // one counter per node
+  bool force_mask = false;    // every gathered column gets a mask (rows may be -1)
 
   // Node `i` gathered at the rows; a key column keeps a mask under INCLUDE
   // only (EXCLUDE dropped its null rows), a struct member whenever it or an
@@ -242,7 +297,8 @@ struct KeyGather {
     out.view.type_id = kv.type_id;
     out.view.scale   = kv.scale;
     out.view.size    = G;
-    const bool with_mask = rc.top ? (rc.mask != nullptr && include) : (rc.mask != nullptr || rc.nanc > 0);
+    const bool with_mask =
+      force_mask || (rc.top ? (rc.mask != nullptr && include) : (rc.mask != nullptr || rc.nanc > 0));
     if (kv.type_id == GBX_TYPE_STRUCT) {
       internal->arrays.emplace_back();
       auto& members = internal->arrays.back();
@@ -582,6 +638,204 @@ int aggregate_presorted(gbx_groupby* gb, const std::vector<gbx_column_view>& key
   ir->requests      = nullptr;
   ir->num_requests  = 0;
   *out = res;
+  return GBX_OK;
+}
+
+bool needs_string_extrema(const gbx_request* requests, int32_t num_requests)
+{
+  for (int q = 0; q < num_requests; ++q) {
+    if (requests[q].values.type_id != GBX_TYPE_STRING) continue;
+    for (int k = 0; k < requests[q].num_aggregations; ++k) {
+      const int32_t kind = requests[q].aggregations[k].kind;
+      if (kind == GBX_AGG_MIN || kind == GBX_AGG_MAX) return true;
+    }
+  }
+  return false;
+}
+
+int aggregate_string_extrema(gbx_groupby* gb, const std::vector<gbx_column_view>& keys, int32_t null_policy,
+                             const gbx_request* requests, int32_t num_requests, void* stream,
+                             const gbx_allocator* mr, gbx_result** out, gbx_stats* stats)
+{
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Alloc a;
+  a.st = s;
+  if (mr && mr->allocate && mr->deallocate) {
+    a.user     = *mr;
+    a.has_user = true;
+  }
+  const int64_t n   = keys.empty() ? 0 : keys[0].size;
+  const int num_sms = current_device().num_sms;
+  Scratch sc(&a);
+  const size_t n4 = static_cast<size_t>(std::max<int64_t>(n, 1)) * 4;
+
+  // every row's group: the representative row of its key
+  const KeyTree tree = key_tree(keys, null_policy);
+  const RepKeys& rk  = tree.rk;
+  const uint64_t cap = next_pow2(std::max<uint64_t>(2 * static_cast<uint64_t>(n) + 2, 64));
+  auto* slots  = static_cast<int32_t*>(sc.get(cap * 4));
+  auto* rep    = static_cast<int32_t*>(sc.get(n4));
+  auto* status = static_cast<int32_t*>(sc.get(8));
+  auto* mask   = static_cast<uint32_t*>(sc.get(static_cast<size_t>((n + 31) / 32) * 4 + 64));
+  GBX_CUDA(cudaMemsetAsync(status, 0, 8, s));
+  k_fill_i32<<<grid_of(static_cast<int64_t>(cap), num_sms), kRepBlock, 0, s>>>(slots, -1, static_cast<int64_t>(cap));
+  GBX_CUDA(cudaGetLastError());
+  if (n > 0) {
+    k_rep_insert<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rk, n, slots, cap, rep, status);
+    if (rk.exclude_nulls) k_rep_mask<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(rep, n, mask);
+    GBX_CUDA(cudaGetLastError());
+  }
+
+  // the requests the groupby on the label answers: every non-STRING
+  // request, and the COUNTs of the STRING ones over a stand-in of zeros with
+  // their validity; MIN / MAX of the strings each keep a best row per group
+  struct Where {
+    int q, k;   // original position
+    int iq, ik; // position in the inner result (-1: a string extreme)
+    int ext;    // index of the string extreme
+  };
+  struct Extreme {
+    RepCol col;
+    bool for_min;
+    int32_t* best;
+  };
+  std::vector<Where> where;
+  std::vector<Extreme> ext;
+  std::vector<gbx_request> reqs;
+  std::vector<std::vector<gbx_aggregation>> aggs;
+  aggs.reserve(static_cast<size_t>(num_requests) + 1);
+  int64_t zbytes = 1;
+  for (int q = 0; q < num_requests; ++q)
+    if (requests[q].values.type_id == GBX_TYPE_STRING) zbytes = std::max(zbytes, requests[q].values.offset + n);
+  void* zeros = sc.get(static_cast<size_t>(zbytes));
+  GBX_CUDA(cudaMemsetAsync(zeros, 0, static_cast<size_t>(zbytes), s));
+  for (int q = 0; q < num_requests; ++q) {
+    const gbx_request& r = requests[q];
+    const bool str       = r.values.type_id == GBX_TYPE_STRING;
+    int iq               = -1;
+    for (int k = 0; k < r.num_aggregations; ++k) {
+      const gbx_aggregation& ag = r.aggregations[k];
+      if (str && (ag.kind == GBX_AGG_MIN || ag.kind == GBX_AGG_MAX)) {
+        const std::vector<gbx_column_view> one{r.values};
+        Extreme e{key_tree(one, GBX_NULL_INCLUDE).rk.cols[0], ag.kind == GBX_AGG_MIN,
+                  static_cast<int32_t*>(sc.get(n4))};
+        where.push_back({q, k, -1, -1, static_cast<int>(ext.size())});
+        ext.push_back(e);
+        continue;
+      }
+      if (iq < 0) {
+        gbx_request ir = r;
+        if (str) {
+          gbx_column_view v{};
+          v.type_id    = GBX_TYPE_INT8;
+          v.size       = r.values.size;
+          v.offset     = r.values.offset;
+          v.data       = zeros;
+          v.null_mask  = r.values.null_mask;
+          v.null_count = r.values.null_count;
+          ir.values    = v;
+        }
+        reqs.push_back(ir);
+        aggs.emplace_back();
+        iq = static_cast<int>(reqs.size()) - 1;
+      }
+      where.push_back({q, k, iq, static_cast<int>(aggs[iq].size()), -1});
+      aggs[iq].push_back(ag);
+    }
+  }
+  if (reqs.empty()) {
+    // only string extremes: the groupby still needs one request to run
+    gbx_request r{};
+    r.values.type_id = GBX_TYPE_INT8;
+    r.values.size    = n;
+    r.values.data    = zeros;
+    reqs.push_back(r);
+    aggs.emplace_back(1, gbx_aggregation{});
+    aggs.back()[0].kind = GBX_AGG_COUNT_ALL;
+  }
+  for (size_t i = 0; i < reqs.size(); ++i) {
+    reqs[i].num_aggregations = static_cast<int32_t>(aggs[i].size());
+    reqs[i].aggregations     = aggs[i].data();
+  }
+  for (const Extreme& e : ext) {
+    k_fill_i32<<<grid_of(std::max<int64_t>(n, 1), num_sms), kRepBlock, 0, s>>>(e.best, -1, std::max<int64_t>(n, 1));
+    if (n > 0)
+      k_str_extreme<<<grid_of(n, num_sms), kRepBlock, 0, s>>>(e.col, rep, n, e.for_min, e.best, status);
+    GBX_CUDA(cudaGetLastError());
+  }
+  int32_t h_status = 0;
+  GBX_CUDA(cudaMemcpyAsync(&h_status, status, 4, cudaMemcpyDeviceToHost, s));
+  GBX_CUDA(cudaStreamSynchronize(s));
+  if (h_status & S_TABLE_FULL) fail(GBX_ERR_DEVICE, "representative table overflow (status 0x%x)", h_status);
+  if (h_status & S_SPIN_LIMIT) fail(GBX_ERR_DEVICE, "string MIN / MAX update gave up (status 0x%x)", h_status);
+
+  // the groupby on the label
+  gbx_column_view lv{};
+  lv.type_id    = GBX_TYPE_INT32;
+  lv.size       = n;
+  lv.data       = rep;
+  lv.null_mask  = rk.exclude_nulls ? mask : nullptr;
+  lv.null_count = rk.exclude_nulls ? -1 : 0;
+  gbx_table_view tv{1, 0, &lv};
+  gbx_groupby* inner = nullptr;
+  ResultHold inner_res;
+  int st = gbx_groupby_create(&tv, GBX_NULL_EXCLUDE, 0, &inner);
+  if (st == GBX_OK) st = gbx_groupby_set_strategy(inner, groupby_strategy(gb));
+  if (st == GBX_OK)
+    st = gbx_groupby_aggregate(inner, reqs.data(), static_cast<int32_t>(reqs.size()), stream, mr, &inner_res.r);
+  if (st == GBX_OK && stats) gbx_groupby_last_stats(inner, stats);
+  if (inner) gbx_groupby_destroy(inner);
+  if (st != GBX_OK) fail(st, "%s", g_last_error.c_str());
+  gbx_result* ir = inner_res.r;
+
+  // the result: keys at the labels, the inner columns moved over, each
+  // string extreme gathered at its best rows
+  const int64_t G     = ir->num_groups;
+  const auto* labels  = static_cast<const int32_t*>(ir->keys[0].data);
+  ResultHold hold;
+  hold.r              = result_with_keys(a, sc, keys, null_policy, tree, labels, G, num_sms, s);
+  gbx_result* res     = hold.r;
+  auto* internal      = static_cast<ResultInternal*>(res->internal);
+  res->num_requests   = num_requests;
+  res->requests       = new gbx_aggregation_result[num_requests > 0 ? num_requests : 1]();
+  for (int q = 0; q < num_requests; ++q) {
+    res->requests[q].num_results = requests[q].num_aggregations;
+    res->requests[q].results = new gbx_column[requests[q].num_aggregations > 0 ? requests[q].num_aggregations : 1]();
+  }
+  auto* rows  = static_cast<int32_t*>(sc.get(static_cast<size_t>(std::max<int64_t>(G, 1)) * 4));
+  auto* nulls = static_cast<unsigned long long*>(sc.get(8));
+  for (const Where& w : where) {
+    gbx_column& dst = res->requests[w.q].results[w.k];
+    if (w.ext < 0) {
+      gbx_column& src = ir->requests[w.iq].results[w.ik];
+      dst             = src;
+      std::memset(&src, 0, sizeof(src));
+      continue;
+    }
+    const Extreme& e = ext[static_cast<size_t>(w.ext)];
+    if (G > 0) {
+      k_pick_rows<<<grid_of(G, num_sms), kRepBlock, 0, s>>>(labels, G, e.best, rows);
+      GBX_CUDA(cudaGetLastError());
+    }
+    // a one-leaf tree over the value column gathers it like a STRING key,
+    // with a mask for the groups that had no valid value (row -1)
+    const std::vector<gbx_column_view> one{requests[w.q].values};
+    const KeyTree vt = key_tree(one, GBX_NULL_INCLUDE);
+    GBX_CUDA(cudaMemsetAsync(nulls, 0, 8, s));
+    KeyGather kg{a, sc, internal, vt, rows, G, num_sms, s, true, nulls, true};
+    Gathered g = kg.node(vt.roots[0]);
+    dst.view       = g.view;
+    dst.data       = g.data;
+    dst.data_bytes = g.data_bytes;
+    dst.null_mask  = g.mask;
+    dst.mask_bytes = g.mask_bytes;
+    unsigned long long h_nulls = 0;
+    GBX_CUDA(cudaMemcpyAsync(&h_nulls, nulls, 8, cudaMemcpyDeviceToHost, s));
+    GBX_CUDA(cudaStreamSynchronize(s));
+    dst.view.null_count = static_cast<int64_t>(h_nulls);
+  }
+  GBX_CUDA(cudaStreamSynchronize(s));
+  *out = hold.take();
   return GBX_OK;
 }
 

@@ -112,7 +112,8 @@ class groupby {
     for (int q = 0; q < res->num_requests; ++q) {
       for (int k = 0; k < res->requests[q].num_results; ++k) {
         gbx_column& gc = res->requests[q].results[k];
-        out[q].results.push_back(std::make_unique<column>(gc, mr.allocator, stream.value()));
+        out[q].results.push_back(std::make_unique<column>(gc, mr.allocator, stream.value(), column_view{},
+                                                          gc.view.type_id == GBX_TYPE_STRING ? shell : nullptr));
         gc.data      = nullptr;
         gc.null_mask = nullptr;
       }

@@ -115,8 +115,9 @@ def test_size_mismatch_is_logic_error():
 @pytest.mark.parametrize("vtype", [TypeId.STRING, TypeId.STRUCT, TypeId.LIST, TypeId.DECIMAL128])
 def test_values_only_counted(vtype):
     """STRING / STRUCT / LIST / DECIMAL128 values: COUNT is computed (through
-    a stand-in, on the device), any other kind is UNSUPPORTED before device
-    work; the no-allocation entry point refuses them all."""
+    a stand-in, on the device), and MIN / MAX of strings; any other kind is
+    UNSUPPORTED before device work; the no-allocation entry point refuses
+    them all."""
     lib = _lib.lib()
     tv, keep = _keys_view(3)
     h = C.c_void_p()
@@ -125,13 +126,40 @@ def test_values_only_counted(vtype):
         r, keep2 = _request(3, kind)
         r.values.type_id = int(vtype)
         out = C.POINTER(_abi.gbx_result)()
-        assert lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out)) == _abi.Status.ERR_UNSUPPORTED
+        st = lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out))
+        if vtype == TypeId.STRING and kind == Kind.MIN:
+            # MIN / MAX of strings are computed; this view lacks its offsets
+            assert st == _abi.Status.ERR_LOGIC and b"offsets" in lib.gbx_last_error()
+        else:
+            assert st == _abi.Status.ERR_UNSUPPORTED
     r, keep2 = _request(3, Kind.COUNT_VALID)
     r.values.type_id = int(vtype)
     res = (_abi.gbx_column * 1)()
     ng = C.c_int64()
     assert lib.gbx_groupby_aggregate_noalloc(h, C.byref(r), 1, None, None, res, 8, C.byref(ng)) == \
         _abi.Status.ERR_UNSUPPORTED
+    lib.gbx_groupby_destroy(h)
+
+
+def test_string_extremes_with_sorted_keys_refused():
+    """MIN / MAX of strings run on unsorted keys only."""
+    lib = _lib.lib()
+    tv, keep = _keys_view(3)
+    h = C.c_void_p()
+    assert lib.gbx_groupby_create(C.byref(tv), 0, 1, C.byref(h)) == 0
+    offs = np.array([0, 1, 2, 3], np.int32)
+    chars = np.frombuffer(b"abc", np.uint8).copy()
+    ov = _abi.gbx_column_view()
+    ov.type_id = TypeId.INT32
+    ov.size = 4
+    ov.data = offs.ctypes.data
+    r, keep2 = _request(3, Kind.MAX)
+    r.values.type_id = int(TypeId.STRING)
+    r.values.data = chars.ctypes.data
+    r.values.dict_keys = C.pointer(ov)
+    out = C.POINTER(_abi.gbx_result)()
+    assert lib.gbx_groupby_aggregate(h, C.byref(r), 1, None, None, C.byref(out)) == _abi.Status.ERR_UNSUPPORTED
+    assert b"sorted" in lib.gbx_last_error()
     lib.gbx_groupby_destroy(h)
 
 

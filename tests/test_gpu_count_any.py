@@ -2,8 +2,8 @@
 (STRING, STRUCT): the reference answers them on its hash path (COUNT has a
 size_type target whatever the values, hash/groupby.cu:73-84); here through
 the C ABI against the oracle given an INT8 column with the same validity
-(a count depends on nothing else).  Other kinds over such values stay
-GBX_ERR_UNSUPPORTED."""
+(a count depends on nothing else).  Kinds other than COUNT (and MIN / MAX
+of strings, tests/test_gpu_string_values.py) stay GBX_ERR_UNSUPPORTED."""
 from __future__ import annotations
 
 import numpy as np
@@ -59,4 +59,4 @@ def test_sliced_string_values_and_other_kinds_refused():
     for j in range(2):
         T.compare_values(COUNTS[j][0], got["results"][0][j], want["results"][0][j], go, wo)
     with pytest.raises(UnsupportedError):
-        T.run_gpu([HostCol(k)], [(s, [(Kind.MIN, 0)])])
+        T.run_gpu([HostCol(k)], [(s, [(Kind.SUM, 0)])])
