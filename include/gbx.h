@@ -250,9 +250,11 @@ GBX_API int gbx_groupby_create(const gbx_table_view* keys,
  * and returns owning results allocated from `mr` (NULL: cudaMallocAsync).
  * Synchronises `stream` once, to learn the number of groups (the reference's
  * retrieve_all does the same).  STRING, STRUCT, LIST and DECIMAL128 value
- * columns take COUNT_VALID / COUNT_ALL only (their rows' validity); other
- * kinds over them are GBX_ERR_UNSUPPORTED (libcudf's sort path).  On success
- * *out must be freed with gbx_result_release. */
+ * columns take COUNT_VALID / COUNT_ALL (their rows' validity), and STRING
+ * values MIN / MAX too (a STRING result, byte order, null for a group with
+ * no valid value; not with keys_are_sorted 1); other kinds over them are
+ * GBX_ERR_UNSUPPORTED (libcudf's sort path).  On success *out must be freed
+ * with gbx_result_release. */
 GBX_API int gbx_groupby_aggregate(gbx_groupby* gb,
                           const gbx_request* requests,
                           int32_t num_requests,
